@@ -1,0 +1,24 @@
+"""Shared pytest setup: the `gpu` marker and import paths.
+
+Tests marked `gpu` need a CUDA device and the built library; everything else
+runs on a CPU-only host.
+"""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
+
+
+@pytest.fixture(scope="session")
+def oracle_mod():
+    from oracle import oracle as O
+    O.build_oracle()
+    return O
