@@ -1,0 +1,84 @@
+"""ctypes binding of the engine's C ABI (include/adaptive_trees_b200.h).
+
+The shared library is built in-tree (python -m adaptive_trees_b200.build);
+importing this module without it raises ImportError.  There is no fallback
+implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libadaptive_trees_b200.so")
+
+AO_OK = 0
+STATUS_NAMES = {1: "invalid argument", 2: "logic error", 3: "length error", 4: "CUDA error", 5: "out of memory",
+                6: "runtime error"}
+
+# Exported entry points and their prototypes.
+vp, sz, ci, cu = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_uint
+
+
+class AoConfig(ctypes.Structure):
+    _fields_ = [("max_depth", ci), ("max_particles_per_leaf", cu), ("update_iterations", ci),
+                ("box", ctypes.c_double * 6), ("split_criterion", ci), ("sfc_kind", ci),
+                ("views_tree_structure", ci), ("views_particle_counts", ci), ("views_particle_mapping", ci)]
+
+
+class AoViewConfig(ctypes.Structure):
+    _fields_ = [("tree_structure", ci), ("particle_counts_per_box", ci), ("particle_mapping", ci)]
+
+
+class AoTreeInfo(ctypes.Structure):
+    _fields_ = [("num_particles", sz), ("num_active_particles", sz), ("num_nodes", sz), ("num_leaves", sz),
+                ("leaf_capacity", sz), ("max_achieved_depth", cu), ("split_criterion", ci), ("sfc_kind", ci)]
+
+
+PROTOTYPES = {
+    "ao_tree_create": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(AoConfig), vp, ctypes.POINTER(vp)],
+    "ao_tree_destroy": [vp],
+    "ao_tree_build": [vp],
+    "ao_tree_update": [vp],
+    "ao_tree_compute_views": [vp, ctypes.POINTER(AoViewConfig)],
+    "ao_tree_needs_resize": [vp, ctypes.POINTER(ci)],
+    "ao_tree_resize_buffers": [vp],
+    "ao_tree_get_buffer": [vp, ci, ctypes.POINTER(vp), ctypes.POINTER(sz), ctypes.POINTER(sz)],
+    "ao_tree_counters": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)],
+    "ao_tree_get_info": [vp, ctypes.POINTER(AoTreeInfo)],
+    "ao_compute_sfc_keys": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_double), ci, cu, vp, vp, vp],
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+class AoError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+def load():
+    """Load the built library (no build is attempted here)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(f"{LIB_PATH} is missing: build it with `python -m adaptive_trees_b200.build`")
+            lib = ctypes.CDLL(LIB_PATH)
+            lib.ao_last_error.restype = ctypes.c_char_p
+            lib.ao_last_error.argtypes = []
+            for name, args in PROTOTYPES.items():
+                f = getattr(lib, name)
+                f.argtypes = args
+                f.restype = ci
+            _lib = lib
+    return _lib
+
+
+def check(status: int):
+    if status != AO_OK:
+        raise AoError(status, load().ao_last_error().decode())

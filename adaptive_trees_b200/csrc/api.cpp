@@ -1,0 +1,424 @@
+// api.cpp -- adaptive_octree::Octree<Real> / KDTree3D<Real> and the C ABI over TreeEngine.
+#include <cstring>
+#include <new>
+#include <ostream>
+#include <string>
+
+#include "adaptive_octree/tree.hpp"
+#include "adaptive_trees_b200.h"
+#include "engine.hpp"
+
+namespace adaptive_octree
+{
+namespace
+{
+template <class Real>
+aot::EngineConfig octreeEngineConfig(const OctreeConfig<Real> &c)
+{
+    aot::EngineConfig e;
+    e.kind = 0;
+    e.real = sizeof(Real) == 4 ? 0 : 1;
+    e.bucket = c.maxParticlesPerLeaf;
+    e.maxDepth = c.maxDepth;
+    e.iterations = c.updateIterations;
+    e.nf = c.splitCriterion == SplitCriterion::NFCount;
+    e.hilbert = c.sfcKind == SfcKind::Hilbert;
+    const double b[6] = {double(c.box.xmin), double(c.box.xmax), double(c.box.ymin),
+                         double(c.box.ymax), double(c.box.zmin), double(c.box.zmax)};
+    std::memcpy(e.box, b, sizeof(b));
+    e.views = c.views;
+    e.stream = c.stream;
+    return e;
+}
+template <class Real>
+aot::EngineConfig binaryEngineConfig(const KDTree3DConfig<Real> &c)
+{
+    aot::EngineConfig e;
+    e.kind = 1;
+    e.real = sizeof(Real) == 4 ? 0 : 1;
+    e.bucket = c.maxParticlesPerLeaf;
+    e.maxDepth = c.maxDepth;
+    e.iterations = c.updateIterations;
+    const double b[6] = {double(c.box.xmin), double(c.box.xmax), double(c.box.ymin),
+                         double(c.box.ymax), double(c.box.zmin), double(c.box.zmax)};
+    std::memcpy(e.box, b, sizeof(b));
+    e.views = c.views;
+    e.stream = c.stream;
+    return e;
+}
+template <class T>
+DeviceVector<T> view(const aot::TreeEngine &e, int which)
+{
+    const void *p = nullptr;
+    size_t len = 0, cap = 0, elem = 0;
+    e.buffer(which, &p, &len, &cap, &elem);
+    return DeviceVector<T>(static_cast<const T *>(p), len, cap);
+}
+void printSummary(std::ostream &out, const aot::TreeEngine &e, const char *name)
+{
+    out << name << ": " << e.numParticles() << " particle slots, " << e.numActiveParticles() << " active, "
+        << e.leafCapacity() << " leaf capacity, " << e.numNodes() << " view nodes\n";
+}
+}  // namespace
+
+// ---------------------------------------------------------------- Octree<Real>
+template <class Real>
+Octree<Real>::Octree(const Real *x, const Real *y, const Real *z, std::size_t n, Config config)
+    : engine_(std::make_unique<aot::TreeEngine>(x, y, z, n, octreeEngineConfig(config)))
+{
+}
+template <class Real> Octree<Real>::~Octree() = default;
+template <class Real> Octree<Real>::Octree(Octree &&) noexcept = default;
+template <class Real> Octree<Real> &Octree<Real>::operator=(Octree &&) noexcept = default;
+template <class Real> void Octree<Real>::print(std::ostream &out) const { printSummary(out, *engine_, "Octree"); }
+template <class Real> void Octree<Real>::build() { engine_->build(); }
+template <class Real> void Octree<Real>::update() { engine_->update(); }
+template <class Real> void Octree<Real>::computeViews(ViewConfig v) { engine_->computeViews(v); }
+template <class Real> void Octree<Real>::computeViews() { engine_->computeViews(engine_->config().views); }
+template <class Real> bool Octree<Real>::doBuffersNeedResize() const { return engine_->doBuffersNeedResize(); }
+template <class Real> void Octree<Real>::resizeBuffers() { engine_->resizeBuffers(); }
+template <class Real> const NodeIndex *Octree<Real>::numLeaves_d() const { return engine_->numLeavesDevice(); }
+template <class Real> const NodeIndex *Octree<Real>::numNodes_d() const { return engine_->numNodesDevice(); }
+template <class Real> const unsigned *Octree<Real>::numActiveParticles_d() const
+{
+    return engine_->numActiveParticlesDevice();
+}
+template <class Real> DeviceVector<KeyType> Octree<Real>::particleKeys_d() const { return view<KeyType>(*engine_, 0); }
+template <class Real> DeviceVector<PermIndex> Octree<Real>::perm_d() const { return view<PermIndex>(*engine_, 1); }
+template <class Real> DeviceVector<KeyType> Octree<Real>::cornerstone_d() const { return view<KeyType>(*engine_, 2); }
+template <class Real> DeviceVector<unsigned> Octree<Real>::leafCounts_d() const { return view<unsigned>(*engine_, 3); }
+template <class Real> DeviceVector<unsigned> Octree<Real>::nearFieldCounts_d() const
+{
+    return view<unsigned>(*engine_, 4);
+}
+template <class Real> DeviceVector<KeyType> Octree<Real>::sfcBoxIndex_d() const { return view<KeyType>(*engine_, 5); }
+template <class Real> DeviceVector<std::uint8_t> Octree<Real>::hasBoxSplit_d() const
+{
+    return view<std::uint8_t>(*engine_, 6);
+}
+template <class Real> DeviceVector<std::uint8_t> Octree<Real>::boxDepth_d() const
+{
+    return view<std::uint8_t>(*engine_, 7);
+}
+template <class Real> DeviceVector<NodeIndex> Octree<Real>::parentIndex_d() const
+{
+    return view<NodeIndex>(*engine_, 8);
+}
+template <class Real> DeviceVector<NodeIndex> Octree<Real>::childIndex_d() const
+{
+    return view<NodeIndex>(*engine_, 9);
+}
+template <class Real> DeviceVector<NodeIndex> Octree<Real>::levelOffset_d() const
+{
+    return view<NodeIndex>(*engine_, 10);
+}
+template <class Real> unsigned Octree<Real>::maxAchievedDepth() const { return engine_->maxAchievedDepth(); }
+template <class Real> DeviceVector<unsigned> Octree<Real>::particleBeginIndex_d() const
+{
+    return view<unsigned>(*engine_, 11);
+}
+template <class Real> DeviceVector<unsigned> Octree<Real>::particleCounts_d() const
+{
+    return view<unsigned>(*engine_, 12);
+}
+template <class Real> DeviceVector<KeyType> Octree<Real>::sfcParticleIndex_d() const
+{
+    return view<KeyType>(*engine_, 13);
+}
+template <class Real> std::size_t Octree<Real>::numParticles() const { return engine_->numParticles(); }
+template <class Real> std::size_t Octree<Real>::numActiveParticles() const { return engine_->numActiveParticles(); }
+template <class Real> std::size_t Octree<Real>::numNodes() const { return engine_->numNodes(); }
+template <class Real> SplitCriterion Octree<Real>::splitCriterion() const
+{
+    return engine_->config().nf ? SplitCriterion::NFCount : SplitCriterion::LeafCount;
+}
+template <class Real> SfcKind Octree<Real>::sfcKind() const
+{
+    return engine_->config().hilbert ? SfcKind::Hilbert : SfcKind::Morton;
+}
+template class Octree<float>;
+template class Octree<double>;
+
+// ---------------------------------------------------------------- KDTree3D<Real>
+template <class Real>
+KDTree3D<Real>::KDTree3D(const Real *x, const Real *y, const Real *z, std::size_t n, Config config)
+    : engine_(std::make_unique<aot::TreeEngine>(x, y, z, n, binaryEngineConfig(config)))
+{
+}
+template <class Real> KDTree3D<Real>::~KDTree3D() = default;
+template <class Real> KDTree3D<Real>::KDTree3D(KDTree3D &&) noexcept = default;
+template <class Real> KDTree3D<Real> &KDTree3D<Real>::operator=(KDTree3D &&) noexcept = default;
+template <class Real> void KDTree3D<Real>::print(std::ostream &out) const { printSummary(out, *engine_, "KDTree3D"); }
+template <class Real> void KDTree3D<Real>::build() { engine_->build(); }
+template <class Real> void KDTree3D<Real>::update() { engine_->update(); }
+template <class Real> void KDTree3D<Real>::computeViews(ViewConfig v) { engine_->computeViews(v); }
+template <class Real> void KDTree3D<Real>::computeViews() { engine_->computeViews(engine_->config().views); }
+template <class Real> bool KDTree3D<Real>::doBuffersNeedResize() const { return engine_->doBuffersNeedResize(); }
+template <class Real> void KDTree3D<Real>::resizeBuffers() { engine_->resizeBuffers(); }
+template <class Real> const NodeIndex *KDTree3D<Real>::numLeaves_d() const { return engine_->numLeavesDevice(); }
+template <class Real> const NodeIndex *KDTree3D<Real>::numNodes_d() const { return engine_->numNodesDevice(); }
+template <class Real> const unsigned *KDTree3D<Real>::numActiveParticles_d() const
+{
+    return engine_->numActiveParticlesDevice();
+}
+template <class Real> DeviceVector<KeyType> KDTree3D<Real>::particleKeys_d() const { return view<KeyType>(*engine_, 0); }
+template <class Real> DeviceVector<PermIndex> KDTree3D<Real>::perm_d() const { return view<PermIndex>(*engine_, 1); }
+template <class Real> DeviceVector<KeyType> KDTree3D<Real>::cornerstone_d() const { return view<KeyType>(*engine_, 2); }
+template <class Real> DeviceVector<unsigned> KDTree3D<Real>::leafCounts_d() const
+{
+    return view<unsigned>(*engine_, 3);
+}
+template <class Real> DeviceVector<KeyType> KDTree3D<Real>::sfcBoxIndex_d() const { return view<KeyType>(*engine_, 5); }
+template <class Real> DeviceVector<std::uint8_t> KDTree3D<Real>::hasBoxSplit_d() const
+{
+    return view<std::uint8_t>(*engine_, 6);
+}
+template <class Real> DeviceVector<std::uint8_t> KDTree3D<Real>::boxDepth_d() const
+{
+    return view<std::uint8_t>(*engine_, 7);
+}
+template <class Real> DeviceVector<NodeIndex> KDTree3D<Real>::parentIndex_d() const
+{
+    return view<NodeIndex>(*engine_, 8);
+}
+template <class Real> DeviceVector<NodeIndex> KDTree3D<Real>::childIndex_d() const
+{
+    return view<NodeIndex>(*engine_, 9);
+}
+template <class Real> DeviceVector<NodeIndex> KDTree3D<Real>::levelOffset_d() const
+{
+    return view<NodeIndex>(*engine_, 10);
+}
+template <class Real> unsigned KDTree3D<Real>::maxAchievedDepth() const { return engine_->maxAchievedDepth(); }
+template <class Real> DeviceVector<unsigned> KDTree3D<Real>::particleBeginIndex_d() const
+{
+    return view<unsigned>(*engine_, 11);
+}
+template <class Real> DeviceVector<unsigned> KDTree3D<Real>::particleCounts_d() const
+{
+    return view<unsigned>(*engine_, 12);
+}
+template <class Real> DeviceVector<KeyType> KDTree3D<Real>::sfcParticleIndex_d() const
+{
+    return view<KeyType>(*engine_, 13);
+}
+template <class Real> std::size_t KDTree3D<Real>::numParticles() const { return engine_->numParticles(); }
+template <class Real> std::size_t KDTree3D<Real>::numActiveParticles() const { return engine_->numActiveParticles(); }
+template <class Real> std::size_t KDTree3D<Real>::numNodes() const { return engine_->numNodes(); }
+template class KDTree3D<float>;
+template class KDTree3D<double>;
+}  // namespace adaptive_octree
+
+// =========================================================================
+// C ABI
+// =========================================================================
+struct ao_tree
+{
+    std::unique_ptr<aot::TreeEngine> engine;
+};
+
+namespace
+{
+thread_local std::string g_lastError;
+
+ao_status fail(ao_status s, const char *msg)
+{
+    g_lastError = msg ? msg : "";
+    return s;
+}
+
+template <class F>
+ao_status guarded(F &&f)
+{
+    try
+    {
+        f();
+        return AO_OK;
+    }
+    catch (const std::invalid_argument &e)
+    {
+        return fail(AO_ERR_INVALID_ARGUMENT, e.what());
+    }
+    catch (const std::length_error &e)
+    {
+        return fail(AO_ERR_LENGTH, e.what());
+    }
+    catch (const std::logic_error &e)
+    {
+        return fail(AO_ERR_LOGIC, e.what());
+    }
+    catch (const aot::CudaError &e)
+    {
+        return fail(e.code == cudaErrorMemoryAllocation ? AO_ERR_OUT_OF_MEMORY : AO_ERR_CUDA, e.what());
+    }
+    catch (const std::bad_alloc &e)
+    {
+        return fail(AO_ERR_OUT_OF_MEMORY, e.what());
+    }
+    catch (const std::exception &e)
+    {
+        return fail(AO_ERR_RUNTIME, e.what());
+    }
+    catch (...)
+    {
+        return fail(AO_ERR_RUNTIME, "unknown error");
+    }
+}
+
+// Tree<Real, Kind>::backendConfig (tree.hpp:108-133) + backend defaults.
+aot::EngineConfig engineConfig(int kind, int real, const ao_config &c, void *stream)
+{
+    if (kind != AO_OCTREE && kind != AO_BINARY) throw std::invalid_argument("ao_tree_create: unknown tree kind");
+    if (real != AO_FLOAT32 && real != AO_FLOAT64) throw std::invalid_argument("ao_tree_create: unknown real type");
+    if (c.max_depth < -1 || c.update_iterations < -1) throw std::invalid_argument("Tree: use -1 for backend defaults");
+    aot::EngineConfig e;
+    e.kind = kind;
+    e.real = real;
+    e.bucket = c.max_particles_per_leaf;
+    e.maxDepth = c.max_depth >= 0 ? unsigned(c.max_depth) : (kind == AO_OCTREE ? 21u : 63u);
+    e.iterations = c.update_iterations >= 0 ? unsigned(c.update_iterations) : (kind == AO_OCTREE ? 2u : 6u);
+    std::memcpy(e.box, c.box, sizeof(e.box));
+    e.views.treeStructure = c.views_tree_structure != 0;
+    e.views.particleCountsPerBox = c.views_particle_counts != 0;
+    e.views.particleMapping = c.views_particle_mapping != 0;
+    e.stream = static_cast<cudaStream_t>(stream);
+    if (kind == AO_OCTREE)
+    {
+        e.nf = c.split_criterion == AO_NF_COUNT;
+        e.hilbert = c.sfc_kind == AO_HILBERT;
+    }
+    else
+    {
+        if (c.split_criterion != AO_LEAF_COUNT)
+            throw std::invalid_argument("Tree: Binary NFCount is not implemented yet");
+        if (c.sfc_kind != AO_MORTON) throw std::invalid_argument("Tree: Binary uses longest-side keys, not Hilbert");
+    }
+    return e;
+}
+}  // namespace
+
+extern "C" {
+
+const char *ao_last_error(void) { return g_lastError.c_str(); }
+
+ao_status ao_tree_create(int kind, int real_type, const void *x, const void *y, const void *z, size_t n,
+                         const ao_config *config, void *stream, ao_tree **out)
+{
+    return guarded([&] {
+        if (!out || !config) throw std::invalid_argument("ao_tree_create: null argument");
+        *out = nullptr;
+        auto e = std::make_unique<aot::TreeEngine>(x, y, z, n, engineConfig(kind, real_type, *config, stream));
+        *out = new ao_tree{std::move(e)};
+    });
+}
+
+ao_status ao_tree_destroy(ao_tree *tree)
+{
+    return guarded([&] { delete tree; });
+}
+
+#define AO_NEED_TREE()                                                     \
+    if (!tree) throw std::invalid_argument("null ao_tree handle")
+
+ao_status ao_tree_build(ao_tree *tree)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        tree->engine->build();
+    });
+}
+
+ao_status ao_tree_update(ao_tree *tree)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        tree->engine->update();
+    });
+}
+
+ao_status ao_tree_compute_views(ao_tree *tree, const ao_view_config *views)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        adaptive_octree::ViewConfig v = tree->engine->config().views;
+        if (views)
+        {
+            v.treeStructure = views->tree_structure != 0;
+            v.particleCountsPerBox = views->particle_counts_per_box != 0;
+            v.particleMapping = views->particle_mapping != 0;
+        }
+        tree->engine->computeViews(v);
+    });
+}
+
+ao_status ao_tree_needs_resize(ao_tree *tree, int *out)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        if (!out) throw std::invalid_argument("ao_tree_needs_resize: null output");
+        *out = tree->engine->doBuffersNeedResize() ? 1 : 0;
+    });
+}
+
+ao_status ao_tree_resize_buffers(ao_tree *tree)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        tree->engine->resizeBuffers();
+    });
+}
+
+ao_status ao_tree_get_buffer(ao_tree *tree, int which, const void **dptr, size_t *len, size_t *capacity)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        tree->engine->buffer(which, dptr, len, capacity, nullptr);
+    });
+}
+
+ao_status ao_tree_counters(ao_tree *tree, const int **num_leaves_d, const int **num_nodes_d,
+                           const unsigned **num_active_particles_d)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        if (num_leaves_d) *num_leaves_d = tree->engine->numLeavesDevice();
+        if (num_nodes_d) *num_nodes_d = tree->engine->numNodesDevice();
+        if (num_active_particles_d) *num_active_particles_d = tree->engine->numActiveParticlesDevice();
+    });
+}
+
+ao_status ao_tree_get_info(ao_tree *tree, ao_tree_info *info)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        if (!info) throw std::invalid_argument("ao_tree_get_info: null output");
+        const aot::TreeEngine &e = *tree->engine;
+        size_t leaves = 0;
+        e.buffer(aot::TreeEngine::LeafCounts, nullptr, &leaves, nullptr, nullptr);
+        info->num_particles = e.numParticles();
+        info->num_active_particles = e.numActiveParticles();
+        info->num_nodes = e.numNodes();
+        info->num_leaves = leaves;
+        info->leaf_capacity = e.leafCapacity();
+        info->max_achieved_depth = e.maxAchievedDepth();
+        info->split_criterion = e.config().nf ? AO_NF_COUNT : AO_LEAF_COUNT;
+        info->sfc_kind = e.config().kind == AO_BINARY ? -1 : (e.config().hilbert ? AO_HILBERT : AO_MORTON);
+    });
+}
+
+ao_status ao_compute_sfc_keys(int kind, int real_type, const void *x, const void *y, const void *z, size_t n,
+                              const double *box, int sfc_kind, unsigned max_depth, unsigned long long *keys_d,
+                              unsigned *perm_d, void *stream)
+{
+    return guarded([&] {
+        if (kind != AO_OCTREE && kind != AO_BINARY) throw std::invalid_argument("ao_compute_sfc_keys: unknown kind");
+        if (real_type != AO_FLOAT32 && real_type != AO_FLOAT64)
+            throw std::invalid_argument("ao_compute_sfc_keys: unknown real type");
+        if (n > 0 && (!x || !y || !z || !keys_d || !box))
+            throw std::invalid_argument("ao_compute_sfc_keys: null argument");
+        aot::TreeEngine::computeKeys(kind, real_type, x, y, z, n, box, sfc_kind == AO_HILBERT, max_depth, keys_d,
+                                     perm_d, static_cast<cudaStream_t>(stream));
+    });
+}
+
+}  // extern "C"

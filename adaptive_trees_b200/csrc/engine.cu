@@ -1,0 +1,1063 @@
+// engine.cu -- host orchestration of the B200 adaptive-tree engine.
+//
+// Follows the reference's control flow for build/update/views
+// (octree.cu:427-551, kdtree3d.cu:227-297, tree_view.cu:814-1134) with
+// B200-specific choices:
+//   * keygen + onesweep sort replace computeSfcKeys + CUB SortPairs;
+//   * the octree build runs its split/merge rounds on the device without a
+//     host round-trip per round: rounds are issued in batches, every kernel
+//     stops as soon as the device state says the tree converged, and the host
+//     reads the state once per batch; the reference's vector capacity growth,
+//     which decides leafCapacity, is replayed on the host from the per-round
+//     proposals recorded on the device;
+//   * the binary build emulates the reference's reject/grow/retry capacity
+//     loop on the device (25% steps) instead of a host sync per pass.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+
+#include "keygen.cuh"
+#include "rebalance.cuh"
+#include "tree_view.cuh"
+
+namespace aot
+{
+// --------------------------------------------------------------------------
+// DevMem
+// --------------------------------------------------------------------------
+DevMem::~DevMem()
+{
+    if (p) cudaFree(p);
+}
+void DevMem::reserve(size_t b)
+{
+    if (b <= bytes) return;
+    if (p) AOT_CHECK(cudaFree(p));
+    p = nullptr;
+    bytes = 0;
+    AOT_CHECK(cudaMalloc(&p, b));
+    bytes = b;
+}
+void DevMem::grow(size_t b, size_t keep, cudaStream_t s)
+{
+    if (b <= bytes) return;
+    void *q = nullptr;
+    AOT_CHECK(cudaMalloc(&q, b));
+    keep = std::min(keep, bytes);
+    if (keep && p)
+    {
+        AOT_CHECK(cudaMemcpyAsync(q, p, keep, cudaMemcpyDeviceToDevice, s));
+        AOT_CHECK(cudaStreamSynchronize(s));
+    }
+    if (p) AOT_CHECK(cudaFree(p));
+    p = q;
+    bytes = b;
+}
+
+namespace
+{
+int smCount()
+{
+    static int sms = 0;
+    if (!sms)
+    {
+        int dev = 0;
+        AOT_CHECK(cudaGetDevice(&dev));
+        AOT_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+const HilbertTables &hilbertTables()
+{
+    static const HilbertTables t = makeHilbertTables();
+    return t;
+}
+
+template <class T>
+QuantBox<T> makeQuantBox(const double *b)
+{
+    // Box<T> (sfc_keys.cuh:420-465): inverse lengths and per-axis bits in T
+    const T xmin = T(b[0]), xmax = T(b[1]), ymin = T(b[2]), ymax = T(b[3]), zmin = T(b[4]), zmax = T(b[5]);
+    QuantBox<T> q;
+    q.xmin = xmin;
+    q.ymin = ymin;
+    q.zmin = zmin;
+    q.ilx = T(1) / (xmax - xmin);
+    q.ily = T(1) / (ymax - ymin);
+    q.ilz = T(1) / (zmax - zmin);
+    const T lx = xmax - xmin, ly = ymax - ymin, lz = zmax - zmin;
+    const T md = std::max(std::max(lx, ly), lz);
+    const T bias = T(0.5849625007211563);
+    q.bx = kOctLevels - unsigned(std::floor(std::log2(md / lx) + bias));
+    q.by = kOctLevels - unsigned(std::floor(std::log2(md / ly) + bias));
+    q.bz = kOctLevels - unsigned(std::floor(std::log2(md / lz) + bias));
+    return q;
+}
+
+// makeBinaryGeometry (binary_node.cuh:17-40): the longest side is halved at
+// every depth, first axis wins ties.
+BinaryGeometry makeGeometry(const double *b, unsigned maxDepth, int real)
+{
+    if (maxDepth > kBinDepth) throw std::invalid_argument("Binary maxDepth exceeds key precision");
+    double bx[6];
+    for (int k = 0; k < 6; ++k) bx[k] = real == 0 ? double(float(b[k])) : b[k];
+    long double len[3] = {(long double)bx[1] - bx[0], (long double)bx[3] - bx[2], (long double)bx[5] - bx[4]};
+    for (auto s : len)
+        if (!(s > 0) || !std::isfinite(s)) throw std::invalid_argument("Tree box must have finite positive sides");
+    BinaryGeometry g{};
+    g.mortonOrder = 1;
+    for (unsigned d = 0; d < kBinDepth; ++d)
+    {
+        unsigned a = 0;
+        if (len[1] > len[a]) a = 1;
+        if (len[2] > len[a]) a = 2;
+        g.axis[d] = (unsigned char)a;
+        if (a != d % 3) g.mortonOrder = 0;
+        len[a] *= 0.5L;
+    }
+    g.xmin = bx[0];
+    g.xmax = bx[1];
+    g.ymin = bx[2];
+    g.ymax = bx[3];
+    g.zmin = bx[4];
+    g.zmax = bx[5];
+    return g;
+}
+
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+template <class Real, Curve C>
+void launchKeygenT(const Real *x, const Real *y, const Real *z, size_t n, const KeygenParams<Real> &prm, u64 *keys,
+                   u32 *hist, int passes, cudaStream_t s)
+{
+    const bool vec = aligned16(x) && aligned16(y) && aligned16(z);
+    constexpr int V = sizeof(Real) == 4 ? 4 : 2;
+    const size_t groups = vec ? n / V : n;
+    const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(std::max<size_t>(groups, 1), kKeygenThreads),
+                                                             unsigned(smCount()) * 8u));
+    if (vec) keygenKernel<Real, C, V><<<blocks, kKeygenThreads, 0, s>>>(x, y, z, n, prm, keys, hist, passes);
+    else keygenKernel<Real, C, 1><<<blocks, kKeygenThreads, 0, s>>>(x, y, z, n, prm, keys, hist, passes);
+    AOT_LAUNCH_CHECK();
+}
+
+template <class Real>
+void launchKeygen(int kind, bool hilbert, const Real *x, const Real *y, const Real *z, size_t n,
+                  const KeygenParams<Real> &prm, u64 *keys, u32 *hist, int passes, cudaStream_t s)
+{
+    if (kind == 1) launchKeygenT<Real, Curve::Binary>(x, y, z, n, prm, keys, hist, passes, s);
+    else if (hilbert) launchKeygenT<Real, Curve::Hilbert>(x, y, z, n, prm, keys, hist, passes, s);
+    else launchKeygenT<Real, Curve::Morton>(x, y, z, n, prm, keys, hist, passes, s);
+}
+
+__global__ void iotaKernel(u32 *perm, size_t n)
+{
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        perm[i] = u32(i);
+}
+
+// Sort scratch layout: hist[8][256] | bins[8][256] | tileCounters[8] (u32),
+// then status words (u64) for `passes` passes.
+struct SortArena
+{
+    DevMem counters, status;
+    size_t tilesCap = 0;
+    void ensure(size_t n)
+    {
+        const size_t tiles = std::max<size_t>(1, (n + sort::kTile - 1) / sort::kTile);
+        counters.reserve((2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses) * sizeof(u32));
+        if (tiles > tilesCap)
+        {
+            status.reserve(size_t(sort::kMaxPasses) * tiles * sort::kRadix * sizeof(u64));
+            tilesCap = tiles;
+        }
+    }
+    u32 *hist() const { return counters.as<u32>(); }
+    u32 *bins() const { return counters.as<u32>() + sort::kMaxPasses * sort::kRadix; }
+    u32 *tileCounters() const { return counters.as<u32>() + 2 * sort::kMaxPasses * sort::kRadix; }
+};
+
+void setPassSmem()
+{
+    static bool done = false;
+    if (!done)
+    {
+        AOT_CHECK(cudaFuncSetAttribute(sort::onesweepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(sort::passSmem())));
+        done = true;
+    }
+}
+
+// Onesweep passes over (k[0], v[0]) -> ... ; counts must already be in
+// hist.  valsAreIndices: the first pass generates the values.  Returns the
+// index (0/1) of the buffers holding the result.
+int runPasses(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int beginBit, int passes, bool valsAreIndices,
+              SortArena &a, int *error)
+{
+    setPassSmem();
+    const size_t tiles = (n + sort::kTile - 1) / sort::kTile;
+    sort::binsKernel<<<1, sort::kRadix, 0, s>>>(a.hist(), a.bins(), passes);
+    AOT_LAUNCH_CHECK();
+    for (int p = 0; p < passes; ++p)
+    {
+        const int in = p & 1, out = in ^ 1;
+        sort::onesweepKernel<<<unsigned(tiles), sort::kThreads, sort::passSmem(), s>>>(
+            k[in], (p == 0 && valsAreIndices) ? nullptr : v[in], k[out], v[out], n, beginBit + p * sort::kRadixBits,
+            a.bins() + p * sort::kRadix, a.tileCounters() + p, a.status.as<u64>() + size_t(p) * tiles * sort::kRadix,
+            error);
+        AOT_LAUNCH_CHECK();
+    }
+    return passes & 1;
+}
+
+void clearArena(cudaStream_t s, SortArena &a, size_t n, int passes)
+{
+    const size_t tiles = std::max<size_t>(1, (n + sort::kTile - 1) / sort::kTile);
+    AOT_CHECK(cudaMemsetAsync(a.counters.p, 0, a.counters.bytes, s));
+    AOT_CHECK(cudaMemsetAsync(a.status.p, 0, size_t(passes) * tiles * sort::kRadix * sizeof(u64), s));
+}
+
+// Generic stable sort of (keys, identity indices) by bits [0, 8*passes).
+int sortWithIndices(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int passes, SortArena &a, int *error)
+{
+    if (n == 0) return 0;
+    a.ensure(n);
+    clearArena(s, a, n, passes);
+    const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n, sort::kThreads), unsigned(smCount()) * 8u));
+    sort::histogramKernel<<<blocks, sort::kThreads, 0, s>>>(k[0], n, 0, passes, a.hist());
+    AOT_LAUNCH_CHECK();
+    return runPasses(s, k, v, n, 0, passes, true, a, error);
+}
+
+unsigned gridFor(size_t n, unsigned threads) { return std::max(1u, ceilDiv(std::max<size_t>(n, 1), threads)); }
+
+}  // namespace
+
+// --------------------------------------------------------------------------
+// Impl
+// --------------------------------------------------------------------------
+struct TreeEngine::Impl
+{
+    // particles
+    DevMem P[2], Perm[2], sample;
+    SortArena sortArena;
+    // state
+    DeviceState *st = nullptr;   // device
+    DeviceState *hst = nullptr;  // pinned mirror
+    cudaStream_t d2h = nullptr;
+    cudaEvent_t ready = nullptr;
+    DevMem history;
+    // tree
+    DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, groups, scan;
+    size_t scanTiles = 0;
+    // views
+    DevMem vBox, vSplit, vDepth, vParent, vChild, vLevelOffset, vPbegin, vPcount, vPmap, vMaxDepth;
+    DevMem vLeafLevel, vLeafToNode, vLevels, vCandStart, vCandLevel, vLvKeys[2], vLvVals[2], vLayKeys[2], vLayVals[2];
+    DevMem vIntStartSfc, vIntLevelSfc, vIntM, vIntStartLay, vIntLevelLay;
+    SortArena viewSort;
+    size_t viewLeafCap = 0, viewParticleCap = 0;
+    bool viewScratch = false;
+    adaptive_octree::ViewConfig viewPrepared{};
+    size_t viewNodesLogical = 0, mappingLogical = 0;
+    // keys
+    KeygenParams<float> kpf{};
+    KeygenParams<double> kpd{};
+
+    ~Impl()
+    {
+        if (st) cudaFree(st);
+        if (hst) cudaFreeHost(hst);
+        if (ready) cudaEventDestroy(ready);
+        if (d2h) cudaStreamDestroy(d2h);
+    }
+
+    rb::TreeBufs bufs() const
+    {
+        rb::TreeBufs t{};
+        for (int k = 0; k < 2; ++k)
+        {
+            t.K[k] = K[k].as<u64>();
+            t.B[k] = B[k].as<u32>();
+            t.NF[k] = NF[k].as<u32>();
+            t.G[k] = G[k].as<u8>();
+            t.N[k] = N[k].as<u32>();
+        }
+        t.offs = offs.as<i64>();
+        t.dirty = dirty.as<int>();
+        t.groups = groups.as<int>();
+        t.scanStatus = scan.as<u64>();
+        t.scanTile = reinterpret_cast<u32 *>(scan.as<u64>() + scanTiles);
+        t.st = st;
+        return t;
+    }
+    KeyIndex keyIndex(size_t n) const
+    {
+        KeyIndex k{};
+        k.keys = P[0].as<u64>();
+        k.sample = sample.as<u64>();
+        k.n = n;
+        k.ns = (n + kSampleStride - 1) >> kSampleShift;
+        return k;
+    }
+    tv::ViewBufs viewBufs() const
+    {
+        tv::ViewBufs v{};
+        v.box = vBox.as<u64>();
+        v.split = vSplit.as<u8>();
+        v.depth = vDepth.as<u8>();
+        v.parent = vParent.as<int>();
+        v.child = vChild.as<int>();
+        v.levelOffset = vLevelOffset.as<int>();
+        v.pbegin = vPbegin.as<u32>();
+        v.pcount = vPcount.as<u32>();
+        v.pmap = vPmap.as<u64>();
+        v.maxDepth = vMaxDepth.as<u8>();
+        v.leafLevel = vLeafLevel.as<u8>();
+        v.leafToNode = vLeafToNode.as<int>();
+        int *lv = vLevels.as<int>();
+        v.leavesPerLevel = lv;
+        v.internalPerLevel = lv + 66;
+        v.nodesPerLevel = lv + 2 * 66;
+        v.levelOffsetInternal = lv + 3 * 66;
+        v.candStart = vCandStart.as<u64>();
+        v.candLevel = vCandLevel.as<u8>();
+        v.lvKeys = vLvKeys[0].as<u64>();
+        v.lvKeysAlt = vLvKeys[1].as<u64>();
+        v.lvVals = vLvVals[0].as<u32>();
+        v.lvValsAlt = vLvVals[1].as<u32>();
+        v.layKeys = vLayKeys[0].as<u64>();
+        v.layKeysAlt = vLayKeys[1].as<u64>();
+        v.layVals = vLayVals[0].as<u32>();
+        v.layValsAlt = vLayVals[1].as<u32>();
+        v.intStartSfc = vIntStartSfc.as<u64>();
+        v.intLevelSfc = vIntLevelSfc.as<u8>();
+        v.intMBySfc = vIntM.as<int>();
+        v.intStartLay = vIntStartLay.as<u64>();
+        v.intLevelLay = vIntLevelLay.as<u8>();
+        return v;
+    }
+};
+
+// --------------------------------------------------------------------------
+// construction
+// --------------------------------------------------------------------------
+TreeEngine::TreeEngine(const void *x, const void *y, const void *z, size_t n, const EngineConfig &cfg)
+    : m_(std::make_unique<Impl>()), cfg_(cfg), n_(n), x_(x), y_(y), z_(z)
+{
+    // Backend constructor checks (octree.cu:321-416, kdtree3d.cu:175-216).
+    if (n > 0 && (!x || !y || !z))
+        throw std::invalid_argument("adaptive_octree: coordinate device pointers must not be null");
+    if (cfg.bucket == 0) throw std::invalid_argument("adaptive_octree: particle limit must be positive");
+    if (cfg.iterations == 0) throw std::invalid_argument("adaptive_octree: updateIterations must be positive");
+    if (cfg.kind == 1) m_->kpd.g = makeGeometry(cfg.box, cfg.maxDepth, cfg.real), m_->kpf.g = m_->kpd.g;
+    if (n > size_t(std::numeric_limits<std::uint32_t>::max()))
+        throw std::invalid_argument(
+            "adaptive_octree: particle count exceeds 32-bit permutation index range");
+    m_->kpf.q = makeQuantBox<float>(cfg.box);
+    m_->kpd.q = makeQuantBox<double>(cfg.box);
+    m_->kpf.h = hilbertTables();
+    m_->kpd.h = hilbertTables();
+    prepared_ = cfg.views;
+
+    AOT_CHECK(cudaMalloc(&m_->st, sizeof(DeviceState)));
+    AOT_CHECK(cudaMemset(m_->st, 0, sizeof(DeviceState)));
+    AOT_CHECK(cudaMallocHost(&m_->hst, sizeof(DeviceState)));
+    std::memset(m_->hst, 0, sizeof(DeviceState));
+    AOT_CHECK(cudaStreamCreateWithFlags(&m_->d2h, cudaStreamNonBlocking));
+    AOT_CHECK(cudaEventCreateWithFlags(&m_->ready, cudaEventDisableTiming));
+    if (n)
+    {
+        for (int k = 0; k < 2; ++k)
+        {
+            m_->P[k].reserve(n * sizeof(u64));
+            m_->Perm[k].reserve(n * sizeof(u32));
+        }
+        m_->sample.reserve(((n + kSampleStride - 1) >> kSampleShift) * sizeof(u64));
+        m_->sortArena.ensure(n);
+    }
+    // K_d.resize(2) in the constructor (octree.cu:149)
+    kSize_ = 2;
+    kCap_ = 2;
+    ensurePhysical(16);
+    if (cfg.kind == 0)
+    {
+        const u64 root[2] = {0, kMaxKey};
+        AOT_CHECK(cudaMemcpy(m_->K[0].p, root, sizeof(root), cudaMemcpyHostToDevice));
+    }
+}
+
+TreeEngine::~TreeEngine() = default;
+
+void TreeEngine::setCoordinates(const void *x, const void *y, const void *z)
+{
+    if (n_ > 0 && (!x || !y || !z))
+        throw std::invalid_argument("adaptive_octree: coordinate device pointers must not be null");
+    x_ = x;
+    y_ = y;
+    z_ = z;
+}
+
+// Physical capacity of the leaf buffers (>= leafCapacity at all times).
+void TreeEngine::ensurePhysical(size_t capacity)
+{
+    if (capacity <= physCap_ && m_->K[0].p) return;
+    cudaStream_t s = cfg_.stream;
+    const size_t c = std::max(capacity, physCap_);
+    for (int k = 0; k < 2; ++k)
+    {
+        m_->K[k].grow((c + 1) * sizeof(u64), m_->K[k].bytes, s);
+        m_->B[k].grow((c + 1) * sizeof(u32), m_->B[k].bytes, s);
+        m_->N[k].grow((c + 1) * sizeof(u32), m_->N[k].bytes, s);
+        if (cfg_.kind == 0 && cfg_.nf)
+        {
+            m_->NF[k].grow((c + 1) * sizeof(u32), m_->NF[k].bytes, s);
+            m_->G[k].grow((c + 1) * sizeof(u8), m_->G[k].bytes, s);
+        }
+        else
+        {
+            m_->NF[k].grow(sizeof(u32) * (c + 1), m_->NF[k].bytes, s);
+            m_->G[k].grow(16, m_->G[k].bytes, s);
+        }
+    }
+    m_->offs.reserve((c + 1) * sizeof(i64));
+    m_->dirty.reserve((c + 1) * sizeof(int));
+    // candidate group leaders are first children of distinct internal nodes: <= (L - 1) / 7
+    m_->groups.reserve((c / 7 + 8) * sizeof(int));
+    m_->scanTiles = (c + 1 + rb::kScanTile - 1) / rb::kScanTile;
+    m_->scan.reserve((m_->scanTiles + 1) * sizeof(u64));
+    physCap_ = c;
+}
+
+// --------------------------------------------------------------------------
+// keys + sort (octree.cu:285-307, kdtree3d.cu:161-172)
+// --------------------------------------------------------------------------
+void TreeEngine::sortParticles()
+{
+    if (n_ == 0) return;
+    cudaStream_t s = cfg_.stream;
+    SortArena &a = m_->sortArena;
+    a.ensure(n_);
+    clearArena(s, a, n_, sort::kMaxPasses);
+    u64 *k[2] = {m_->P[0].as<u64>(), m_->P[1].as<u64>()};
+    u32 *v[2] = {m_->Perm[0].as<u32>(), m_->Perm[1].as<u32>()};
+    if (cfg_.real == 0)
+        launchKeygen<float>(cfg_.kind, cfg_.hilbert, static_cast<const float *>(x_), static_cast<const float *>(y_),
+                            static_cast<const float *>(z_), n_, m_->kpf, k[0], a.hist(), sort::kMaxPasses, s);
+    else
+        launchKeygen<double>(cfg_.kind, cfg_.hilbert, static_cast<const double *>(x_), static_cast<const double *>(y_),
+                             static_cast<const double *>(z_), n_, m_->kpd, k[0], a.hist(), sort::kMaxPasses, s);
+    const int where = runPasses(s, k, v, n_, 0, sort::kMaxPasses, true, a, &m_->st->error);
+    (void)where;  // eight passes end in buffer 0
+    const size_t ns = (n_ + kSampleStride - 1) >> kSampleShift;
+    rb::sampleKeysKernel<<<gridFor(ns, 256), 256, 0, s>>>(k[0], n_, m_->sample.as<u64>(), ns);
+    AOT_LAUNCH_CHECK();
+}
+
+void TreeEngine::computeKeys(int kind, int real, const void *x, const void *y, const void *z, size_t n,
+                             const double *box, bool hilbert, unsigned maxDepth, unsigned long long *keys,
+                             unsigned *perm, cudaStream_t s)
+{
+    if (n == 0) return;
+    if (n > size_t(std::numeric_limits<std::uint32_t>::max()))
+        throw std::invalid_argument("adaptive_octree: particle count exceeds 32-bit permutation index range");
+    KeygenParams<float> pf{};
+    KeygenParams<double> pd{};
+    if (kind == 1) pd.g = pf.g = makeGeometry(box, maxDepth, real);
+    pf.q = makeQuantBox<float>(box);
+    pd.q = makeQuantBox<double>(box);
+    pf.h = pd.h = hilbertTables();
+    if (real == 0)
+        launchKeygen<float>(kind, hilbert, static_cast<const float *>(x), static_cast<const float *>(y),
+                            static_cast<const float *>(z), n, pf, reinterpret_cast<u64 *>(keys), nullptr, 0, s);
+    else
+        launchKeygen<double>(kind, hilbert, static_cast<const double *>(x), static_cast<const double *>(y),
+                             static_cast<const double *>(z), n, pd, reinterpret_cast<u64 *>(keys), nullptr, 0, s);
+    if (perm)
+    {
+        iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(perm, n);
+        AOT_LAUNCH_CHECK();
+    }
+}
+
+// --------------------------------------------------------------------------
+// rebalance passes
+// --------------------------------------------------------------------------
+namespace
+{
+__global__ void octInitRootKernel(rb::TreeBufs tb, const u64 *P, size_t n)
+{
+    DeviceState *st = tb.st;
+    const unsigned active = n ? unsigned(lowerBoundDev(P, n, kMaxKey)) : 0u;
+    tb.K[0][0] = 0;
+    tb.K[0][1] = kMaxKey;
+    tb.B[0][0] = 0;
+    tb.B[0][1] = active;
+    const u64 sq = u64(active) * active;
+    tb.NF[0][0] = sq > 0xffffffffull / 27ull ? 0xffffffffu : u32(27ull * sq);  // octree.cu:23-38
+    const int err = st->error;
+    *st = DeviceState{};
+    st->error = err;
+    st->numLeaves = 1;
+    st->newNumLeaves = 1;
+    st->numActiveParticles = active;
+}
+
+// finishBuildStateKernel (octree.cu:40-47)
+__global__ void octFinishBuildKernel(DeviceState *st)
+{
+    st->newNumLeaves = st->numLeaves;
+    st->changed = st->converged = st->needsResize = 0;
+    st->numNodes = 0;
+    st->activeBuffer = 0;
+    st->overflow = 0;
+}
+
+// initBinaryRootKernel (kdtree3d.cu:24-30)
+__global__ void binInitRootKernel(rb::TreeBufs tb, long long logicalCap)
+{
+    DeviceState *st = tb.st;
+    tb.K[0][0] = 0;
+    tb.K[0][1] = kMaxKey;
+    const int err = st->error;
+    *st = DeviceState{};
+    st->error = err;
+    st->numLeaves = 1;
+    st->newNumLeaves = 1;
+    st->numNodes = 1;
+    st->logicalCap = logicalCap;
+}
+
+__global__ void clearOverflowKernel(DeviceState *st) { st->overflow = 0; }
+}  // namespace
+
+void TreeEngine::octreePass(bool buildMode, long long limit)
+{
+    cudaStream_t s = cfg_.stream;
+    const rb::TreeBufs tb = m_->bufs();
+    const size_t cap = buildMode ? physCap_ : leafCapacity_;
+    const size_t tiles = (cap + 1 + rb::kScanTile - 1) / rb::kScanTile;
+    rb::beginPassKernel<<<1, 1, 0, s>>>(m_->st);
+    AOT_CHECK(cudaMemsetAsync(m_->scan.p, 0, (m_->scanTiles + 1) * sizeof(u64), s));
+    const KeyIndex idx = m_->keyIndex(n_);
+    const int mode = buildMode ? kModeOctreeBuild : kModeUpdate;
+    long long *hist = buildMode ? m_->history.as<long long>() : nullptr;
+    const unsigned scatterBlocks = gridFor(cap, rb::kScatterThreads);
+    const unsigned refreshBlocks = unsigned(smCount()) * 8u;
+    if (cfg_.nf)
+    {
+        rb::octDecideScanKernel<true><<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket);
+        rb::octScatterKernel<true><<<scatterBlocks, rb::kScatterThreads, 0, s>>>(tb, limit, mode, hist);
+        if (cfg_.hilbert)
+            rb::octRefreshKernel<true, true, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(
+                tb, idx, cfg_.bucket, m_->kpd.h);
+        else
+            rb::octRefreshKernel<true, false, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(
+                tb, idx, cfg_.bucket, m_->kpd.h);
+    }
+    else
+    {
+        rb::octDecideScanKernel<false><<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket);
+        rb::octScatterKernel<false><<<scatterBlocks, rb::kScatterThreads, 0, s>>>(tb, limit, mode, hist);
+        rb::octRefreshKernel<false, false, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
+                                                                                                m_->kpd.h);
+    }
+    AOT_LAUNCH_CHECK();
+}
+
+void TreeEngine::binaryPass(bool buildMode, long long limit)
+{
+    cudaStream_t s = cfg_.stream;
+    const rb::TreeBufs tb = m_->bufs();
+    const size_t cap = buildMode ? physCap_ : leafCapacity_;
+    const size_t tiles = (cap + 1 + rb::kScanTile - 1) / rb::kScanTile;
+    rb::beginPassKernel<<<1, 1, 0, s>>>(m_->st);
+    AOT_CHECK(cudaMemsetAsync(m_->scan.p, 0, (m_->scanTiles + 1) * sizeof(u64), s));
+    const KeyIndex idx = m_->keyIndex(n_);
+    rb::binDecideScanKernel<<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket, cfg_.maxDepth);
+    rb::binScatterKernel<<<gridFor(cap, rb::kScatterThreads), rb::kScatterThreads, 0, s>>>(
+        tb, limit, buildMode ? kModeBinaryBuild : kModeUpdate);
+    rb::binRefreshKernel<false><<<unsigned(smCount()) * 8u, 256, 0, s>>>(tb, idx);
+    AOT_LAUNCH_CHECK();
+}
+
+// Full refresh of the per-leaf quantities of the active tree, after the
+// reset of changed/converged/active count (resetRebalanceStateKernel +
+// refreshGraphCountsGpu without dirty lists).
+void TreeEngine::refreshAll()
+{
+    cudaStream_t s = cfg_.stream;
+    const rb::TreeBufs tb = m_->bufs();
+    const KeyIndex idx = m_->keyIndex(n_);
+    rb::resetForUpdateKernel<<<1, 1, 0, s>>>(m_->st, m_->P[0].as<u64>(), n_);
+    const unsigned blocks = unsigned(smCount()) * 8u;
+    if (cfg_.kind == 1)
+        rb::binRefreshKernel<true><<<blocks, 256, 0, s>>>(tb, idx);
+    else if (!cfg_.nf)
+        rb::octRefreshKernel<false, false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
+                                                                                        m_->kpd.h);
+    else if (cfg_.hilbert)
+        rb::octRefreshKernel<true, true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, m_->kpd.h);
+    else
+        rb::octRefreshKernel<true, false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
+                                                                                       m_->kpd.h);
+    AOT_LAUNCH_CHECK();
+}
+
+void TreeEngine::materializeCounts()
+{
+    rb::materializeCountsKernel<<<gridFor(std::max(leafCapacity_, physCap_), 256), 256, 0, cfg_.stream>>>(m_->bufs());
+    AOT_LAUNCH_CHECK();
+}
+
+// --------------------------------------------------------------------------
+// state readback (octree.cu:498-537, kdtree3d.cu:127-137)
+// --------------------------------------------------------------------------
+void TreeEngine::readState()
+{
+    AOT_CHECK(cudaEventRecord(m_->ready, cfg_.stream));
+    AOT_CHECK(cudaStreamWaitEvent(m_->d2h, m_->ready, 0));
+    AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, m_->d2h));
+    AOT_CHECK(cudaStreamSynchronize(m_->d2h));
+    const DeviceState &h = *m_->hst;
+    if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
+    hostActiveBuffer_ = h.activeBuffer;
+    hostLeaves_ = size_t(std::max(h.numLeaves, 0));
+    hostActive_ = h.numActiveParticles;
+    hostNodes_ = size_t(std::max(h.numNodes, 0));
+    if (cfg_.kind == 0)
+    {
+        kSize_ = hostLeaves_ + 1;
+        tSize_ = hostLeaves_ + 1;
+    }
+    syncViewSizes();
+}
+
+bool TreeEngine::doBuffersNeedResize()
+{
+    if (!built_) return false;
+    readState();
+    return m_->hst->needsResize != 0;
+}
+
+// --------------------------------------------------------------------------
+// capacity (octree.cu:182-241, kdtree3d.cu:96-116)
+// --------------------------------------------------------------------------
+namespace
+{
+void capResize(size_t &size, size_t &cap, size_t n)  // vector growth (append)
+{
+    if (n > cap) cap = std::max(size + std::max(size, n - size), 2 * cap);
+    size = n;
+}
+void capReserve(size_t &cap, size_t n) { cap = std::max(cap, n); }
+}  // namespace
+
+void TreeEngine::prepareGraphBuffers(size_t capacity)
+{
+    if (cfg_.kind == 0)
+    {
+        const size_t maxLeaves = (size_t(std::numeric_limits<int>::max()) - 1) / 8 * 7 + 1;
+        if (capacity > maxLeaves) throw std::length_error("adaptive_octree: buffer capacity exceeds node index range");
+        const size_t leaves = kSize_ - 1;
+        leafCapacity_ = capacity;
+        capReserve(kCap_, capacity + 1);
+        capResize(kSize_, kCap_, capacity + 1);
+        capReserve(tCap_, capacity + 1);
+        capResize(tSize_, tCap_, capacity + 1);
+        ensurePhysical(capacity);
+        prepareViews(capacity, prepared_);
+        kSize_ = tSize_ = leaves + 1;
+        syncViewSizes();
+    }
+    else
+    {
+        const size_t maxLeaves = size_t(std::numeric_limits<int>::max()) / 2 + 1;
+        if (capacity > maxLeaves) throw std::length_error("adaptive_octree: buffer capacity exceeds node index range");
+        leafCapacity_ = capacity;
+        ensurePhysical(capacity);
+        if (built_ && prepared_.treeStructure | prepared_.particleCountsPerBox | prepared_.particleMapping)
+            prepareViews(capacity, prepared_);
+        syncViewSizes();
+    }
+}
+
+void TreeEngine::resizeBuffers()
+{
+    if (!built_) throw std::logic_error("adaptive_octree: call build() before resizeBuffers()");
+    readState();
+    prepareGraphBuffers(leafCapacity_ + (leafCapacity_ + 3) / 4);
+    AOT_CHECK(cudaMemsetAsync(&m_->st->needsResize, 0, sizeof(int), cfg_.stream));
+    AOT_CHECK(cudaStreamSynchronize(cfg_.stream));
+}
+
+// --------------------------------------------------------------------------
+// build / update
+// --------------------------------------------------------------------------
+void TreeEngine::build()
+{
+    if (cfg_.kind == 0) octreeBuild();
+    else binaryBuild();
+}
+
+void TreeEngine::octreeBuild()
+{
+    cudaStream_t s = cfg_.stream;
+    AOT_CHECK(cudaStreamSynchronize(s));
+    kSize_ = 2;
+    sortParticles();
+    // Room for the build rounds; grown on overflow.
+    const size_t estimate = std::max<size_t>(4096, cfg_.nf ? n_ + 4096 : n_ / 4 + 4096);
+    ensurePhysical(std::max(physCap_, estimate));
+    m_->history.reserve(std::max<size_t>(cfg_.maxDepth, 1) * sizeof(long long));
+    rb::TreeBufs tb = m_->bufs();
+    octInitRootKernel<<<1, 1, 0, s>>>(tb, m_->P[0].as<u64>(), n_);
+    AOT_LAUNCH_CHECK();
+    // rebalanceBuild (octree.cu:159-180): at most maxDepth decision rounds
+    int done = 0;
+    const int maxRounds = int(cfg_.maxDepth);
+    while (done < maxRounds)
+    {
+        const int batch = std::min(4, maxRounds - done);
+        for (int r = 0; r < batch; ++r) octreePass(true, (long long)physCap_);
+        AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
+        AOT_CHECK(cudaStreamSynchronize(s));
+        const DeviceState h = *m_->hst;
+        if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
+        done = h.rounds;
+        if (h.converged) break;
+        if (h.overflow)
+        {
+            const size_t need = size_t(h.proposal);
+            ensurePhysical(std::max(need + need / 4, 2 * physCap_));
+            clearOverflowKernel<<<1, 1, 0, s>>>(m_->st);
+            AOT_LAUNCH_CHECK();
+        }
+    }
+    AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
+    AOT_CHECK(cudaStreamSynchronize(s));
+    const DeviceState h = *m_->hst;
+    buildRounds_ = h.iteration;
+    // Replay the reference's K_d/tmpTree capacity history (octree.cu:159-180,
+    // 453-457; resizeWithHeadroom, helpers.cuh:122-141).
+    std::vector<long long> proposals(size_t(h.iteration));
+    if (h.iteration)
+        AOT_CHECK(cudaMemcpy(proposals.data(), m_->history.p, proposals.size() * sizeof(long long),
+                             cudaMemcpyDeviceToHost));
+    for (long long p : proposals)
+    {
+        const size_t req = size_t(p) + 1;
+        if (req > tCap_) tCap_ = req + req / 4;
+        tSize_ = req;
+        std::swap(kSize_, tSize_);
+        std::swap(kCap_, tCap_);
+    }
+    const size_t leaves = size_t(h.numLeaves);
+    kSize_ = leaves + 1;
+    hostLeaves_ = leaves;
+    const size_t cap = std::max({kCap_ - 1, tSize_ == 0 ? size_t(0) : tCap_ - 1, leaves + (leaves + 3) / 4});
+    // The final tree must sit in buffer 0 (finishBuildStateKernel resets the
+    // active buffer).
+    if (h.activeBuffer == 1)
+    {
+        AOT_CHECK(cudaMemcpyAsync(m_->K[0].p, m_->K[1].p, (leaves + 1) * sizeof(u64), cudaMemcpyDeviceToDevice, s));
+        AOT_CHECK(cudaMemcpyAsync(m_->B[0].p, m_->B[1].p, (leaves + 1) * sizeof(u32), cudaMemcpyDeviceToDevice, s));
+        if (cfg_.nf)
+        {
+            AOT_CHECK(cudaMemcpyAsync(m_->NF[0].p, m_->NF[1].p, leaves * sizeof(u32), cudaMemcpyDeviceToDevice, s));
+            AOT_CHECK(cudaMemcpyAsync(m_->G[0].p, m_->G[1].p, leaves * sizeof(u8), cudaMemcpyDeviceToDevice, s));
+        }
+    }
+    octFinishBuildKernel<<<1, 1, 0, s>>>(m_->st);
+    AOT_LAUNCH_CHECK();
+    prepareGraphBuffers(cap);
+    built_ = true;
+    materializeCounts();
+    buildViews(cfg_.views);
+    (void)doBuffersNeedResize();
+}
+
+void TreeEngine::binaryBuild()
+{
+    cudaStream_t s = cfg_.stream;
+    AOT_CHECK(cudaStreamSynchronize(s));
+    built_ = false;
+    hostLeaves_ = 1;
+    prepareGraphBuffers(std::max<size_t>(2, leafCapacity_));
+    sortParticles();
+    const size_t estimate = std::max<size_t>(4096, 4 * (n_ / std::max(1u, cfg_.bucket)) + 4096);
+    ensurePhysical(std::max({physCap_, estimate, leafCapacity_}));
+    rb::TreeBufs tb = m_->bufs();
+    binInitRootKernel<<<1, 1, 0, s>>>(tb, (long long)leafCapacity_);
+    AOT_LAUNCH_CHECK();
+    refreshAll();
+    // build loop (kdtree3d.cu:239-249): passes until converged
+    long long passes = 0;
+    for (;;)
+    {
+        const int batch = 8;
+        for (int r = 0; r < batch; ++r) binaryPass(true, (long long)physCap_);
+        passes += batch;
+        AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
+        AOT_CHECK(cudaStreamSynchronize(s));
+        const DeviceState h = *m_->hst;
+        if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
+        if (h.converged) break;
+        if (h.overflow)
+        {
+            const size_t need = size_t(h.proposal);
+            ensurePhysical(std::max(need + need / 4, 2 * physCap_));
+            clearOverflowKernel<<<1, 1, 0, s>>>(m_->st);
+            AOT_LAUNCH_CHECK();
+        }
+        if (passes > 200000) throw std::runtime_error("adaptive_octree: binary build did not converge");
+    }
+    buildRounds_ = m_->hst->iteration;
+    leafCapacity_ = size_t(m_->hst->logicalCap);
+    ensurePhysical(leafCapacity_);
+    built_ = true;
+    if (prepared_.treeStructure | prepared_.particleCountsPerBox | prepared_.particleMapping)
+        prepareViews(leafCapacity_, prepared_);
+    materializeCounts();
+    buildViews(cfg_.views);
+    readState();
+}
+
+void TreeEngine::update()
+{
+    if (!built_) throw std::logic_error("adaptive_octree: call build() before update()");
+    sortParticles();
+    refreshAll();
+    for (unsigned i = 0; i < cfg_.iterations; ++i)
+    {
+        if (cfg_.kind == 0) octreePass(false, (long long)leafCapacity_);
+        else binaryPass(false, (long long)leafCapacity_);
+    }
+    materializeCounts();
+    buildViews(cfg_.views);
+}
+
+void TreeEngine::computeViews(const adaptive_octree::ViewConfig &v)
+{
+    if (!built_) throw std::logic_error("adaptive_octree: call build() before computeViews()");
+    buildViews(v);
+}
+
+// --------------------------------------------------------------------------
+// views (tree_view.cu:755-1134)
+// --------------------------------------------------------------------------
+void TreeEngine::prepareViews(size_t capacity, const adaptive_octree::ViewConfig &v)
+{
+    if (!(v.treeStructure | v.particleCountsPerBox | v.particleMapping)) return;
+    Impl &m = *m_;
+    cudaStream_t s = cfg_.stream;
+    m.viewLeafCap = std::max(m.viewLeafCap, capacity);
+    m.viewParticleCap = std::max(m.viewParticleCap, n_);
+    m.viewPrepared.treeStructure |= v.treeStructure;
+    m.viewPrepared.particleCountsPerBox |= v.particleCountsPerBox;
+    m.viewPrepared.particleMapping |= v.particleMapping;
+    m.viewScratch = true;
+    const int b = cfg_.kind == 0 ? 3 : 1;
+    const size_t L = std::max<size_t>(m.viewLeafCap, 1);
+    const size_t I = (L - 1) / ((size_t(1) << b) - 1);
+    const size_t nodes = L + I;
+    m.vBox.grow(nodes * 8, m.vBox.bytes, s);
+    m.vSplit.grow(nodes, m.vSplit.bytes, s);
+    m.vDepth.grow(nodes, m.vDepth.bytes, s);
+    m.vParent.grow(nodes * 4, m.vParent.bytes, s);
+    m.vChild.grow(nodes * 4, m.vChild.bytes, s);
+    m.vLevelOffset.grow(66 * 4, m.vLevelOffset.bytes, s);
+    m.vMaxDepth.grow(16, m.vMaxDepth.bytes, s);
+    if (m.viewPrepared.particleCountsPerBox)
+    {
+        m.vPbegin.grow(nodes * 4, m.vPbegin.bytes, s);
+        m.vPcount.grow((nodes + 1) * 4, m.vPcount.bytes, s);
+    }
+    if (m.viewPrepared.particleMapping) m.vPmap.grow(std::max<size_t>(m.viewParticleCap, 1) * 8, m.vPmap.bytes, s);
+    m.vLeafLevel.reserve(L);
+    m.vLeafToNode.reserve(L * 4);
+    m.vLevels.reserve(4 * 66 * 4);
+    m.vCandStart.reserve(L * 8);
+    m.vCandLevel.reserve(L);
+    for (int k = 0; k < 2; ++k)
+    {
+        m.vLvKeys[k].reserve(L * 8);
+        m.vLvVals[k].reserve(L * 4);
+        m.vLayKeys[k].reserve(std::max<size_t>(I, 1) * 8);
+        m.vLayVals[k].reserve(std::max<size_t>(I, 1) * 4);
+    }
+    m.vIntStartSfc.reserve(std::max<size_t>(I, 1) * 8);
+    m.vIntLevelSfc.reserve(std::max<size_t>(I, 1));
+    m.vIntM.reserve(std::max<size_t>(I, 1) * 4);
+    m.vIntStartLay.reserve(std::max<size_t>(I, 1) * 8);
+    m.vIntLevelLay.reserve(std::max<size_t>(I, 1));
+    m.viewSort.ensure(L);
+}
+
+void TreeEngine::syncViewSizes()
+{
+    Impl &m = *m_;
+    if (!m.viewScratch || hostLeaves_ > m.viewLeafCap) return;
+    const size_t k = cfg_.kind == 0 ? 7 : 1;
+    m.viewNodesLogical = hostLeaves_ + (hostLeaves_ - 1) / k;
+    if (m.viewPrepared.particleMapping) m.mappingLogical = hostActive_;
+}
+
+void TreeEngine::buildViews(const adaptive_octree::ViewConfig &v)
+{
+    prepared_.treeStructure |= v.treeStructure;
+    prepared_.particleCountsPerBox |= v.particleCountsPerBox;
+    prepared_.particleMapping |= v.particleMapping;
+    if (!(v.treeStructure | v.particleCountsPerBox | v.particleMapping)) return;
+    Impl &m = *m_;
+    cudaStream_t s = cfg_.stream;
+    if (!m.viewScratch || (v.particleCountsPerBox && !m.viewPrepared.particleCountsPerBox) ||
+        (v.particleMapping && (!m.viewPrepared.particleMapping || n_ > m.viewParticleCap)))
+    {
+        tv::flagResizeKernel<<<1, 1, 0, s>>>(m.st);
+        AOT_LAUNCH_CHECK();
+        return;
+    }
+    const int b = cfg_.kind == 0 ? 3 : 1;
+    const int leafCap = int(m.viewLeafCap);
+    const int intCap = (leafCap - 1) / ((1 << b) - 1);
+    const tv::ViewBufs vb = m.viewBufs();
+    const u64 *K0 = m.K[0].as<u64>(), *K1 = m.K[1].as<u64>();
+    const u32 *B0 = m.B[0].as<u32>(), *B1 = m.B[1].as<u32>();
+    const KeyIndex idx = m.keyIndex(n_);
+    const int counts = v.particleCountsPerBox ? 1 : 0;
+    AOT_CHECK(cudaMemsetAsync(vb.leavesPerLevel, 0, 66 * sizeof(int), s));
+    if (b == 3)
+    {
+        tv::classifyKernel<3><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, m.st, leafCap, vb);
+        tv::metadataKernel<3><<<1, 1, 0, s>>>(m.st, leafCap, vb);
+    }
+    else
+    {
+        tv::classifyKernel<1><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, m.st, leafCap, vb);
+        tv::metadataKernel<1><<<1, 1, 0, s>>>(m.st, leafCap, vb);
+    }
+    AOT_LAUNCH_CHECK();
+    if (intCap > 0)
+    {
+        // stable order of internal nodes by level (non-internal boundaries last)
+        u64 *lk[2] = {vb.lvKeys, vb.lvKeysAlt};
+        u32 *lv[2] = {vb.lvVals, vb.lvValsAlt};
+        const int w1 = sortWithIndices(s, lk, lv, size_t(leafCap - 1), 1, m.viewSort, &m.st->error);
+        if (b == 3)
+            tv::layoutKeysKernel<3><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(lk[w1], lv[w1], intCap, vb);
+        else
+            tv::layoutKeysKernel<1><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(lk[w1], lv[w1], intCap, vb);
+        AOT_LAUNCH_CHECK();
+        u64 *yk[2] = {vb.layKeys, vb.layKeysAlt};
+        u32 *yv[2] = {vb.layVals, vb.layValsAlt};
+        const int w2 = sortWithIndices(s, yk, yv, size_t(intCap), 8, m.viewSort, &m.st->error);
+        tv::materializeKernel<<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(yk[w2], yv[w2], intCap, vb);
+        if (b == 3)
+            tv::internalNodesKernel<3><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(m.st, leafCap, intCap,
+                                                                                              idx, counts, vb);
+        else
+            tv::internalNodesKernel<1><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(m.st, leafCap, intCap,
+                                                                                              idx, counts, vb);
+        AOT_LAUNCH_CHECK();
+    }
+    if (b == 3)
+        tv::leafNodesKernel<3><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, B0, B1, m.st, leafCap,
+                                                                                      counts, vb);
+    else
+        tv::leafNodesKernel<1><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, B0, B1, m.st, leafCap,
+                                                                                      counts, vb);
+    AOT_LAUNCH_CHECK();
+    if (v.particleMapping && n_ > 0)
+    {
+        tv::mappingKernel<<<gridFor(n_, tv::kThreads), tv::kThreads, 0, s>>>(B0, B1, m.st, leafCap, n_, vb);
+        AOT_LAUNCH_CHECK();
+    }
+}
+
+// --------------------------------------------------------------------------
+// getters
+// --------------------------------------------------------------------------
+void TreeEngine::buffer(int which, const void **ptr, size_t *len, size_t *cap, size_t *elem) const
+{
+    const Impl &m = *m_;
+    const int a = hostActiveBuffer_;
+    const size_t nodes = m.viewScratch ? m.viewNodesLogical : 0;
+    const size_t nodeCap = m.viewScratch ? m.vBox.bytes / 8 : 0;
+    const void *p = nullptr;
+    size_t l = 0, c = 0, e = 1;
+    switch (which)
+    {
+    case ParticleKeys: p = m.P[0].p; l = c = n_; e = 8; break;
+    case Perm: p = m.Perm[0].p; l = c = n_; e = 4; break;
+    case Cornerstone: p = m.K[a].p; l = hostLeaves_ + 1; c = physCap_ + 1; e = 8; break;
+    case LeafCounts: p = m.N[a].p; l = hostLeaves_; c = physCap_; e = 4; break;
+    case NearFieldCounts:
+        if (cfg_.kind == 1) throw std::logic_error("Tree: Binary NFCount is not implemented yet");
+        p = m.NF[a].p; l = hostLeaves_; c = physCap_; e = 4; break;
+    case SfcBoxIndex: p = m.vBox.p; l = nodes; c = nodeCap; e = 8; break;
+    case HasBoxSplit: p = m.vSplit.p; l = nodes; c = nodeCap; e = 1; break;
+    case BoxDepth: p = m.vDepth.p; l = nodes; c = nodeCap; e = 1; break;
+    case ParentIndex: p = m.vParent.p; l = nodes; c = nodeCap; e = 4; break;
+    case ChildIndex: p = m.vChild.p; l = nodes; c = nodeCap; e = 4; break;
+    case LevelOffset:
+        p = m.vLevelOffset.p;
+        l = c = m.viewScratch ? (cfg_.kind == 0 ? 23 : 65) : 0;
+        e = 4;
+        break;
+    case ParticleBeginIndex:
+        p = m.vPbegin.p;
+        l = (m.viewScratch && m.viewPrepared.particleCountsPerBox) ? nodes : 0;
+        c = m.vPbegin.bytes / 4;
+        e = 4;
+        break;
+    case ParticleCounts:
+        p = m.vPcount.p;
+        l = (m.viewScratch && m.viewPrepared.particleCountsPerBox) ? nodes + 1 : 0;
+        c = m.vPcount.bytes / 4;
+        e = 4;
+        break;
+    case SfcParticleIndex:
+        p = m.vPmap.p;
+        l = (m.viewScratch && m.viewPrepared.particleMapping) ? m.mappingLogical : 0;
+        c = m.vPmap.bytes / 8;
+        e = 8;
+        break;
+    default: throw std::invalid_argument("adaptive_octree: unknown buffer");
+    }
+    if (ptr) *ptr = p;
+    if (len) *len = l;
+    if (cap) *cap = c;
+    if (elem) *elem = e;
+}
+
+const int *TreeEngine::numLeavesDevice() const { return &m_->st->numLeaves; }
+const int *TreeEngine::numNodesDevice() const { return &m_->st->numNodes; }
+const unsigned *TreeEngine::numActiveParticlesDevice() const { return &m_->st->numActiveParticles; }
+
+unsigned TreeEngine::maxAchievedDepth() const
+{
+    const Impl &m = *m_;
+    cudaStream_t s = cfg_.stream;
+    if (cfg_.kind == 1 && !(cfg_.views.treeStructure | cfg_.views.particleCountsPerBox | cfg_.views.particleMapping))
+    {
+        // kdtree3d.cu: maxAchievedDepth from the cornerstone when no view is configured
+        std::vector<u64> k(hostLeaves_ + 1);
+        AOT_CHECK(cudaMemcpyAsync(k.data(), m.K[hostActiveBuffer_].p, k.size() * 8, cudaMemcpyDeviceToHost, s));
+        AOT_CHECK(cudaStreamSynchronize(s));
+        unsigned d = 0;
+        for (size_t i = 0; i + 1 < k.size(); ++i) d = std::max(d, unsigned(clz64(k[i + 1] - k[i])));
+        return d;
+    }
+    if (!m.viewScratch) return 0;
+    u8 v = 0;
+    AOT_CHECK(cudaMemcpyAsync(&v, m.vMaxDepth.p, 1, cudaMemcpyDeviceToHost, s));
+    AOT_CHECK(cudaStreamSynchronize(s));
+    return v;
+}
+
+}  // namespace aot

@@ -1,0 +1,137 @@
+// engine.hpp -- host-side engine shared by Octree<Real>, KDTree3D<Real> and the C ABI.
+//
+// One TreeEngine holds one tree: borrowed device coordinates, the sorted keys
+// P and permutation Perm, the A/B leaf buffers, the device-resident state,
+// the capacity bookkeeping of the reference and the view arrays.  All work is
+// issued on the caller's stream; update() and computeViews() issue only
+// kernel launches and memsets and can be captured into a CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "adaptive_octree/config.hpp"
+
+namespace aot
+{
+struct DeviceState;
+
+// A CUDA runtime failure inside the engine.
+struct CudaError : std::runtime_error
+{
+    cudaError_t code;
+    CudaError(cudaError_t c, const char *what)
+        : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+inline void check(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) throw CudaError(e, what);
+}
+#define AOT_CHECK(x) ::aot::check((x), #x)
+#define AOT_LAUNCH_CHECK() ::aot::check(cudaGetLastError(), "kernel launch")
+
+struct EngineConfig
+{
+    int kind = 0;   // 0 octree, 1 binary
+    int real = 1;   // 0 float, 1 double
+    unsigned bucket = 64;
+    unsigned maxDepth = 21;
+    unsigned iterations = 2;
+    bool nf = false;
+    bool hilbert = false;
+    double box[6] = {0, 1, 0, 1, 0, 1};
+    adaptive_octree::ViewConfig views{};
+    cudaStream_t stream = nullptr;
+};
+
+// Raw device allocation that only grows.
+struct DevMem
+{
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevMem() = default;
+    DevMem(const DevMem &) = delete;
+    DevMem &operator=(const DevMem &) = delete;
+    ~DevMem();
+    void reserve(size_t b);                        // discard contents
+    void grow(size_t b, size_t keep, cudaStream_t s);  // keep the first `keep` bytes
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+class TreeEngine
+{
+public:
+    TreeEngine(const void *x, const void *y, const void *z, size_t n, const EngineConfig &cfg);
+    ~TreeEngine();
+    TreeEngine(const TreeEngine &) = delete;
+    TreeEngine &operator=(const TreeEngine &) = delete;
+
+    void build();
+    void update();
+    void computeViews(const adaptive_octree::ViewConfig &v);
+    bool doBuffersNeedResize();
+    void resizeBuffers();
+    void setCoordinates(const void *x, const void *y, const void *z);
+
+    // getters (logical sizes from the last host readback)
+    enum Buffer
+    {
+        ParticleKeys = 0, Perm, Cornerstone, LeafCounts, NearFieldCounts, SfcBoxIndex, HasBoxSplit, BoxDepth,
+        ParentIndex, ChildIndex, LevelOffset, ParticleBeginIndex, ParticleCounts, SfcParticleIndex, NumBuffers
+    };
+    void buffer(int which, const void **ptr, size_t *len, size_t *cap, size_t *elemBytes) const;
+    const int *numLeavesDevice() const;
+    const int *numNodesDevice() const;
+    const unsigned *numActiveParticlesDevice() const;
+    size_t numParticles() const { return n_; }
+    size_t numActiveParticles() const { return hostActive_; }
+    size_t numNodes() const { return hostNodes_; }
+    unsigned maxAchievedDepth() const;
+    size_t leafCapacity() const { return leafCapacity_; }
+    const EngineConfig &config() const { return cfg_; }
+    // diagnostics: committed build rounds, physical leaf capacity
+    int buildRounds() const { return buildRounds_; }
+    size_t physicalCapacity() const { return physCap_; }
+    // one-shot key generation without a sort (computeSfcKeys semantics)
+    static void computeKeys(int kind, int real, const void *x, const void *y, const void *z, size_t n,
+                            const double *box, bool hilbert, unsigned maxDepth, unsigned long long *keys,
+                            unsigned *perm, cudaStream_t s);
+
+private:
+    struct Impl;
+    std::unique_ptr<Impl> m_;
+    EngineConfig cfg_;
+    size_t n_ = 0;
+    const void *x_ = nullptr, *y_ = nullptr, *z_ = nullptr;
+    size_t leafCapacity_ = 0, physCap_ = 0;
+    size_t hostLeaves_ = 1, hostActive_ = 0, hostNodes_ = 0;
+    int hostActiveBuffer_ = 0;
+    bool built_ = false;
+    int buildRounds_ = 0;
+    // thrust capacity model of K_d / tmpTree (octree.cu:453-457)
+    size_t kSize_ = 0, kCap_ = 0, tSize_ = 0, tCap_ = 0;
+    adaptive_octree::ViewConfig prepared_{};
+
+    void sortParticles();
+    void octreeBuild();
+    void binaryBuild();
+    void octreePass(bool buildMode, long long limit);
+    void binaryPass(bool buildMode, long long limit);
+    void refreshAll();
+    void prepareGraphBuffers(size_t capacity);
+    void ensurePhysical(size_t capacity);
+    void buildViews(const adaptive_octree::ViewConfig &v);
+    void prepareViews(size_t capacity, const adaptive_octree::ViewConfig &v);
+    void syncViewSizes();
+    void readState();
+    void materializeCounts();
+};
+
+}  // namespace aot

@@ -1,0 +1,281 @@
+// radix_sort.cuh -- onesweep LSD radix sort of 64-bit keys carrying 32-bit values.
+//
+// Replaces cub::DeviceRadixSort::SortPairs on the particle keys
+// (octree.cu:301-304, kdtree3d.cu:168-170) and on the view's internal-node keys
+// (tree_view.cu:664-689).  Stable: equal keys keep their input order, which
+// for the particle sort makes Perm ascend within runs of equal keys.
+//
+// Structure (one read of the keys per 8-bit digit):
+//   1. a histogram kernel counts all digit positions at once (fused into key
+//      generation for the particle sort, so the keys are never re-read);
+//   2. a tiny kernel turns the counts into per-digit global start offsets;
+//   3. one onesweep kernel per digit: each CTA takes a tile of 4096 keys in
+//      arrival order (atomic tile counter), ranks them per warp with
+//      __match_any_sync, publishes its per-digit counts, resolves its global
+//      offsets by decoupled look-back over earlier tiles, reorders the tile in
+//      shared memory and writes digit runs out contiguously.
+// The look-back wait is bounded: after kLookbackSpins polls it records
+// kErrLookback in the device error word and proceeds, so a broken invariant
+// surfaces as an error status instead of a hung GPU.
+#pragma once
+
+#include "common.cuh"
+
+namespace aot
+{
+namespace sort
+{
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = 16;
+constexpr int kTile = kThreads * kItems;
+constexpr int kMaxPasses = 8;
+constexpr u64 kFlagAgg = u64(1) << 62;
+constexpr u64 kFlagPrefix = u64(2) << 62;
+constexpr u64 kValueMask = (u64(1) << 62) - 1;
+constexpr unsigned kLookbackSpins = 1u << 22;
+
+__device__ __forceinline__ u64 ldRelaxed(const u64 *p)
+{
+    u64 v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void stRelaxed(u64 *p, u64 v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned laneMaskLt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Per-sort scratch laid out by the host (see SortScratch):
+//   hist[kMaxPasses][256] u32 counts, bins[kMaxPasses][256] u32 exclusive
+//   starts, tileCounters[kMaxPasses] u32, status[kMaxPasses][tiles][256] u64.
+struct Scratch
+{
+    u32 *hist;
+    u32 *bins;
+    u32 *tileCounters;
+    u64 *status;
+    int *error;
+    size_t tiles;
+};
+
+inline size_t scratchBytes(size_t n)
+{
+    const size_t tiles = (n + kTile - 1) / kTile;
+    return size_t(kMaxPasses) * kRadix * 4 * 2 + 64 + size_t(kMaxPasses) * (tiles ? tiles : 1) * kRadix * 8;
+}
+
+// Histogram of the digits of keys[0, n) for passes covering [beginBit, endBit).
+__global__ void __launch_bounds__(kThreads) histogramKernel(const u64 *__restrict__ keys, size_t n, int beginBit,
+                                                             int passes, u32 *__restrict__ hist)
+{
+    __shared__ u32 sh[kMaxPasses][kRadix];
+    for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kThreads) (&sh[0][0])[i] = 0;
+    __syncthreads();
+    for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n; i += size_t(gridDim.x) * kThreads)
+    {
+        const u64 k = __ldg(keys + i);
+        for (int p = 0; p < passes; ++p) atomicAdd(&sh[p][(k >> (beginBit + p * kRadixBits)) & (kRadix - 1)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * kRadix; i += kThreads)
+    {
+        const u32 v = (&sh[0][0])[i];
+        if (v) atomicAdd(hist + i, v);
+    }
+}
+
+// Exclusive scan of each pass' 256 digit counts.
+__global__ void __launch_bounds__(kRadix) binsKernel(const u32 *__restrict__ hist, u32 *__restrict__ bins, int passes)
+{
+    __shared__ u32 s[kRadix];
+    const int d = threadIdx.x;
+    for (int p = 0; p < passes; ++p)
+    {
+        const u32 v = hist[p * kRadix + d];
+        s[d] = v;
+        __syncthreads();
+        // Hillis-Steele inclusive scan over 256 entries
+        for (int off = 1; off < kRadix; off <<= 1)
+        {
+            const u32 t = d >= off ? s[d - off] : 0u;
+            __syncthreads();
+            s[d] += t;
+            __syncthreads();
+        }
+        bins[p * kRadix + d] = s[d] - v;
+        __syncthreads();
+    }
+}
+
+struct SharedPass
+{
+    u64 keys[kTile];
+    u32 vals[kTile];
+    u32 warpHist[kWarps][kRadix];  // per-warp digit counts, then exclusive warp offsets
+    u32 localStart[kRadix];
+    long long gstart[kRadix];      // global position of local index 0 of each digit
+    u32 count[kRadix];
+    u32 warpSums[kWarps];
+    u32 tile;
+};
+
+// One onesweep pass over keys[0, n): digit at bit `shift`.
+// valsIn == nullptr means values are the input indices (first pass).
+__global__ void __launch_bounds__(kThreads) onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn,
+                                                            u64 *__restrict__ keysOut, u32 *__restrict__ valsOut,
+                                                            size_t n, int shift, const u32 *__restrict__ bins,
+                                                            u32 *tileCounter, u64 *status, int *error)
+{
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    SharedPass &sm = *reinterpret_cast<SharedPass *>(smemRaw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    for (int i = tid; i < kWarps * kRadix; i += kThreads) (&sm.warpHist[0][0])[i] = 0;
+    if (tid == 0) sm.tile = atomicAdd(tileCounter, 1u);
+    __syncthreads();
+    const size_t tile = sm.tile;
+    const size_t tileBase = tile * kTile;
+    const size_t warpBase = tileBase + size_t(warp) * (32 * kItems);
+
+    u64 key[kItems];
+    u32 val[kItems];
+    int digit[kItems];
+    u32 rank[kItems];
+#pragma unroll
+    for (int i = 0; i < kItems; ++i)
+    {
+        const size_t idx = warpBase + size_t(i) * 32 + lane;
+        if (idx < n)
+        {
+            key[i] = __ldcs(keysIn + idx);
+            val[i] = valsIn ? __ldcs(valsIn + idx) : u32(idx);
+            digit[i] = int((key[i] >> shift) & (kRadix - 1));
+        }
+        else
+        {
+            key[i] = 0;
+            val[i] = 0;
+            digit[i] = kRadix;  // outside every bucket
+        }
+    }
+    // Rank within the warp, items in memory order (item-major, lane-minor).
+    u32 *wh = sm.warpHist[warp];
+    const unsigned ltMask = laneMaskLt();
+#pragma unroll
+    for (int i = 0; i < kItems; ++i)
+    {
+        const unsigned peers = __match_any_sync(0xffffffffu, digit[i]);
+        const bool valid = digit[i] < kRadix;
+        u32 base = 0;
+        if (valid) base = wh[digit[i]];
+        __syncwarp();
+        if (valid && (peers & ltMask) == 0) wh[digit[i]] = base + __popc(peers);
+        __syncwarp();
+        rank[i] = base + __popc(peers & ltMask);
+    }
+    __syncthreads();
+    // Per digit: warp exclusive offsets and tile total (thread = digit).
+    {
+        const int d = tid;
+        u32 acc = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w)
+        {
+            const u32 c = sm.warpHist[w][d];
+            sm.warpHist[w][d] = acc;
+            acc += c;
+        }
+        sm.count[d] = acc;
+    }
+    // Publish this tile's digit counts; tile 0 publishes final prefixes.
+    {
+        const int d = tid;
+        const u64 total = sm.count[d];
+        u64 *st = status + tile * kRadix + d;
+        stRelaxed(st, (tile == 0 ? kFlagPrefix : kFlagAgg) | total);
+        u64 excl = 0;
+        if (tile > 0)
+        {
+            long long j = (long long)tile - 1;
+            unsigned spins = 0;
+            while (j >= 0)
+            {
+                const u64 v = ldRelaxed(status + size_t(j) * kRadix + d);
+                const u64 flag = v & ~kValueMask;
+                if (flag == 0)
+                {
+                    if (++spins > kLookbackSpins)
+                    {
+                        atomicExch(error, kErrLookback);
+                        break;
+                    }
+                    if (spins > 64) __nanosleep(64);
+                    continue;
+                }
+                excl += v & kValueMask;
+                if (flag == kFlagPrefix) break;
+                --j;
+            }
+            stRelaxed(st, kFlagPrefix | (excl + total));
+        }
+        sm.gstart[d] = (long long)bins[d] + (long long)excl;
+    }
+    // Exclusive scan of the tile's digit counts -> local starts.
+    {
+        const int d = tid;
+        u32 v = sm.count[d];
+        // warp inclusive scan
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const u32 t = __shfl_up_sync(0xffffffffu, v, off);
+            if (lane >= off) v += t;
+        }
+        if (lane == 31) sm.warpSums[warp] = v;
+        __syncthreads();
+        u32 wOff = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w)
+            if (w < warp) wOff += sm.warpSums[w];
+        const u32 local = wOff + v - sm.count[d];
+        sm.localStart[d] = local;
+        sm.gstart[d] -= (long long)local;
+    }
+    __syncthreads();
+    // Reorder the tile in shared memory.
+#pragma unroll
+    for (int i = 0; i < kItems; ++i)
+    {
+        if (digit[i] < kRadix)
+        {
+            const u32 pos = sm.localStart[digit[i]] + sm.warpHist[warp][digit[i]] + rank[i];
+            sm.keys[pos] = key[i];
+            sm.vals[pos] = val[i];
+        }
+    }
+    __syncthreads();
+    const size_t remain = n - tileBase;
+    const int valid = remain < size_t(kTile) ? int(remain) : kTile;
+    for (int j = tid; j < valid; j += kThreads)
+    {
+        const u64 k = sm.keys[j];
+        const int d = int((k >> shift) & (kRadix - 1));
+        const size_t out = size_t(sm.gstart[d] + j);
+        keysOut[out] = k;
+        valsOut[out] = sm.vals[j];
+    }
+}
+
+inline size_t passSmem() { return sizeof(SharedPass); }
+
+}  // namespace sort
+}  // namespace aot

@@ -1,0 +1,696 @@
+// rebalance.cuh -- device kernels of the split/merge rebalance passes.
+//
+// One pass (octree or binary) is three kernels, all reading sizes and the
+// A/B selection from DeviceState so a captured CUDA graph stays valid while
+// the topology changes (the reference's graph path, octree_rebalance.cuh:
+// 1177-1322 and kdtree3d_rebalance.cuh:160-245):
+//   decide+scan   per-leaf op code and its exclusive prefix in ONE kernel
+//                 (decoupled look-back over 2048-entry tiles); the tile that
+//                 holds entry numLeaves records the proposed leaf count;
+//   scatter       writes the proposal into the inactive buffer when it is
+//                 accepted; the last CTA to finish applies the reference's
+//                 capacity check and commit (graphCheckCapacityKernel +
+//                 graphCommitNodesKernel) and the work lists for the refresh;
+//   refresh       recomputes per-leaf quantities of new leaves only.
+// Per leaf the engine keeps B[i] = lowerBound(P, K[i]) (B[L] = active count):
+// the leaf count is B[i+1] - B[i] and a sibling group's count is
+// B[first+8] - B[first], so LeafCount decisions need no count array and
+// unchanged leaves keep B without a search.
+#pragma once
+
+#include "common.cuh"
+#include "sfc.cuh"
+
+namespace aot
+{
+namespace rb
+{
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr u64 kFlagAgg = u64(1) << 62;
+constexpr u64 kFlagPrefix = u64(2) << 62;
+constexpr u64 kValueMask = (u64(1) << 62) - 1;
+constexpr unsigned kLookbackSpins = 1u << 22;
+constexpr int kScatterThreads = 256;
+constexpr int kRefreshThreads = 256;
+
+// Buffers of one tree (A/B pairs are indexed by DeviceState::activeBuffer).
+struct TreeBufs
+{
+    u64 *K[2];    // leaf boundaries, numLeaves + 1 used
+    u32 *B[2];    // begin index of every boundary in P
+    u32 *NF[2];   // near-field counts (NFCount octrees)
+    u8 *G[2];     // group-can-merge flag at each complete group's first leaf
+    u32 *N[2];    // leaf counts, materialised for getters and views
+    i64 *offs;    // decision scan, capacity + 1
+    int *dirty;   // new leaves that need a search (and NF)
+    int *groups;  // candidate group leaders that need a parent NF
+    u64 *scanStatus;
+    u32 *scanTile;
+    DeviceState *st;
+};
+
+__device__ __forceinline__ bool halted(const DeviceState *st)
+{
+    return st->converged | st->overflow | st->error;
+}
+
+__device__ __forceinline__ u64 ldRelaxed(const u64 *p)
+{
+    u64 v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void stRelaxed(u64 *p, u64 v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Block-wide exclusive scan of one value per thread (kScanThreads threads).
+__device__ __forceinline__ i64 blockExclusiveScan(i64 v, i64 *sWarp, i64 &total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    i64 inc = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1)
+    {
+        const i64 t = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += t;
+    }
+    if (lane == 31) sWarp[warp] = inc;
+    __syncthreads();
+    i64 wOff = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kScanThreads / 32; ++w)
+    {
+        const i64 s = sWarp[w];
+        if (w < warp) wOff += s;
+        tot += s;
+    }
+    total = tot;
+    return wOff + inc - v;
+}
+
+// Decoupled look-back: returns the exclusive prefix of `tile` given its
+// aggregate.  Called by one thread.
+__device__ __forceinline__ i64 lookback(u64 *status, u32 tile, i64 aggregate, int *error)
+{
+    if (tile == 0)
+    {
+        stRelaxed(status, kFlagPrefix | u64(aggregate));
+        return 0;
+    }
+    stRelaxed(status + tile, kFlagAgg | u64(aggregate));
+    i64 excl = 0;
+    long long j = (long long)tile - 1;
+    unsigned spins = 0;
+    while (j >= 0)
+    {
+        const u64 v = ldRelaxed(status + j);
+        const u64 flag = v & ~kValueMask;
+        if (flag == 0)
+        {
+            if (++spins > kLookbackSpins)
+            {
+                atomicExch(error, kErrLookback);
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        excl += i64(v & kValueMask);
+        if (flag == kFlagPrefix) break;
+        --j;
+    }
+    stRelaxed(status + tile, kFlagPrefix | u64(excl + aggregate));
+    return excl;
+}
+
+// Generic single-pass decide+scan.  OpFn(i, L) returns the op code of leaf
+// i < L; entry L is 0.  Writes offs[0..L] (exclusive), state->proposal and
+// state->changed.
+template <class OpFn>
+__device__ void decideScan(const OpFn &opOf, TreeBufs tb)
+{
+    __shared__ i64 sWarp[kScanThreads / 32];
+    __shared__ u32 sTile;
+    __shared__ i64 sPrefix;
+    __shared__ int sChanged;
+    DeviceState *st = tb.st;
+    if (halted(st) || st->needsResize) return;
+    const int L = st->numLeaves;
+    const size_t entries = size_t(L) + 1;
+    const u32 numTiles = u32((entries + kScanTile - 1) / kScanTile);
+    if (threadIdx.x == 0)
+    {
+        sTile = atomicAdd(tb.scanTile, 1u);
+        sChanged = 0;
+    }
+    __syncthreads();
+    const u32 tile = sTile;
+    if (tile >= numTiles) return;
+    const size_t first = size_t(tile) * kScanTile + size_t(threadIdx.x) * kScanItems;
+    int ops[kScanItems];
+    i64 sum = 0;
+    bool changed = false;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j)
+    {
+        const size_t i = first + j;
+        int op = 0;
+        if (i < size_t(L))
+        {
+            op = opOf(int(i), L);
+            changed |= op != 1;
+        }
+        ops[j] = op;
+        sum += op;
+    }
+    if (changed) sChanged = 1;
+    i64 total;
+    const i64 excl = blockExclusiveScan(sum, sWarp, total);
+    if (threadIdx.x == 0)
+    {
+        sPrefix = lookback(tb.scanStatus, tile, total, &st->error);
+        if (sChanged) atomicOr(&st->changed, 1);
+    }
+    __syncthreads();
+    i64 run = sPrefix + excl;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j)
+    {
+        const size_t i = first + j;
+        if (i <= size_t(L))
+        {
+            tb.offs[i] = run;
+            if (i == size_t(L)) st->proposal = run;
+        }
+        run += ops[j];
+    }
+}
+
+// Warp-aggregated append of `count` consecutive items to a list; returns the
+// first slot of this thread.
+__device__ __forceinline__ int warpAppend(int *counter, int count)
+{
+    const int lane = threadIdx.x & 31;
+    int inc = count;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1)
+    {
+        const int t = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += t;
+    }
+    const int warpTotal = __shfl_sync(0xffffffffu, inc, 31);
+    int base = 0;
+    if (lane == 31 && warpTotal) base = atomicAdd(counter, warpTotal);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    return base + inc - count;
+}
+
+// Completion of a scatter kernel: the last CTA applies the capacity check and
+// the commit (graphCheckCapacityKernel + graphCommitNodesKernel semantics,
+// octree_rebalance.cuh:1211-1273).  `limit` is the leaf capacity the scatter
+// wrote against: the reference's leafCapacity in kModeUpdate, the physical
+// buffer size in the build modes (exceeding it is an overflow the host repairs
+// by growing the buffers and repeating the round).  In kModeBinaryBuild the
+// reference's leafCapacity (st->logicalCap) grows by 25% steps until the
+// proposal fits, as its build loop does through needsResize/growBuffers
+// (kdtree3d.cu:239-249).
+__device__ __forceinline__ void commitIfLast(DeviceState *st, long long limit, int mode, bool binary,
+                                             long long *history)
+{
+    __shared__ bool sLast;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        sLast = atomicAdd(&st->doneBlocks, 1) == int(gridDim.x) - 1;
+    }
+    __syncthreads();
+    if (!sLast || threadIdx.x != 0) return;
+    __threadfence();
+    st->doneBlocks = 0;
+    const long long total = st->proposal;
+    if (st->needsResize || !st->changed)
+    {
+        st->converged = 1;
+        if (mode != kModeUpdate) st->rounds += 1;
+        return;
+    }
+    if (total > limit)
+    {
+        if (mode == kModeUpdate)
+        {
+            st->needsResize = 1;
+            st->converged = 1;
+        }
+        else
+        {
+            st->overflow = 1;
+        }
+        return;
+    }
+    if (mode == kModeBinaryBuild)
+    {
+        long long c = st->logicalCap < 1 ? 1 : st->logicalCap;
+        while (total > c) c += (c + 3) / 4;  // c >= 1 grows by >= 1 per step
+        st->logicalCap = c;
+    }
+    st->newNumLeaves = int(total);
+    st->numLeaves = int(total);
+    if (binary) st->numNodes = (int(total) - 1) * 2 + 1;
+    st->activeBuffer ^= 1;
+    if (mode != kModeUpdate)
+    {
+        if (history) history[st->iteration] = total;
+        st->iteration += 1;
+        st->rounds += 1;
+    }
+}
+
+// --------------------------------------------------------------------------
+// Octree
+// --------------------------------------------------------------------------
+// siblingIndexAndLevel (octree_rebalance.cuh:26-50)
+__device__ __forceinline__ int siblingIndex(const u64 *K, int L, int i, unsigned &level)
+{
+    const u64 s = K[i];
+    level = octLevel(K[i + 1] - s);
+    if (level == 0) return -1;
+    const int sib = int(octDigit(s, level));
+    const int first = i - sib;
+    if (first < 0 || first > L - 8) return -1;
+    return K[first + 8] == K[first] + octRange(level - 1) ? sib : -1;
+}
+
+// calculateNodeOp (octree_rebalance.cuh:174-249)
+template <bool NF>
+struct OctreeOp
+{
+    const u64 *K;
+    const u32 *B;
+    const u32 *NFc;
+    const u8 *G;
+    unsigned bucket;
+    __device__ __forceinline__ int operator()(int i, int L) const
+    {
+        unsigned level = 0;
+        const int sib = siblingIndex(K, L, i, level);
+        if constexpr (!NF)
+        {
+            if (sib > 0)
+            {
+                const int first = i - sib;
+                const u64 parent = u64(B[first + 8] - B[first]);
+                if (parent <= u64(bucket)) return 0;
+            }
+            const u32 c = B[i + 1] - B[i];
+            if (c > bucket * 512u && level + 3 < kOctLevels) return 4096;
+            if (c > bucket * 64u && level + 2 < kOctLevels) return 512;
+            if (c > bucket * 8u && level + 1 < kOctLevels) return 64;
+            if (c > bucket && level < kOctLevels) return 8;
+            return 1;
+        }
+        else
+        {
+            if (sib >= 0)
+            {
+                const int first = i - sib;
+                if (first + 8 <= L && G[first]) return sib == 0 ? 1 : 0;
+            }
+            const u64 c = NFc[i], b = bucket;
+            if (c > b * 262144 && level + 3 < kOctLevels) return 4096;
+            if (c > b * 4096 && level + 2 < kOctLevels) return 512;
+            if (c > b * 64 && level + 1 < kOctLevels) return 64;
+            if (c > b && level < kOctLevels) return 8;
+            return 1;
+        }
+    }
+};
+
+template <bool NF>
+__global__ void __launch_bounds__(kScanThreads) octDecideScanKernel(TreeBufs tb, unsigned bucket)
+{
+    const int a = tb.st->activeBuffer;
+    const OctreeOp<NF> op{tb.K[a], tb.B[a], tb.NF[a], tb.G[a], bucket};
+    decideScan(op, tb);
+}
+
+__device__ __forceinline__ int opAt(const i64 *offs, int i) { return int(offs[i + 1] - offs[i]); }
+
+// log8ceil of a split op code (octree_rebalance.cuh:349): 8->1, 64->2, 512->3, 4096->4
+__device__ __forceinline__ unsigned splitLevels(int op) { return op == 8 ? 1u : op == 64 ? 2u : op == 512 ? 3u : 4u; }
+
+// processNode (octree_rebalance.cuh:253-365) for every old leaf, plus the
+// work lists of the refresh: new leaves needing a search (and NF) and
+// candidate group leaders needing a parent NF.
+template <bool NF>
+__global__ void __launch_bounds__(kScatterThreads)
+    octScatterKernel(TreeBufs tb, long long limit, int mode, long long *history)
+{
+    DeviceState *st = tb.st;
+    if (halted(st)) return;  // uniform: the state does not change before the last CTA
+    const long long total = st->proposal;
+    const bool proceed = !st->needsResize && st->changed && total <= limit;
+    const int L = st->numLeaves;
+    const int a = st->activeBuffer, b = a ^ 1;
+    const int i = int(blockIdx.x * blockDim.x + threadIdx.x);
+    int nDirty = 0, nGroup = 0;
+    int op = 0;
+    unsigned level = 0;
+    u64 start = 0;
+    bool leader = false, reusable = false;
+    if (proceed && i < L)
+    {
+        const u64 *K = tb.K[a];
+        const i64 *offs = tb.offs;
+        op = opAt(offs, i);
+        start = K[i];
+        level = octLevel(K[i + 1] - start);
+        const i64 ni = offs[i];
+        u64 *Kn = tb.K[b];
+        u32 *Bn = tb.B[b];
+        if (op == 1)
+        {
+            Kn[ni] = start;
+            Bn[ni] = tb.B[a][i];
+            if constexpr (NF)
+            {
+                leader = i + 1 < L && opAt(offs, i + 1) == 0;
+                if (leader)
+                {
+                    nDirty = 1;
+                    nGroup = (level - 1 > 0 && octDigit(start, level - 1) == 0) ? 1 : 0;
+                }
+                else
+                {
+                    tb.NF[b][ni] = tb.NF[a][i];
+                    unsigned sl = 0;
+                    const int sib = siblingIndex(K, L, i, sl);
+                    if (sib == 0 && i + 8 <= L)
+                    {
+                        reusable = true;
+                        for (int s = 0; s < 8; ++s)
+                            if (opAt(offs, i + s) != 1) reusable = false;
+                    }
+                    if (reusable) tb.G[b][ni] = tb.G[a][i];
+                    else nGroup = (level > 0 && octDigit(start, level) == 0) ? 1 : 0;
+                }
+            }
+        }
+        else if (op > 1)
+        {
+            const u64 nr = octRange(level + splitLevels(op));
+            for (int c = 0; c < op; ++c) Kn[ni + c] = start + u64(c) * nr;
+            Bn[ni] = tb.B[a][i];  // the first child starts where the parent did
+            nDirty = NF ? op : op - 1;
+            nGroup = NF ? op / 8 : 0;
+        }
+        if (i == 0)
+        {
+            Kn[total] = kMaxKey;
+            Bn[total] = st->numActiveParticles;
+        }
+    }
+    // work lists (warp-aggregated appends; list order is irrelevant)
+    if (proceed)
+    {
+        const int d0 = warpAppend(&st->dirtyCount, nDirty);
+        if (nDirty)
+        {
+            const int ni = int(tb.offs[i]);
+            if (op > 1)
+            {
+                const int c0 = NF ? 0 : 1;
+                for (int c = c0; c < op; ++c) tb.dirty[d0 + c - c0] = ni + c;
+            }
+            else
+            {
+                tb.dirty[d0] = ni;
+            }
+        }
+        if constexpr (NF)
+        {
+            const int g0 = warpAppend(&st->groupCount, nGroup);
+            if (nGroup)
+            {
+                const int ni = int(tb.offs[i]);
+                if (op > 1)
+                    for (int c = 0; c < nGroup; ++c) tb.groups[g0 + c] = ni + 8 * c;
+                else
+                    tb.groups[g0] = ni;
+            }
+        }
+    }
+    commitIfLast(st, limit, mode, false, history);
+}
+
+// Near-field count of the octree cell [start, start + range(level)):
+// own count x sum of the 27 periodic same-level neighbour counts
+// (computeNFCooperative, octree_rebalance.cuh:579-634), one lane per cell.
+// Returns the product on every lane; `own` and `begin` (lower bound of the
+// cell start) are valid on every lane.
+template <bool Hilbert>
+__device__ __forceinline__ u64 warpNearField(const KeyIndex &idx, u64 start, unsigned level, const unsigned char *sEnc,
+                                             const unsigned char *sNext, const unsigned char *sDec, u32 &own,
+                                             u32 &begin)
+{
+    const int lane = threadIdx.x & 31;
+    if (level > kOctLevels) level = kOctLevels;  // only a malformed tree gets here
+    const u64 range = octRange(level);
+    u32 cx, cy, cz;
+    if constexpr (Hilbert)
+    {
+        hilbertCorner(start, level, sDec, sNext, cx, cy, cz);
+    }
+    else
+    {
+        cx = compact3(start >> 2);
+        cy = compact3(start >> 1);
+        cz = compact3(start);
+    }
+    const u32 cube = 1u << (kOctLevels - level);
+    u64 cnt = 0;
+    u32 lo = 0;
+    if (lane < 27)
+    {
+        u64 key = start;
+        if (lane != 13)
+        {
+            const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+            const u32 x = (cx + u32(dx) * cube) & 0x1fffffu;
+            const u32 y = (cy + u32(dy) * cube) & 0x1fffffu;
+            const u32 z = (cz + u32(dz) * cube) & 0x1fffffu;
+            if constexpr (Hilbert) key = hilbertPrefix(x, y, z, level, sEnc, sNext);
+            else key = mortonKey(x, y, z);
+        }
+        lo = u32(idx.lower(key));
+        const u32 hi = u32(idx.lower(key + range));
+        cnt = hi - lo;
+    }
+    u64 sum = cnt;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    const u64 centre = __shfl_sync(0xffffffffu, cnt, 13);
+    begin = __shfl_sync(0xffffffffu, lo, 13);
+    own = u32(centre);
+    return centre * sum;
+}
+
+// Refresh of new leaves (All = every leaf, at the start of update()).
+template <bool NF, bool Hilbert, bool All>
+__global__ void __launch_bounds__(kRefreshThreads)
+    octRefreshKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h)
+{
+    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
+    DeviceState *st = tb.st;
+    if (halted(st)) return;
+    if constexpr (NF && Hilbert)
+    {
+        for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
+        {
+            sEnc[k] = h.enc[k];
+            sNext[k] = h.encNext[k];
+            sDec[k] = h.decOct[k];
+        }
+        __syncthreads();
+    }
+    const int a = st->activeBuffer;
+    const int L = st->numLeaves;
+    const u64 *K = tb.K[a];
+    u32 *B = tb.B[a];
+    if (All && blockIdx.x == 0 && threadIdx.x == 0) B[L] = st->numActiveParticles;
+    if constexpr (!NF)
+    {
+        const int count = All ? L : st->dirtyCount;
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
+        {
+            const int i = All ? j : tb.dirty[j];
+            B[i] = u32(idx.lower(K[i]));
+        }
+    }
+    else
+    {
+        const int warpsTotal = gridDim.x * (blockDim.x / 32);
+        const int w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+        const int lane = threadIdx.x & 31;
+        const int count = All ? L : st->dirtyCount;
+        for (int j = w0; j < count; j += warpsTotal)
+        {
+            const int i = All ? j : tb.dirty[j];
+            const u64 s = K[i];
+            const unsigned level = octLevel(K[i + 1] - s);
+            u32 own, begin;
+            const u64 v = warpNearField<Hilbert>(idx, s, level, sEnc, sNext, sDec, own, begin);
+            if (lane == 0)
+            {
+                tb.NF[a][i] = v > 0xffffffffull ? 0xffffffffu : u32(v);
+                B[i] = begin;
+            }
+        }
+        const int gcount = All ? L : st->groupCount;
+        for (int j = w0; j < gcount; j += warpsTotal)
+        {
+            const int i = All ? j : tb.groups[j];
+            const u64 s = K[i];
+            const unsigned level = octLevel(K[i + 1] - s);
+            if (level == 0 || octDigit(s, level) != 0) continue;           // not a first sibling
+            if (i + 8 > L || K[i + 8] != s + octRange(level - 1)) continue;  // incomplete group
+            u32 own, begin;
+            const u64 parentNF = warpNearField<Hilbert>(idx, s, level - 1, sEnc, sNext, sDec, own, begin);
+            if (lane == 0) tb.G[a][i] = parentNF <= u64(bucket) ? 1 : 0;
+        }
+    }
+}
+
+// N[i] = B[i+1] - B[i] on the active buffer.
+__global__ void materializeCountsKernel(TreeBufs tb)
+{
+    const DeviceState *st = tb.st;
+    const int a = st->activeBuffer, L = st->numLeaves;
+    const u32 *B = tb.B[a];
+    u32 *N = tb.N[a];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) N[i] = B[i + 1] - B[i];
+}
+
+// --------------------------------------------------------------------------
+// Binary (kdtree3d_rebalance.cuh:61-125)
+// --------------------------------------------------------------------------
+struct BinaryOp
+{
+    const u64 *K;
+    const u32 *B;
+    unsigned bucket, maxDepth;
+    __device__ __forceinline__ bool siblings(int L, int first) const  // binarySiblings, binary_node.cuh:91-98
+    {
+        if (first < 0 || first + 1 >= L) return false;
+        const u64 r = K[first + 1] - K[first];
+        return !(K[first] & r) && K[first + 2] - K[first + 1] == r;
+    }
+    __device__ __forceinline__ int operator()(int i, int L) const
+    {
+        const u32 ci = B[i + 1] - B[i];
+        const bool merge = i && siblings(L, i - 1) && u64(B[i] - B[i - 1]) + ci <= bucket;
+        if (merge) return 0;
+        return (ci > bucket && unsigned(clz64(K[i + 1] - K[i])) < maxDepth) ? 2 : 1;
+    }
+};
+
+__global__ void __launch_bounds__(kScanThreads) binDecideScanKernel(TreeBufs tb, unsigned bucket, unsigned maxDepth)
+{
+    const int a = tb.st->activeBuffer;
+    const BinaryOp op{tb.K[a], tb.B[a], bucket, maxDepth};
+    decideScan(op, tb);
+}
+
+__global__ void __launch_bounds__(kScatterThreads)
+    binScatterKernel(TreeBufs tb, long long limit, int mode)
+{
+    DeviceState *st = tb.st;
+    if (halted(st)) return;
+    const long long total = st->proposal;
+    const bool proceed = !st->needsResize && st->changed && total <= limit;
+    const int L = st->numLeaves;
+    const int a = st->activeBuffer, b = a ^ 1;
+    const int i = int(blockIdx.x * blockDim.x + threadIdx.x);
+    int nDirty = 0;
+    i64 ni = 0;
+    if (proceed && i < L)
+    {
+        const int op = opAt(tb.offs, i);
+        if (op)
+        {
+            ni = tb.offs[i];
+            const u64 s = tb.K[a][i];
+            tb.K[b][ni] = s;
+            tb.B[b][ni] = tb.B[a][i];
+            if (op == 2)
+            {
+                tb.K[b][ni + 1] = s + (tb.K[a][i + 1] - s) / 2;
+                nDirty = 1;
+            }
+        }
+        if (i == 0)
+        {
+            tb.K[b][total] = kMaxKey;
+            tb.B[b][total] = st->numActiveParticles;
+        }
+    }
+    if (proceed)
+    {
+        const int d0 = warpAppend(&st->dirtyCount, nDirty);
+        if (nDirty) tb.dirty[d0] = int(ni) + 1;
+    }
+    commitIfLast(st, limit, mode, true, nullptr);
+}
+
+// Binary count refresh: B of new split points (All: every boundary).  The
+// reference counts over the active prefix of P (binaryLeafCountsKernel,
+// kdtree3d_rebalance.cuh:127-138); lower bounds of keys below 2^63 agree.
+template <bool All>
+__global__ void binRefreshKernel(TreeBufs tb, KeyIndex idx)
+{
+    DeviceState *st = tb.st;
+    if (halted(st)) return;
+    const int a = st->activeBuffer, L = st->numLeaves;
+    const u64 *K = tb.K[a];
+    u32 *B = tb.B[a];
+    if (All && blockIdx.x == 0 && threadIdx.x == 0) B[L] = st->numActiveParticles;
+    const int count = All ? L : st->dirtyCount;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
+    {
+        const int i = All ? j : tb.dirty[j];
+        B[i] = u32(idx.lower(K[i]));
+    }
+}
+
+// Reset at the start of update() (resetRebalanceStateKernel,
+// octree_rebalance.cuh:62-73): changed, converged and the active count.
+__global__ void resetForUpdateKernel(DeviceState *st, const u64 *P, size_t n)
+{
+    st->changed = 0;
+    st->converged = 0;
+    st->numActiveParticles = n ? u32(lowerBoundDev(P, n, kMaxKey)) : 0u;
+    st->dirtyCount = 0;
+    st->groupCount = 0;
+}
+
+// Per-pass reset of the flags the decision accumulates.
+__global__ void beginPassKernel(DeviceState *st)
+{
+    st->changed = 0;
+    st->dirtyCount = 0;
+    st->groupCount = 0;
+}
+
+// Sample every kSampleStride-th key for KeyIndex.
+__global__ void sampleKeysKernel(const u64 *P, size_t n, u64 *sample, size_t ns)
+{
+    for (size_t j = blockIdx.x * size_t(blockDim.x) + threadIdx.x; j < ns; j += size_t(gridDim.x) * blockDim.x)
+        sample[j] = P[j << kSampleShift];
+}
+
+}  // namespace rb
+}  // namespace aot

@@ -1,0 +1,158 @@
+/* adaptive_trees_b200.h -- C ABI of the B200 adaptive-tree engine.
+ *
+ * Plain C: handles, pointers, sizes and status codes; no C++ or framework
+ * types.  Each entry point replaces one member of the reference's C++ surface
+ * (nrottstegge/Adaptive_Trees, include/adaptive_octree/tree.hpp), cited at
+ * the declaration.  Coordinates and returned buffers are DEVICE pointers; the
+ * stream is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Error behaviour: the reference throws std::invalid_argument,
+ * std::logic_error and std::length_error from its C++ API and calls
+ * std::exit() on CUDA errors.  Here every entry point returns an ao_status;
+ * ao_last_error() returns the message of the last failure on the calling
+ * thread.  Nothing in the library exits the process.
+ */
+#ifndef ADAPTIVE_TREES_B200_H
+#define ADAPTIVE_TREES_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define AO_API __attribute__((visibility("default")))
+#else
+#define AO_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ao_status
+{
+    AO_OK = 0,
+    AO_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+    AO_ERR_LOGIC = 2,            /* std::logic_error (wrong call order, unsupported getter) */
+    AO_ERR_LENGTH = 3,           /* std::length_error (capacity beyond the node index range) */
+    AO_ERR_CUDA = 4,             /* CUDA runtime failure (the reference exits the process) */
+    AO_ERR_OUT_OF_MEMORY = 5,    /* device or host allocation failed */
+    AO_ERR_RUNTIME = 6           /* other failure, e.g. a bounded device wait gave up */
+} ao_status;
+
+enum { AO_OCTREE = 0, AO_BINARY = 1 };          /* TreeType (config.hpp:50) */
+enum { AO_FLOAT32 = 0, AO_FLOAT64 = 1 };        /* Real */
+enum { AO_LEAF_COUNT = 0, AO_NF_COUNT = 1 };    /* SplitCriterion (config.hpp:51) */
+enum { AO_MORTON = 0, AO_HILBERT = 1 };         /* SfcKind (config.hpp:52) */
+
+/* Getter selectors: the reference's device_vector getters (tree.hpp:72-97, 113). */
+enum
+{
+    AO_BUF_PARTICLE_KEYS = 0,        /* particleKeys_d      u64, numParticles             */
+    AO_BUF_PERM = 1,                 /* perm_d              u32, numParticles             */
+    AO_BUF_CORNERSTONE = 2,          /* cornerstone_d       u64, numLeaves + 1            */
+    AO_BUF_LEAF_COUNTS = 3,          /* leafCounts_d        u32, numLeaves                */
+    AO_BUF_NEAR_FIELD_COUNTS = 4,    /* nearFieldCounts_d   u32, numLeaves (octree only)  */
+    AO_BUF_SFC_BOX_INDEX = 5,        /* sfcBoxIndex_d       u64, numNodes                 */
+    AO_BUF_HAS_BOX_SPLIT = 6,        /* hasBoxSplit_d       u8,  numNodes                 */
+    AO_BUF_BOX_DEPTH = 7,            /* boxDepth_d          u8,  numNodes                 */
+    AO_BUF_PARENT_INDEX = 8,         /* parentIndex_d       i32, numNodes                 */
+    AO_BUF_CHILD_INDEX = 9,          /* childIndex_d        i32, numNodes                 */
+    AO_BUF_LEVEL_OFFSET = 10,        /* levelOffset_d       i32, 23 (octree) / 65 (binary) */
+    AO_BUF_PARTICLE_BEGIN_INDEX = 11,/* particleBeginIndex_d u32, numNodes                */
+    AO_BUF_PARTICLE_COUNTS = 12,     /* particleCounts_d    u32, numNodes + 1             */
+    AO_BUF_SFC_PARTICLE_INDEX = 13   /* sfcParticleIndex_d  u64, numActiveParticles       */
+};
+
+/* TreeConfig<Real> (config.hpp:147-160); the box is given in double and
+ * converted to Real. */
+typedef struct ao_config
+{
+    int max_depth;                   /* -1: backend default (21 octree build rounds / 63 binary depth) */
+    unsigned max_particles_per_leaf; /* LeafCount bucket, or the near-field limit for NFCount */
+    int update_iterations;           /* -1: backend default (2 octree / 6 binary) */
+    double box[6];                   /* xmin, xmax, ymin, ymax, zmin, zmax */
+    int split_criterion;             /* AO_LEAF_COUNT / AO_NF_COUNT */
+    int sfc_kind;                    /* AO_MORTON / AO_HILBERT */
+    int views_tree_structure;        /* ViewConfig (config.hpp:115-120) */
+    int views_particle_counts;
+    int views_particle_mapping;
+} ao_config;
+
+typedef struct ao_view_config
+{
+    int tree_structure;
+    int particle_counts_per_box;
+    int particle_mapping;
+} ao_view_config;
+
+typedef struct ao_tree_info
+{
+    size_t num_particles;        /* numParticles()        tree.hpp:64-65 */
+    size_t num_active_particles; /* numActiveParticles()  tree.hpp:66-67 */
+    size_t num_nodes;            /* numNodes()            tree.hpp:68-69 */
+    size_t num_leaves;           /* cornerstone_d().size() - 1 */
+    size_t leaf_capacity;        /* capacity that bounds update() before needsResize */
+    unsigned max_achieved_depth; /* maxAchievedDepth()    tree.hpp:70-71 */
+    int split_criterion;         /* splitCriterion()      tree.hpp:99-103 */
+    int sfc_kind;                /* sfcKind() tree.hpp:104-108; -1 for Binary (the C++ facade throws) */
+} ao_tree_info;
+
+typedef struct ao_tree ao_tree;
+
+/* Tree<Real, Kind>::Tree(x, y, z, count, config) -- tree.hpp:35-37 (with the
+ * backend constructors octree.cu:321-416, kdtree3d.cu:175-216).  x, y, z are
+ * borrowed device arrays of `n` Real values; they are read at every build()
+ * and update() and may be changed in place between calls. */
+AO_API ao_status ao_tree_create(int kind, int real_type, const void *x, const void *y, const void *z, size_t n,
+                         const ao_config *config, void *stream, ao_tree **out);
+
+/* ~Tree() */
+AO_API ao_status ao_tree_destroy(ao_tree *tree);
+
+/* Tree::build() -- tree.hpp:45 (octree.cu:427-469, kdtree3d.cu:227-257).  Not capturable. */
+AO_API ao_status ao_tree_build(ao_tree *tree);
+
+/* Tree::update() -- tree.hpp:46 (octree.cu:471-481, kdtree3d.cu:259-270).
+ * Capturable into a CUDA graph on the tree's stream. */
+AO_API ao_status ao_tree_update(ao_tree *tree);
+
+/* Tree::computeViews() / computeViews(ViewConfig) -- tree.hpp:49-53.
+ * views == NULL uses the configured views. */
+AO_API ao_status ao_tree_compute_views(ao_tree *tree, const ao_view_config *views);
+
+/* Tree::doBuffersNeedResize() -- tree.hpp:56-57.  Refreshes the host-visible
+ * sizes from the device state; *out = 1 when resizeBuffers() is needed. */
+AO_API ao_status ao_tree_needs_resize(ao_tree *tree, int *out);
+
+/* Tree::resizeBuffers() -- tree.hpp:47.  Grows the leaf capacity by 25%;
+ * graphs captured before must be captured again. */
+AO_API ao_status ao_tree_resize_buffers(ao_tree *tree);
+
+/* Getters particleKeys_d() ... sfcParticleIndex_d() -- tree.hpp:72-97, 113:
+ * device pointer, logical length (elements) and allocated capacity. */
+AO_API ao_status ao_tree_get_buffer(ao_tree *tree, int which, const void **dptr, size_t *len, size_t *capacity);
+
+/* numLeaves_d() / numNodes_d() / numActiveParticles_d() -- tree.hpp:58-63:
+ * device-resident counters for kernels recorded in the same graph. */
+AO_API ao_status ao_tree_counters(ao_tree *tree, const int **num_leaves_d, const int **num_nodes_d,
+                           const unsigned **num_active_particles_d);
+
+/* numParticles(), numActiveParticles(), numNodes(), maxAchievedDepth(),
+ * splitCriterion(), sfcKind() -- tree.hpp:64-71, 99-108. */
+AO_API ao_status ao_tree_get_info(ao_tree *tree, ao_tree_info *info);
+
+/* computeSfcKeys (sfc_keys.cuh:517-532) / computeSfcKeysBinary
+ * (kdtree3d_rebalance.cuh:261-273): unsorted keys of n particles and, if
+ * perm_d is not NULL, the identity permutation.  kind AO_OCTREE uses
+ * sfc_kind; AO_BINARY uses the longest-side schedule of `box` and max_depth. */
+AO_API ao_status ao_compute_sfc_keys(int kind, int real_type, const void *x, const void *y, const void *z, size_t n,
+                              const double *box, int sfc_kind, unsigned max_depth, unsigned long long *keys_d,
+                              unsigned *perm_d, void *stream);
+
+/* Message of the last failed call on this thread ("" if none). */
+AO_API const char *ao_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ADAPTIVE_TREES_B200_H */

@@ -1,0 +1,233 @@
+// ref_driver.cu -- runs the REFERENCE library (nrottstegge/Adaptive_Trees,
+// compiled from its own sources by oracle/Makefile into oracle/_ref/) on a
+// scenario file and dumps every output array.
+//
+// TEST INFRASTRUCTURE ONLY: used by tests/ to pin parity of the B200 engine
+// against the reference itself, and by bench.py to time the reference's GPU
+// path on the same box.  Written against the reference's public API
+// (adaptive_octree::Tree<Real, Kind>, tree.hpp:11-134).
+//
+// Input file (little-endian):
+//   u32 magic 'AOSC', u32 kind, u32 real, u32 frames, u64 n,
+//   i32 maxDepth, u32 bucket, i32 updateIterations, u32 nf, u32 hilbert,
+//   u32 views[3], u32 timingReps, f64 box[6],
+//   then `frames` x (x[n], y[n], z[n]) in Real.
+// Output file: per frame, for each of 14 arrays: u32 id, u64 count,
+//   u64 elemBytes, bytes; then u32 0xFFFFFFFF, u64 scalars[6]
+//   (numParticles, numActive, numNodes, maxAchievedDepth, resizes, 0).
+// With timingReps > 0 it instead prints one JSON line of timings:
+//   build_ms (median of reps, each a fresh tree), update_ms (median of
+//   captured-graph replays of update() over frame 1).
+#include <cuda_runtime.h>
+#include <thrust/device_vector.h>
+#include <thrust/host_vector.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <stdexcept>
+#include <vector>
+
+#include "adaptive_octree/tree.hpp"
+
+namespace
+{
+struct Header
+{
+    std::uint32_t magic, kind, real, frames;
+    std::uint64_t n;
+    std::int32_t maxDepth;
+    std::uint32_t bucket;
+    std::int32_t updateIterations;
+    std::uint32_t nf, hilbert, views[3], timingReps;
+    double box[6];
+};
+
+void check(cudaError_t e, const char *w)
+{
+    if (e != cudaSuccess) throw std::runtime_error(std::string(w) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+void dump(std::ofstream &out, std::uint32_t id, const thrust::device_vector<T> &v)
+{
+    thrust::host_vector<T> h = v;
+    const std::uint64_t count = h.size(), eb = sizeof(T);
+    out.write(reinterpret_cast<const char *>(&id), 4);
+    out.write(reinterpret_cast<const char *>(&count), 8);
+    out.write(reinterpret_cast<const char *>(&eb), 8);
+    if (count) out.write(reinterpret_cast<const char *>(h.data()), std::streamsize(count * eb));
+}
+
+template <class Real, adaptive_octree::TreeType Kind>
+int run(const Header &h, const std::vector<char> &payload, const char *outPath)
+{
+    using Tree = adaptive_octree::Tree<Real, Kind>;
+    const size_t n = h.n;
+    const Real *frames = reinterpret_cast<const Real *>(payload.data());
+    thrust::device_vector<Real> x(n), y(n), z(n);
+    auto load = [&](unsigned f) {
+        const Real *base = frames + size_t(f) * 3 * n;
+        if (n)
+        {
+            check(cudaMemcpy(thrust::raw_pointer_cast(x.data()), base, n * sizeof(Real), cudaMemcpyHostToDevice), "x");
+            check(cudaMemcpy(thrust::raw_pointer_cast(y.data()), base + n, n * sizeof(Real), cudaMemcpyHostToDevice),
+                  "y");
+            check(cudaMemcpy(thrust::raw_pointer_cast(z.data()), base + 2 * n, n * sizeof(Real),
+                             cudaMemcpyHostToDevice),
+                  "z");
+        }
+    };
+    typename Tree::Config c;
+    c.maxDepth = h.maxDepth;
+    c.maxParticlesPerLeaf = h.bucket;
+    c.updateIterations = h.updateIterations;
+    c.box = {Real(h.box[0]), Real(h.box[1]), Real(h.box[2]), Real(h.box[3]), Real(h.box[4]), Real(h.box[5])};
+    c.splitCriterion = h.nf ? adaptive_octree::SplitCriterion::NFCount : adaptive_octree::SplitCriterion::LeafCount;
+    c.sfcKind = h.hilbert ? adaptive_octree::SfcKind::Hilbert : adaptive_octree::SfcKind::Morton;
+    c.views = {h.views[0] != 0, h.views[1] != 0, h.views[2] != 0};
+    cudaStream_t stream;
+    check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "stream");
+    c.stream = stream;
+    const Real *xp = thrust::raw_pointer_cast(x.data()), *yp = thrust::raw_pointer_cast(y.data()),
+               *zp = thrust::raw_pointer_cast(z.data());
+
+    if (h.timingReps > 0)
+    {
+        cudaEvent_t a, b;
+        check(cudaEventCreate(&a), "ev");
+        check(cudaEventCreate(&b), "ev");
+        std::vector<double> builds, updates;
+        load(0);
+        check(cudaDeviceSynchronize(), "sync");
+        for (unsigned r = 0; r < h.timingReps + 1; ++r)
+        {
+            Tree tree(xp, yp, zp, n, c);
+            check(cudaStreamSynchronize(stream), "sync");
+            check(cudaEventRecord(a, stream), "rec");
+            tree.build();
+            check(cudaEventRecord(b, stream), "rec");
+            check(cudaEventSynchronize(b), "sync");
+            float ms = 0;
+            check(cudaEventElapsedTime(&ms, a, b), "elapsed");
+            if (r > 0) builds.push_back(ms);  // first build warms the process up
+        }
+        Tree tree(xp, yp, zp, n, c);
+        tree.build();
+        if (h.frames > 1) load(1);
+        check(cudaDeviceSynchronize(), "sync");
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+        check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeGlobal), "capture");
+        tree.update();
+        check(cudaStreamEndCapture(stream, &graph), "capture");
+        check(cudaGraphInstantiate(&exec, graph, 0), "instantiate");
+        for (unsigned r = 0; r < h.timingReps + 3; ++r)
+        {
+            check(cudaEventRecord(a, stream), "rec");
+            check(cudaGraphLaunch(exec, stream), "launch");
+            check(cudaEventRecord(b, stream), "rec");
+            check(cudaEventSynchronize(b), "sync");
+            float ms = 0;
+            check(cudaEventElapsedTime(&ms, a, b), "elapsed");
+            if (r >= 3) updates.push_back(ms);
+            if (tree.doBuffersNeedResize())
+            {
+                cudaGraphExecDestroy(exec);
+                cudaGraphDestroy(graph);
+                tree.resizeBuffers();
+                check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeGlobal), "capture");
+                tree.update();
+                check(cudaStreamEndCapture(stream, &graph), "capture");
+                check(cudaGraphInstantiate(&exec, graph, 0), "instantiate");
+            }
+        }
+        std::sort(builds.begin(), builds.end());
+        std::sort(updates.begin(), updates.end());
+        std::printf("{\"build_ms\": %.6f, \"update_ms\": %.6f, \"build_min_ms\": %.6f, \"update_min_ms\": %.6f}\n",
+                    builds[builds.size() / 2], updates[updates.size() / 2], builds.front(), updates.front());
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        return 0;
+    }
+
+    std::ofstream out(outPath, std::ios::binary);
+    Tree tree(xp, yp, zp, n, c);
+    std::uint64_t resizes = 0;
+    for (unsigned f = 0; f < h.frames; ++f)
+    {
+        load(f);
+        check(cudaDeviceSynchronize(), "sync");
+        if (f == 0)
+        {
+            tree.build();
+        }
+        else
+        {
+            tree.update();
+            while (tree.doBuffersNeedResize())
+            {
+                ++resizes;
+                tree.resizeBuffers();
+                tree.update();
+            }
+        }
+        (void)tree.doBuffersNeedResize();
+        check(cudaDeviceSynchronize(), "sync");
+        dump(out, 0, tree.particleKeys_d());
+        dump(out, 1, tree.perm_d());
+        dump(out, 2, tree.cornerstone_d());
+        dump(out, 3, tree.leafCounts_d());
+        if constexpr (Kind == adaptive_octree::TreeType::Octree) dump(out, 4, tree.nearFieldCounts_d());
+        dump(out, 5, tree.sfcBoxIndex_d());
+        dump(out, 6, tree.hasBoxSplit_d());
+        dump(out, 7, tree.boxDepth_d());
+        dump(out, 8, tree.parentIndex_d());
+        dump(out, 9, tree.childIndex_d());
+        dump(out, 10, tree.levelOffset_d());
+        dump(out, 11, tree.particleBeginIndex_d());
+        dump(out, 12, tree.particleCounts_d());
+        dump(out, 13, tree.sfcParticleIndex_d());
+        const std::uint32_t end = 0xFFFFFFFFu;
+        const std::uint64_t sc[6] = {tree.numParticles(), tree.numActiveParticles(), tree.numNodes(),
+                                     tree.maxAchievedDepth(), resizes, 0};
+        out.write(reinterpret_cast<const char *>(&end), 4);
+        out.write(reinterpret_cast<const char *>(sc), sizeof(sc));
+    }
+    return 0;
+}
+}  // namespace
+
+int main(int argc, char **argv)
+{
+    if (argc < 3)
+    {
+        std::fprintf(stderr, "usage: ref_driver scenario.bin out.bin\n");
+        return 2;
+    }
+    try
+    {
+        std::ifstream in(argv[1], std::ios::binary);
+        Header h{};
+        in.read(reinterpret_cast<char *>(&h), sizeof(h));
+        if (!in || h.magic != 0x43534f41u) throw std::runtime_error("bad scenario header");
+        const size_t bytes = size_t(h.frames) * 3 * h.n * (h.real ? 8 : 4);
+        std::vector<char> payload(bytes);
+        in.read(payload.data(), std::streamsize(bytes));
+        if (!in) throw std::runtime_error("short scenario file");
+        using adaptive_octree::TreeType;
+        if (h.kind == 0 && h.real == 0) return run<float, TreeType::Octree>(h, payload, argv[2]);
+        if (h.kind == 0 && h.real == 1) return run<double, TreeType::Octree>(h, payload, argv[2]);
+        if (h.kind == 1 && h.real == 0) return run<float, TreeType::Binary>(h, payload, argv[2]);
+        return run<double, TreeType::Binary>(h, payload, argv[2]);
+    }
+    catch (const std::exception &e)
+    {
+        std::fprintf(stderr, "ref_driver: %s\n", e.what());
+        return 1;
+    }
+}
