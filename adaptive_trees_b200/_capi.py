@@ -33,7 +33,8 @@ class AoViewConfig(ctypes.Structure):
 
 class AoTreeInfo(ctypes.Structure):
     _fields_ = [("num_particles", sz), ("num_active_particles", sz), ("num_nodes", sz), ("num_leaves", sz),
-                ("leaf_capacity", sz), ("max_achieved_depth", cu), ("split_criterion", ci), ("sfc_kind", ci)]
+                ("leaf_capacity", sz), ("max_achieved_depth", cu), ("split_criterion", ci), ("sfc_kind", ci),
+                ("kernel_launches", ctypes.c_ulonglong)]
 
 
 PROTOTYPES = {
@@ -48,6 +49,7 @@ PROTOTYPES = {
     "ao_tree_counters": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)],
     "ao_tree_get_info": [vp, ctypes.POINTER(AoTreeInfo)],
     "ao_compute_sfc_keys": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_double), ci, cu, vp, vp, vp],
+    "ao_sort_pairs": [vp, ctypes.POINTER(sz), vp, vp, vp, vp, sz, ci, ci, vp],
 }
 
 _lock = threading.Lock()

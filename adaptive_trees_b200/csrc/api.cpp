@@ -403,6 +403,7 @@ ao_status ao_tree_get_info(ao_tree *tree, ao_tree_info *info)
         info->max_achieved_depth = e.maxAchievedDepth();
         info->split_criterion = e.config().nf ? AO_NF_COUNT : AO_LEAF_COUNT;
         info->sfc_kind = e.config().kind == AO_BINARY ? -1 : (e.config().hilbert ? AO_HILBERT : AO_MORTON);
+        info->kernel_launches = aot::TreeEngine::kernelLaunches();
     });
 }
 
@@ -418,6 +419,16 @@ ao_status ao_compute_sfc_keys(int kind, int real_type, const void *x, const void
             throw std::invalid_argument("ao_compute_sfc_keys: null argument");
         aot::TreeEngine::computeKeys(kind, real_type, x, y, z, n, box, sfc_kind == AO_HILBERT, max_depth, keys_d,
                                      perm_d, static_cast<cudaStream_t>(stream));
+    });
+}
+
+ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsigned long long *keys_in,
+                        unsigned long long *keys_out, const unsigned *values_in, unsigned *values_out, size_t n,
+                        int begin_bit, int end_bit, void *stream)
+{
+    return guarded([&] {
+        aot::TreeEngine::sortPairs(scratch, scratch_bytes, keys_in, keys_out, values_in, values_out, n, begin_bit,
+                                   end_bit, static_cast<cudaStream_t>(stream));
     });
 }
 

@@ -15,6 +15,7 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -60,6 +61,11 @@ void DevMem::grow(size_t b, size_t keep, cudaStream_t s)
 
 namespace
 {
+// Kernel launches issued by this process (all trees); reported by
+// ao_tree_get_info so a benchmark can state how many engine kernels ran.
+std::atomic<unsigned long long> g_launches{0};
+inline void noteLaunch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 int smCount()
 {
     static int sms = 0;
@@ -141,8 +147,8 @@ void launchKeygenT(const Real *x, const Real *y, const Real *z, size_t n, const 
     const size_t groups = vec ? n / V : n;
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(std::max<size_t>(groups, 1), kKeygenThreads),
                                                              unsigned(smCount()) * 8u));
-    if (vec) keygenKernel<Real, C, V><<<blocks, kKeygenThreads, 0, s>>>(x, y, z, n, prm, keys, hist, passes);
-    else keygenKernel<Real, C, 1><<<blocks, kKeygenThreads, 0, s>>>(x, y, z, n, prm, keys, hist, passes);
+    if (vec) keygenKernel<Real, C, V><<<blocks, kKeygenThreads, 0, s>>>(x, y, z, n, prm, keys, hist, passes), noteLaunch();
+    else keygenKernel<Real, C, 1><<<blocks, kKeygenThreads, 0, s>>>(x, y, z, n, prm, keys, hist, passes), noteLaunch();
     AOT_LAUNCH_CHECK();
 }
 
@@ -201,7 +207,7 @@ int runPasses(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int beginBit, int 
 {
     setPassSmem();
     const size_t tiles = (n + sort::kTile - 1) / sort::kTile;
-    sort::binsKernel<<<1, sort::kRadix, 0, s>>>(a.hist(), a.bins(), passes);
+    sort::binsKernel<<<1, sort::kRadix, 0, s>>>(a.hist(), a.bins(), passes), noteLaunch();
     AOT_LAUNCH_CHECK();
     for (int p = 0; p < passes; ++p)
     {
@@ -209,7 +215,7 @@ int runPasses(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int beginBit, int 
         sort::onesweepKernel<<<unsigned(tiles), sort::kThreads, sort::passSmem(), s>>>(
             k[in], (p == 0 && valsAreIndices) ? nullptr : v[in], k[out], v[out], n, beginBit + p * sort::kRadixBits,
             a.bins() + p * sort::kRadix, a.tileCounters() + p, a.status.as<u64>() + size_t(p) * tiles * sort::kRadix,
-            error);
+            error), noteLaunch();
         AOT_LAUNCH_CHECK();
     }
     return passes & 1;
@@ -229,7 +235,7 @@ int sortWithIndices(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int passes, 
     a.ensure(n);
     clearArena(s, a, n, passes);
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n, sort::kThreads), unsigned(smCount()) * 8u));
-    sort::histogramKernel<<<blocks, sort::kThreads, 0, s>>>(k[0], n, 0, passes, a.hist());
+    sort::histogramKernel<<<blocks, sort::kThreads, 0, s>>>(k[0], n, 0, passes, a.hist()), noteLaunch();
     AOT_LAUNCH_CHECK();
     return runPasses(s, k, v, n, 0, passes, true, a, error);
 }
@@ -237,6 +243,91 @@ int sortWithIndices(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int passes, 
 unsigned gridFor(size_t n, unsigned threads) { return std::max(1u, ceilDiv(std::max<size_t>(n, 1), threads)); }
 
 }  // namespace
+
+unsigned long long TreeEngine::kernelLaunches() { return g_launches.load(std::memory_order_relaxed); }
+
+// --------------------------------------------------------------------------
+// stand-alone stable pair sort (cub::DeviceRadixSort::SortPairs semantics)
+// --------------------------------------------------------------------------
+namespace
+{
+struct PairSortLayout
+{
+    size_t altKeys = 0, altVals = 0, counters = 0, status = 0, total = 0, tiles = 0;
+    explicit PairSortLayout(size_t n)
+    {
+        auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+        tiles = std::max<size_t>(1, (n + sort::kTile - 1) / sort::kTile);
+        altKeys = 0;
+        altVals = up(altKeys + n * sizeof(u64));
+        counters = up(altVals + n * sizeof(u32));
+        status = up(counters + (2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses + 2) * sizeof(u32));
+        total = up(status + size_t(sort::kMaxPasses) * tiles * sort::kRadix * sizeof(u64));
+    }
+};
+}  // namespace
+
+void TreeEngine::sortPairs(void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
+                           unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
+                           int beginBit, int endBit, cudaStream_t s)
+{
+    if (!scratchBytes) throw std::invalid_argument("ao_sort_pairs: scratch_bytes must not be null");
+    if (beginBit < 0 || endBit > 64 || beginBit > endBit)
+        throw std::invalid_argument("ao_sort_pairs: need 0 <= begin_bit <= end_bit <= 64");
+    if (n > size_t(std::numeric_limits<std::uint32_t>::max()))
+        throw std::invalid_argument("ao_sort_pairs: more than 2^32 - 1 items");
+    const PairSortLayout lay(n);
+    if (!scratch)
+    {
+        *scratchBytes = lay.total;
+        return;
+    }
+    if (*scratchBytes < lay.total) throw std::invalid_argument("ao_sort_pairs: scratch too small");
+    if (n == 0) return;
+    if (!keysIn || !keysOut || !valsOut) throw std::invalid_argument("ao_sort_pairs: null array");
+    if (keysIn == keysOut) throw std::invalid_argument("ao_sort_pairs: keys_in and keys_out must differ");
+    char *base = static_cast<char *>(scratch);
+    u64 *altK = reinterpret_cast<u64 *>(base + lay.altKeys);
+    u32 *altV = reinterpret_cast<u32 *>(base + lay.altVals);
+    u32 *ctr = reinterpret_cast<u32 *>(base + lay.counters);
+    u64 *status = reinterpret_cast<u64 *>(base + lay.status);
+    int *error = reinterpret_cast<int *>(ctr + 2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses);
+    const int passes = (endBit - beginBit + sort::kRadixBits - 1) / sort::kRadixBits;
+    if (passes == 0)
+    {
+        AOT_CHECK(cudaMemcpyAsync(keysOut, keysIn, n * sizeof(u64), cudaMemcpyDeviceToDevice, s));
+        if (valsIn) AOT_CHECK(cudaMemcpyAsync(valsOut, valsIn, n * sizeof(u32), cudaMemcpyDeviceToDevice, s));
+        else iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(valsOut, n), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        return;
+    }
+    AOT_CHECK(cudaMemsetAsync(ctr, 0, (2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses + 2) * sizeof(u32), s));
+    AOT_CHECK(cudaMemsetAsync(status, 0, size_t(passes) * lay.tiles * sort::kRadix * sizeof(u64), s));
+    const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n, sort::kThreads), unsigned(smCount()) * 8u));
+    sort::histogramKernel<<<blocks, sort::kThreads, 0, s>>>(reinterpret_cast<const u64 *>(keysIn), n, beginBit, passes,
+                                                             ctr, endBit), noteLaunch();
+    sort::binsKernel<<<1, sort::kRadix, 0, s>>>(ctr, ctr + sort::kMaxPasses * sort::kRadix, passes), noteLaunch();
+    AOT_LAUNCH_CHECK();
+    setPassSmem();
+    const u64 *kin = reinterpret_cast<const u64 *>(keysIn);
+    const u32 *vin = valsIn;
+    for (int p = 0; p < passes; ++p)
+    {
+        // the last pass writes keysOut; earlier passes alternate backwards from it
+        const bool toOut = ((passes - 1 - p) & 1) == 0;
+        u64 *kout = toOut ? reinterpret_cast<u64 *>(keysOut) : altK;
+        u32 *vout = toOut ? valsOut : altV;
+        const int shift = beginBit + p * sort::kRadixBits;
+        const int bits = std::min(sort::kRadixBits, endBit - shift);
+        sort::onesweepKernel<<<unsigned(lay.tiles), sort::kThreads, sort::passSmem(), s>>>(
+            kin, vin, kout, vout, n, shift, ctr + sort::kMaxPasses * sort::kRadix + p * sort::kRadix,
+            ctr + 2 * sort::kMaxPasses * sort::kRadix + p, status + size_t(p) * lay.tiles * sort::kRadix, error,
+            bits), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        kin = kout;
+        vin = vout;
+    }
+}
 
 // --------------------------------------------------------------------------
 // Impl
@@ -454,7 +545,7 @@ void TreeEngine::sortParticles()
     const int where = runPasses(s, k, v, n_, 0, sort::kMaxPasses, true, a, &m_->st->error);
     (void)where;  // eight passes end in buffer 0
     const size_t ns = (n_ + kSampleStride - 1) >> kSampleShift;
-    rb::sampleKeysKernel<<<gridFor(ns, 256), 256, 0, s>>>(k[0], n_, m_->sample.as<u64>(), ns);
+    rb::sampleKeysKernel<<<gridFor(ns, 256), 256, 0, s>>>(k[0], n_, m_->sample.as<u64>(), ns), noteLaunch();
     AOT_LAUNCH_CHECK();
 }
 
@@ -479,7 +570,7 @@ void TreeEngine::computeKeys(int kind, int real, const void *x, const void *y, c
                              static_cast<const double *>(z), n, pd, reinterpret_cast<u64 *>(keys), nullptr, 0, s);
     if (perm)
     {
-        iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(perm, n);
+        iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(perm, n), noteLaunch();
         AOT_LAUNCH_CHECK();
     }
 }
@@ -541,7 +632,7 @@ void TreeEngine::octreePass(bool buildMode, long long limit)
     const rb::TreeBufs tb = m_->bufs();
     const size_t cap = buildMode ? physCap_ : leafCapacity_;
     const size_t tiles = (cap + 1 + rb::kScanTile - 1) / rb::kScanTile;
-    rb::beginPassKernel<<<1, 1, 0, s>>>(m_->st);
+    rb::beginPassKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
     AOT_CHECK(cudaMemsetAsync(m_->scan.p, 0, (m_->scanTiles + 1) * sizeof(u64), s));
     const KeyIndex idx = m_->keyIndex(n_);
     const int mode = buildMode ? kModeOctreeBuild : kModeUpdate;
@@ -550,21 +641,21 @@ void TreeEngine::octreePass(bool buildMode, long long limit)
     const unsigned refreshBlocks = unsigned(smCount()) * 8u;
     if (cfg_.nf)
     {
-        rb::octDecideScanKernel<true><<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket);
-        rb::octScatterKernel<true><<<scatterBlocks, rb::kScatterThreads, 0, s>>>(tb, limit, mode, hist);
+        rb::octDecideScanKernel<true><<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket), noteLaunch();
+        rb::octScatterKernel<true><<<scatterBlocks, rb::kScatterThreads, 0, s>>>(tb, limit, mode, hist), noteLaunch();
         if (cfg_.hilbert)
             rb::octRefreshKernel<true, true, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(
-                tb, idx, cfg_.bucket, m_->kpd.h);
+                tb, idx, cfg_.bucket, m_->kpd.h), noteLaunch();
         else
             rb::octRefreshKernel<true, false, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(
-                tb, idx, cfg_.bucket, m_->kpd.h);
+                tb, idx, cfg_.bucket, m_->kpd.h), noteLaunch();
     }
     else
     {
-        rb::octDecideScanKernel<false><<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket);
-        rb::octScatterKernel<false><<<scatterBlocks, rb::kScatterThreads, 0, s>>>(tb, limit, mode, hist);
+        rb::octDecideScanKernel<false><<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket), noteLaunch();
+        rb::octScatterKernel<false><<<scatterBlocks, rb::kScatterThreads, 0, s>>>(tb, limit, mode, hist), noteLaunch();
         rb::octRefreshKernel<false, false, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
-                                                                                                m_->kpd.h);
+                                                                                                m_->kpd.h), noteLaunch();
     }
     AOT_LAUNCH_CHECK();
 }
@@ -575,13 +666,13 @@ void TreeEngine::binaryPass(bool buildMode, long long limit)
     const rb::TreeBufs tb = m_->bufs();
     const size_t cap = buildMode ? physCap_ : leafCapacity_;
     const size_t tiles = (cap + 1 + rb::kScanTile - 1) / rb::kScanTile;
-    rb::beginPassKernel<<<1, 1, 0, s>>>(m_->st);
+    rb::beginPassKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
     AOT_CHECK(cudaMemsetAsync(m_->scan.p, 0, (m_->scanTiles + 1) * sizeof(u64), s));
     const KeyIndex idx = m_->keyIndex(n_);
-    rb::binDecideScanKernel<<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket, cfg_.maxDepth);
+    rb::binDecideScanKernel<<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket, cfg_.maxDepth), noteLaunch();
     rb::binScatterKernel<<<gridFor(cap, rb::kScatterThreads), rb::kScatterThreads, 0, s>>>(
-        tb, limit, buildMode ? kModeBinaryBuild : kModeUpdate);
-    rb::binRefreshKernel<false><<<unsigned(smCount()) * 8u, 256, 0, s>>>(tb, idx);
+        tb, limit, buildMode ? kModeBinaryBuild : kModeUpdate), noteLaunch();
+    rb::binRefreshKernel<false><<<unsigned(smCount()) * 8u, 256, 0, s>>>(tb, idx), noteLaunch();
     AOT_LAUNCH_CHECK();
 }
 
@@ -593,24 +684,24 @@ void TreeEngine::refreshAll()
     cudaStream_t s = cfg_.stream;
     const rb::TreeBufs tb = m_->bufs();
     const KeyIndex idx = m_->keyIndex(n_);
-    rb::resetForUpdateKernel<<<1, 1, 0, s>>>(m_->st, m_->P[0].as<u64>(), n_);
+    rb::resetForUpdateKernel<<<1, 1, 0, s>>>(m_->st, m_->P[0].as<u64>(), n_), noteLaunch();
     const unsigned blocks = unsigned(smCount()) * 8u;
     if (cfg_.kind == 1)
-        rb::binRefreshKernel<true><<<blocks, 256, 0, s>>>(tb, idx);
+        rb::binRefreshKernel<true><<<blocks, 256, 0, s>>>(tb, idx), noteLaunch();
     else if (!cfg_.nf)
         rb::octRefreshKernel<false, false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
-                                                                                        m_->kpd.h);
+                                                                                        m_->kpd.h), noteLaunch();
     else if (cfg_.hilbert)
-        rb::octRefreshKernel<true, true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, m_->kpd.h);
+        rb::octRefreshKernel<true, true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, m_->kpd.h), noteLaunch();
     else
         rb::octRefreshKernel<true, false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
-                                                                                       m_->kpd.h);
+                                                                                       m_->kpd.h), noteLaunch();
     AOT_LAUNCH_CHECK();
 }
 
 void TreeEngine::materializeCounts()
 {
-    rb::materializeCountsKernel<<<gridFor(std::max(leafCapacity_, physCap_), 256), 256, 0, cfg_.stream>>>(m_->bufs());
+    rb::materializeCountsKernel<<<gridFor(std::max(leafCapacity_, physCap_), 256), 256, 0, cfg_.stream>>>(m_->bufs()), noteLaunch();
     AOT_LAUNCH_CHECK();
 }
 
@@ -715,7 +806,7 @@ void TreeEngine::octreeBuild()
     ensurePhysical(std::max(physCap_, estimate));
     m_->history.reserve(std::max<size_t>(cfg_.maxDepth, 1) * sizeof(long long));
     rb::TreeBufs tb = m_->bufs();
-    octInitRootKernel<<<1, 1, 0, s>>>(tb, m_->P[0].as<u64>(), n_);
+    octInitRootKernel<<<1, 1, 0, s>>>(tb, m_->P[0].as<u64>(), n_), noteLaunch();
     AOT_LAUNCH_CHECK();
     // rebalanceBuild (octree.cu:159-180): at most maxDepth decision rounds
     int done = 0;
@@ -734,7 +825,7 @@ void TreeEngine::octreeBuild()
         {
             const size_t need = size_t(h.proposal);
             ensurePhysical(std::max(need + need / 4, 2 * physCap_));
-            clearOverflowKernel<<<1, 1, 0, s>>>(m_->st);
+            clearOverflowKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
             AOT_LAUNCH_CHECK();
         }
     }
@@ -772,7 +863,7 @@ void TreeEngine::octreeBuild()
             AOT_CHECK(cudaMemcpyAsync(m_->G[0].p, m_->G[1].p, leaves * sizeof(u8), cudaMemcpyDeviceToDevice, s));
         }
     }
-    octFinishBuildKernel<<<1, 1, 0, s>>>(m_->st);
+    octFinishBuildKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
     AOT_LAUNCH_CHECK();
     prepareGraphBuffers(cap);
     built_ = true;
@@ -792,7 +883,7 @@ void TreeEngine::binaryBuild()
     const size_t estimate = std::max<size_t>(4096, 4 * (n_ / std::max(1u, cfg_.bucket)) + 4096);
     ensurePhysical(std::max({physCap_, estimate, leafCapacity_}));
     rb::TreeBufs tb = m_->bufs();
-    binInitRootKernel<<<1, 1, 0, s>>>(tb, (long long)leafCapacity_);
+    binInitRootKernel<<<1, 1, 0, s>>>(tb, (long long)leafCapacity_), noteLaunch();
     AOT_LAUNCH_CHECK();
     refreshAll();
     // build loop (kdtree3d.cu:239-249): passes until converged
@@ -811,7 +902,7 @@ void TreeEngine::binaryBuild()
         {
             const size_t need = size_t(h.proposal);
             ensurePhysical(std::max(need + need / 4, 2 * physCap_));
-            clearOverflowKernel<<<1, 1, 0, s>>>(m_->st);
+            clearOverflowKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
             AOT_LAUNCH_CHECK();
         }
         if (passes > 200000) throw std::runtime_error("adaptive_octree: binary build did not converge");
@@ -918,7 +1009,7 @@ void TreeEngine::buildViews(const adaptive_octree::ViewConfig &v)
     if (!m.viewScratch || (v.particleCountsPerBox && !m.viewPrepared.particleCountsPerBox) ||
         (v.particleMapping && (!m.viewPrepared.particleMapping || n_ > m.viewParticleCap)))
     {
-        tv::flagResizeKernel<<<1, 1, 0, s>>>(m.st);
+        tv::flagResizeKernel<<<1, 1, 0, s>>>(m.st), noteLaunch();
         AOT_LAUNCH_CHECK();
         return;
     }
@@ -933,13 +1024,13 @@ void TreeEngine::buildViews(const adaptive_octree::ViewConfig &v)
     AOT_CHECK(cudaMemsetAsync(vb.leavesPerLevel, 0, 66 * sizeof(int), s));
     if (b == 3)
     {
-        tv::classifyKernel<3><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, m.st, leafCap, vb);
-        tv::metadataKernel<3><<<1, 1, 0, s>>>(m.st, leafCap, vb);
+        tv::classifyKernel<3><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, m.st, leafCap, vb), noteLaunch();
+        tv::metadataKernel<3><<<1, 1, 0, s>>>(m.st, leafCap, vb), noteLaunch();
     }
     else
     {
-        tv::classifyKernel<1><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, m.st, leafCap, vb);
-        tv::metadataKernel<1><<<1, 1, 0, s>>>(m.st, leafCap, vb);
+        tv::classifyKernel<1><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, m.st, leafCap, vb), noteLaunch();
+        tv::metadataKernel<1><<<1, 1, 0, s>>>(m.st, leafCap, vb), noteLaunch();
     }
     AOT_LAUNCH_CHECK();
     if (intCap > 0)
@@ -949,32 +1040,32 @@ void TreeEngine::buildViews(const adaptive_octree::ViewConfig &v)
         u32 *lv[2] = {vb.lvVals, vb.lvValsAlt};
         const int w1 = sortWithIndices(s, lk, lv, size_t(leafCap - 1), 1, m.viewSort, &m.st->error);
         if (b == 3)
-            tv::layoutKeysKernel<3><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(lk[w1], lv[w1], intCap, vb);
+            tv::layoutKeysKernel<3><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(lk[w1], lv[w1], intCap, vb), noteLaunch();
         else
-            tv::layoutKeysKernel<1><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(lk[w1], lv[w1], intCap, vb);
+            tv::layoutKeysKernel<1><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(lk[w1], lv[w1], intCap, vb), noteLaunch();
         AOT_LAUNCH_CHECK();
         u64 *yk[2] = {vb.layKeys, vb.layKeysAlt};
         u32 *yv[2] = {vb.layVals, vb.layValsAlt};
         const int w2 = sortWithIndices(s, yk, yv, size_t(intCap), 8, m.viewSort, &m.st->error);
-        tv::materializeKernel<<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(yk[w2], yv[w2], intCap, vb);
+        tv::materializeKernel<<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(yk[w2], yv[w2], intCap, vb), noteLaunch();
         if (b == 3)
             tv::internalNodesKernel<3><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(m.st, leafCap, intCap,
-                                                                                              idx, counts, vb);
+                                                                                              idx, counts, vb), noteLaunch();
         else
             tv::internalNodesKernel<1><<<gridFor(intCap, tv::kThreads), tv::kThreads, 0, s>>>(m.st, leafCap, intCap,
-                                                                                              idx, counts, vb);
+                                                                                              idx, counts, vb), noteLaunch();
         AOT_LAUNCH_CHECK();
     }
     if (b == 3)
         tv::leafNodesKernel<3><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, B0, B1, m.st, leafCap,
-                                                                                      counts, vb);
+                                                                                      counts, vb), noteLaunch();
     else
         tv::leafNodesKernel<1><<<gridFor(leafCap, tv::kThreads), tv::kThreads, 0, s>>>(K0, K1, B0, B1, m.st, leafCap,
-                                                                                      counts, vb);
+                                                                                      counts, vb), noteLaunch();
     AOT_LAUNCH_CHECK();
     if (v.particleMapping && n_ > 0)
     {
-        tv::mappingKernel<<<gridFor(n_, tv::kThreads), tv::kThreads, 0, s>>>(B0, B1, m.st, leafCap, n_, vb);
+        tv::mappingKernel<<<gridFor(n_, tv::kThreads), tv::kThreads, 0, s>>>(B0, B1, m.st, leafCap, n_, vb), noteLaunch();
         AOT_LAUNCH_CHECK();
     }
 }

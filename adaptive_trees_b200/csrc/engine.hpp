@@ -99,6 +99,14 @@ public:
     // diagnostics: committed build rounds, physical leaf capacity
     int buildRounds() const { return buildRounds_; }
     size_t physicalCapacity() const { return physCap_; }
+    // kernel launches issued by the engine in this process
+    static unsigned long long kernelLaunches();
+    // stable sort of (key, value) pairs by bits [beginBit, endBit)
+    // (cub::DeviceRadixSort::SortPairs semantics; scratch == nullptr queries
+    // the scratch size; valsIn == nullptr sorts the indices 0..n-1)
+    static void sortPairs(void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
+                          unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
+                          int beginBit, int endBit, cudaStream_t s);
     // one-shot key generation without a sort (computeSfcKeys semantics)
     static void computeKeys(int kind, int real, const void *x, const void *y, const void *z, size_t n,
                             const double *box, bool hilbert, unsigned maxDepth, unsigned long long *keys,

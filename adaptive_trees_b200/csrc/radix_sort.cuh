@@ -75,7 +75,7 @@ inline size_t scratchBytes(size_t n)
 
 // Histogram of the digits of keys[0, n) for passes covering [beginBit, endBit).
 __global__ void __launch_bounds__(kThreads) histogramKernel(const u64 *__restrict__ keys, size_t n, int beginBit,
-                                                             int passes, u32 *__restrict__ hist)
+                                                             int passes, u32 *__restrict__ hist, int endBit = 64)
 {
     __shared__ u32 sh[kMaxPasses][kRadix];
     for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kThreads) (&sh[0][0])[i] = 0;
@@ -83,7 +83,12 @@ __global__ void __launch_bounds__(kThreads) histogramKernel(const u64 *__restric
     for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n; i += size_t(gridDim.x) * kThreads)
     {
         const u64 k = __ldg(keys + i);
-        for (int p = 0; p < passes; ++p) atomicAdd(&sh[p][(k >> (beginBit + p * kRadixBits)) & (kRadix - 1)], 1u);
+        for (int p = 0; p < passes; ++p)
+        {
+            const int shift = beginBit + p * kRadixBits;
+            const int bits = endBit - shift < kRadixBits ? endBit - shift : kRadixBits;
+            atomicAdd(&sh[p][(k >> shift) & ((1u << bits) - 1)], 1u);
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < passes * kRadix; i += kThreads)
@@ -133,8 +138,10 @@ struct SharedPass
 __global__ void __launch_bounds__(kThreads) onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn,
                                                             u64 *__restrict__ keysOut, u32 *__restrict__ valsOut,
                                                             size_t n, int shift, const u32 *__restrict__ bins,
-                                                            u32 *tileCounter, u64 *status, int *error)
+                                                            u32 *tileCounter, u64 *status, int *error,
+                                                            int bits = kRadixBits)
 {
+    const unsigned dmask = (1u << bits) - 1;
     extern __shared__ __align__(16) unsigned char smemRaw[];
     SharedPass &sm = *reinterpret_cast<SharedPass *>(smemRaw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -158,7 +165,7 @@ __global__ void __launch_bounds__(kThreads) onesweepKernel(const u64 *__restrict
         {
             key[i] = __ldcs(keysIn + idx);
             val[i] = valsIn ? __ldcs(valsIn + idx) : u32(idx);
-            digit[i] = int((key[i] >> shift) & (kRadix - 1));
+            digit[i] = int((key[i] >> shift) & dmask);
         }
         else
         {
@@ -268,7 +275,7 @@ __global__ void __launch_bounds__(kThreads) onesweepKernel(const u64 *__restrict
     for (int j = tid; j < valid; j += kThreads)
     {
         const u64 k = sm.keys[j];
-        const int d = int((k >> shift) & (kRadix - 1));
+        const int d = int((k >> shift) & dmask);
         const size_t out = size_t(sm.gstart[d] + j);
         keysOut[out] = k;
         valsOut[out] = sm.vals[j];

@@ -1,0 +1,387 @@
+"""Benchmark of the B200 adaptive-tree engine on the 16Mi-particle octree workload.
+
+Workload (one GPU): octree, 16,777,216 fp32 particles in a Plummer sphere
+(scale 0.05, centre (0.5,0.5,0.5), truncated at r = 0.5), Hilbert keys,
+NFCount refinement with near-field limit 512.  A step is one build() of the
+tree from the root over the resident coordinates; the same run also times
+graph-replayed update() steps on jittered coordinates (N(0, 1e-3), clamped to
+the box).  Multi-GPU runs are replicas (one independent tree per GPU, no
+collective on the path); the value is the total particles of all ranks over
+the slowest rank's time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  --impl reference times the CPU oracle port of
+the reference algorithm on a bounded sample (the reference has no CPU
+implementation of this path); the reference library's own GPU time on this
+box is reported by the default run under "reference_gpu".
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 1 << 24
+BUCKET = 512
+METRIC = "particles/s (octree build, 16Mi Plummer fp32, Hilbert, NFCount 512)"
+WORKLOAD = "octree build + graph-replayed update, 16Mi Plummer fp32 (a=0.05, r<=0.5), Hilbert keys, NFCount 512"
+# DRAM bytes of one 16Mi-key onesweep pass (key+value in and out), from the ncu
+# capture summarised in profiles/onesweep_pass_16Mi.txt; None until captured.
+ONESWEEP_TRAFFIC_BYTES = None
+
+
+def plummer(n, seed, scale=0.05, rmax=0.5):
+    rng = np.random.default_rng(seed)
+    out = np.empty((n, 3), dtype=np.float64)
+    filled = 0
+    while filled < n:
+        m = int((n - filled) * 1.05) + 1024
+        u = np.clip(rng.random(m), 1e-12, 1 - 1e-12)
+        r = scale / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+        r = r[r <= rmax]
+        v = rng.normal(size=(r.size, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        take = min(r.size, n - filled)
+        out[filled:filled + take] = v[:take] * r[:take, None] + 0.5
+        filled += take
+    np.clip(out, 0.0, np.nextafter(1.0, 0.0), out=out)
+    return tuple(np.ascontiguousarray(out[:, i].astype(np.float32)) for i in range(3))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_build(n_sample, seed=7):
+    """Single-threaded CPU port (oracle) of the reference build on a subset; particles/s."""
+    from oracle import oracle as O
+    x, y, z = plummer(n_sample, seed)
+    cfg = O.make_config(max_particles_per_leaf=BUCKET, split_criterion=1, sfc_kind=1)
+    t = O.OracleTree(0, x, y, z, cfg)
+    t0 = time.perf_counter()
+    t.build()
+    dt = time.perf_counter() - t0
+    return n_sample / dt, dt
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sample = args.cpu_sample
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, _ = cpu_oracle_build(sample, seed=7 + i)
+        if i >= args.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particles/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sample / v * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": sample, "sample_of_n": args.n},
+            "cpu_baseline": {"value": v, "unit": "particles/s", "cores": 1, "kind": "port",
+                             "sample": f"one build of {sample} Plummer particles per step (CPU oracle port)"},
+            "e2e": {"value": v, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--cpu-sample", type=int, default=1 << 20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import adaptive_trees_b200 as ab
+    from adaptive_trees_b200 import _capi as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    s = torch.cuda.Stream(device=dev)
+    n = args.n
+    hx = plummer(n, seed=1234 + rank)
+    pinned = [torch.from_numpy(a).pin_memory() for a in hx]
+    xs = [p.to(dev) for p in pinned]
+    torch.cuda.synchronize()
+    cfg = ab.TreeConfig(maxParticlesPerLeaf=BUCKET, splitCriterion=ab.SplitCriterion.NFCount,
+                        sfcKind=ab.SfcKind.Hilbert)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    with torch.cuda.stream(s):
+        tree = ab.Tree(0, *xs, cfg, stream=s)
+        # ---------------- warm-up builds
+        for _ in range(args.warmup):
+            tree.build()
+        s.synchronize()
+        launches0 = tree.info().kernel_launches
+        # ---------------- timed builds (inputs 192 MiB > L2: no flush needed)
+        barrier()
+        build_ms = []
+        with ClockSampler(local) as clocks:
+            for _ in range(args.steps):
+                a, b = ev(), ev()
+                a.record(s)
+                tree.build()
+                b.record(s)
+                b.synchronize()
+                build_ms.append(a.elapsed_time(b))
+            barrier()
+        launches = tree.info().kernel_launches - launches0
+        info = tree.info()
+        leaves, depth = info.num_leaves, info.max_achieved_depth
+
+        # ---------------- graph-replayed updates
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(99 + rank)
+        upper = float(np.nextafter(np.float32(1.0), np.float32(0.0)))
+
+        def jitter():
+            for t in xs:
+                t.add_(torch.randn(t.shape, generator=gen, device=dev, dtype=t.dtype) * 1e-3).clamp_(0.0, upper)
+
+        def capture():
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                tree.update()
+            return g
+
+        jitter()
+        tree.update()
+        while tree.doBuffersNeedResize():
+            tree.resizeBuffers()
+            tree.update()
+        graph = capture()
+        update_ms, resizes = [], 0
+        for i in range(args.warmup + args.steps):
+            jitter()
+            s.synchronize()
+            a, b = ev(), ev()
+            a.record(s)
+            graph.replay()
+            b.record(s)
+            b.synchronize()
+            if i >= args.warmup:
+                update_ms.append(a.elapsed_time(b))
+            if tree.doBuffersNeedResize():
+                resizes += 1
+                del graph
+                tree.resizeBuffers()
+                tree.update()
+                graph = capture()
+        del graph
+
+        # ---------------- end to end: host coordinates -> build -> counters to host
+        cnt_ptr = tree.counters()
+        host_counters = torch.zeros(3, dtype=torch.int32).pin_memory()
+        e2e_ms = []
+        for i in range(args.warmup + args.steps):
+            a, b = ev(), ev()
+            a.record(s)
+            for d, p in zip(xs, pinned):
+                d.copy_(p, non_blocking=True)
+            tree.build()
+            nl = ab.device_tensor(cnt_ptr[0], 1, "<i4")
+            nn = ab.device_tensor(cnt_ptr[1], 1, "<i4")
+            na = ab.device_tensor(cnt_ptr[2], 1, "<u4").view(torch.int32)
+            host_counters[0:1].copy_(nl, non_blocking=True)
+            host_counters[1:2].copy_(nn, non_blocking=True)
+            host_counters[2:3].copy_(na, non_blocking=True)
+            b.record(s)
+            b.synchronize()
+            if i >= args.warmup:
+                e2e_ms.append(a.elapsed_time(b))
+        assert int(host_counters[0]) == leaves
+
+        # ---------------- roofline: onesweep pass timed live via ao_sort_pairs
+        keys_ptr = tree.buffer_info("particleKeys_d")[0]
+        keys_in = ab.device_tensor(keys_ptr, n, "<u8").clone()
+        keys_out = torch.empty_like(keys_in)
+        vals_out = torch.empty(n, dtype=torch.uint32, device=dev)
+        nbytes = ctypes.c_size_t()
+        C.check(C.load().ao_sort_pairs(None, ctypes.byref(nbytes), None, None, None, None, n, 0, 64, None))
+        scratch = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
+        st = ctypes.c_void_p(s.cuda_stream)
+
+        def sort_ms(end_bit, reps=5):
+            out = []
+            for _ in range(reps + 2):
+                a, b = ev(), ev()
+                a.record(s)
+                C.check(C.load().ao_sort_pairs(ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(nbytes),
+                                               ctypes.c_void_p(keys_in.data_ptr()),
+                                               ctypes.c_void_p(keys_out.data_ptr()), None,
+                                               ctypes.c_void_p(vals_out.data_ptr()), n, 0, end_bit, st))
+                b.record(s)
+                b.synchronize()
+                out.append(a.elapsed_time(b))
+            return statistics.median(out[2:])
+
+        t64, t8 = sort_ms(64), sort_ms(8)
+        pass_ms = (t64 - t8) / 7.0
+        # keygen alone (computeSfcKeys): coordinates in, keys out
+        kg = []
+        for _ in range(7):
+            a, b = ev(), ev()
+            a.record(s)
+            ab.compute_sfc_keys(0, *xs, sfc_kind=ab.SfcKind.Hilbert, stream=s)
+            b.record(s)
+            b.synchronize()
+            kg.append(a.elapsed_time(b))
+        keygen_ms = statistics.median(kg[2:])
+    barrier()
+
+    step_ms = max_over_ranks(statistics.median(build_ms))
+    upd_ms = max_over_ranks(statistics.median(update_ms))
+    e2e = max_over_ranks(statistics.median(e2e_ms))
+    total = n * world
+    hbm, peak_kind = peaks()
+    pass_bytes = 24.0 * n
+    achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": "onesweepKernel (one 8-bit pass of the 64-bit key + 32-bit value sort)",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+            "traffic": ONESWEEP_TRAFFIC_BYTES, "algorithmic_bytes_per_launch": pass_bytes,
+            "launch_ms": pass_ms, "sort_64bit_ms": t64,
+            "keygen": {"ms": keygen_ms, "achieved_gbs": (20.0 * n) / (keygen_ms * 1e-3) / 1e9}}
+    line = {"metric": METRIC, "value": total / (step_ms * 1e-3), "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_per_gpu": n, "coords": "float32", "leaves": leaves,
+                       "max_depth": depth, "l2": "inputs 192 MiB > 126 MB L2; no flush", "views": "off",
+                       "parallelism": f"replicas{world}"},
+            "clocks": clocks.summary(), "gpu_launches": int(launches),
+            "update": {"value": total / (upd_ms * 1e-3), "unit": "particles/s", "ms_per_step": upd_ms,
+                       "graph_replayed": True, "resizes": resizes},
+            "e2e": {"value": total / (e2e * 1e-3), "unit": "particles/s", "ms_per_step": e2e,
+                    "h2d_bytes_per_step": 3 * 4 * n, "d2h_bytes_per_step": 12},
+            "roofline": roof}
+    if rank == 0 and not args.no_cpu_baseline:
+        v, dt = cpu_oracle_build(args.cpu_sample)
+        line["cpu_baseline"] = {"value": v, "unit": "particles/s", "cores": 1, "kind": "port",
+                                "sample": f"one build of {args.cpu_sample} Plummer particles (CPU oracle port)"}
+    if rank == 0 and not args.no_reference_gpu:
+        try:
+            from oracle import refrun
+            if refrun.available():
+                rng = np.random.default_rng(5)
+                frame1 = tuple(np.clip(a + rng.normal(0, 1e-3, a.size).astype(np.float32), 0, upper).astype(
+                    np.float32) for a in hx)
+                r = refrun.time_reference(0, [hx, frame1], reps=3, bucket=BUCKET, nf=True, hilbert=True,
+                                          views=(False, False, False))
+                line["reference_gpu"] = {"build_ms": r["build_ms"], "update_ms": r["update_ms"],
+                                         "build_value": n / (r["build_ms"] * 1e-3),
+                                         "update_value": n / (r["update_ms"] * 1e-3), "unit": "particles/s",
+                                         "what": "reference library compiled for sm_100a, same inputs and GPU"}
+        except Exception as e:  # the reference run is informational
+            line["reference_gpu"] = {"error": str(e)[:200]}
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

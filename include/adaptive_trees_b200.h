@@ -94,6 +94,7 @@ typedef struct ao_tree_info
     unsigned max_achieved_depth; /* maxAchievedDepth()    tree.hpp:70-71 */
     int split_criterion;         /* splitCriterion()      tree.hpp:99-103 */
     int sfc_kind;                /* sfcKind() tree.hpp:104-108; -1 for Binary (the C++ facade throws) */
+    unsigned long long kernel_launches; /* engine kernels launched by this process so far */
 } ao_tree_info;
 
 typedef struct ao_tree ao_tree;
@@ -147,6 +148,18 @@ AO_API ao_status ao_tree_get_info(ao_tree *tree, ao_tree_info *info);
 AO_API ao_status ao_compute_sfc_keys(int kind, int real_type, const void *x, const void *y, const void *z, size_t n,
                               const double *box, int sfc_kind, unsigned max_depth, unsigned long long *keys_d,
                               unsigned *perm_d, void *stream);
+
+/* cub::DeviceRadixSort::SortPairs(d_temp_storage, temp_storage_bytes,
+ * d_keys_in, d_keys_out, d_values_in, d_values_out, num_items, begin_bit,
+ * end_bit, stream) as called at octree.cu:301-304 and kdtree3d.cu:168-170:
+ * stable LSD sort of 64-bit keys carrying 32-bit values by bits
+ * [begin_bit, end_bit), onesweep with decoupled look-back.  With scratch ==
+ * NULL only *scratch_bytes is set.  values_in == NULL sorts the indices
+ * 0..n-1 (the identity permutation).  keys_in/values_in are not modified and
+ * must not alias the outputs.  No allocation; capturable. */
+AO_API ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsigned long long *keys_in,
+                               unsigned long long *keys_out, const unsigned *values_in, unsigned *values_out,
+                               size_t n, int begin_bit, int end_bit, void *stream);
 
 /* Message of the last failed call on this thread ("" if none). */
 AO_API const char *ao_last_error(void);

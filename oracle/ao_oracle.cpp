@@ -1267,8 +1267,11 @@ int aoo_tree_copy_buffer(void *h, int which, void *dst, size_t dst_bytes, size_t
         case 2: src = t->K.data(); count = t->hostLeaves + 1; elem = 8; break;
         case 3: src = t->N.data(); count = t->hostLeaves; elem = 4; break;
         case 4:
+            // NF_d is sized like N_d in both criteria (octree.cu:527-530); its
+            // contents are only defined for NFCount (zeros here otherwise).
             if (t->kind == 1) throw std::logic_error("Tree: Binary NFCount is not implemented yet");
-            src = t->NF.data(); count = t->nf ? t->hostLeaves : 0; elem = 4; break;
+            if (!t->nf && t->NF.size() < t->hostLeaves) t->NF.assign(t->hostLeaves, 0u);
+            src = t->NF.data(); count = t->hostLeaves; elem = 4; break;
         case 5: src = t->view.box.data(); count = v ? nodes : 0; elem = 8; break;
         case 6: src = t->view.split.data(); count = v ? nodes : 0; elem = 1; break;
         case 7: src = t->view.depth.data(); count = v ? nodes : 0; elem = 1; break;

@@ -123,6 +123,7 @@ class OracleTree:
         self.kind = kind
         self._set_arrays(x, y, z)
         self.real = 0 if self._x.dtype == np.float32 else 1
+        self.nf = kind == 0 and config.split_criterion == 1
         h = ctypes.c_void_p()
         _check(lib().aoo_tree_create(kind, self.real, self._ptr(self._x), self._ptr(self._y), self._ptr(self._z),
                                      len(self._x), ctypes.byref(config), ctypes.byref(h)))

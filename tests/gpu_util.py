@@ -61,6 +61,8 @@ def compare(gpu_tree, oracle_tree, names=None, skip=()):
         a = gpu_get(gpu_tree, name)
         assert a.dtype == e.dtype, (name, a.dtype, e.dtype)
         assert a.size == e.size, f"{name}: size {a.size} != oracle {e.size}"
+        if name == "nearFieldCounts" and not getattr(oracle_tree, "nf", True):
+            continue  # defined only for NFCount trees
         bad = np.nonzero(a != e)[0]
         assert bad.size == 0, f"{name}: {bad.size} mismatches, first at {bad[:5]}: gpu {a[bad[:5]]} oracle {e[bad[:5]]}"
         done.append(name)
