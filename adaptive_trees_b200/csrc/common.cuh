@@ -114,9 +114,24 @@ __device__ __forceinline__ size_t upperBoundDev(const u64 *__restrict__ a, size_
     return lo;
 }
 
+// First index in a[0, n) whose key is >= v, 32-bit index arithmetic.
+__device__ __forceinline__ u32 lowerBound32(const u64 *__restrict__ a, u32 n, u64 v)
+{
+    u32 lo = 0;
+    while (n > 0)
+    {
+        const u32 half = n >> 1;
+        const bool less = __ldg(a + lo + half) < v;
+        lo = less ? lo + half + 1 : lo;
+        n = less ? n - half - 1 : half;
+    }
+    return lo;
+}
+
 // Sorted-key search accelerated by a sampled index.  `sample[j]` holds
 // keys[j * kSampleStride]; the search first narrows to one stride window with
 // the sample (small, L2-resident) and then searches that window of the keys.
+// Key counts are below 2^32 (32-bit permutation), so indices are 32-bit.
 constexpr unsigned kSampleShift = 5;
 constexpr unsigned kSampleStride = 1u << kSampleShift;
 
@@ -128,19 +143,54 @@ struct KeyIndex
     size_t ns;       // samples = ceil(n / stride)
 
     // lowerBound(keys, n, v)
-    __device__ __forceinline__ size_t lower(u64 v) const
+    __device__ __forceinline__ u32 lower(u64 v) const
     {
         if (n == 0) return 0;
         // first sample >= v; the answer lies in the window before it
-        const size_t s = lowerBoundDev(sample, ns, v);
+        const u32 s = lowerBound32(sample, u32(ns), v);
         if (s == 0) return 0;
-        const size_t base = (s - 1) << kSampleShift;
-        size_t len = n - base;
+        const u32 base = (s - 1) << kSampleShift;
+        u32 len = u32(n) - base;
         if (len > kSampleStride) len = kSampleStride;
-        return base + lowerBoundDev(keys + base, len, v);
+        return base + lowerBound32(keys + base, len, v);
+    }
+
+    // lowerBound(keys, n, v) for a target expected near index `hint`:
+    // gallop up to 4 probes each way from the hint, then fall back to lower().
+    __device__ __forceinline__ u32 lowerNear(u32 hint, u64 v) const
+    {
+        const u32 m = u32(n);
+        if (hint < m && __ldg(keys + hint) < v)
+        {
+            u32 base = hint, step = 1;  // keys[base] < v
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+            {
+                const u32 probe = base + step;
+                if (probe >= m || __ldg(keys + probe) >= v)
+                {
+                    const u32 end = probe < m ? probe : m;
+                    return base + 1 + lowerBound32(keys + base + 1, end - base - 1, v);
+                }
+                base = probe;
+                step <<= 1;
+            }
+            return lower(v);
+        }
+        u32 top = hint < m ? hint : m, step = 1;  // answer <= top
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+        {
+            if (top < step) return lowerBound32(keys, top, v);
+            const u32 probe = top - step;
+            if (__ldg(keys + probe) < v) return probe + 1 + lowerBound32(keys + probe + 1, top - probe - 1, v);
+            top = probe;
+            step <<= 1;
+        }
+        return lower(v);
     }
     // number of keys in [a, b)
-    __device__ __forceinline__ unsigned count(u64 a, u64 b) const { return unsigned(lower(b) - lower(a)); }
+    __device__ __forceinline__ unsigned count(u64 a, u64 b) const { return lower(b) - lower(a); }
 };
 
 }  // namespace aot

@@ -637,26 +637,20 @@ void TreeEngine::octreePass(bool buildMode, long long limit)
     const KeyIndex idx = m_->keyIndex(n_);
     const int mode = buildMode ? kModeOctreeBuild : kModeUpdate;
     long long *hist = buildMode ? m_->history.as<long long>() : nullptr;
-    const unsigned scatterBlocks = gridFor(cap, rb::kScatterThreads);
+    const unsigned scatterBlocks = std::min(gridFor(cap, rb::kScatterThreads), unsigned(smCount()) * 8u);
     const unsigned refreshBlocks = unsigned(smCount()) * 8u;
     if (cfg_.nf)
     {
         rb::octDecideScanKernel<true><<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket), noteLaunch();
         rb::octScatterKernel<true><<<scatterBlocks, rb::kScatterThreads, 0, s>>>(tb, limit, mode, hist), noteLaunch();
-        if (cfg_.hilbert)
-            rb::octRefreshKernel<true, true, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(
-                tb, idx, cfg_.bucket, m_->kpd.h), noteLaunch();
-        else
-            rb::octRefreshKernel<true, false, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(
-                tb, idx, cfg_.bucket, m_->kpd.h), noteLaunch();
     }
     else
     {
         rb::octDecideScanKernel<false><<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket), noteLaunch();
         rb::octScatterKernel<false><<<scatterBlocks, rb::kScatterThreads, 0, s>>>(tb, limit, mode, hist), noteLaunch();
-        rb::octRefreshKernel<false, false, false><<<refreshBlocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
-                                                                                                m_->kpd.h), noteLaunch();
     }
+    AOT_LAUNCH_CHECK();
+    refreshCounts(false, refreshBlocks);
     AOT_LAUNCH_CHECK();
 }
 
@@ -670,7 +664,7 @@ void TreeEngine::binaryPass(bool buildMode, long long limit)
     AOT_CHECK(cudaMemsetAsync(m_->scan.p, 0, (m_->scanTiles + 1) * sizeof(u64), s));
     const KeyIndex idx = m_->keyIndex(n_);
     rb::binDecideScanKernel<<<unsigned(tiles), rb::kScanThreads, 0, s>>>(tb, cfg_.bucket, cfg_.maxDepth), noteLaunch();
-    rb::binScatterKernel<<<gridFor(cap, rb::kScatterThreads), rb::kScatterThreads, 0, s>>>(
+    rb::binScatterKernel<<<std::min(gridFor(cap, rb::kScatterThreads), unsigned(smCount()) * 8u), rb::kScatterThreads, 0, s>>>(
         tb, limit, buildMode ? kModeBinaryBuild : kModeUpdate), noteLaunch();
     rb::binRefreshKernel<false><<<unsigned(smCount()) * 8u, 256, 0, s>>>(tb, idx), noteLaunch();
     AOT_LAUNCH_CHECK();
@@ -687,15 +681,38 @@ void TreeEngine::refreshAll()
     rb::resetForUpdateKernel<<<1, 1, 0, s>>>(m_->st, m_->P[0].as<u64>(), n_), noteLaunch();
     const unsigned blocks = unsigned(smCount()) * 8u;
     if (cfg_.kind == 1)
+    {
         rb::binRefreshKernel<true><<<blocks, 256, 0, s>>>(tb, idx), noteLaunch();
-    else if (!cfg_.nf)
-        rb::octRefreshKernel<false, false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
-                                                                                        m_->kpd.h), noteLaunch();
-    else if (cfg_.hilbert)
-        rb::octRefreshKernel<true, true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, m_->kpd.h), noteLaunch();
+        AOT_LAUNCH_CHECK();
+    }
     else
-        rb::octRefreshKernel<true, false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket,
-                                                                                       m_->kpd.h), noteLaunch();
+    {
+        refreshCounts(true, blocks);
+    }
+}
+
+// Per-leaf quantities of the active octree: begin indices, then (NFCount)
+// near-field counts and group-merge flags.  all = every leaf, else the work
+// lists of the last materialisation.
+void TreeEngine::refreshCounts(bool all, unsigned blocks)
+{
+    cudaStream_t s = cfg_.stream;
+    const rb::TreeBufs tb = m_->bufs();
+    const KeyIndex idx = m_->keyIndex(n_);
+    if (all) rb::octBeginKernel<true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx), noteLaunch();
+    else rb::octBeginKernel<false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx), noteLaunch();
+    if (cfg_.nf)
+    {
+        const HilbertTables &h = m_->kpd.h;
+        if (all && cfg_.hilbert)
+            rb::octNearFieldKernel<true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h), noteLaunch();
+        else if (all)
+            rb::octNearFieldKernel<false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h), noteLaunch();
+        else if (cfg_.hilbert)
+            rb::octNearFieldKernel<true, false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h), noteLaunch();
+        else
+            rb::octNearFieldKernel<false, false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h), noteLaunch();
+    }
     AOT_LAUNCH_CHECK();
 }
 

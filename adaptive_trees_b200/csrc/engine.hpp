@@ -133,6 +133,7 @@ private:
     void octreePass(bool buildMode, long long limit);
     void binaryPass(bool buildMode, long long limit);
     void refreshAll();
+    void refreshCounts(bool all, unsigned blocks);
     void prepareGraphBuffers(size_t capacity);
     void ensurePhysical(size_t capacity);
     void buildViews(const adaptive_octree::ViewConfig &v);

@@ -36,6 +36,7 @@ constexpr u64 kFlagAgg = u64(1) << 62;
 constexpr u64 kFlagPrefix = u64(2) << 62;
 constexpr u64 kValueMask = (u64(1) << 62) - 1;
 constexpr unsigned kLookbackSpins = 1u << 22;
+constexpr int kLookbackWindow = 8;
 
 __device__ __forceinline__ u64 ldRelaxed(const u64 *p)
 {
@@ -127,19 +128,36 @@ struct SharedPass
     u32 vals[kTile];
     u32 warpHist[kWarps][kRadix];  // per-warp digit counts, then exclusive warp offsets
     u32 localStart[kRadix];
-    long long gstart[kRadix];      // global position of local index 0 of each digit
+    u32 gstart[kRadix];            // global position of local index 0 of each digit (mod 2^32)
     u32 count[kRadix];
     u32 warpSums[kWarps];
     u32 tile;
 };
 
-// One onesweep pass over keys[0, n): digit at bit `shift`.
+// Lanes of the warp whose (valid) digit equals this lane's: eight ballots, one
+// per digit bit, instead of __match_any_sync.
+__device__ __forceinline__ unsigned peerLanes(unsigned digit, int bits, unsigned validMask)
+{
+    unsigned peers = validMask;
+#pragma unroll
+    for (int b = 0; b < kRadixBits; ++b)
+    {
+        if (b < bits)
+        {
+            const bool set = (digit >> b) & 1u;
+            const unsigned m = __ballot_sync(0xffffffffu, set);
+            peers &= set ? m : ~m;
+        }
+    }
+    return peers;
+}
+
+// One onesweep pass over keys[0, n): digit at bit `shift` (`bits` wide).
 // valsIn == nullptr means values are the input indices (first pass).
-__global__ void __launch_bounds__(kThreads) onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn,
-                                                            u64 *__restrict__ keysOut, u32 *__restrict__ valsOut,
-                                                            size_t n, int shift, const u32 *__restrict__ bins,
-                                                            u32 *tileCounter, u64 *status, int *error,
-                                                            int bits = kRadixBits)
+__global__ void __launch_bounds__(kThreads, 3)
+    onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
+                   u32 *__restrict__ valsOut, size_t n, int shift, const u32 *__restrict__ bins, u32 *tileCounter,
+                   u64 *status, int *error, int bits = kRadixBits)
 {
     const unsigned dmask = (1u << bits) - 1;
     extern __shared__ __align__(16) unsigned char smemRaw[];
@@ -154,40 +172,34 @@ __global__ void __launch_bounds__(kThreads) onesweepKernel(const u64 *__restrict
     const size_t warpBase = tileBase + size_t(warp) * (32 * kItems);
 
     u64 key[kItems];
-    u32 val[kItems];
-    int digit[kItems];
-    u32 rank[kItems];
 #pragma unroll
     for (int i = 0; i < kItems; ++i)
     {
         const size_t idx = warpBase + size_t(i) * 32 + lane;
-        if (idx < n)
-        {
-            key[i] = __ldcs(keysIn + idx);
-            val[i] = valsIn ? __ldcs(valsIn + idx) : u32(idx);
-            digit[i] = int((key[i] >> shift) & dmask);
-        }
-        else
-        {
-            key[i] = 0;
-            val[i] = 0;
-            digit[i] = kRadix;  // outside every bucket
-        }
+        key[i] = idx < n ? __ldcs(keysIn + idx) : 0ull;
     }
-    // Rank within the warp, items in memory order (item-major, lane-minor).
+    // Rank within the warp, items in memory order (item-major, lane-minor):
+    // the lowest lane of each digit group adds the group size to the warp's
+    // counter and broadcasts the old value.
     u32 *wh = sm.warpHist[warp];
     const unsigned ltMask = laneMaskLt();
+    u32 rank2[kItems / 2];
 #pragma unroll
     for (int i = 0; i < kItems; ++i)
     {
-        const unsigned peers = __match_any_sync(0xffffffffu, digit[i]);
-        const bool valid = digit[i] < kRadix;
+        const size_t idx = warpBase + size_t(i) * 32 + lane;
+        const bool valid = idx < n;
+        const unsigned validMask = __ballot_sync(0xffffffffu, valid);
+        const unsigned d = unsigned(key[i] >> shift) & dmask;
+        const unsigned peers = peerLanes(d, bits, validMask);
+        const int leader = __ffs(peers) - 1;
         u32 base = 0;
-        if (valid) base = wh[digit[i]];
+        if (valid && lane == leader) base = atomicAdd(&wh[d], u32(__popc(peers)));
+        base = __shfl_sync(0xffffffffu, base, leader < 0 ? 0 : leader);
         __syncwarp();
-        if (valid && (peers & ltMask) == 0) wh[digit[i]] = base + __popc(peers);
-        __syncwarp();
-        rank[i] = base + __popc(peers & ltMask);
+        const u32 r = base + __popc(peers & ltMask);
+        if (i & 1) rank2[i >> 1] |= r << 16;
+        else rank2[i >> 1] = r;
     }
     __syncthreads();
     // Per digit: warp exclusive offsets and tile total (thread = digit).
@@ -203,44 +215,14 @@ __global__ void __launch_bounds__(kThreads) onesweepKernel(const u64 *__restrict
         }
         sm.count[d] = acc;
     }
-    // Publish this tile's digit counts; tile 0 publishes final prefixes.
+    // Publish this tile's digit counts early (tile 0 publishes final prefixes),
+    // then build the tile-local order; the look-back comes last so earlier
+    // tiles have had time to publish inclusive prefixes.
     {
         const int d = tid;
-        const u64 total = sm.count[d];
-        u64 *st = status + tile * kRadix + d;
-        stRelaxed(st, (tile == 0 ? kFlagPrefix : kFlagAgg) | total);
-        u64 excl = 0;
-        if (tile > 0)
-        {
-            long long j = (long long)tile - 1;
-            unsigned spins = 0;
-            while (j >= 0)
-            {
-                const u64 v = ldRelaxed(status + size_t(j) * kRadix + d);
-                const u64 flag = v & ~kValueMask;
-                if (flag == 0)
-                {
-                    if (++spins > kLookbackSpins)
-                    {
-                        atomicExch(error, kErrLookback);
-                        break;
-                    }
-                    if (spins > 64) __nanosleep(64);
-                    continue;
-                }
-                excl += v & kValueMask;
-                if (flag == kFlagPrefix) break;
-                --j;
-            }
-            stRelaxed(st, kFlagPrefix | (excl + total));
-        }
-        sm.gstart[d] = (long long)bins[d] + (long long)excl;
-    }
-    // Exclusive scan of the tile's digit counts -> local starts.
-    {
-        const int d = tid;
+        stRelaxed(status + tile * kRadix + d, (tile == 0 ? kFlagPrefix : kFlagAgg) | u64(sm.count[d]));
+        // exclusive scan of the tile's digit counts -> local starts
         u32 v = sm.count[d];
-        // warp inclusive scan
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1)
         {
@@ -253,30 +235,79 @@ __global__ void __launch_bounds__(kThreads) onesweepKernel(const u64 *__restrict
 #pragma unroll
         for (int w = 0; w < kWarps; ++w)
             if (w < warp) wOff += sm.warpSums[w];
-        const u32 local = wOff + v - sm.count[d];
-        sm.localStart[d] = local;
-        sm.gstart[d] -= (long long)local;
+        sm.localStart[d] = wOff + v - sm.count[d];
     }
     __syncthreads();
     // Reorder the tile in shared memory.
 #pragma unroll
     for (int i = 0; i < kItems; ++i)
     {
-        if (digit[i] < kRadix)
+        const size_t idx = warpBase + size_t(i) * 32 + lane;
+        if (idx < n)
         {
-            const u32 pos = sm.localStart[digit[i]] + sm.warpHist[warp][digit[i]] + rank[i];
+            const unsigned d = unsigned(key[i] >> shift) & dmask;
+            const u32 r = (rank2[i >> 1] >> ((i & 1) * 16)) & 0xffffu;
+            const u32 pos = sm.localStart[d] + sm.warpHist[warp][d] + r;
             sm.keys[pos] = key[i];
-            sm.vals[pos] = val[i];
+            sm.vals[pos] = valsIn ? __ldcs(valsIn + idx) : u32(idx);
         }
+    }
+    // Look-back: global start of each digit for this tile.
+    {
+        const int d = tid;
+        const u64 total = sm.count[d];
+        u64 excl = 0;
+        if (tile > 0)
+        {
+            // Walk back over earlier tiles, eight status words per round trip,
+            // summing aggregates until an inclusive prefix is found.
+            long long j = (long long)tile - 1;
+            unsigned spins = 0;
+            while (j >= 0)
+            {
+                u64 w8[kLookbackWindow];
+#pragma unroll
+                for (int k = 0; k < kLookbackWindow; ++k)
+                    w8[k] = j - k >= 0 ? ldRelaxed(status + size_t(j - k) * kRadix + d) : kFlagPrefix;
+                int k = 0;
+                bool done = false;
+                for (; k < kLookbackWindow; ++k)
+                {
+                    const u64 flag = w8[k] & ~kValueMask;
+                    if (flag == 0) break;
+                    excl += w8[k] & kValueMask;
+                    if (flag == kFlagPrefix)
+                    {
+                        done = true;
+                        break;
+                    }
+                }
+                if (done) break;
+                j -= k;
+                if (k < kLookbackWindow)  // tile j has not published yet
+                {
+                    if (++spins > kLookbackSpins)
+                    {
+                        atomicExch(error, kErrLookback);
+                        break;
+                    }
+                    if (spins > 64) __nanosleep(64);
+                }
+            }
+            stRelaxed(status + tile * kRadix + d, kFlagPrefix | (excl + total));
+        }
+        // modulo 2^32: gstart + j is exact for every key of digit d
+        sm.gstart[d] = bins[d] + u32(excl) - sm.localStart[d];
     }
     __syncthreads();
     const size_t remain = n - tileBase;
     const int valid = remain < size_t(kTile) ? int(remain) : kTile;
+#pragma unroll 4
     for (int j = tid; j < valid; j += kThreads)
     {
         const u64 k = sm.keys[j];
-        const int d = int((k >> shift) & dmask);
-        const size_t out = size_t(sm.gstart[d] + j);
+        const unsigned d = unsigned(k >> shift) & dmask;
+        const u32 out = sm.gstart[d] + u32(j);
         keysOut[out] = k;
         valsOut[out] = sm.vals[j];
     }

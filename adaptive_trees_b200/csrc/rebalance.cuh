@@ -49,6 +49,13 @@ struct TreeBufs
     u64 *scanStatus;
     u32 *scanTile;
     DeviceState *st;
+    // A/B selection without dynamic indexing of the (by-value) arrays, which
+    // would move the whole struct to local memory
+    __device__ __forceinline__ u64 *k(int a) const { return a ? K[1] : K[0]; }
+    __device__ __forceinline__ u32 *b(int a) const { return a ? B[1] : B[0]; }
+    __device__ __forceinline__ u32 *nf(int a) const { return a ? NF[1] : NF[0]; }
+    __device__ __forceinline__ u8 *g(int a) const { return a ? G[1] : G[0]; }
+    __device__ __forceinline__ u32 *n(int a) const { return a ? N[1] : N[0]; }
 };
 
 __device__ __forceinline__ bool halted(const DeviceState *st)
@@ -107,9 +114,25 @@ __device__ __forceinline__ i64 lookback(u64 *status, u32 tile, i64 aggregate, in
     unsigned spins = 0;
     while (j >= 0)
     {
-        const u64 v = ldRelaxed(status + j);
-        const u64 flag = v & ~kValueMask;
-        if (flag == 0)
+        u64 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = j - k >= 0 ? ldRelaxed(status + (j - k)) : kFlagPrefix;
+        int k = 0;
+        bool done = false;
+        for (; k < 8; ++k)
+        {
+            const u64 flag = v[k] & ~kValueMask;
+            if (flag == 0) break;
+            excl += i64(v[k] & kValueMask);
+            if (flag == kFlagPrefix)
+            {
+                done = true;
+                break;
+            }
+        }
+        if (done) break;
+        j -= k;
+        if (k < 8)
         {
             if (++spins > kLookbackSpins)
             {
@@ -117,11 +140,7 @@ __device__ __forceinline__ i64 lookback(u64 *status, u32 tile, i64 aggregate, in
                 break;
             }
             if (spins > 64) __nanosleep(64);
-            continue;
         }
-        excl += i64(v & kValueMask);
-        if (flag == kFlagPrefix) break;
-        --j;
     }
     stRelaxed(status + tile, kFlagPrefix | u64(excl + aggregate));
     return excl;
@@ -334,7 +353,7 @@ template <bool NF>
 __global__ void __launch_bounds__(kScanThreads) octDecideScanKernel(TreeBufs tb, unsigned bucket)
 {
     const int a = tb.st->activeBuffer;
-    const OctreeOp<NF> op{tb.K[a], tb.B[a], tb.NF[a], tb.G[a], bucket};
+    const OctreeOp<NF> op{tb.k(a), tb.b(a), tb.nf(a), tb.g(a), bucket};
     decideScan(op, tb);
 }
 
@@ -347,38 +366,28 @@ __device__ __forceinline__ unsigned splitLevels(int op) { return op == 8 ? 1u : 
 // work lists of the refresh: new leaves needing a search (and NF) and
 // candidate group leaders needing a parent NF.
 template <bool NF>
-__global__ void __launch_bounds__(kScatterThreads)
-    octScatterKernel(TreeBufs tb, long long limit, int mode, long long *history)
+__device__ __forceinline__ void octScatterLeaf(const TreeBufs &tb, DeviceState *st, int i, int L, int a, int b,
+                                               long long total)
 {
-    DeviceState *st = tb.st;
-    if (halted(st)) return;  // uniform: the state does not change before the last CTA
-    const long long total = st->proposal;
-    const bool proceed = !st->needsResize && st->changed && total <= limit;
-    const int L = st->numLeaves;
-    const int a = st->activeBuffer, b = a ^ 1;
-    const int i = int(blockIdx.x * blockDim.x + threadIdx.x);
-    int nDirty = 0, nGroup = 0;
-    int op = 0;
-    unsigned level = 0;
-    u64 start = 0;
-    bool leader = false, reusable = false;
-    if (proceed && i < L)
+    int nDirty = 0, nGroup = 0, op = 0;
+    i64 ni = 0;
+    if (i < L)
     {
-        const u64 *K = tb.K[a];
+        const u64 *K = tb.k(a);
         const i64 *offs = tb.offs;
         op = opAt(offs, i);
-        start = K[i];
-        level = octLevel(K[i + 1] - start);
-        const i64 ni = offs[i];
-        u64 *Kn = tb.K[b];
-        u32 *Bn = tb.B[b];
+        const u64 start = K[i];
+        const unsigned level = octLevel(K[i + 1] - start);
+        ni = offs[i];
+        u64 *Kn = tb.k(b);
+        u32 *Bn = tb.b(b);
         if (op == 1)
         {
             Kn[ni] = start;
-            Bn[ni] = tb.B[a][i];
+            Bn[ni] = tb.b(a)[i];
             if constexpr (NF)
             {
-                leader = i + 1 < L && opAt(offs, i + 1) == 0;
+                const bool leader = i + 1 < L && opAt(offs, i + 1) == 0;
                 if (leader)
                 {
                     nDirty = 1;
@@ -386,16 +395,17 @@ __global__ void __launch_bounds__(kScatterThreads)
                 }
                 else
                 {
-                    tb.NF[b][ni] = tb.NF[a][i];
+                    tb.nf(b)[ni] = tb.nf(a)[i];
                     unsigned sl = 0;
                     const int sib = siblingIndex(K, L, i, sl);
+                    bool reusable = false;
                     if (sib == 0 && i + 8 <= L)
                     {
                         reusable = true;
                         for (int s = 0; s < 8; ++s)
                             if (opAt(offs, i + s) != 1) reusable = false;
                     }
-                    if (reusable) tb.G[b][ni] = tb.G[a][i];
+                    if (reusable) tb.g(b)[ni] = tb.g(a)[i];
                     else nGroup = (level > 0 && octDigit(start, level) == 0) ? 1 : 0;
                 }
             }
@@ -404,7 +414,7 @@ __global__ void __launch_bounds__(kScatterThreads)
         {
             const u64 nr = octRange(level + splitLevels(op));
             for (int c = 0; c < op; ++c) Kn[ni + c] = start + u64(c) * nr;
-            Bn[ni] = tb.B[a][i];  // the first child starts where the parent did
+            Bn[ni] = tb.b(a)[i];  // the first child starts where the parent did
             nDirty = NF ? op : op - 1;
             nGroup = NF ? op / 8 : 0;
         }
@@ -415,55 +425,117 @@ __global__ void __launch_bounds__(kScatterThreads)
         }
     }
     // work lists (warp-aggregated appends; list order is irrelevant)
+    const int d0 = warpAppend(&st->dirtyCount, nDirty);
+    if (nDirty)
+    {
+        if (op > 1)
+        {
+            const int c0 = NF ? 0 : 1;
+            for (int c = c0; c < op; ++c) tb.dirty[d0 + c - c0] = int(ni) + c;
+        }
+        else
+        {
+            tb.dirty[d0] = int(ni);
+        }
+    }
+    if constexpr (NF)
+    {
+        const int g0 = warpAppend(&st->groupCount, nGroup);
+        if (nGroup)
+        {
+            if (op > 1)
+                for (int c = 0; c < nGroup; ++c) tb.groups[g0 + c] = int(ni) + 8 * c;
+            else
+                tb.groups[g0] = int(ni);
+        }
+    }
+}
+
+// processNode (octree_rebalance.cuh:253-365) for every old leaf, plus the
+// work lists of the refresh: new leaves needing a search (and NF) and
+// candidate group leaders needing a parent NF.  Persistent grid: each warp
+// strides over the leaves 32 at a time, so every lane takes part in the
+// warp-aggregated appends.
+template <bool NF>
+__global__ void __launch_bounds__(kScatterThreads)
+    octScatterKernel(TreeBufs tb, long long limit, int mode, long long *history)
+{
+    DeviceState *st = tb.st;
+    if (halted(st)) return;  // uniform: the state does not change before the last CTA
+    const long long total = st->proposal;
+    const bool proceed = !st->needsResize && st->changed && total <= limit;
     if (proceed)
     {
-        const int d0 = warpAppend(&st->dirtyCount, nDirty);
-        if (nDirty)
-        {
-            const int ni = int(tb.offs[i]);
-            if (op > 1)
-            {
-                const int c0 = NF ? 0 : 1;
-                for (int c = c0; c < op; ++c) tb.dirty[d0 + c - c0] = ni + c;
-            }
-            else
-            {
-                tb.dirty[d0] = ni;
-            }
-        }
-        if constexpr (NF)
-        {
-            const int g0 = warpAppend(&st->groupCount, nGroup);
-            if (nGroup)
-            {
-                const int ni = int(tb.offs[i]);
-                if (op > 1)
-                    for (int c = 0; c < nGroup; ++c) tb.groups[g0 + c] = ni + 8 * c;
-                else
-                    tb.groups[g0] = ni;
-            }
-        }
+        const int L = st->numLeaves;
+        const int a = st->activeBuffer, b = a ^ 1;
+        const int lane = threadIdx.x & 31;
+        const int warpsTotal = gridDim.x * (blockDim.x / 32);
+        const int w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+        for (int base = w0 * 32; base < L; base += warpsTotal * 32) octScatterLeaf<NF>(tb, st, base + lane, L, a, b, total);
     }
     commitIfLast(st, limit, mode, false, history);
 }
 
-// Near-field count of the octree cell [start, start + range(level)):
-// own count x sum of the 27 periodic same-level neighbour counts
-// (computeNFCooperative, octree_rebalance.cuh:579-634), one lane per cell.
-// Returns the product on every lane; `own` and `begin` (lower bound of the
-// cell start) are valid on every lane.
-template <bool Hilbert>
-__device__ __forceinline__ u64 warpNearField(const KeyIndex &idx, u64 start, unsigned level, const unsigned char *sEnc,
-                                             const unsigned char *sNext, const unsigned char *sDec, u32 &own,
-                                             u32 &begin)
+// Lower bound of v in the sorted keys when `lo` is already a lower bound of a
+// key <= v (so the answer is >= lo): gallop forward from lo (exponential
+// probes, then a binary search of the bracket).  Near-field cells hold few
+// particles, so the upper end of a cell is usually found in the cache line of
+// its lower end.  Far targets fall back to the sampled index.
+__device__ __forceinline__ u32 lowerFrom(const KeyIndex &idx, u32 lo, u64 v)
 {
-    const int lane = threadIdx.x & 31;
+    const u64 *P = idx.keys;
+    const u32 n = u32(idx.n);
+    if (lo >= n || __ldg(P + lo) >= v) return lo;
+    u32 base = lo, step = 1;  // P[base] < v
+    for (int k = 0; k < 12; ++k)
+    {
+        const u32 probe = base + step;
+        if (probe >= n || __ldg(P + probe) >= v)
+        {
+            const u32 end = probe < n ? probe : n;
+            return base + 1 + lowerBound32(P + base + 1, end - base - 1, v);
+        }
+        base = probe;
+        step <<= 1;
+    }
+    return idx.lower(v);
+}
+
+// Population of the 27 periodic same-level cells around the cell
+// [start, start + range(level)), the centre included (the population sum of
+// computeNFCooperative, octree_rebalance.cuh:579-634), computed by ONE lane.
+// `own` is the centre's count (known from the begin indices) and `hint` its
+// first particle.  Neighbour keys: Morton by bit spreading; Hilbert
+// incrementally -- a neighbour agrees with the centre cell on the leading
+// levels where its coordinates agree, so its key keeps that prefix and only the
+// differing suffix is encoded, starting from the centre's state at the first
+// differing level.  Lower bounds gallop from the previous neighbour's.
+template <bool Hilbert>
+__device__ __forceinline__ u64 laneStencilPopulation(const KeyIndex &idx, u64 start, unsigned level, u32 own,
+                                                     u32 hint, const unsigned char *sEnc,
+                                                     const unsigned char *sNext, const unsigned char *sDec)
+{
     if (level > kOctLevels) level = kOctLevels;  // only a malformed tree gets here
     const u64 range = octRange(level);
-    u32 cx, cy, cz;
+    u32 cx = 0, cy = 0, cz = 0;
+    u64 st0 = 0, st1 = 0, st2 = 0;  // 6-bit state before each level: levels 0-9, 10-19, 20
     if constexpr (Hilbert)
     {
-        hilbertCorner(start, level, sDec, sNext, cx, cy, cz);
+        int st = kHilbertStart;
+        for (unsigned k = 0; k < level; ++k)
+        {
+            const u64 bitsv = u64(st) << (6 * (k < 10 ? k : (k < 20 ? k - 10 : k - 20)));
+            if (k < 10) st0 |= bitsv;
+            else if (k < 20) st1 |= bitsv;
+            else st2 |= bitsv;
+            const unsigned b = kOctLevels - 1 - k;
+            const unsigned d = unsigned(start >> (3u * b)) & 7u;
+            const unsigned o = sDec[st * 8 + int(d)];
+            cx |= ((o >> 2) & 1u) << b;
+            cy |= ((o >> 1) & 1u) << b;
+            cz |= (o & 1u) << b;
+            st = sNext[st * 8 + int(o)];
+        }
     }
     else
     {
@@ -472,42 +544,88 @@ __device__ __forceinline__ u64 warpNearField(const KeyIndex &idx, u64 start, uns
         cz = compact3(start);
     }
     const u32 cube = 1u << (kOctLevels - level);
-    u64 cnt = 0;
-    u32 lo = 0;
-    if (lane < 27)
+    u64 pop = own;
+    u32 h = hint;
+#pragma unroll 1
+    for (int cell = 0; cell < 27; ++cell)
     {
-        u64 key = start;
-        if (lane != 13)
+        if (cell == 13) continue;
+        const int dx = cell % 3 - 1, dy = (cell / 3) % 3 - 1, dz = cell / 9 - 1;
+        const u32 x = (cx + u32(dx) * cube) & 0x1fffffu;
+        const u32 y = (cy + u32(dy) * cube) & 0x1fffffu;
+        const u32 z = (cz + u32(dz) * cube) & 0x1fffffu;
+        u64 key;
+        if constexpr (Hilbert)
         {
-            const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
-            const u32 x = (cx + u32(dx) * cube) & 0x1fffffu;
-            const u32 y = (cy + u32(dy) * cube) & 0x1fffffu;
-            const u32 z = (cz + u32(dz) * cube) & 0x1fffffu;
-            if constexpr (Hilbert) key = hilbertPrefix(x, y, z, level, sEnc, sNext);
-            else key = mortonKey(x, y, z);
+            // first level (from the root) whose bit differs on some axis
+            const u32 diff = (x ^ cx) | (y ^ cy) | (z ^ cz);  // nonzero: the neighbour is another cell
+            const unsigned m = unsigned(__clz(diff)) - (32u - kOctLevels);  // levels 0..m-1 agree
+            const u64 word = m < 10 ? st0 : (m < 20 ? st1 : st2);
+            int st = int((word >> (6 * (m < 10 ? m : (m < 20 ? m - 10 : m - 20)))) & 63u);
+            u64 suffix = 0;
+            for (unsigned k = m; k < level; ++k)
+            {
+                const unsigned b = kOctLevels - 1 - k;
+                const unsigned o = (((x >> b) & 1u) << 2) | (((y >> b) & 1u) << 1) | ((z >> b) & 1u);
+                const int e = st * 8 + int(o);
+                suffix = (suffix << 3) | sEnc[e];
+                st = sNext[e];
+            }
+            const unsigned keep = 3u * m;  // prefix bits from the top of the 63-bit key
+            const u64 prefix = keep ? (start >> (63u - keep)) << (63u - keep) : 0ull;
+            key = prefix | (suffix << (3u * (kOctLevels - level)));
         }
-        lo = u32(idx.lower(key));
-        const u32 hi = u32(idx.lower(key + range));
-        cnt = hi - lo;
+        else
+        {
+            key = mortonKey(x, y, z);
+        }
+        const u32 lo = idx.lowerNear(h, key);
+        pop += lowerFrom(idx, lo, key + range) - lo;
+        h = lo;
     }
-    u64 sum = cnt;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-    const u64 centre = __shfl_sync(0xffffffffu, cnt, 13);
-    begin = __shfl_sync(0xffffffffu, lo, 13);
-    own = u32(centre);
-    return centre * sum;
+    return pop;
 }
 
-// Refresh of new leaves (All = every leaf, at the start of update()).
-template <bool NF, bool Hilbert, bool All>
-__global__ void __launch_bounds__(kRefreshThreads)
-    octRefreshKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h)
+// Begin index B[i] = lowerBound(P, K[i]) of new leaves (All: of every leaf and
+// the end sentinel).  This is the whole count refresh of LeafCount trees: the
+// counts are differences of B.
+template <bool All>
+__global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBufs tb, KeyIndex idx)
 {
-    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
     DeviceState *st = tb.st;
     if (halted(st)) return;
-    if constexpr (NF && Hilbert)
+    const int a = st->activeBuffer;
+    const int L = st->numLeaves;
+    const u64 *K = tb.k(a);
+    u32 *B = tb.b(a);
+    if (All && blockIdx.x == 0 && threadIdx.x == 0) B[L] = st->numActiveParticles;
+    const int count = All ? L : st->dirtyCount;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
+    {
+        const int i = All ? j : tb.dirty[j];
+        B[i] = u32(idx.lower(K[i]));
+    }
+}
+
+// Near-field counts of new leaves and group-merge flags of new candidate
+// group leaders (All: of every leaf / group), after octBeginKernel.
+// NF(leaf) = own x (population of the 27-cell stencil): an empty leaf has NF
+// 0 without any search, and the own count is B[i+1] - B[i].  A group's parent
+// count is B[first+8] - B[first]; an empty parent can always merge.  Each CTA
+// queues the non-empty entries of a chunk in shared memory and gives one to
+// each thread, so lanes are not left idle by empty leaves.
+template <bool Hilbert, bool All>
+__global__ void __launch_bounds__(kRefreshThreads)
+    octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h)
+{
+    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
+    __shared__ int sIdx[kRefreshThreads];
+    __shared__ u32 sCnt[kRefreshThreads];
+    __shared__ unsigned char sLev[kRefreshThreads];
+    __shared__ int sQueued;
+    DeviceState *st = tb.st;
+    if (halted(st)) return;
+    if constexpr (Hilbert)
     {
         for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
         {
@@ -515,53 +633,94 @@ __global__ void __launch_bounds__(kRefreshThreads)
             sNext[k] = h.encNext[k];
             sDec[k] = h.decOct[k];
         }
-        __syncthreads();
     }
+    if (threadIdx.x == 0) sQueued = 0;
+    __syncthreads();
     const int a = st->activeBuffer;
     const int L = st->numLeaves;
-    const u64 *K = tb.K[a];
-    u32 *B = tb.B[a];
-    if (All && blockIdx.x == 0 && threadIdx.x == 0) B[L] = st->numActiveParticles;
-    if constexpr (!NF)
+    const u64 *K = tb.k(a);
+    const u32 *B = tb.b(a);
+    u32 *NF = tb.nf(a);
+    u8 *G = tb.g(a);
+
+    // leaves
+    const int count = All ? L : st->dirtyCount;
+    for (int base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x)
     {
-        const int count = All ? L : st->dirtyCount;
-        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
+        const int j = base + threadIdx.x;
+        if (j < count)
         {
             const int i = All ? j : tb.dirty[j];
-            B[i] = u32(idx.lower(K[i]));
-        }
-    }
-    else
-    {
-        const int warpsTotal = gridDim.x * (blockDim.x / 32);
-        const int w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-        const int lane = threadIdx.x & 31;
-        const int count = All ? L : st->dirtyCount;
-        for (int j = w0; j < count; j += warpsTotal)
-        {
-            const int i = All ? j : tb.dirty[j];
-            const u64 s = K[i];
-            const unsigned level = octLevel(K[i + 1] - s);
-            u32 own, begin;
-            const u64 v = warpNearField<Hilbert>(idx, s, level, sEnc, sNext, sDec, own, begin);
-            if (lane == 0)
+            const u32 c = B[i + 1] - B[i];
+            if (c == 0)
             {
-                tb.NF[a][i] = v > 0xffffffffull ? 0xffffffffu : u32(v);
-                B[i] = begin;
+                NF[i] = 0;
+            }
+            else
+            {
+                const int q = atomicAdd(&sQueued, 1);
+                sIdx[q] = i;
+                sCnt[q] = c;
             }
         }
-        const int gcount = All ? L : st->groupCount;
-        for (int j = w0; j < gcount; j += warpsTotal)
+        __syncthreads();
+        const int nq = sQueued;
+        if (int(threadIdx.x) < nq)
+        {
+            const int i = sIdx[threadIdx.x];
+            const u32 c = sCnt[threadIdx.x];
+            const u64 s = K[i];
+            const unsigned level = octLevel(K[i + 1] - s);
+            const u64 v = u64(c) * laneStencilPopulation<Hilbert>(idx, s, level, c, B[i], sEnc, sNext, sDec);
+            NF[i] = v > 0xffffffffull ? 0xffffffffu : u32(v);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) sQueued = 0;
+        __syncthreads();
+    }
+
+    // candidate group leaders: first leaf of a complete group of 8
+    // (IsDirtyGroupLeader, octree_rebalance.cuh:83-105)
+    const int gcount = All ? L : st->groupCount;
+    for (int base = blockIdx.x * blockDim.x; base < gcount; base += gridDim.x * blockDim.x)
+    {
+        const int j = base + threadIdx.x;
+        if (j < gcount)
         {
             const int i = All ? j : tb.groups[j];
             const u64 s = K[i];
             const unsigned level = octLevel(K[i + 1] - s);
-            if (level == 0 || octDigit(s, level) != 0) continue;           // not a first sibling
-            if (i + 8 > L || K[i + 8] != s + octRange(level - 1)) continue;  // incomplete group
-            u32 own, begin;
-            const u64 parentNF = warpNearField<Hilbert>(idx, s, level - 1, sEnc, sNext, sDec, own, begin);
-            if (lane == 0) tb.G[a][i] = parentNF <= u64(bucket) ? 1 : 0;
+            const bool leader = level > 0 && level <= kOctLevels && octDigit(s, level) == 0 && i + 8 <= L &&
+                                K[i + 8] == s + octRange(level - 1);
+            if (leader)
+            {
+                const u32 pc = B[i + 8] - B[i];
+                if (pc == 0)
+                {
+                    G[i] = 1;
+                }
+                else
+                {
+                    const int q = atomicAdd(&sQueued, 1);
+                    sIdx[q] = i;
+                    sCnt[q] = pc;
+                    sLev[q] = (unsigned char)(level - 1);
+                }
+            }
         }
+        __syncthreads();
+        const int nq = sQueued;
+        if (int(threadIdx.x) < nq)
+        {
+            const int i = sIdx[threadIdx.x];
+            const u32 pc = sCnt[threadIdx.x];
+            const unsigned plevel = sLev[threadIdx.x];
+            const u64 v = u64(pc) * laneStencilPopulation<Hilbert>(idx, K[i], plevel, pc, B[i], sEnc, sNext, sDec);
+            G[i] = v <= u64(bucket) ? 1 : 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) sQueued = 0;
+        __syncthreads();
     }
 }
 
@@ -570,8 +729,8 @@ __global__ void materializeCountsKernel(TreeBufs tb)
 {
     const DeviceState *st = tb.st;
     const int a = st->activeBuffer, L = st->numLeaves;
-    const u32 *B = tb.B[a];
-    u32 *N = tb.N[a];
+    const u32 *B = tb.b(a);
+    u32 *N = tb.n(a);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) N[i] = B[i + 1] - B[i];
 }
 
@@ -601,7 +760,7 @@ struct BinaryOp
 __global__ void __launch_bounds__(kScanThreads) binDecideScanKernel(TreeBufs tb, unsigned bucket, unsigned maxDepth)
 {
     const int a = tb.st->activeBuffer;
-    const BinaryOp op{tb.K[a], tb.B[a], bucket, maxDepth};
+    const BinaryOp op{tb.k(a), tb.b(a), bucket, maxDepth};
     decideScan(op, tb);
 }
 
@@ -612,36 +771,42 @@ __global__ void __launch_bounds__(kScatterThreads)
     if (halted(st)) return;
     const long long total = st->proposal;
     const bool proceed = !st->needsResize && st->changed && total <= limit;
-    const int L = st->numLeaves;
-    const int a = st->activeBuffer, b = a ^ 1;
-    const int i = int(blockIdx.x * blockDim.x + threadIdx.x);
-    int nDirty = 0;
-    i64 ni = 0;
-    if (proceed && i < L)
-    {
-        const int op = opAt(tb.offs, i);
-        if (op)
-        {
-            ni = tb.offs[i];
-            const u64 s = tb.K[a][i];
-            tb.K[b][ni] = s;
-            tb.B[b][ni] = tb.B[a][i];
-            if (op == 2)
-            {
-                tb.K[b][ni + 1] = s + (tb.K[a][i + 1] - s) / 2;
-                nDirty = 1;
-            }
-        }
-        if (i == 0)
-        {
-            tb.K[b][total] = kMaxKey;
-            tb.B[b][total] = st->numActiveParticles;
-        }
-    }
     if (proceed)
     {
-        const int d0 = warpAppend(&st->dirtyCount, nDirty);
-        if (nDirty) tb.dirty[d0] = int(ni) + 1;
+        const int L = st->numLeaves;
+        const int a = st->activeBuffer, b = a ^ 1;
+        const int lane = threadIdx.x & 31;
+        const int warpsTotal = gridDim.x * (blockDim.x / 32);
+        const int w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+        for (int base = w0 * 32; base < L; base += warpsTotal * 32)
+        {
+            const int i = base + lane;
+            int nDirty = 0;
+            i64 ni = 0;
+            if (i < L)
+            {
+                const int op = opAt(tb.offs, i);
+                if (op)
+                {
+                    ni = tb.offs[i];
+                    const u64 s = tb.k(a)[i];
+                    tb.k(b)[ni] = s;
+                    tb.b(b)[ni] = tb.b(a)[i];
+                    if (op == 2)
+                    {
+                        tb.k(b)[ni + 1] = s + (tb.k(a)[i + 1] - s) / 2;
+                        nDirty = 1;
+                    }
+                }
+                if (i == 0)
+                {
+                    tb.k(b)[total] = kMaxKey;
+                    tb.b(b)[total] = st->numActiveParticles;
+                }
+            }
+            const int d0 = warpAppend(&st->dirtyCount, nDirty);
+            if (nDirty) tb.dirty[d0] = int(ni) + 1;
+        }
     }
     commitIfLast(st, limit, mode, true, nullptr);
 }
@@ -655,8 +820,8 @@ __global__ void binRefreshKernel(TreeBufs tb, KeyIndex idx)
     DeviceState *st = tb.st;
     if (halted(st)) return;
     const int a = st->activeBuffer, L = st->numLeaves;
-    const u64 *K = tb.K[a];
-    u32 *B = tb.B[a];
+    const u64 *K = tb.k(a);
+    u32 *B = tb.b(a);
     if (All && blockIdx.x == 0 && threadIdx.x == 0) B[L] = st->numActiveParticles;
     const int count = All ? L : st->dirtyCount;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)

@@ -158,6 +158,88 @@ def reference_arm(args):
     return 0
 
 
+def graph_ms(fn, stream, reps, warm=2):
+    """Median device time of `fn` replayed from a CUDA graph (no host launch cost inside)."""
+    import torch
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream):
+        fn()
+    out = []
+    for i in range(reps + warm):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        g.replay()
+        b.record(stream)
+        b.synchronize()
+        if i >= warm:
+            out.append(a.elapsed_time(b))
+    del g
+    return statistics.median(out)
+
+
+class SortRig:
+    """ao_sort_pairs on device keys with caller-owned scratch."""
+
+    def __init__(self, keys, stream):
+        import torch
+        from adaptive_trees_b200 import _capi as C
+        self.C, self.lib = C, C.load()
+        self.n = keys.numel()
+        self.keys = keys
+        self.out = torch.empty_like(keys)
+        self.vals = torch.empty(self.n, dtype=torch.uint32, device=keys.device)
+        self.nbytes = ctypes.c_size_t()
+        C.check(self.lib.ao_sort_pairs(None, ctypes.byref(self.nbytes), None, None, None, None, self.n, 0, 64, None))
+        self.scratch = torch.empty(self.nbytes.value, dtype=torch.uint8, device=keys.device)
+        self.stream = stream
+
+    def __call__(self, end_bit=64):
+        self.C.check(self.lib.ao_sort_pairs(ctypes.c_void_p(self.scratch.data_ptr()), ctypes.byref(self.nbytes),
+                                            ctypes.c_void_p(self.keys.data_ptr()),
+                                            ctypes.c_void_p(self.out.data_ptr()), None,
+                                            ctypes.c_void_p(self.vals.data_ptr()), self.n, 0, end_bit,
+                                            ctypes.c_void_p(self.stream.cuda_stream)))
+
+
+def kernels_only(args):
+    """Key generation and the 64-bit pair sort of the workload's keys, `reps` times each."""
+    import torch
+    import adaptive_trees_b200 as ab
+    torch.cuda.set_device(0)
+    s = torch.cuda.Stream()
+    xs = [torch.from_numpy(a).cuda() for a in plummer(args.n, seed=1234)]
+    with torch.cuda.stream(s):
+        keys = ab.compute_sfc_keys(0, *xs, sfc_kind=ab.SfcKind.Hilbert, stream=s)
+        rig = SortRig(keys, s)
+        for _ in range(args.reps):
+            ab.compute_sfc_keys(0, *xs, sfc_kind=ab.SfcKind.Hilbert, stream=s)
+            rig(64)
+    s.synchronize()
+    print(json.dumps({"mode": "kernels", "n": args.n, "reps": args.reps}))
+    return 0
+
+
+def build_only(args):
+    """One build and one update of the workload's tree at size --n."""
+    import torch
+    import adaptive_trees_b200 as ab
+    torch.cuda.set_device(0)
+    s = torch.cuda.Stream()
+    xs = [torch.from_numpy(a).cuda() for a in plummer(args.n, seed=1234)]
+    cfg = ab.TreeConfig(maxParticlesPerLeaf=BUCKET, splitCriterion=ab.SplitCriterion.NFCount,
+                        sfcKind=ab.SfcKind.Hilbert)
+    with torch.cuda.stream(s):
+        t = ab.Tree(0, *xs, cfg, stream=s)
+        t.build()
+        for x in xs:
+            x.add_(1e-3 * torch.randn_like(x)).clamp_(0.0, 0.99999994)
+        t.update()
+        t.doBuffersNeedResize()
+    s.synchronize()
+    print(json.dumps({"mode": "build", "n": args.n, "leaves": t.info().num_leaves}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -168,9 +250,17 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1 << 20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--mode", default="bench", choices=["bench", "kernels", "build"],
+                    help="kernels: only key generation + the 64-bit pair sort of the workload's keys; "
+                         "build: one build + one update of the workload's tree (small commands for ncu)")
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.mode == "kernels":
+        return kernels_only(args)
+    if args.mode == "build":
+        return build_only(args)
 
     import torch
     import torch.distributed as dist
@@ -295,42 +385,15 @@ def main():
                 e2e_ms.append(a.elapsed_time(b))
         assert int(host_counters[0]) == leaves
 
-        # ---------------- roofline: onesweep pass timed live via ao_sort_pairs
+        # ---------------- roofline: onesweep pass timed live via ao_sort_pairs,
+        # replayed from CUDA graphs so no host launch time is inside the events
         keys_ptr = tree.buffer_info("particleKeys_d")[0]
         keys_in = ab.device_tensor(keys_ptr, n, "<u8").clone()
-        keys_out = torch.empty_like(keys_in)
-        vals_out = torch.empty(n, dtype=torch.uint32, device=dev)
-        nbytes = ctypes.c_size_t()
-        C.check(C.load().ao_sort_pairs(None, ctypes.byref(nbytes), None, None, None, None, n, 0, 64, None))
-        scratch = torch.empty(nbytes.value, dtype=torch.uint8, device=dev)
-        st = ctypes.c_void_p(s.cuda_stream)
-
-        def sort_ms(end_bit, reps=5):
-            out = []
-            for _ in range(reps + 2):
-                a, b = ev(), ev()
-                a.record(s)
-                C.check(C.load().ao_sort_pairs(ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(nbytes),
-                                               ctypes.c_void_p(keys_in.data_ptr()),
-                                               ctypes.c_void_p(keys_out.data_ptr()), None,
-                                               ctypes.c_void_p(vals_out.data_ptr()), n, 0, end_bit, st))
-                b.record(s)
-                b.synchronize()
-                out.append(a.elapsed_time(b))
-            return statistics.median(out[2:])
-
-        t64, t8 = sort_ms(64), sort_ms(8)
+        rig = SortRig(keys_in, s)
+        t64 = graph_ms(lambda: rig(64), s, 7)
+        t8 = graph_ms(lambda: rig(8), s, 7)
         pass_ms = (t64 - t8) / 7.0
-        # keygen alone (computeSfcKeys): coordinates in, keys out
-        kg = []
-        for _ in range(7):
-            a, b = ev(), ev()
-            a.record(s)
-            ab.compute_sfc_keys(0, *xs, sfc_kind=ab.SfcKind.Hilbert, stream=s)
-            b.record(s)
-            b.synchronize()
-            kg.append(a.elapsed_time(b))
-        keygen_ms = statistics.median(kg[2:])
+        keygen_ms = graph_ms(lambda: ab.compute_sfc_keys(0, *xs, sfc_kind=ab.SfcKind.Hilbert, stream=s), s, 7)
     barrier()
 
     step_ms = max_over_ranks(statistics.median(build_ms))
