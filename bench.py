@@ -321,7 +321,7 @@ def main():
             barrier()
         launches = tree.info().kernel_launches - launches0
         info = tree.info()
-        leaves, depth = info.num_leaves, info.max_achieved_depth
+        leaves = info.num_leaves
 
         # ---------------- graph-replayed updates
         gen = torch.Generator(device=dev)
@@ -412,7 +412,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n_per_gpu": n, "coords": "float32", "leaves": leaves,
-                       "max_depth": depth, "l2": "inputs 192 MiB > 126 MB L2; no flush", "views": "off",
+                       "l2": "inputs 192 MiB > 126 MB L2; no flush", "views": "off",
                        "parallelism": f"replicas{world}"},
             "clocks": clocks.summary(), "gpu_launches": int(launches),
             "update": {"value": total / (upd_ms * 1e-3), "unit": "particles/s", "ms_per_step": upd_ms,
