@@ -50,7 +50,11 @@ PROTOTYPES = {
     "ao_tree_get_info": [vp, ctypes.POINTER(AoTreeInfo)],
     "ao_compute_sfc_keys": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_double), ci, cu, vp, vp, vp],
     "ao_sort_pairs": [vp, ctypes.POINTER(sz), vp, vp, vp, vp, sz, ci, ci, vp],
+    "ao_sort_pairs_noalloc": [vp, vp, vp, vp, sz, ci, ci, vp],
 }
+
+# n limit of ao_sort_pairs_noalloc (AO_SORT_PAIRS_NOALLOC_MAX_ITEMS)
+SORT_PAIRS_NOALLOC_MAX_ITEMS = 1 << 20
 
 _lock = threading.Lock()
 _lib = None

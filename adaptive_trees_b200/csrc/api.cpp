@@ -432,4 +432,14 @@ ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsigned lon
     });
 }
 
+ao_status ao_sort_pairs_noalloc(const unsigned long long *keys_in, unsigned long long *keys_out,
+                                const unsigned *values_in, unsigned *values_out, size_t n, int begin_bit,
+                                int end_bit, void *stream)
+{
+    return guarded([&] {
+        aot::sortPairsNoAlloc(keys_in, keys_out, values_in, values_out, n, begin_bit, end_bit,
+                              static_cast<cudaStream_t>(stream));
+    });
+}
+
 }  // extern "C"

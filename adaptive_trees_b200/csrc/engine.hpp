@@ -143,4 +143,11 @@ private:
     void materializeCounts();
 };
 
+// TreeEngine::sortPairs with its scratch in a fixed device array of
+// sort_noalloc.cu (no allocation; at most sortPairsNoAllocMaxItems() items;
+// concurrent calls on one device race).
+void sortPairsNoAlloc(const unsigned long long *keysIn, unsigned long long *keysOut, const unsigned *valsIn,
+                      unsigned *valsOut, size_t n, int beginBit, int endBit, cudaStream_t s);
+size_t sortPairsNoAllocMaxItems();
+
 }  // namespace aot

@@ -1,0 +1,90 @@
+// Allocation-free pair sort: ao_sort_pairs with its scratch in a fixed device
+// array of this file instead of caller-provided memory.
+//
+// Who needs it: callers that cannot allocate device memory where they sort --
+// a serving process that reserves its whole device budget at start-up and
+// must not grow it afterwards, or a plain C / FFI host that has no device
+// allocator of its own to hand a scratch buffer to ao_sort_pairs.
+//
+// Limits and rules:
+//  * at most kNoAllocMaxItems (1,048,576) items per call; larger n is rejected
+//    with std::invalid_argument before any CUDA call;
+//  * the array is one per device: calls that overlap in time on the same
+//    device (from other streams or threads) share it and race, corrupting
+//    each other's results.  Serialise them (one stream, or host-side order);
+//  * the first call on a device does the set-up (it looks up the array's
+//    address on that device, which also loads this file's module there);
+//    make that call before any stream capture;
+//  * what must start at zero -- the sort's digit counters, pass counters,
+//    error word and decoupled look-back status words -- is cleared by the sort
+//    itself on the caller's stream (cudaMemsetAsync) before its kernels run,
+//    so whatever an earlier call left in the array is harmless.  The
+//    key/value ping-pong halves need no clearing.
+// Nothing here calls cudaMalloc/cudaFree or a routine that allocates.
+#include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+#include "engine.hpp"
+
+namespace aot
+{
+namespace
+{
+// Scratch layout of the pair sort for kNoAllocMaxItems items: alternate keys
+// (8 B/item), alternate values (4 B/item), counters (2 x 8 passes x 256
+// digits + 8 + 2 words), look-back status (8 passes x tiles of 4096 items x
+// 256 digits x 8 B), each part rounded up to 256 bytes.  The call checks the
+// sort's own size query against this before using the array.
+constexpr size_t kNoAllocMaxItems = size_t(1) << 20;
+constexpr size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t kNoAllocTiles = (kNoAllocMaxItems + 4095) / 4096;
+constexpr size_t kNoAllocScratchBytes =
+    up256(up256(up256(up256(kNoAllocMaxItems * 8) + kNoAllocMaxItems * 4) + (2 * 8 * 256 + 8 + 2) * 4) +
+          size_t(8) * kNoAllocTiles * 256 * 8);  // 16,793,600 bytes
+
+static __device__ __align__(256) unsigned char g_noAllocScratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setupMutex;
+void *g_scratchAddress[kMaxDevices] = {};
+
+// Address of g_noAllocScratch on the current device, looked up once per
+// device with that device current.
+void *noAllocScratch()
+{
+    int dev = 0;
+    AOT_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices)
+        throw std::runtime_error("ao_sort_pairs_noalloc: device ordinal " + std::to_string(dev) +
+                                 " is beyond the supported " + std::to_string(kMaxDevices));
+    std::lock_guard<std::mutex> lock(g_setupMutex);
+    if (!g_scratchAddress[dev])
+    {
+        void *p = nullptr;
+        AOT_CHECK(cudaGetSymbolAddress(&p, g_noAllocScratch));
+        g_scratchAddress[dev] = p;
+    }
+    return g_scratchAddress[dev];
+}
+}  // namespace
+
+size_t sortPairsNoAllocMaxItems() { return kNoAllocMaxItems; }
+
+void sortPairsNoAlloc(const unsigned long long *keysIn, unsigned long long *keysOut, const unsigned *valsIn,
+                      unsigned *valsOut, size_t n, int beginBit, int endBit, cudaStream_t s)
+{
+    if (n > kNoAllocMaxItems)
+        throw std::invalid_argument("ao_sort_pairs_noalloc: n = " + std::to_string(n) +
+                                    " exceeds the fixed scratch limit of " + std::to_string(kNoAllocMaxItems) +
+                                    " items; use ao_sort_pairs with caller scratch");
+    size_t need = 0;
+    TreeEngine::sortPairs(nullptr, &need, keysIn, keysOut, valsIn, valsOut, n, beginBit, endBit, s);
+    if (need > kNoAllocScratchBytes)
+        throw std::logic_error("ao_sort_pairs_noalloc: the sort needs " + std::to_string(need) +
+                               " scratch bytes, more than the fixed " + std::to_string(kNoAllocScratchBytes));
+    size_t have = kNoAllocScratchBytes;
+    TreeEngine::sortPairs(noAllocScratch(), &have, keysIn, keysOut, valsIn, valsOut, n, beginBit, endBit, s);
+}
+}  // namespace aot

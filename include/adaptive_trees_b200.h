@@ -161,6 +161,24 @@ AO_API ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsig
                                unsigned long long *keys_out, const unsigned *values_in, unsigned *values_out,
                                size_t n, int begin_bit, int end_bit, void *stream);
 
+/* Allocation-free variant of ao_sort_pairs; it has no counterpart in the
+ * reference.  The same sort, with its scratch in a fixed device array inside
+ * this library instead of caller memory, for callers that cannot allocate
+ * device memory where they sort: a process that reserves its whole device
+ * budget at start-up and must not grow it, or a plain C / FFI host without a
+ * device allocator of its own.
+ *  - n <= AO_SORT_PAIRS_NOALLOC_MAX_ITEMS, else AO_ERR_INVALID_ARGUMENT.
+ *  - The first call on a device does the set-up (it looks up the array's
+ *    address on that device); make it before any stream capture.
+ *  - One array per device: calls that overlap in time on the same device
+ *    (other streams, other threads) race and corrupt each other's results.
+ *    Serialise them.
+ *  - Arguments otherwise as ao_sort_pairs. */
+#define AO_SORT_PAIRS_NOALLOC_MAX_ITEMS 1048576
+AO_API ao_status ao_sort_pairs_noalloc(const unsigned long long *keys_in, unsigned long long *keys_out,
+                                       const unsigned *values_in, unsigned *values_out, size_t n, int begin_bit,
+                                       int end_bit, void *stream);
+
 /* Message of the last failed call on this thread ("" if none). */
 AO_API const char *ao_last_error(void);
 
