@@ -501,91 +501,6 @@ __device__ __forceinline__ u32 lowerFrom(const KeyIndex &idx, u32 lo, u64 v)
     return idx.lower(v);
 }
 
-// Population of the 27 periodic same-level cells around the cell
-// [start, start + range(level)), the centre included (the population sum of
-// computeNFCooperative, octree_rebalance.cuh:579-634), computed by ONE lane.
-// `own` is the centre's count (known from the begin indices) and `hint` its
-// first particle.  Neighbour keys: Morton by bit spreading; Hilbert
-// incrementally -- a neighbour agrees with the centre cell on the leading
-// levels where its coordinates agree, so its key keeps that prefix and only the
-// differing suffix is encoded, starting from the centre's state at the first
-// differing level.  Lower bounds gallop from the previous neighbour's.
-template <bool Hilbert>
-__device__ __forceinline__ u64 laneStencilPopulation(const KeyIndex &idx, u64 start, unsigned level, u32 own,
-                                                     u32 hint, const unsigned char *sEnc,
-                                                     const unsigned char *sNext, const unsigned char *sDec)
-{
-    if (level > kOctLevels) level = kOctLevels;  // only a malformed tree gets here
-    const u64 range = octRange(level);
-    u32 cx = 0, cy = 0, cz = 0;
-    u64 st0 = 0, st1 = 0, st2 = 0;  // 6-bit state before each level: levels 0-9, 10-19, 20
-    if constexpr (Hilbert)
-    {
-        int st = kHilbertStart;
-        for (unsigned k = 0; k < level; ++k)
-        {
-            const u64 bitsv = u64(st) << (6 * (k < 10 ? k : (k < 20 ? k - 10 : k - 20)));
-            if (k < 10) st0 |= bitsv;
-            else if (k < 20) st1 |= bitsv;
-            else st2 |= bitsv;
-            const unsigned b = kOctLevels - 1 - k;
-            const unsigned d = unsigned(start >> (3u * b)) & 7u;
-            const unsigned o = sDec[st * 8 + int(d)];
-            cx |= ((o >> 2) & 1u) << b;
-            cy |= ((o >> 1) & 1u) << b;
-            cz |= (o & 1u) << b;
-            st = sNext[st * 8 + int(o)];
-        }
-    }
-    else
-    {
-        cx = compact3(start >> 2);
-        cy = compact3(start >> 1);
-        cz = compact3(start);
-    }
-    const u32 cube = 1u << (kOctLevels - level);
-    u64 pop = own;
-    u32 h = hint;
-#pragma unroll 1
-    for (int cell = 0; cell < 27; ++cell)
-    {
-        if (cell == 13) continue;
-        const int dx = cell % 3 - 1, dy = (cell / 3) % 3 - 1, dz = cell / 9 - 1;
-        const u32 x = (cx + u32(dx) * cube) & 0x1fffffu;
-        const u32 y = (cy + u32(dy) * cube) & 0x1fffffu;
-        const u32 z = (cz + u32(dz) * cube) & 0x1fffffu;
-        u64 key;
-        if constexpr (Hilbert)
-        {
-            // first level (from the root) whose bit differs on some axis
-            const u32 diff = (x ^ cx) | (y ^ cy) | (z ^ cz);  // nonzero: the neighbour is another cell
-            const unsigned m = unsigned(__clz(diff)) - (32u - kOctLevels);  // levels 0..m-1 agree
-            const u64 word = m < 10 ? st0 : (m < 20 ? st1 : st2);
-            int st = int((word >> (6 * (m < 10 ? m : (m < 20 ? m - 10 : m - 20)))) & 63u);
-            u64 suffix = 0;
-            for (unsigned k = m; k < level; ++k)
-            {
-                const unsigned b = kOctLevels - 1 - k;
-                const unsigned o = (((x >> b) & 1u) << 2) | (((y >> b) & 1u) << 1) | ((z >> b) & 1u);
-                const int e = st * 8 + int(o);
-                suffix = (suffix << 3) | sEnc[e];
-                st = sNext[e];
-            }
-            const unsigned keep = 3u * m;  // prefix bits from the top of the 63-bit key
-            const u64 prefix = keep ? (start >> (63u - keep)) << (63u - keep) : 0ull;
-            key = prefix | (suffix << (3u * (kOctLevels - level)));
-        }
-        else
-        {
-            key = mortonKey(x, y, z);
-        }
-        const u32 lo = idx.lowerNear(h, key);
-        pop += lowerFrom(idx, lo, key + range) - lo;
-        h = lo;
-    }
-    return pop;
-}
-
 // Begin index B[i] = lowerBound(P, K[i]) of new leaves (All: of every leaf and
 // the end sentinel).  This is the whole count refresh of LeafCount trees: the
 // counts are differences of B.
@@ -607,22 +522,206 @@ __global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBufs tb, K
     }
 }
 
-// Near-field counts of new leaves and group-merge flags of new candidate
-// group leaders (All: of every leaf / group), after octBeginKernel.
-// NF(leaf) = own x (population of the 27-cell stencil): an empty leaf has NF
-// 0 without any search, and the own count is B[i+1] - B[i].  A group's parent
-// count is B[first+8] - B[first]; an empty parent can always merge.  Each CTA
-// queues the non-empty entries of a chunk in shared memory and gives one to
-// each thread, so lanes are not left idle by empty leaves.
+// Near-field counts by parent cell.
+//
+// NF(leaf) = own x (population of the 27 periodic same-level cells around the
+// leaf) (computeNFCooperative, octree_rebalance.cuh:579-634), and a complete
+// sibling group may merge when parent count x (population of the 27 cells
+// around the parent, one level up) <= bucket (computeGroupCanMergeKernel,
+// octree_rebalance.cuh:636-700).  Both depend only on the particles, not on
+// the tree, so they are computed per parent cell P at level l-1 (a "unit"):
+//   * the 27 parent-level cells Q around P (P included) are found by two
+//     lower bounds each, one lane per Q;
+//   * the 8 children of P have their 27-cell stencils inside the 4 x 4 x 4
+//     block of level-l cells around P, and that block is partitioned by the
+//     children of the Q's that touch P (per axis: offset -1 gives the upper
+//     child, 0 both, +1 the lower): each lane counts its Q's particles into
+//     its block positions (a scan of a short range, or binary searches of
+//     its child boundaries when the range is long);
+//   * each leaf of P sums its 3 x 3 x 3 sub-block, and the group flag is the
+//     sum of the 27 Q populations.
+// Periodic wrap at low levels makes several offsets name the same cell;
+// every offset is counted, as in the per-leaf stencil.  One warp per unit:
+// 54 lower bounds serve up to 8 leaves and the group flag.
+constexpr u32 kNFScanMax = 32;  // Q ranges up to this length are scanned
+
+// Leaf index of child 0 of the parent at `pStart` if all 8 children are
+// leaves (a complete group), else -1.
+__device__ __forceinline__ int completeGroup(const u64 *K, int L, int h, unsigned level, u64 pStart, u64 pRange)
+{
+    const int i0 = h - int(octDigit(K[h], level));
+    if (i0 < 0 || i0 + 8 > L) return -1;
+    if (K[i0] != pStart || K[i0 + 8] != pStart + pRange) return -1;
+    return i0;
+}
+
+template <bool Hilbert>
+__device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, const u64 *K, const u32 *B, u32 *NF,
+                                              u8 *G, int L, unsigned bucket, int h, int run, unsigned level,
+                                              u32 &hint, const unsigned char *sEnc, const unsigned char *sNext,
+                                              const unsigned char *sDec)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned pl = level - 1;  // parent level
+    const u64 pRange = octRange(pl);
+    const u64 pStart = K[h] & ~(pRange - 1);
+
+    // parent coordinates (cell origin, 21-bit grid) and, for Hilbert, the
+    // curve state before each level (6 bits per level, levels 0-9, 10-19, 20)
+    u32 cx = 0, cy = 0, cz = 0;
+    u64 st0 = 0, st1 = 0, st2 = 0;
+    int pState = kHilbertStart;
+    if constexpr (Hilbert)
+    {
+        for (unsigned k = 0; k < pl; ++k)
+        {
+            const u64 bitsv = u64(pState) << (6 * (k < 10 ? k : (k < 20 ? k - 10 : k - 20)));
+            if (k < 10) st0 |= bitsv;
+            else if (k < 20) st1 |= bitsv;
+            else st2 |= bitsv;
+            const unsigned b = kOctLevels - 1 - k;
+            const unsigned o = sDec[pState * 8 + int((pStart >> (3u * b)) & 7u)];
+            cx |= ((o >> 2) & 1u) << b;
+            cy |= ((o >> 1) & 1u) << b;
+            cz |= (o & 1u) << b;
+            pState = sNext[pState * 8 + int(o)];
+        }
+    }
+    else
+    {
+        cx = compact3(pStart >> 2);
+        cy = compact3(pStart >> 1);
+        cz = compact3(pStart);
+    }
+
+    // lane q < 27: the parent-level cell Q at offset (dx, dy, dz)
+    u32 lo = 0, hi = 0;
+    if (lane < 27)
+    {
+        const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+        const u32 cube = 1u << (kOctLevels - pl);
+        const u32 x = (cx + u32(dx) * cube) & 0x1fffffu;
+        const u32 y = (cy + u32(dy) * cube) & 0x1fffffu;
+        const u32 z = (cz + u32(dz) * cube) & 0x1fffffu;
+        u64 qKey = pStart;
+        int qState = pState;  // Hilbert state of Q's children
+        const u32 diff = (x ^ cx) | (y ^ cy) | (z ^ cz);  // zero only when the wrap maps Q onto P
+        if (diff != 0)
+        {
+            if constexpr (Hilbert)
+            {
+                // Q agrees with P on the levels above the first differing bit:
+                // keep that key prefix and encode the suffix from P's state there
+                const unsigned m = unsigned(__clz(diff)) - (32u - kOctLevels);
+                const u64 word = m < 10 ? st0 : (m < 20 ? st1 : st2);
+                int st = int((word >> (6 * (m < 10 ? m : (m < 20 ? m - 10 : m - 20)))) & 63u);
+                u64 suffix = 0;
+                for (unsigned k = m; k < pl; ++k)
+                {
+                    const unsigned b = kOctLevels - 1 - k;
+                    const unsigned o = (((x >> b) & 1u) << 2) | (((y >> b) & 1u) << 1) | ((z >> b) & 1u);
+                    const int e = st * 8 + int(o);
+                    suffix = (suffix << 3) | sEnc[e];
+                    st = sNext[e];
+                }
+                qState = st;
+                const unsigned keep = 3u * m;
+                const u64 prefix = keep ? (pStart >> (63u - keep)) << (63u - keep) : 0ull;
+                qKey = prefix | (suffix << (3u * (kOctLevels - pl)));
+            }
+            else
+            {
+                qKey = mortonKey(x, y, z);
+            }
+        }
+        lo = idx.lowerNear(hint, qKey);
+        hi = lowerFrom(idx, lo, qKey + pRange);
+        hint = lo;
+
+        // this lane's block positions: per axis 2*d + bit + 1, bit allowed by d
+        const int xb0 = dx > 0 ? 0 : (dx < 0 ? 1 : 0), xb1 = dx < 0 ? 1 : (dx > 0 ? 0 : 1);
+        const int yb0 = dy > 0 ? 0 : (dy < 0 ? 1 : 0), yb1 = dy < 0 ? 1 : (dy > 0 ? 0 : 1);
+        const int zb0 = dz > 0 ? 0 : (dz < 0 ? 1 : 0), zb1 = dz < 0 ? 1 : (dz > 0 ? 0 : 1);
+        for (int bx = xb0; bx <= xb1; ++bx)
+            for (int by = yb0; by <= yb1; ++by)
+                for (int bz = zb0; bz <= zb1; ++bz)
+                    block[(2 * dx + bx + 1) * 16 + (2 * dy + by + 1) * 4 + (2 * dz + bz + 1)] = 0;
+        const u32 n = hi - lo;
+        const unsigned cShift = 3u * (kOctLevels - level);
+        if (n <= kNFScanMax)
+        {
+            const u64 *P = idx.keys + lo;
+            for (u32 t = 0; t < n; ++t)
+            {
+                const unsigned d = unsigned(__ldg(P + t) >> cShift) & 7u;
+                const unsigned o = Hilbert ? unsigned(sDec[qState * 8 + int(d)]) : d;
+                const int ox = int(o >> 2), oy = int((o >> 1) & 1u), oz = int(o & 1u);
+                if (ox >= xb0 && ox <= xb1 && oy >= yb0 && oy <= yb1 && oz >= zb0 && oz <= zb1)
+                    ++block[(2 * dx + ox + 1) * 16 + (2 * dy + oy + 1) * 4 + (2 * dz + oz + 1)];
+            }
+        }
+        else
+        {
+            const u64 cr = octRange(level);
+            const u64 *P = idx.keys + lo;
+            for (int bx = xb0; bx <= xb1; ++bx)
+                for (int by = yb0; by <= yb1; ++by)
+                    for (int bz = zb0; bz <= zb1; ++bz)
+                    {
+                        const unsigned o = unsigned(bx << 2 | by << 1 | bz);
+                        const unsigned dg = Hilbert ? unsigned(sEnc[qState * 8 + int(o)]) : o;
+                        const u64 cs = qKey + u64(dg) * cr;
+                        const u32 c = lowerBound32(P, n, cs + cr) - lowerBound32(P, n, cs);
+                        block[(2 * dx + bx + 1) * 16 + (2 * dy + by + 1) * 4 + (2 * dz + bz + 1)] = c;
+                    }
+        }
+    }
+    __syncwarp();
+
+    // the unit's leaves: own count x sum of the 3 x 3 x 3 sub-block
+    if (lane < run)
+    {
+        const int i = h + lane;
+        const u32 c = B[i + 1] - B[i];
+        u32 out = 0;
+        if (c)
+        {
+            const unsigned d = octDigit(K[i], level);
+            const unsigned o = Hilbert ? unsigned(sDec[pState * 8 + int(d)]) : d;
+            const int ox = int(o >> 2), oy = int((o >> 1) & 1u), oz = int(o & 1u);
+            u64 pop = 0;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int e = 0; e < 3; ++e) pop += block[(ox + a) * 16 + (oy + b) * 4 + (oz + e)];
+            const u64 v = u64(c) * pop;
+            out = v > 0xffffffffull ? 0xffffffffu : u32(v);
+        }
+        NF[i] = out;
+    }
+
+    // group flag of a complete group: parent count x population around the parent
+    u64 qpop = lane < 27 ? u64(hi - lo) : 0;
+    for (int off = 16; off > 0; off >>= 1) qpop += __shfl_xor_sync(0xffffffffu, qpop, off);
+    const u32 pc = __shfl_sync(0xffffffffu, hi - lo, 13);
+    if (lane == 0)
+    {
+        const int i0 = completeGroup(K, L, h, level, pStart, pRange);
+        if (i0 >= 0) G[i0] = u64(pc) * qpop <= u64(bucket) ? 1 : 0;
+    }
+    __syncwarp();
+}
+
+// Near-field counts and group flags of the new leaves (All: of every leaf),
+// after octBeginKernel.  Each warp takes 32 list entries at a time, cuts them
+// into runs of consecutive leaves with the same parent, and processes each
+// run as one unit.  A run of empty leaves whose group is incomplete or empty
+// needs no search (NF 0; an empty parent can always merge).
 template <bool Hilbert, bool All>
 __global__ void __launch_bounds__(kRefreshThreads)
     octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h)
 {
     __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
-    __shared__ int sIdx[kRefreshThreads];
-    __shared__ u32 sCnt[kRefreshThreads];
-    __shared__ unsigned char sLev[kRefreshThreads];
-    __shared__ int sQueued;
+    __shared__ u32 sBlock[kRefreshThreads / 32][64];
     DeviceState *st = tb.st;
     if (halted(st)) return;
     if constexpr (Hilbert)
@@ -633,94 +732,75 @@ __global__ void __launch_bounds__(kRefreshThreads)
             sNext[k] = h.encNext[k];
             sDec[k] = h.decOct[k];
         }
+        __syncthreads();
     }
-    if (threadIdx.x == 0) sQueued = 0;
-    __syncthreads();
     const int a = st->activeBuffer;
     const int L = st->numLeaves;
     const u64 *K = tb.k(a);
     const u32 *B = tb.b(a);
     u32 *NF = tb.nf(a);
-    u8 *G = tb.g(a);
-
-    // leaves
+    u8 *Gf = tb.g(a);
+    u32 *block = sBlock[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int warpsTotal = gridDim.x * (blockDim.x / 32);
+    const int w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     const int count = All ? L : st->dirtyCount;
-    for (int base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x)
+    u32 hint = 0;
+    for (int base = w0 * 32; base < count; base += warpsTotal * 32)
     {
-        const int j = base + threadIdx.x;
-        if (j < count)
+        const int j = base + lane;
+        const bool valid = j < count;
+        const int i = valid ? (All ? j : tb.dirty[j]) : 0;
+        const u64 s = valid ? K[i] : 0;
+        const unsigned lev = valid ? octLevel(K[i + 1] - s) : 0;
+        const u32 c = valid ? B[i + 1] - B[i] : 0;
+        const u64 pk = lev > 0 ? (s & ~(octRange(lev - 1) - 1)) : 0;
+        const int iPrev = __shfl_up_sync(0xffffffffu, i, 1);
+        const u64 pkPrev = __shfl_up_sync(0xffffffffu, pk, 1);
+        const unsigned levPrev = __shfl_up_sync(0xffffffffu, lev, 1);
+        const bool head = valid && (lane == 0 || i != iPrev + 1 || pk != pkPrev || lev != levPrev || lev == 0);
+        unsigned heads = __ballot_sync(0xffffffffu, head);
+        const unsigned validMask = __ballot_sync(0xffffffffu, valid);
+        const unsigned nonEmpty = __ballot_sync(0xffffffffu, c != 0);
+        const int endLane = 32 - __clz(validMask);
+        while (heads)
         {
-            const int i = All ? j : tb.dirty[j];
-            const u32 c = B[i + 1] - B[i];
-            if (c == 0)
+            const int hl = __ffs(heads) - 1;
+            heads &= heads - 1;
+            const int next = heads ? __ffs(heads) - 1 : endLane;
+            const int hIdx = __shfl_sync(0xffffffffu, i, hl);
+            const unsigned lv = __shfl_sync(0xffffffffu, lev, hl);
+            const int run = next - hl;
+            if (lv == 0)
             {
-                NF[i] = 0;
-            }
-            else
-            {
-                const int q = atomicAdd(&sQueued, 1);
-                sIdx[q] = i;
-                sCnt[q] = c;
-            }
-        }
-        __syncthreads();
-        const int nq = sQueued;
-        if (int(threadIdx.x) < nq)
-        {
-            const int i = sIdx[threadIdx.x];
-            const u32 c = sCnt[threadIdx.x];
-            const u64 s = K[i];
-            const unsigned level = octLevel(K[i + 1] - s);
-            const u64 v = u64(c) * laneStencilPopulation<Hilbert>(idx, s, level, c, B[i], sEnc, sNext, sDec);
-            NF[i] = v > 0xffffffffull ? 0xffffffffu : u32(v);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) sQueued = 0;
-        __syncthreads();
-    }
-
-    // candidate group leaders: first leaf of a complete group of 8
-    // (IsDirtyGroupLeader, octree_rebalance.cuh:83-105)
-    const int gcount = All ? L : st->groupCount;
-    for (int base = blockIdx.x * blockDim.x; base < gcount; base += gridDim.x * blockDim.x)
-    {
-        const int j = base + threadIdx.x;
-        if (j < gcount)
-        {
-            const int i = All ? j : tb.groups[j];
-            const u64 s = K[i];
-            const unsigned level = octLevel(K[i + 1] - s);
-            const bool leader = level > 0 && level <= kOctLevels && octDigit(s, level) == 0 && i + 8 <= L &&
-                                K[i + 8] == s + octRange(level - 1);
-            if (leader)
-            {
-                const u32 pc = B[i + 8] - B[i];
-                if (pc == 0)
+                // the root leaf: all 27 periodic cells are the root itself
+                if (lane == 0)
                 {
-                    G[i] = 1;
+                    const u64 cr = B[hIdx + 1] - B[hIdx];
+                    const u64 v = cr * cr * 27ull;
+                    NF[hIdx] = v > 0xffffffffull ? 0xffffffffu : u32(v);
                 }
-                else
+                continue;
+            }
+            const unsigned runMask = (next == 32 ? 0xffffffffu : ((1u << next) - 1u)) & ~((1u << hl) - 1u);
+            if ((nonEmpty & runMask) == 0)
+            {
+                // empty run: NF 0; the group flag needs a search only if the parent holds particles
+                const u64 pRange = octRange(lv - 1);
+                const u64 pStart = __shfl_sync(0xffffffffu, s, hl) & ~(pRange - 1);
+                int i0 = -1;
+                if (lane == 0) i0 = completeGroup(K, L, hIdx, lv, pStart, pRange);
+                i0 = __shfl_sync(0xffffffffu, i0, 0);
+                const bool parentEmpty = i0 < 0 || B[i0 + 8] == B[i0];
+                if (parentEmpty)
                 {
-                    const int q = atomicAdd(&sQueued, 1);
-                    sIdx[q] = i;
-                    sCnt[q] = pc;
-                    sLev[q] = (unsigned char)(level - 1);
+                    if (lane >= hl && lane < next) NF[i] = 0;
+                    if (lane == 0 && i0 >= 0) Gf[i0] = 1;
+                    continue;
                 }
             }
+            nearFieldUnit<Hilbert>(idx, block, K, B, NF, Gf, L, bucket, hIdx, run, lv, hint, sEnc, sNext, sDec);
         }
-        __syncthreads();
-        const int nq = sQueued;
-        if (int(threadIdx.x) < nq)
-        {
-            const int i = sIdx[threadIdx.x];
-            const u32 pc = sCnt[threadIdx.x];
-            const unsigned plevel = sLev[threadIdx.x];
-            const u64 v = u64(pc) * laneStencilPopulation<Hilbert>(idx, K[i], plevel, pc, B[i], sEnc, sNext, sDec);
-            G[i] = v <= u64(bucket) ? 1 : 0;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) sQueued = 0;
-        __syncthreads();
     }
 }
 
