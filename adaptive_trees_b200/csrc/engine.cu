@@ -344,7 +344,7 @@ struct TreeEngine::Impl
     cudaEvent_t ready = nullptr;
     DevMem history;
     // tree
-    DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, groups, scan;
+    DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
     size_t scanTiles = 0;
     // views
     DevMem vBox, vSplit, vDepth, vParent, vChild, vLevelOffset, vPbegin, vPcount, vPmap, vMaxDepth;
@@ -380,7 +380,6 @@ struct TreeEngine::Impl
         }
         t.offs = offs.as<i64>();
         t.dirty = dirty.as<int>();
-        t.groups = groups.as<int>();
         t.scanStatus = scan.as<u64>();
         t.scanTile = reinterpret_cast<u32 *>(scan.as<u64>() + scanTiles);
         t.st = st;
@@ -518,7 +517,6 @@ void TreeEngine::ensurePhysical(size_t capacity)
     m_->offs.reserve((c + 1) * sizeof(i64));
     m_->dirty.reserve((c + 1) * sizeof(int));
     // candidate group leaders are first children of distinct internal nodes: <= (L - 1) / 7
-    m_->groups.reserve((c / 7 + 8) * sizeof(int));
     m_->scanTiles = (c + 1 + rb::kScanTile - 1) / rb::kScanTile;
     m_->scan.reserve((m_->scanTiles + 1) * sizeof(u64));
     physCap_ = c;

@@ -45,7 +45,6 @@ struct TreeBufs
     u32 *N[2];    // leaf counts, materialised for getters and views
     i64 *offs;    // decision scan, capacity + 1
     int *dirty;   // new leaves that need a search (and NF)
-    int *groups;  // candidate group leaders that need a parent NF
     u64 *scanStatus;
     u32 *scanTile;
     DeviceState *st;
@@ -369,7 +368,7 @@ template <bool NF>
 __device__ __forceinline__ void octScatterLeaf(const TreeBufs &tb, DeviceState *st, int i, int L, int a, int b,
                                                long long total)
 {
-    int nDirty = 0, nGroup = 0, op = 0;
+    int nDirty = 0, op = 0;
     i64 ni = 0;
     if (i < L)
     {
@@ -387,26 +386,19 @@ __device__ __forceinline__ void octScatterLeaf(const TreeBufs &tb, DeviceState *
             Bn[ni] = tb.b(a)[i];
             if constexpr (NF)
             {
+                // a merge leader becomes a new leaf; a kept leaf keeps its NF
+                // and its group flag (both depend on the particles only; a
+                // group completed in this pass holds a new leaf, and the
+                // refresh of that leaf's parent rewrites the flag)
                 const bool leader = i + 1 < L && opAt(offs, i + 1) == 0;
                 if (leader)
                 {
                     nDirty = 1;
-                    nGroup = (level - 1 > 0 && octDigit(start, level - 1) == 0) ? 1 : 0;
                 }
                 else
                 {
                     tb.nf(b)[ni] = tb.nf(a)[i];
-                    unsigned sl = 0;
-                    const int sib = siblingIndex(K, L, i, sl);
-                    bool reusable = false;
-                    if (sib == 0 && i + 8 <= L)
-                    {
-                        reusable = true;
-                        for (int s = 0; s < 8; ++s)
-                            if (opAt(offs, i + s) != 1) reusable = false;
-                    }
-                    if (reusable) tb.g(b)[ni] = tb.g(a)[i];
-                    else nGroup = (level > 0 && octDigit(start, level) == 0) ? 1 : 0;
+                    tb.g(b)[ni] = tb.g(a)[i];
                 }
             }
         }
@@ -416,7 +408,6 @@ __device__ __forceinline__ void octScatterLeaf(const TreeBufs &tb, DeviceState *
             for (int c = 0; c < op; ++c) Kn[ni + c] = start + u64(c) * nr;
             Bn[ni] = tb.b(a)[i];  // the first child starts where the parent did
             nDirty = NF ? op : op - 1;
-            nGroup = NF ? op / 8 : 0;
         }
         if (i == 0)
         {
@@ -436,17 +427,6 @@ __device__ __forceinline__ void octScatterLeaf(const TreeBufs &tb, DeviceState *
         else
         {
             tb.dirty[d0] = int(ni);
-        }
-    }
-    if constexpr (NF)
-    {
-        const int g0 = warpAppend(&st->groupCount, nGroup);
-        if (nGroup)
-        {
-            if (op > 1)
-                for (int c = 0; c < nGroup; ++c) tb.groups[g0 + c] = int(ni) + 8 * c;
-            else
-                tb.groups[g0] = int(ni);
         }
     }
 }
@@ -919,7 +899,6 @@ __global__ void resetForUpdateKernel(DeviceState *st, const u64 *P, size_t n)
     st->converged = 0;
     st->numActiveParticles = n ? u32(lowerBoundDev(P, n, kMaxKey)) : 0u;
     st->dirtyCount = 0;
-    st->groupCount = 0;
 }
 
 // Per-pass reset of the flags the decision accumulates.
@@ -927,7 +906,6 @@ __global__ void beginPassKernel(DeviceState *st)
 {
     st->changed = 0;
     st->dirtyCount = 0;
-    st->groupCount = 0;
 }
 
 // Sample every kSampleStride-th key for KeyIndex.
