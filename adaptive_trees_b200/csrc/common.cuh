@@ -156,7 +156,9 @@ struct KeyIndex
     }
 
     // lowerBound(keys, n, v) for a target expected near index `hint`:
-    // gallop up to 4 probes each way from the hint, then fall back to lower().
+    // gallop up to Probes probes each way from the hint (a window of
+    // 2^Probes - 1 keys), then fall back to lower().
+    template <int Probes = 4>
     __device__ __forceinline__ u32 lowerNear(u32 hint, u64 v) const
     {
         const u32 m = u32(n);
@@ -164,7 +166,7 @@ struct KeyIndex
         {
             u32 base = hint, step = 1;  // keys[base] < v
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
+            for (int k = 0; k < Probes; ++k)
             {
                 const u32 probe = base + step;
                 if (probe >= m || __ldg(keys + probe) >= v)
@@ -179,7 +181,7 @@ struct KeyIndex
         }
         u32 top = hint < m ? hint : m, step = 1;  // answer <= top
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
+        for (int k = 0; k < Probes; ++k)
         {
             if (top < step) return lowerBound32(keys, top, v);
             const u32 probe = top - step;

@@ -524,6 +524,7 @@ __global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBufs tb, K
 // every offset is counted, as in the per-leaf stencil.  One warp per unit:
 // 54 lower bounds serve up to 8 leaves and the group flag.
 constexpr u32 kNFScanMax = 32;  // Q ranges up to this length are scanned
+constexpr int kNFGallop = 8;    // gallop window of the Q searches: 255 keys from the last unit's
 
 // Leaf index of child 0 of the parent at `pStart` if all 8 children are
 // leaves (a complete group), else -1.
@@ -535,57 +536,89 @@ __device__ __forceinline__ int completeGroup(const u64 *K, int L, int h, unsigne
     return i0;
 }
 
+// Cell of `start` at level `pl`: grid coordinates of its origin (21-bit) and,
+// for Hilbert, the curve state before each level (6 bits per level; levels
+// 0-9 in st0, 10-19 in st1, 20 in st2) and the state of its children.
+struct CellPath
+{
+    u32 x, y, z;
+    u64 st0, st1, st2;
+    int childState;
+};
+
+template <bool Hilbert>
+__device__ __forceinline__ CellPath decodeCell(u64 start, unsigned pl, const unsigned char *sNext,
+                                               const unsigned char *sDec)
+{
+    CellPath c{0, 0, 0, 0, 0, 0, kHilbertStart};
+    if constexpr (Hilbert)
+    {
+        int st = kHilbertStart;
+        for (unsigned k = 0; k < pl; ++k)
+        {
+            const u64 bitsv = u64(st) << (6 * (k < 10 ? k : (k < 20 ? k - 10 : k - 20)));
+            if (k < 10) c.st0 |= bitsv;
+            else if (k < 20) c.st1 |= bitsv;
+            else c.st2 |= bitsv;
+            const unsigned b = kOctLevels - 1 - k;
+            const unsigned o = sDec[st * 8 + int((start >> (3u * b)) & 7u)];
+            c.x |= ((o >> 2) & 1u) << b;
+            c.y |= ((o >> 1) & 1u) << b;
+            c.z |= (o & 1u) << b;
+            st = sNext[st * 8 + int(o)];
+        }
+        c.childState = st;
+    }
+    else
+    {
+        c.x = compact3(start >> 2);
+        c.y = compact3(start >> 1);
+        c.z = compact3(start);
+    }
+    return c;
+}
+
+__device__ __forceinline__ CellPath shflPath(const CellPath &c, int src)
+{
+    CellPath r;
+    r.x = __shfl_sync(0xffffffffu, c.x, src);
+    r.y = __shfl_sync(0xffffffffu, c.y, src);
+    r.z = __shfl_sync(0xffffffffu, c.z, src);
+    r.st0 = __shfl_sync(0xffffffffu, c.st0, src);
+    r.st1 = __shfl_sync(0xffffffffu, c.st1, src);
+    r.st2 = __shfl_sync(0xffffffffu, c.st2, src);
+    r.childState = __shfl_sync(0xffffffffu, c.childState, src);
+    return r;
+}
+
+// One unit: the leaves h..h+run-1 (children of the parent P at level
+// level-1, decoded in `pp`) and the group flag of P's complete group.
+// sPos[q * 8 + o] is the block position of child octant o of the Q at lane q,
+// or 0xff where that child does not touch P.
 template <bool Hilbert>
 __device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, const u64 *K, const u32 *B, u32 *NF,
                                               u8 *G, int L, unsigned bucket, int h, int run, unsigned level,
-                                              u32 &hint, const unsigned char *sEnc, const unsigned char *sNext,
-                                              const unsigned char *sDec)
+                                              const CellPath &pp, u32 &hint, const unsigned char *sEnc,
+                                              const unsigned char *sNext, const unsigned char *sDec,
+                                              const unsigned char *sPos)
 {
     const int lane = threadIdx.x & 31;
     const unsigned pl = level - 1;  // parent level
     const u64 pRange = octRange(pl);
     const u64 pStart = K[h] & ~(pRange - 1);
 
-    // parent coordinates (cell origin, 21-bit grid) and, for Hilbert, the
-    // curve state before each level (6 bits per level, levels 0-9, 10-19, 20)
-    u32 cx = 0, cy = 0, cz = 0;
-    u64 st0 = 0, st1 = 0, st2 = 0;
-    int pState = kHilbertStart;
-    if constexpr (Hilbert)
-    {
-        for (unsigned k = 0; k < pl; ++k)
-        {
-            const u64 bitsv = u64(pState) << (6 * (k < 10 ? k : (k < 20 ? k - 10 : k - 20)));
-            if (k < 10) st0 |= bitsv;
-            else if (k < 20) st1 |= bitsv;
-            else st2 |= bitsv;
-            const unsigned b = kOctLevels - 1 - k;
-            const unsigned o = sDec[pState * 8 + int((pStart >> (3u * b)) & 7u)];
-            cx |= ((o >> 2) & 1u) << b;
-            cy |= ((o >> 1) & 1u) << b;
-            cz |= (o & 1u) << b;
-            pState = sNext[pState * 8 + int(o)];
-        }
-    }
-    else
-    {
-        cx = compact3(pStart >> 2);
-        cy = compact3(pStart >> 1);
-        cz = compact3(pStart);
-    }
-
-    // lane q < 27: the parent-level cell Q at offset (dx, dy, dz)
+    // lane q < 27: the parent-level cell Q at offset (q%3-1, q/3%3-1, q/9-1)
     u32 lo = 0, hi = 0;
     if (lane < 27)
     {
         const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
         const u32 cube = 1u << (kOctLevels - pl);
-        const u32 x = (cx + u32(dx) * cube) & 0x1fffffu;
-        const u32 y = (cy + u32(dy) * cube) & 0x1fffffu;
-        const u32 z = (cz + u32(dz) * cube) & 0x1fffffu;
+        const u32 x = (pp.x + u32(dx) * cube) & 0x1fffffu;
+        const u32 y = (pp.y + u32(dy) * cube) & 0x1fffffu;
+        const u32 z = (pp.z + u32(dz) * cube) & 0x1fffffu;
         u64 qKey = pStart;
-        int qState = pState;  // Hilbert state of Q's children
-        const u32 diff = (x ^ cx) | (y ^ cy) | (z ^ cz);  // zero only when the wrap maps Q onto P
+        int qState = pp.childState;  // Hilbert state of Q's children
+        const u32 diff = (x ^ pp.x) | (y ^ pp.y) | (z ^ pp.z);  // zero only when the wrap maps Q onto P
         if (diff != 0)
         {
             if constexpr (Hilbert)
@@ -593,7 +626,7 @@ __device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, c
                 // Q agrees with P on the levels above the first differing bit:
                 // keep that key prefix and encode the suffix from P's state there
                 const unsigned m = unsigned(__clz(diff)) - (32u - kOctLevels);
-                const u64 word = m < 10 ? st0 : (m < 20 ? st1 : st2);
+                const u64 word = m < 10 ? pp.st0 : (m < 20 ? pp.st1 : pp.st2);
                 int st = int((word >> (6 * (m < 10 ? m : (m < 20 ? m - 10 : m - 20)))) & 63u);
                 u64 suffix = 0;
                 for (unsigned k = m; k < pl; ++k)
@@ -614,51 +647,46 @@ __device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, c
                 qKey = mortonKey(x, y, z);
             }
         }
-        lo = idx.lowerNear(hint, qKey);
+        lo = idx.lowerNear<kNFGallop>(hint, qKey);
         hi = lowerFrom(idx, lo, qKey + pRange);
         hint = lo;
 
-        // this lane's block positions: per axis 2*d + bit + 1, bit allowed by d
-        const int xb0 = dx > 0 ? 0 : (dx < 0 ? 1 : 0), xb1 = dx < 0 ? 1 : (dx > 0 ? 0 : 1);
-        const int yb0 = dy > 0 ? 0 : (dy < 0 ? 1 : 0), yb1 = dy < 0 ? 1 : (dy > 0 ? 0 : 1);
-        const int zb0 = dz > 0 ? 0 : (dz < 0 ? 1 : 0), zb1 = dz < 0 ? 1 : (dz > 0 ? 0 : 1);
-        for (int bx = xb0; bx <= xb1; ++bx)
-            for (int by = yb0; by <= yb1; ++by)
-                for (int bz = zb0; bz <= zb1; ++bz)
-                    block[(2 * dx + bx + 1) * 16 + (2 * dy + by + 1) * 4 + (2 * dz + bz + 1)] = 0;
+        const unsigned char *pos = sPos + lane * 8;
+#pragma unroll
+        for (int o = 0; o < 8; ++o)
+            if (pos[o] != 0xff) block[pos[o]] = 0;
         const u32 n = hi - lo;
         const unsigned cShift = 3u * (kOctLevels - level);
+        const u64 *P = idx.keys + lo;
         if (n <= kNFScanMax)
         {
-            const u64 *P = idx.keys + lo;
             for (u32 t = 0; t < n; ++t)
             {
                 const unsigned d = unsigned(__ldg(P + t) >> cShift) & 7u;
                 const unsigned o = Hilbert ? unsigned(sDec[qState * 8 + int(d)]) : d;
-                const int ox = int(o >> 2), oy = int((o >> 1) & 1u), oz = int(o & 1u);
-                if (ox >= xb0 && ox <= xb1 && oy >= yb0 && oy <= yb1 && oz >= zb0 && oz <= zb1)
-                    ++block[(2 * dx + ox + 1) * 16 + (2 * dy + oy + 1) * 4 + (2 * dz + oz + 1)];
+                const unsigned p = pos[o];
+                if (p != 0xff) ++block[p];
             }
         }
         else
         {
             const u64 cr = octRange(level);
-            const u64 *P = idx.keys + lo;
-            for (int bx = xb0; bx <= xb1; ++bx)
-                for (int by = yb0; by <= yb1; ++by)
-                    for (int bz = zb0; bz <= zb1; ++bz)
-                    {
-                        const unsigned o = unsigned(bx << 2 | by << 1 | bz);
-                        const unsigned dg = Hilbert ? unsigned(sEnc[qState * 8 + int(o)]) : o;
-                        const u64 cs = qKey + u64(dg) * cr;
-                        const u32 c = lowerBound32(P, n, cs + cr) - lowerBound32(P, n, cs);
-                        block[(2 * dx + bx + 1) * 16 + (2 * dy + by + 1) * 4 + (2 * dz + bz + 1)] = c;
-                    }
+#pragma unroll 1
+            for (int o = 0; o < 8; ++o)
+            {
+                const unsigned p = pos[o];
+                if (p == 0xff) continue;
+                const unsigned dg = Hilbert ? unsigned(sEnc[qState * 8 + o]) : unsigned(o);
+                const u64 cs = qKey + u64(dg) * cr;
+                block[p] = lowerBound32(P, n, cs + cr) - lowerBound32(P, n, cs);
+            }
         }
     }
     __syncwarp();
 
-    // the unit's leaves: own count x sum of the 3 x 3 x 3 sub-block
+    // the unit's leaves: own count x population of the 3 x 3 x 3 sub-block
+    // (27 distinct cells, so at most n < 2^32, except at level 1 where the
+    // periodic wrap repeats cells)
     if (lane < run)
     {
         const int i = h + lane;
@@ -667,12 +695,27 @@ __device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, c
         if (c)
         {
             const unsigned d = octDigit(K[i], level);
-            const unsigned o = Hilbert ? unsigned(sDec[pState * 8 + int(d)]) : d;
-            const int ox = int(o >> 2), oy = int((o >> 1) & 1u), oz = int(o & 1u);
-            u64 pop = 0;
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b)
-                    for (int e = 0; e < 3; ++e) pop += block[(ox + a) * 16 + (oy + b) * 4 + (oz + e)];
+            const unsigned o = Hilbert ? unsigned(sDec[pp.childState * 8 + int(d)]) : d;
+            const u32 *sub = block + (o >> 2) * 16 + ((o >> 1) & 1u) * 4 + (o & 1u);
+            u64 pop;
+            if (level > 1)
+            {
+                u32 p32 = 0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b)
+#pragma unroll
+                        for (int e = 0; e < 3; ++e) p32 += sub[a * 16 + b * 4 + e];
+                pop = p32;
+            }
+            else
+            {
+                pop = 0;
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        for (int e = 0; e < 3; ++e) pop += sub[a * 16 + b * 4 + e];
+            }
             const u64 v = u64(c) * pop;
             out = v > 0xffffffffull ? 0xffffffffu : u32(v);
         }
@@ -693,14 +736,15 @@ __device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, c
 
 // Near-field counts and group flags of the new leaves (All: of every leaf),
 // after octBeginKernel.  Each warp takes 32 list entries at a time, cuts them
-// into runs of consecutive leaves with the same parent, and processes each
-// run as one unit.  A run of empty leaves whose group is incomplete or empty
-// needs no search (NF 0; an empty parent can always merge).
+// into runs of consecutive leaves with the same parent, decodes the runs'
+// parents lane-parallel and processes each run as one unit.  A run of empty
+// leaves whose group is incomplete or empty needs no search (NF 0; an empty
+// parent can always merge).
 template <bool Hilbert, bool All>
 __global__ void __launch_bounds__(kRefreshThreads)
     octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h)
 {
-    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
+    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8], sPos[27 * 8];
     __shared__ u32 sBlock[kRefreshThreads / 32][64];
     DeviceState *st = tb.st;
     if (halted(st)) return;
@@ -712,8 +756,24 @@ __global__ void __launch_bounds__(kRefreshThreads)
             sNext[k] = h.encNext[k];
             sDec[k] = h.decOct[k];
         }
-        __syncthreads();
     }
+    for (int k = threadIdx.x; k < 27 * 8; k += blockDim.x)
+    {
+        // per axis: offset -1 touches P with its upper child, 0 with both, +1 with its lower;
+        // block coordinate 2 * offset + child bit + 1
+        const int q = k >> 3, o = k & 7;
+        const int d[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+        const int bit[3] = {o >> 2, (o >> 1) & 1, o & 1};
+        bool ok = true;
+        int p = 0;
+        for (int ax = 0; ax < 3; ++ax)
+        {
+            if ((d[ax] < 0 && bit[ax] == 0) || (d[ax] > 0 && bit[ax] == 1)) ok = false;
+            p = p * 4 + (2 * d[ax] + bit[ax] + 1);
+        }
+        sPos[k] = ok ? (unsigned char)p : (unsigned char)0xff;
+    }
+    __syncthreads();
     const int a = st->activeBuffer;
     const int L = st->numLeaves;
     const u64 *K = tb.k(a);
@@ -743,6 +803,9 @@ __global__ void __launch_bounds__(kRefreshThreads)
         const unsigned validMask = __ballot_sync(0xffffffffu, valid);
         const unsigned nonEmpty = __ballot_sync(0xffffffffu, c != 0);
         const int endLane = 32 - __clz(validMask);
+        // decode the parents of all runs at once (head lanes)
+        CellPath path{0, 0, 0, 0, 0, 0, kHilbertStart};
+        if (head && lev > 0) path = decodeCell<Hilbert>(pk, lev - 1, sNext, sDec);
         while (heads)
         {
             const int hl = __ffs(heads) - 1;
@@ -779,7 +842,9 @@ __global__ void __launch_bounds__(kRefreshThreads)
                     continue;
                 }
             }
-            nearFieldUnit<Hilbert>(idx, block, K, B, NF, Gf, L, bucket, hIdx, run, lv, hint, sEnc, sNext, sDec);
+            const CellPath pp = shflPath(path, hl);
+            nearFieldUnit<Hilbert>(idx, block, K, B, NF, Gf, L, bucket, hIdx, run, lv, pp, hint, sEnc, sNext, sDec,
+                                   sPos);
         }
     }
 }
