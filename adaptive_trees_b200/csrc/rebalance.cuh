@@ -523,8 +523,8 @@ __global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBufs tb, K
 // Periodic wrap at low levels makes several offsets name the same cell;
 // every offset is counted, as in the per-leaf stencil.  One warp per unit:
 // 54 lower bounds serve up to 8 leaves and the group flag.
-constexpr u32 kNFScanMax = 32;  // Q ranges up to this length are scanned
-constexpr int kNFGallop = 8;    // gallop window of the Q searches: 255 keys from the last unit's
+constexpr u32 kNFScanMax = 256;  // Q ranges up to this length are scanned
+constexpr int kNFGallop = 4;     // gallop window of the Q searches: 15 keys from the last unit's
 
 // Leaf index of child 0 of the parent at `pStart` if all 8 children are
 // leaves (a complete group), else -1.
