@@ -37,6 +37,11 @@ class AoTreeInfo(ctypes.Structure):
                 ("kernel_launches", ctypes.c_ulonglong)]
 
 
+class AoBatchSystemInfo(ctypes.Structure):
+    _fields_ = [("num_particles", sz), ("num_active_particles", sz), ("num_leaves", sz), ("leaf_capacity", sz),
+                ("needs_resize", ci)]
+
+
 PROTOTYPES = {
     "ao_tree_create": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(AoConfig), vp, ctypes.POINTER(vp)],
     "ao_tree_destroy": [vp],
@@ -51,6 +56,16 @@ PROTOTYPES = {
     "ao_compute_sfc_keys": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_double), ci, cu, vp, vp, vp],
     "ao_sort_pairs": [vp, ctypes.POINTER(sz), vp, vp, vp, vp, sz, ci, ci, vp],
     "ao_sort_pairs_noalloc": [vp, vp, vp, vp, sz, ci, ci, vp],
+    "ao_batch_create": [ci, ci, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(sz),
+                        ctypes.POINTER(AoConfig), vp, ctypes.POINTER(vp)],
+    "ao_batch_destroy": [vp],
+    "ao_batch_build": [vp],
+    "ao_batch_update": [vp, vp],
+    "ao_batch_needs_resize": [vp, ctypes.POINTER(ci)],
+    "ao_batch_resize_buffers": [vp],
+    "ao_batch_set_coordinates": [vp, ci, vp, vp, vp],
+    "ao_batch_get_buffer": [vp, ci, ci, ctypes.POINTER(vp), ctypes.POINTER(sz)],
+    "ao_batch_get_info": [vp, ci, ctypes.POINTER(AoBatchSystemInfo)],
 }
 
 # n limit of ao_sort_pairs_noalloc (AO_SORT_PAIRS_NOALLOC_MAX_ITEMS)

@@ -7,6 +7,7 @@
 #include "adaptive_octree/tree.hpp"
 #include "adaptive_trees_b200.h"
 #include "engine.hpp"
+#include "forest.hpp"
 
 namespace adaptive_octree
 {
@@ -215,6 +216,11 @@ template class KDTree3D<double>;
 struct ao_tree
 {
     std::unique_ptr<aot::TreeEngine> engine;
+};
+
+struct ao_batch
+{
+    std::unique_ptr<aot::ForestEngine> engine;
 };
 
 namespace
@@ -429,6 +435,88 @@ ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsigned lon
     return guarded([&] {
         aot::TreeEngine::sortPairs(scratch, scratch_bytes, keys_in, keys_out, values_in, values_out, n, begin_bit,
                                    end_bit, static_cast<cudaStream_t>(stream));
+    });
+}
+
+ao_status ao_batch_create(int real_type, int num_systems, const void *const *x, const void *const *y,
+                          const void *const *z, const size_t *counts, const ao_config *config, void *stream,
+                          ao_batch **out)
+{
+    return guarded([&] {
+        if (!out || !config) throw std::invalid_argument("ao_batch_create: null argument");
+        *out = nullptr;
+        const aot::EngineConfig cfg = engineConfig(AO_OCTREE, real_type, *config, stream);
+        auto b = std::make_unique<ao_batch>();
+        b->engine = std::make_unique<aot::ForestEngine>(x, y, z, counts, num_systems, cfg);
+        *out = b.release();
+    });
+}
+
+ao_status ao_batch_destroy(ao_batch *batch)
+{
+    return guarded([&] { delete batch; });
+}
+
+ao_status ao_batch_build(ao_batch *batch)
+{
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("ao_batch_build: null batch");
+        batch->engine->build();
+    });
+}
+
+ao_status ao_batch_update(ao_batch *batch, const unsigned char *frozen)
+{
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("ao_batch_update: null batch");
+        batch->engine->update(frozen);
+    });
+}
+
+ao_status ao_batch_needs_resize(ao_batch *batch, int *any)
+{
+    return guarded([&] {
+        if (!batch || !any) throw std::invalid_argument("ao_batch_needs_resize: null argument");
+        *any = batch->engine->needsResize() ? 1 : 0;
+    });
+}
+
+ao_status ao_batch_resize_buffers(ao_batch *batch)
+{
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("ao_batch_resize_buffers: null batch");
+        batch->engine->resizeBuffers();
+    });
+}
+
+ao_status ao_batch_set_coordinates(ao_batch *batch, int system, const void *x, const void *y, const void *z)
+{
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("ao_batch_set_coordinates: null batch");
+        batch->engine->setCoordinates(system, x, y, z);
+    });
+}
+
+ao_status ao_batch_get_buffer(ao_batch *batch, int system, int which, const void **ptr, size_t *size)
+{
+    return guarded([&] {
+        if (!batch || !ptr || !size) throw std::invalid_argument("ao_batch_get_buffer: null argument");
+        if (which < AO_BUF_PARTICLE_KEYS || which > AO_BUF_LEAF_COUNTS)
+            throw std::invalid_argument("ao_batch_get_buffer: a batch exposes keys, perm, cornerstone and counts");
+        batch->engine->buffer(system, which, ptr, size);
+    });
+}
+
+ao_status ao_batch_get_info(ao_batch *batch, int system, ao_batch_system_info *info)
+{
+    return guarded([&] {
+        if (!batch || !info) throw std::invalid_argument("ao_batch_get_info: null argument");
+        const aot::ForestEngine::SystemInfo s = batch->engine->info(system);
+        info->num_particles = s.particles;
+        info->num_active_particles = s.active;
+        info->num_leaves = s.leaves;
+        info->leaf_capacity = s.leafCapacity;
+        info->needs_resize = s.needsResize ? 1 : 0;
     });
 }
 

@@ -21,6 +21,7 @@
 #include <limits>
 #include <stdexcept>
 
+#include "engine_util.cuh"
 #include "keygen.cuh"
 #include "rebalance.cuh"
 #include "tree_view.cuh"
@@ -64,7 +65,9 @@ namespace
 // Kernel launches issued by this process (all trees); reported by
 // ao_tree_get_info so a benchmark can state how many engine kernels ran.
 std::atomic<unsigned long long> g_launches{0};
-inline void noteLaunch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace
+
+void noteLaunch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int smCount()
 {
@@ -85,27 +88,8 @@ const HilbertTables &hilbertTables()
     return t;
 }
 
-template <class T>
-QuantBox<T> makeQuantBox(const double *b)
+namespace
 {
-    // Box<T> (sfc_keys.cuh:420-465): inverse lengths and per-axis bits in T
-    const T xmin = T(b[0]), xmax = T(b[1]), ymin = T(b[2]), ymax = T(b[3]), zmin = T(b[4]), zmax = T(b[5]);
-    QuantBox<T> q;
-    q.xmin = xmin;
-    q.ymin = ymin;
-    q.zmin = zmin;
-    q.ilx = T(1) / (xmax - xmin);
-    q.ily = T(1) / (ymax - ymin);
-    q.ilz = T(1) / (zmax - zmin);
-    const T lx = xmax - xmin, ly = ymax - ymin, lz = zmax - zmin;
-    const T md = std::max(std::max(lx, ly), lz);
-    const T bias = T(0.5849625007211563);
-    q.bx = kOctLevels - unsigned(std::floor(std::log2(md / lx) + bias));
-    q.by = kOctLevels - unsigned(std::floor(std::log2(md / ly) + bias));
-    q.bz = kOctLevels - unsigned(std::floor(std::log2(md / lz) + bias));
-    return q;
-}
-
 // makeBinaryGeometry (binary_node.cuh:17-40): the longest side is halved at
 // every depth, first axis wins ties.
 BinaryGeometry makeGeometry(const double *b, unsigned maxDepth, int real)
@@ -240,9 +224,9 @@ int sortWithIndices(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int passes, 
     return runPasses(s, k, v, n, 0, passes, true, a, error);
 }
 
-unsigned gridFor(size_t n, unsigned threads) { return std::max(1u, ceilDiv(std::max<size_t>(n, 1), threads)); }
-
 }  // namespace
+
+unsigned gridFor(size_t n, unsigned threads) { return std::max(1u, ceilDiv(std::max<size_t>(n, 1), threads)); }
 
 unsigned long long TreeEngine::kernelLaunches() { return g_launches.load(std::memory_order_relaxed); }
 
@@ -470,9 +454,6 @@ TreeEngine::TreeEngine(const void *x, const void *y, const void *z, size_t n, co
         m_->sample.reserve(((n + kSampleStride - 1) >> kSampleShift) * sizeof(u64));
         m_->sortArena.ensure(n);
     }
-    // K_d.resize(2) in the constructor (octree.cu:149)
-    kSize_ = 2;
-    kCap_ = 2;
     ensurePhysical(16);
     if (cfg.kind == 0)
     {
@@ -735,11 +716,7 @@ void TreeEngine::readState()
     hostLeaves_ = size_t(std::max(h.numLeaves, 0));
     hostActive_ = h.numActiveParticles;
     hostNodes_ = size_t(std::max(h.numNodes, 0));
-    if (cfg_.kind == 0)
-    {
-        kSize_ = hostLeaves_ + 1;
-        tSize_ = hostLeaves_ + 1;
-    }
+    if (cfg_.kind == 0) capModel_.stateRead(hostLeaves_);
     syncViewSizes();
 }
 
@@ -753,15 +730,6 @@ bool TreeEngine::doBuffersNeedResize()
 // --------------------------------------------------------------------------
 // capacity (octree.cu:182-241, kdtree3d.cu:96-116)
 // --------------------------------------------------------------------------
-namespace
-{
-void capResize(size_t &size, size_t &cap, size_t n)  // vector growth (append)
-{
-    if (n > cap) cap = std::max(size + std::max(size, n - size), 2 * cap);
-    size = n;
-}
-void capReserve(size_t &cap, size_t n) { cap = std::max(cap, n); }
-}  // namespace
 
 void TreeEngine::prepareGraphBuffers(size_t capacity)
 {
@@ -769,15 +737,10 @@ void TreeEngine::prepareGraphBuffers(size_t capacity)
     {
         const size_t maxLeaves = (size_t(std::numeric_limits<int>::max()) - 1) / 8 * 7 + 1;
         if (capacity > maxLeaves) throw std::length_error("adaptive_octree: buffer capacity exceeds node index range");
-        const size_t leaves = kSize_ - 1;
         leafCapacity_ = capacity;
-        capReserve(kCap_, capacity + 1);
-        capResize(kSize_, kCap_, capacity + 1);
-        capReserve(tCap_, capacity + 1);
-        capResize(tSize_, tCap_, capacity + 1);
+        capModel_.prepare(capacity);
         ensurePhysical(capacity);
         prepareViews(capacity, prepared_);
-        kSize_ = tSize_ = leaves + 1;
         syncViewSizes();
     }
     else
@@ -814,7 +777,7 @@ void TreeEngine::octreeBuild()
 {
     cudaStream_t s = cfg_.stream;
     AOT_CHECK(cudaStreamSynchronize(s));
-    kSize_ = 2;
+    capModel_.buildStart();
     sortParticles();
     // Room for the build rounds; grown on overflow.
     const size_t estimate = std::max<size_t>(4096, cfg_.nf ? n_ + 4096 : n_ / 4 + 4096);
@@ -854,18 +817,9 @@ void TreeEngine::octreeBuild()
     if (h.iteration)
         AOT_CHECK(cudaMemcpy(proposals.data(), m_->history.p, proposals.size() * sizeof(long long),
                              cudaMemcpyDeviceToHost));
-    for (long long p : proposals)
-    {
-        const size_t req = size_t(p) + 1;
-        if (req > tCap_) tCap_ = req + req / 4;
-        tSize_ = req;
-        std::swap(kSize_, tSize_);
-        std::swap(kCap_, tCap_);
-    }
     const size_t leaves = size_t(h.numLeaves);
-    kSize_ = leaves + 1;
     hostLeaves_ = leaves;
-    const size_t cap = std::max({kCap_ - 1, tSize_ == 0 ? size_t(0) : tCap_ - 1, leaves + (leaves + 3) / 4});
+    const size_t cap = capModel_.finishBuild(proposals.data(), proposals.size(), leaves);
     // The final tree must sit in buffer 0 (finishBuildStateKernel resets the
     // active buffer).
     if (h.activeBuffer == 1)

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "adaptive_octree/config.hpp"
+#include "capacity.hpp"
 
 namespace aot
 {
@@ -124,7 +125,7 @@ private:
     bool built_ = false;
     int buildRounds_ = 0;
     // thrust capacity model of K_d / tmpTree (octree.cu:453-457)
-    size_t kSize_ = 0, kCap_ = 0, tSize_ = 0, tCap_ = 0;
+    OctreeCapacity capModel_;  // reference K_d / tmpTree capacities (octree)
     adaptive_octree::ViewConfig prepared_{};
 
     void sortParticles();

@@ -1,0 +1,459 @@
+// forest.cu -- host orchestration of the forest engine (forest.hpp).
+//
+// build():  keys + segmented sort of all systems, the roots, then build
+//           rounds over all systems until none changes (at most maxDepth,
+//           as rebalanceBuild, octree.cu:159-180), one state readback per
+//           round; each system's leafCapacity is replayed from its own round
+//           history with the same capacity model as a single tree.
+// update(): keys + segmented sort, a full begin-index refresh, then the
+//           configured number of fixed passes with per-system capacity
+//           rejection (updateOctreeGraphGpu, octree_rebalance.cuh:1177-1322);
+//           no host synchronisation.
+#include "forest.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+
+#include "capacity.hpp"
+#include "engine_util.cuh"
+#include "forest.cuh"
+
+namespace aot
+{
+struct ForestEngine::Impl
+{
+    EngineConfig cfg;
+    int S = 0;
+    size_t total = 0;
+    std::vector<forest::System> systems;
+    // segmented sort
+    u32 numTiles = 0;
+    DevMem systemsD, tileSys, tileBegin, tileEnd, segFirstTile, segBase;
+    DevMem P[2], Perm[2], hist, bins, tileCounters, status;
+    // leaf arrays (entries = all systems' leaves + sentinels)
+    size_t entryCap = 0;
+    DevMem K[2], B[2], SEG[2], N, ops, offs, dirty, scanStatus, scanTile;
+    size_t scanTiles = 0;
+    // state
+    DevMem st, sys, history, frozen;
+    forest::State *hst = nullptr;
+    forest::SysState *hsys = nullptr;
+    std::vector<OctreeCapacity> capModel;
+    std::vector<size_t> leafCap;
+    bool built = false;
+    KeygenParams<float> kpf{};
+    KeygenParams<double> kpd{};
+
+    ~Impl()
+    {
+        if (hst) cudaFreeHost(hst);
+        if (hsys) cudaFreeHost(hsys);
+    }
+
+    forest::Bufs bufs() const
+    {
+        forest::Bufs f{};
+        for (int k = 0; k < 2; ++k)
+        {
+            f.K[k] = K[k].as<u64>();
+            f.B[k] = B[k].as<u32>();
+            f.SEG[k] = SEG[k].as<int>();
+        }
+        f.N = N.as<u32>();
+        f.ops = ops.as<int>();
+        f.offs = offs.as<i64>();
+        f.dirty = dirty.as<int>();
+        f.scanStatus = scanStatus.as<u64>();
+        f.scanTile = scanTile.as<u32>();
+        f.st = st.as<forest::State>();
+        f.sys = sys.as<forest::SysState>();
+        f.systems = systemsD.as<forest::System>();
+        f.numSystems = S;
+        f.history = history.as<long long>();
+        f.P = P[0].as<u64>();
+        return f;
+    }
+};
+
+namespace
+{
+bool forestPassSmemSet = false;
+void setForestPassSmem()
+{
+    if (!forestPassSmemSet)
+    {
+        AOT_CHECK(cudaFuncSetAttribute(sort::segmentOnesweepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(sort::passSmem())));
+        forestPassSmemSet = true;
+    }
+}
+}  // namespace
+
+ForestEngine::ForestEngine(const void *const *x, const void *const *y, const void *const *z, const size_t *n,
+                           int numSystems, const EngineConfig &cfg)
+    : m_(std::make_unique<Impl>())
+{
+    Impl &m = *m_;
+    if (numSystems <= 0) throw std::invalid_argument("forest: need at least one system");
+    if (!x || !y || !z || !n) throw std::invalid_argument("forest: null coordinate or count array");
+    if (cfg.kind != 0) throw std::invalid_argument("forest: only octrees are batched");
+    if (cfg.nf) throw std::invalid_argument("forest: only LeafCount refinement is batched");
+    if (cfg.bucket == 0) throw std::invalid_argument("adaptive_octree: particle limit must be positive");
+    if (cfg.iterations == 0) throw std::invalid_argument("adaptive_octree: updateIterations must be positive");
+    if (cfg.views.treeStructure | cfg.views.particleCountsPerBox | cfg.views.particleMapping)
+        throw std::invalid_argument("forest: tree views are not batched");
+    m.cfg = cfg;
+    m.S = numSystems;
+    m.systems.resize(size_t(numSystems));
+    size_t total = 0;
+    for (int s = 0; s < numSystems; ++s)
+    {
+        if (n[s] > 0 && (!x[s] || !y[s] || !z[s]))
+            throw std::invalid_argument("adaptive_octree: coordinate device pointers must not be null");
+        m.systems[s] = forest::System{x[s], y[s], z[s], u32(total), u32(n[s])};
+        total += n[s];
+        if (total > size_t(std::numeric_limits<std::uint32_t>::max()))
+            throw std::invalid_argument("forest: more than 2^32 - 1 particles in total");
+    }
+    m.total = total;
+    m.kpf.q = makeQuantBox<float>(cfg.box);
+    m.kpd.q = makeQuantBox<double>(cfg.box);
+    m.kpf.h = m.kpd.h = hilbertTables();
+    m.capModel.assign(size_t(numSystems), OctreeCapacity{});
+    m.leafCap.assign(size_t(numSystems), 0);
+
+    // tile table of the segmented sort: every system in tiles of sort::kTile
+    std::vector<u32> tSys, tBeg, tEnd;
+    std::vector<u32> first(static_cast<size_t>(numSystems), 0xffffffffu);
+    std::vector<u32> base(static_cast<size_t>(numSystems), 0u);
+    for (int s = 0; s < numSystems; ++s)
+    {
+        const forest::System &sy = m.systems[s];
+        base[s] = sy.base;
+        if (sy.n) first[s] = u32(tSys.size());
+        for (u32 b = 0; b < sy.n; b += u32(sort::kTile))
+        {
+            tSys.push_back(u32(s));
+            tBeg.push_back(sy.base + b);
+            tEnd.push_back(sy.base + std::min<u32>(sy.n, b + u32(sort::kTile)));
+        }
+    }
+    m.numTiles = u32(tSys.size());
+    auto upload = [](DevMem &d, const void *src, size_t bytes) {
+        d.reserve(std::max<size_t>(bytes, 16));
+        if (bytes) AOT_CHECK(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice));
+    };
+    upload(m.systemsD, m.systems.data(), m.systems.size() * sizeof(forest::System));
+    upload(m.tileSys, tSys.data(), tSys.size() * 4);
+    upload(m.tileBegin, tBeg.data(), tBeg.size() * 4);
+    upload(m.tileEnd, tEnd.data(), tEnd.size() * 4);
+    upload(m.segFirstTile, first.data(), first.size() * 4);
+    upload(m.segBase, base.data(), base.size() * 4);
+    for (int k = 0; k < 2; ++k)
+    {
+        m.P[k].reserve(std::max<size_t>(total, 1) * 8);
+        m.Perm[k].reserve(std::max<size_t>(total, 1) * 4);
+    }
+    m.hist.reserve(size_t(numSystems) * sort::kMaxPasses * sort::kRadix * 4);
+    m.bins.reserve(size_t(numSystems) * sort::kMaxPasses * sort::kRadix * 4);
+    m.tileCounters.reserve(sort::kMaxPasses * 4);
+    m.status.reserve(std::max<size_t>(m.numTiles, 1) * sort::kMaxPasses * sort::kRadix * 8);
+    m.st.reserve(sizeof(forest::State));
+    AOT_CHECK(cudaMemset(m.st.p, 0, sizeof(forest::State)));
+    m.sys.reserve(size_t(numSystems) * sizeof(forest::SysState));
+    AOT_CHECK(cudaMemset(m.sys.p, 0, size_t(numSystems) * sizeof(forest::SysState)));
+    m.history.reserve(size_t(std::max(cfg.maxDepth, 1u)) * numSystems * sizeof(long long));
+    m.frozen.reserve(size_t(numSystems));
+    AOT_CHECK(cudaMemset(m.frozen.p, 0, size_t(numSystems)));
+    AOT_CHECK(cudaMallocHost(&m.hst, sizeof(forest::State)));
+    AOT_CHECK(cudaMallocHost(&m.hsys, size_t(numSystems) * sizeof(forest::SysState)));
+    std::memset(m.hst, 0, sizeof(forest::State));
+    std::memset(m.hsys, 0, size_t(numSystems) * sizeof(forest::SysState));
+    ensurePhysical(size_t(4) * numSystems + 4096);
+}
+
+ForestEngine::~ForestEngine() = default;
+
+int ForestEngine::numSystems() const { return m_->S; }
+size_t ForestEngine::numParticles() const { return m_->total; }
+
+void ForestEngine::setCoordinates(int s, const void *x, const void *y, const void *z)
+{
+    Impl &m = *m_;
+    if (s < 0 || s >= m.S) throw std::invalid_argument("forest: system index out of range");
+    if (m.systems[s].n > 0 && (!x || !y || !z))
+        throw std::invalid_argument("adaptive_octree: coordinate device pointers must not be null");
+    m.systems[s].x = x;
+    m.systems[s].y = y;
+    m.systems[s].z = z;
+    AOT_CHECK(cudaMemcpyAsync(m.systemsD.as<forest::System>() + s, &m.systems[s], sizeof(forest::System),
+                              cudaMemcpyHostToDevice, m.cfg.stream));
+    AOT_CHECK(cudaStreamSynchronize(m.cfg.stream));
+}
+
+// Leaf arrays for `entries` entries; the active arrays keep their contents.
+void ForestEngine::ensurePhysical(size_t entries)
+{
+    Impl &m = *m_;
+    if (entries <= m.entryCap && m.K[0].p) return;
+    cudaStream_t s = m.cfg.stream;
+    const size_t c = std::max(entries, m.entryCap + m.entryCap / 2);
+    for (int k = 0; k < 2; ++k)
+    {
+        m.K[k].grow((c + 1) * 8, m.K[k].bytes, s);
+        m.B[k].grow((c + 1) * 4, m.B[k].bytes, s);
+        m.SEG[k].grow((c + 1) * 4, m.SEG[k].bytes, s);
+    }
+    m.N.grow((c + 1) * 4, m.N.bytes, s);
+    m.ops.reserve((c + 1) * 4);
+    m.offs.grow((c + 2) * 8, m.offs.bytes, s);  // a build round grows the arrays between scan and scatter
+    m.dirty.reserve((c + 1) * 4);
+    m.scanTiles = (c + 2 + rb::kScanTile - 1) / rb::kScanTile;
+    m.scanStatus.reserve((m.scanTiles + 1) * 8);
+    m.scanTile.reserve(16);
+    m.entryCap = c;
+}
+
+void ForestEngine::sortParticles()
+{
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    if (m.total)
+    {
+        AOT_CHECK(cudaMemsetAsync(m.hist.p, 0, size_t(m.S) * sort::kMaxPasses * sort::kRadix * 4, s));
+        AOT_CHECK(cudaMemsetAsync(m.tileCounters.p, 0, sort::kMaxPasses * 4, s));
+        AOT_CHECK(cudaMemsetAsync(m.status.p, 0, size_t(m.numTiles) * sort::kMaxPasses * sort::kRadix * 8, s));
+        const unsigned grid = std::max(1u, std::min<unsigned>(m.numTiles, unsigned(smCount()) * 8u));
+        u64 *keys = m.P[0].as<u64>();
+        const Impl &cm = m;
+        auto launch = [&](auto real) {
+            using Real = decltype(real);
+            const KeygenParams<Real> &prm = [&]() -> const KeygenParams<Real> & {
+                if constexpr (sizeof(Real) == 4) return cm.kpf;
+                else return cm.kpd;
+            }();
+            if (m.cfg.hilbert)
+                forest::keygenKernel<Real, Curve::Hilbert><<<grid, forest::kThreads, 0, s>>>(
+                    m.systemsD.as<forest::System>(), m.tileSys.as<u32>(), m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
+                    m.numTiles, prm, keys, m.hist.as<u32>()), noteLaunch();
+            else
+                forest::keygenKernel<Real, Curve::Morton><<<grid, forest::kThreads, 0, s>>>(
+                    m.systemsD.as<forest::System>(), m.tileSys.as<u32>(), m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
+                    m.numTiles, prm, keys, m.hist.as<u32>()), noteLaunch();
+        };
+        if (m.cfg.real == 0) launch(float{});
+        else launch(double{});
+        forest::binsKernel<<<unsigned(m.S), sort::kRadix, 0, s>>>(m.systemsD.as<forest::System>(), m.S,
+                                                                  m.hist.as<u32>(), m.bins.as<u32>()), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        setForestPassSmem();
+        u64 *k[2] = {m.P[0].as<u64>(), m.P[1].as<u64>()};
+        u32 *v[2] = {m.Perm[0].as<u32>(), m.Perm[1].as<u32>()};
+        for (int p = 0; p < sort::kMaxPasses; ++p)
+        {
+            const int in = p & 1, out = in ^ 1;
+            const sort::SegmentTiles tiles{m.tileSys.as<u32>(),      m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
+                                           m.segFirstTile.as<u32>(), m.segBase.as<u32>(),
+                                           m.bins.as<u32>() + size_t(p) * m.S * sort::kRadix};
+            sort::segmentOnesweepKernel<<<m.numTiles, sort::kThreads, sort::passSmem(), s>>>(
+                tiles, k[in], p == 0 ? nullptr : v[in], k[out], v[out], p * sort::kRadixBits,
+                m.tileCounters.as<u32>() + p, m.status.as<u64>() + size_t(p) * m.numTiles * sort::kRadix,
+                &m.st.as<forest::State>()->error), noteLaunch();
+            AOT_LAUNCH_CHECK();
+        }
+        // eight passes end in buffer 0
+    }
+    forest::activeKernel<<<gridFor(size_t(m.S), 256), 256, 0, s>>>(m.bufs()), noteLaunch();
+    AOT_LAUNCH_CHECK();
+}
+
+// One decision round (build) or fixed pass (update) over all systems.
+void ForestEngine::pass(bool build, const unsigned char *frozenDevice)
+{
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    const forest::Bufs f = m.bufs();
+    const unsigned sysGrid = gridFor(size_t(m.S), 256);
+    const unsigned wide = unsigned(smCount()) * 8u;
+    forest::beginPassKernel<<<sysGrid, 256, 0, s>>>(f, frozenDevice), noteLaunch();
+    AOT_CHECK(cudaMemsetAsync(m.scanStatus.p, 0, (m.scanTiles + 1) * 8, s));
+    forest::decideKernel<<<wide, forest::kThreads, 0, s>>>(f, m.cfg.bucket), noteLaunch();
+    if (build) forest::checkKernel<true><<<sysGrid, 256, 0, s>>>(f), noteLaunch();
+    else forest::checkKernel<false><<<sysGrid, 256, 0, s>>>(f), noteLaunch();
+    forest::scanKernel<<<unsigned(m.scanTiles), rb::kScanThreads, 0, s>>>(f), noteLaunch();
+    AOT_LAUNCH_CHECK();
+    if (build)
+    {
+        // the proposal decides the room the scatter needs
+        AOT_CHECK(cudaMemcpyAsync(m.hst, m.st.p, sizeof(forest::State), cudaMemcpyDeviceToHost, s));
+        AOT_CHECK(cudaStreamSynchronize(s));
+        if (m.hst->error) throw std::runtime_error("forest: a device scan gave up waiting (bounded look-back)");
+        if (!m.hst->changed) return;
+        ensurePhysical(size_t(m.hst->proposal));
+    }
+    const forest::Bufs g = m.bufs();
+    forest::scatterKernel<<<wide, forest::kThreads, 0, s>>>(g), noteLaunch();
+    if (build) forest::commitKernel<true><<<1, 256, 0, s>>>(g), noteLaunch();
+    else forest::commitKernel<false><<<1, 256, 0, s>>>(g), noteLaunch();
+    forest::refreshKernel<false><<<wide, forest::kThreads, 0, s>>>(g), noteLaunch();
+    AOT_LAUNCH_CHECK();
+}
+
+// Host mirrors of the device state; model: also the state readback of each
+// system's capacity model (as doBuffersNeedResize of a single tree).
+void ForestEngine::readState(bool model)
+{
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    AOT_CHECK(cudaMemcpyAsync(m.hst, m.st.p, sizeof(forest::State), cudaMemcpyDeviceToHost, s));
+    AOT_CHECK(cudaMemcpyAsync(m.hsys, m.sys.p, size_t(m.S) * sizeof(forest::SysState), cudaMemcpyDeviceToHost, s));
+    AOT_CHECK(cudaStreamSynchronize(s));
+    if (m.hst->error) throw std::runtime_error("forest: a device scan gave up waiting (bounded look-back)");
+    if (model)
+        for (int i = 0; i < m.S; ++i) m.capModel[i].stateRead(size_t(std::max(m.hsys[i].leaves, 0)));
+}
+
+void ForestEngine::build()
+{
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    AOT_CHECK(cudaStreamSynchronize(s));
+    for (auto &c : m.capModel) c.buildStart();
+    sortParticles();
+    ensurePhysical(size_t(2) * m.S);
+    const forest::Bufs f = m.bufs();
+    forest::initKernel<<<gridFor(size_t(m.S), 256), 256, 0, s>>>(f), noteLaunch();
+    AOT_LAUNCH_CHECK();
+    for (unsigned r = 0; r < m.cfg.maxDepth; ++r)
+    {
+        pass(true, nullptr);
+        if (!m.hst->changed) break;
+    }
+    // per-system leafCapacity from each system's round history
+    readState(false);
+    std::vector<long long> hist(size_t(std::max(m.cfg.maxDepth, 1u)) * m.S);
+    AOT_CHECK(cudaMemcpy(hist.data(), m.history.p, hist.size() * sizeof(long long), cudaMemcpyDeviceToHost));
+    size_t entries = 0;
+    for (int i = 0; i < m.S; ++i)
+    {
+        forest::SysState &ss = m.hsys[i];
+        std::vector<long long> rounds(size_t(ss.iteration));
+        for (int r = 0; r < ss.iteration; ++r) rounds[r] = hist[size_t(r) * m.S + i];
+        const size_t leaves = size_t(ss.leaves);
+        const size_t cap = m.capModel[i].finishBuild(rounds.data(), rounds.size(), leaves);
+        const size_t maxLeaves = (size_t(std::numeric_limits<int>::max()) - 1) / 8 * 7 + 1;
+        if (cap > maxLeaves) throw std::length_error("adaptive_octree: buffer capacity exceeds node index range");
+        m.capModel[i].prepare(cap);
+        m.leafCap[i] = cap;
+        ss.cap = int(cap);
+        ss.needsResize = 0;
+        entries += cap + 1;
+    }
+    AOT_CHECK(cudaMemcpyAsync(m.sys.p, m.hsys, size_t(m.S) * sizeof(forest::SysState), cudaMemcpyHostToDevice, s));
+    ensurePhysical(entries);
+    forest::materializeKernel<<<unsigned(smCount()) * 8u, 256, 0, s>>>(m.bufs()), noteLaunch();
+    AOT_LAUNCH_CHECK();
+    m.built = true;
+    readState(true);
+}
+
+void ForestEngine::update(const unsigned char *frozen)
+{
+    Impl &m = *m_;
+    if (!m.built) throw std::logic_error("adaptive_octree: call build() before update()");
+    cudaStream_t s = m.cfg.stream;
+    if (frozen)
+        AOT_CHECK(cudaMemcpyAsync(m.frozen.p, frozen, size_t(m.S), cudaMemcpyHostToDevice, s));
+    else
+        AOT_CHECK(cudaMemsetAsync(m.frozen.p, 0, size_t(m.S), s));
+    sortParticles();
+    const forest::Bufs f = m.bufs();
+    const unsigned wide = unsigned(smCount()) * 8u;
+    forest::refreshKernel<true><<<wide, forest::kThreads, 0, s>>>(f), noteLaunch();
+    AOT_LAUNCH_CHECK();
+    for (unsigned i = 0; i < m.cfg.iterations; ++i) pass(false, m.frozen.as<unsigned char>());
+    forest::materializeKernel<<<wide, 256, 0, s>>>(f), noteLaunch();
+    AOT_LAUNCH_CHECK();
+}
+
+bool ForestEngine::needsResize()
+{
+    Impl &m = *m_;
+    if (!m.built) return false;
+    readState(true);
+    for (int i = 0; i < m.S; ++i)
+        if (m.hsys[i].needsResize) return true;
+    return false;
+}
+
+void ForestEngine::resizeBuffers()
+{
+    Impl &m = *m_;
+    if (!m.built) throw std::logic_error("adaptive_octree: call build() before resizeBuffers()");
+    readState(true);
+    size_t entries = 0;
+    for (int i = 0; i < m.S; ++i)
+    {
+        forest::SysState &ss = m.hsys[i];
+        if (ss.needsResize)
+        {
+            // resizeBuffers (octree.cu:539-551): 25% more capacity
+            const size_t cap = m.leafCap[i] + (m.leafCap[i] + 3) / 4;
+            const size_t maxLeaves = (size_t(std::numeric_limits<int>::max()) - 1) / 8 * 7 + 1;
+            if (cap > maxLeaves) throw std::length_error("adaptive_octree: buffer capacity exceeds node index range");
+            m.capModel[i].prepare(cap);
+            m.leafCap[i] = cap;
+            ss.cap = int(cap);
+            ss.needsResize = 0;
+        }
+        entries += m.leafCap[i] + 1;
+    }
+    ensurePhysical(entries);
+    AOT_CHECK(cudaMemcpyAsync(m.sys.p, m.hsys, size_t(m.S) * sizeof(forest::SysState), cudaMemcpyHostToDevice,
+                              m.cfg.stream));
+    AOT_CHECK(cudaStreamSynchronize(m.cfg.stream));
+}
+
+void ForestEngine::buffer(int s, int which, const void **ptr, size_t *len) const
+{
+    const Impl &m = *m_;
+    if (s < 0 || s >= m.S) throw std::invalid_argument("forest: system index out of range");
+    const forest::System &sy = m.systems[s];
+    const forest::SysState &ss = m.hsys[s];
+    const int a = m.hst->activeBuffer;
+    switch (which)
+    {
+    case ParticleKeys:
+        *ptr = m.P[0].as<u64>() + sy.base;
+        *len = sy.n;
+        break;
+    case Perm:
+        *ptr = m.Perm[0].as<u32>() + sy.base;
+        *len = sy.n;
+        break;
+    case Cornerstone:
+        *ptr = m.K[a].as<u64>() + ss.start;
+        *len = m.built ? size_t(ss.leaves) + 1 : 0;
+        break;
+    case LeafCounts:
+        *ptr = m.N.as<u32>() + ss.start;
+        *len = m.built ? size_t(ss.leaves) : 0;
+        break;
+    default:
+        throw std::invalid_argument("forest: unknown buffer");
+    }
+}
+
+ForestEngine::SystemInfo ForestEngine::info(int s) const
+{
+    const Impl &m = *m_;
+    if (s < 0 || s >= m.S) throw std::invalid_argument("forest: system index out of range");
+    const forest::SysState &ss = m.hsys[s];
+    return SystemInfo{m.systems[s].n, ss.active, m.built ? size_t(ss.leaves) : 0, m.leafCap[s],
+                      ss.needsResize != 0};
+}
+}  // namespace aot

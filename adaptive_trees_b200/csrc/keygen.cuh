@@ -47,7 +47,7 @@ constexpr int kKeygenThreads = 256;
 
 // Vec: particles per thread step (4 for float4, 2 for double2, 1 scalar).
 template <class Real, Curve C, int Vec>
-__global__ void __launch_bounds__(kKeygenThreads)
+static __global__ void __launch_bounds__(kKeygenThreads)
     keygenKernel(const Real *__restrict__ x, const Real *__restrict__ y, const Real *__restrict__ z, size_t n,
                  const KeygenParams<Real> prm, u64 *__restrict__ keys, u32 *__restrict__ hist, int histPasses)
 {

@@ -75,7 +75,7 @@ inline size_t scratchBytes(size_t n)
 }
 
 // Histogram of the digits of keys[0, n) for passes covering [beginBit, endBit).
-__global__ void __launch_bounds__(kThreads) histogramKernel(const u64 *__restrict__ keys, size_t n, int beginBit,
+static __global__ void __launch_bounds__(kThreads) histogramKernel(const u64 *__restrict__ keys, size_t n, int beginBit,
                                                              int passes, u32 *__restrict__ hist, int endBit = 64)
 {
     __shared__ u32 sh[kMaxPasses][kRadix];
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kThreads) histogramKernel(const u64 *__restric
 }
 
 // Exclusive scan of each pass' 256 digit counts.
-__global__ void __launch_bounds__(kRadix) binsKernel(const u32 *__restrict__ hist, u32 *__restrict__ bins, int passes)
+static __global__ void __launch_bounds__(kRadix) binsKernel(const u32 *__restrict__ hist, u32 *__restrict__ bins, int passes)
 {
     __shared__ u32 s[kRadix];
     const int d = threadIdx.x;
@@ -152,12 +152,46 @@ __device__ __forceinline__ unsigned peerLanes(unsigned digit, int bits, unsigned
     return peers;
 }
 
-// One onesweep pass over keys[0, n): digit at bit `shift` (`bits` wide).
-// valsIn == nullptr means values are the input indices (first pass).
-__global__ void __launch_bounds__(kThreads, 3)
-    onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
-                   u32 *__restrict__ valsOut, size_t n, int shift, const u32 *__restrict__ bins, u32 *tileCounter,
-                   u64 *status, int *error, int bits = kRadixBits)
+// Tile geometry of a pass over one contiguous key array keys[0, n).  The
+// accessors are cheap and recomputed where used, so that nothing extra stays
+// live in registers across the pass.
+struct ContiguousTiles
+{
+    size_t n;
+    const u32 *bins;  // [kRadix] global start of each digit
+    // the tile's keys are [base(t), min(base(t) + kTile, end(t)))
+    __device__ __forceinline__ size_t base(size_t tile) const { return tile * kTile; }
+    __device__ __forceinline__ size_t end(size_t) const { return n; }
+    // the tile publishes an inclusive prefix without look-back
+    __device__ __forceinline__ bool chainStart(size_t tile) const { return tile == 0; }
+    __device__ __forceinline__ const u32 *digitBase(size_t) const { return bins; }
+    // generated first-pass value of the key at global index i: i - valueOffset
+    __device__ __forceinline__ u32 valueOffset(size_t) const { return 0; }
+};
+
+// Tile geometry of a segmented pass (the systems of a forest): tile t holds
+// the keys [tileBegin[t], tileEnd[t]) of segment tileSeg[t] (at most kTile,
+// never straddling segments); a look-back chain ends at the segment's first
+// tile; digit starts are per segment, and generated values are indices within
+// the segment.
+struct SegmentTiles
+{
+    const u32 *tileSeg, *tileBegin, *tileEnd, *segFirstTile, *segBase;
+    const u32 *bins;  // [segments][kRadix] global start of each digit of this pass
+    __device__ __forceinline__ size_t base(size_t tile) const { return tileBegin[tile]; }
+    __device__ __forceinline__ size_t end(size_t tile) const { return tileEnd[tile]; }
+    __device__ __forceinline__ bool chainStart(size_t tile) const { return u32(tile) == segFirstTile[tileSeg[tile]]; }
+    __device__ __forceinline__ const u32 *digitBase(size_t tile) const { return bins + size_t(tileSeg[tile]) * kRadix; }
+    __device__ __forceinline__ u32 valueOffset(size_t tile) const { return segBase[tileSeg[tile]]; }
+};
+
+// One onesweep pass: digit at bit `shift` (`bits` wide) of the tiles of
+// `tiles`.  valsIn == nullptr means values are generated (first pass).
+template <class Tiles>
+__device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__restrict__ keysIn,
+                                             const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
+                                             u32 *__restrict__ valsOut, int shift, u32 *tileCounter, u64 *status,
+                                             int *error, int bits)
 {
     const unsigned dmask = (1u << bits) - 1;
     extern __shared__ __align__(16) unsigned char smemRaw[];
@@ -168,7 +202,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     if (tid == 0) sm.tile = atomicAdd(tileCounter, 1u);
     __syncthreads();
     const size_t tile = sm.tile;
-    const size_t tileBase = tile * kTile;
+    const size_t tileBase = tiles.base(tile);
     const size_t warpBase = tileBase + size_t(warp) * (32 * kItems);
 
     u64 key[kItems];
@@ -176,7 +210,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     for (int i = 0; i < kItems; ++i)
     {
         const size_t idx = warpBase + size_t(i) * 32 + lane;
-        key[i] = idx < n ? __ldcs(keysIn + idx) : 0ull;
+        key[i] = idx < tiles.end(tile) ? __ldcs(keysIn + idx) : 0ull;
     }
     // Rank within the warp, items in memory order (item-major, lane-minor):
     // the lowest lane of each digit group adds the group size to the warp's
@@ -188,7 +222,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     for (int i = 0; i < kItems; ++i)
     {
         const size_t idx = warpBase + size_t(i) * 32 + lane;
-        const bool valid = idx < n;
+        const bool valid = idx < tiles.end(tile);
         const unsigned validMask = __ballot_sync(0xffffffffu, valid);
         const unsigned d = unsigned(key[i] >> shift) & dmask;
         const unsigned peers = peerLanes(d, bits, validMask);
@@ -215,12 +249,12 @@ __global__ void __launch_bounds__(kThreads, 3)
         }
         sm.count[d] = acc;
     }
-    // Publish this tile's digit counts early (tile 0 publishes final prefixes),
-    // then build the tile-local order; the look-back comes last so earlier
-    // tiles have had time to publish inclusive prefixes.
+    // Publish this tile's digit counts early (a chain's first tile publishes
+    // final prefixes), then build the tile-local order; the look-back comes
+    // last so earlier tiles have had time to publish inclusive prefixes.
     {
         const int d = tid;
-        stRelaxed(status + tile * kRadix + d, (tile == 0 ? kFlagPrefix : kFlagAgg) | u64(sm.count[d]));
+        stRelaxed(status + tile * kRadix + d, (tiles.chainStart(tile) ? kFlagPrefix : kFlagAgg) | u64(sm.count[d]));
         // exclusive scan of the tile's digit counts -> local starts
         u32 v = sm.count[d];
 #pragma unroll
@@ -243,13 +277,13 @@ __global__ void __launch_bounds__(kThreads, 3)
     for (int i = 0; i < kItems; ++i)
     {
         const size_t idx = warpBase + size_t(i) * 32 + lane;
-        if (idx < n)
+        if (idx < tiles.end(tile))
         {
             const unsigned d = unsigned(key[i] >> shift) & dmask;
             const u32 r = (rank2[i >> 1] >> ((i & 1) * 16)) & 0xffffu;
             const u32 pos = sm.localStart[d] + sm.warpHist[warp][d] + r;
             sm.keys[pos] = key[i];
-            sm.vals[pos] = valsIn ? __ldcs(valsIn + idx) : u32(idx);
+            sm.vals[pos] = valsIn ? __ldcs(valsIn + idx) : u32(idx) - tiles.valueOffset(tile);
         }
     }
     // Look-back: global start of each digit for this tile.
@@ -257,10 +291,11 @@ __global__ void __launch_bounds__(kThreads, 3)
         const int d = tid;
         const u64 total = sm.count[d];
         u64 excl = 0;
-        if (tile > 0)
+        if (!tiles.chainStart(tile))
         {
             // Walk back over earlier tiles, eight status words per round trip,
-            // summing aggregates until an inclusive prefix is found.
+            // summing aggregates until an inclusive prefix is found (the
+            // chain's first tile always holds one).
             long long j = (long long)tile - 1;
             unsigned spins = 0;
             while (j >= 0)
@@ -297,10 +332,10 @@ __global__ void __launch_bounds__(kThreads, 3)
             stRelaxed(status + tile * kRadix + d, kFlagPrefix | (excl + total));
         }
         // modulo 2^32: gstart + j is exact for every key of digit d
-        sm.gstart[d] = bins[d] + u32(excl) - sm.localStart[d];
+        sm.gstart[d] = tiles.digitBase(tile)[d] + u32(excl) - sm.localStart[d];
     }
     __syncthreads();
-    const size_t remain = n - tileBase;
+    const size_t remain = tiles.end(tile) - tileBase;
     const int valid = remain < size_t(kTile) ? int(remain) : kTile;
 #pragma unroll 4
     for (int j = tid; j < valid; j += kThreads)
@@ -311,6 +346,26 @@ __global__ void __launch_bounds__(kThreads, 3)
         keysOut[out] = k;
         valsOut[out] = sm.vals[j];
     }
+}
+
+// One onesweep pass over keys[0, n): digit at bit `shift` (`bits` wide).
+// valsIn == nullptr means values are the input indices (first pass).
+static __global__ void __launch_bounds__(kThreads, 3)
+    onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
+                   u32 *__restrict__ valsOut, size_t n, int shift, const u32 *__restrict__ bins, u32 *tileCounter,
+                   u64 *status, int *error, int bits = kRadixBits)
+{
+    onesweepTile(ContiguousTiles{n, bins}, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);
+}
+
+// One onesweep pass over the segments of a forest: every segment is sorted
+// on its own (stable within the segment), in place in the global arrays.
+static __global__ void __launch_bounds__(kThreads, 3)
+    segmentOnesweepKernel(SegmentTiles tiles, const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn,
+                          u64 *__restrict__ keysOut, u32 *__restrict__ valsOut, int shift, u32 *tileCounter,
+                          u64 *status, int *error)
+{
+    onesweepTile(tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, kRadixBits);
 }
 
 inline size_t passSmem() { return sizeof(SharedPass); }

@@ -349,7 +349,7 @@ struct OctreeOp
 };
 
 template <bool NF>
-__global__ void __launch_bounds__(kScanThreads) octDecideScanKernel(TreeBufs tb, unsigned bucket)
+static __global__ void __launch_bounds__(kScanThreads) octDecideScanKernel(TreeBufs tb, unsigned bucket)
 {
     const int a = tb.st->activeBuffer;
     const OctreeOp<NF> op{tb.k(a), tb.b(a), tb.nf(a), tb.g(a), bucket};
@@ -437,7 +437,7 @@ __device__ __forceinline__ void octScatterLeaf(const TreeBufs &tb, DeviceState *
 // strides over the leaves 32 at a time, so every lane takes part in the
 // warp-aggregated appends.
 template <bool NF>
-__global__ void __launch_bounds__(kScatterThreads)
+static __global__ void __launch_bounds__(kScatterThreads)
     octScatterKernel(TreeBufs tb, long long limit, int mode, long long *history)
 {
     DeviceState *st = tb.st;
@@ -485,7 +485,7 @@ __device__ __forceinline__ u32 lowerFrom(const KeyIndex &idx, u32 lo, u64 v)
 // the end sentinel).  This is the whole count refresh of LeafCount trees: the
 // counts are differences of B.
 template <bool All>
-__global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBufs tb, KeyIndex idx)
+static __global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBufs tb, KeyIndex idx)
 {
     DeviceState *st = tb.st;
     if (halted(st)) return;
@@ -741,7 +741,7 @@ __device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, c
 // leaves whose group is incomplete or empty needs no search (NF 0; an empty
 // parent can always merge).
 template <bool Hilbert, bool All>
-__global__ void __launch_bounds__(kRefreshThreads)
+static __global__ void __launch_bounds__(kRefreshThreads)
     octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h)
 {
     __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8], sPos[27 * 8];
@@ -850,7 +850,7 @@ __global__ void __launch_bounds__(kRefreshThreads)
 }
 
 // N[i] = B[i+1] - B[i] on the active buffer.
-__global__ void materializeCountsKernel(TreeBufs tb)
+static __global__ void materializeCountsKernel(TreeBufs tb)
 {
     const DeviceState *st = tb.st;
     const int a = st->activeBuffer, L = st->numLeaves;
@@ -882,14 +882,14 @@ struct BinaryOp
     }
 };
 
-__global__ void __launch_bounds__(kScanThreads) binDecideScanKernel(TreeBufs tb, unsigned bucket, unsigned maxDepth)
+static __global__ void __launch_bounds__(kScanThreads) binDecideScanKernel(TreeBufs tb, unsigned bucket, unsigned maxDepth)
 {
     const int a = tb.st->activeBuffer;
     const BinaryOp op{tb.k(a), tb.b(a), bucket, maxDepth};
     decideScan(op, tb);
 }
 
-__global__ void __launch_bounds__(kScatterThreads)
+static __global__ void __launch_bounds__(kScatterThreads)
     binScatterKernel(TreeBufs tb, long long limit, int mode)
 {
     DeviceState *st = tb.st;
@@ -940,7 +940,7 @@ __global__ void __launch_bounds__(kScatterThreads)
 // reference counts over the active prefix of P (binaryLeafCountsKernel,
 // kdtree3d_rebalance.cuh:127-138); lower bounds of keys below 2^63 agree.
 template <bool All>
-__global__ void binRefreshKernel(TreeBufs tb, KeyIndex idx)
+static __global__ void binRefreshKernel(TreeBufs tb, KeyIndex idx)
 {
     DeviceState *st = tb.st;
     if (halted(st)) return;
@@ -958,7 +958,7 @@ __global__ void binRefreshKernel(TreeBufs tb, KeyIndex idx)
 
 // Reset at the start of update() (resetRebalanceStateKernel,
 // octree_rebalance.cuh:62-73): changed, converged and the active count.
-__global__ void resetForUpdateKernel(DeviceState *st, const u64 *P, size_t n)
+static __global__ void resetForUpdateKernel(DeviceState *st, const u64 *P, size_t n)
 {
     st->changed = 0;
     st->converged = 0;
@@ -967,14 +967,14 @@ __global__ void resetForUpdateKernel(DeviceState *st, const u64 *P, size_t n)
 }
 
 // Per-pass reset of the flags the decision accumulates.
-__global__ void beginPassKernel(DeviceState *st)
+static __global__ void beginPassKernel(DeviceState *st)
 {
     st->changed = 0;
     st->dirtyCount = 0;
 }
 
 // Sample every kSampleStride-th key for KeyIndex.
-__global__ void sampleKeysKernel(const u64 *P, size_t n, u64 *sample, size_t ns)
+static __global__ void sampleKeysKernel(const u64 *P, size_t n, u64 *sample, size_t ns)
 {
     for (size_t j = blockIdx.x * size_t(blockDim.x) + threadIdx.x; j < ns; j += size_t(gridDim.x) * blockDim.x)
         sample[j] = P[j << kSampleShift];

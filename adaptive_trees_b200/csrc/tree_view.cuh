@@ -76,7 +76,7 @@ __device__ __forceinline__ unsigned lcaLevel(u64 x, u64 y)
 
 // Stage 1 (classifyLeavesAndInternalsKernel, tree_view.cu:151-203).
 template <int b>
-__global__ void classifyKernel(const u64 *Kact0, const u64 *Kact1, DeviceState *st, int leafCap, ViewBufs v)
+static __global__ void classifyKernel(const u64 *Kact0, const u64 *Kact1, DeviceState *st, int leafCap, ViewBufs v)
 {
     __shared__ int sHist[64];
     if (threadIdx.x < 64) sHist[threadIdx.x] = 0;
@@ -118,7 +118,7 @@ __global__ void classifyKernel(const u64 *Kact0, const u64 *Kact1, DeviceState *
 
 // Stage 2 (buildLevelMetadataKernel, tree_view.cu:211-275), one thread.
 template <int b>
-__global__ void metadataKernel(DeviceState *st, int leafCap, ViewBufs v)
+static __global__ void metadataKernel(DeviceState *st, int leafCap, ViewBufs v)
 {
     const int L = st->numLeaves <= leafCap ? st->numLeaves : 0;
     if (L == 0) return;
@@ -151,7 +151,7 @@ __global__ void metadataKernel(DeviceState *st, int leafCap, ViewBufs v)
 // Stages 3-5: internal starts/levels in (level, SFC) order and layout keys
 // (makeInternalLayoutKeysKernel, tree_view.cu:301-339).
 template <int b>
-__global__ void layoutKeysKernel(const u64 *lvSortedKeys, const u32 *lvSortedVals, int intCap, ViewBufs v)
+static __global__ void layoutKeysKernel(const u64 *lvSortedKeys, const u32 *lvSortedVals, int intCap, ViewBufs v)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= intCap) return;
@@ -178,7 +178,7 @@ __global__ void layoutKeysKernel(const u64 *lvSortedKeys, const u32 *lvSortedVal
 }
 
 // materializeInternalLayoutKernel (tree_view.cu:340-358)
-__global__ void materializeKernel(const u64 *laySortedKeys, const u32 *laySortedVals, int intCap, ViewBufs v)
+static __global__ void materializeKernel(const u64 *laySortedKeys, const u32 *laySortedVals, int intCap, ViewBufs v)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= intCap || laySortedKeys[j] == ~u64(0)) return;
@@ -207,7 +207,7 @@ __device__ __forceinline__ int finalNodeIndex(unsigned level, u64 start, const V
 
 // Stage 6 (buildInternalNodesKernel, tree_view.cu:407-482)
 template <int b>
-__global__ void internalNodesKernel(DeviceState *st, int leafCap, int intCap, KeyIndex idx, int counts, ViewBufs v)
+static __global__ void internalNodesKernel(DeviceState *st, int leafCap, int intCap, KeyIndex idx, int counts, ViewBufs v)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int L = st->numLeaves <= leafCap ? st->numLeaves : 0;
@@ -237,7 +237,7 @@ __global__ void internalNodesKernel(DeviceState *st, int leafCap, int intCap, Ke
 
 // Stage 7 (buildLeafNodesKernel, tree_view.cu:488-538)
 template <int b>
-__global__ void leafNodesKernel(const u64 *K0, const u64 *K1, const u32 *B0, const u32 *B1, DeviceState *st,
+static __global__ void leafNodesKernel(const u64 *K0, const u64 *K1, const u32 *B0, const u32 *B1, DeviceState *st,
                                 int leafCap, int counts, ViewBufs v)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -264,7 +264,7 @@ __global__ void leafNodesKernel(const u64 *K0, const u64 *K1, const u32 *B0, con
 
 // Particle mapping (fillSfcParticleIndexKernel, tree_view.cu:542-562): the leaf
 // holding sorted particle p is the last leaf whose begin index is <= p.
-__global__ void mappingKernel(const u32 *B0, const u32 *B1, DeviceState *st, int leafCap, size_t n, ViewBufs v)
+static __global__ void mappingKernel(const u32 *B0, const u32 *B1, DeviceState *st, int leafCap, size_t n, ViewBufs v)
 {
     const size_t p = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
     if (p >= n) return;
@@ -288,7 +288,7 @@ __global__ void mappingKernel(const u32 *B0, const u32 *B1, DeviceState *st, int
     v.pmap[p] = u64((long long)v.leafToNode[lo - 1]);
 }
 
-__global__ void flagResizeKernel(DeviceState *st) { st->needsResize = 1; }
+static __global__ void flagResizeKernel(DeviceState *st) { st->needsResize = 1; }
 
 }  // namespace tv
 }  // namespace aot

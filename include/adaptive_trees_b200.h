@@ -179,6 +179,54 @@ AO_API ao_status ao_sort_pairs_noalloc(const unsigned long long *keys_in, unsign
                                        const unsigned *values_in, unsigned *values_out, size_t n, int begin_bit,
                                        int end_bit, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Batched octrees ("forest").  The reference has no batch API: its callers
+ * loop over one Tree<Real, Octree> per particle system.  A batch holds many
+ * independent systems, each with its own borrowed device coordinates and
+ * count, and one shared config (octree, LeafCount, Morton or Hilbert, no
+ * views).  Every system gets exactly what a Tree built and updated on that
+ * system alone would hold: particleKeys_d, perm_d (indices within the
+ * system), cornerstone_d, leafCounts_d, leafCapacity and needsResize.  The
+ * work of all systems runs in the same kernel launches (a segmented sort and
+ * one decision/scan/scatter per round or pass over all systems' leaves), so
+ * many small systems are not bound by launch latency.
+ * ------------------------------------------------------------------------- */
+typedef struct ao_batch ao_batch;
+
+typedef struct ao_batch_system_info
+{
+    size_t num_particles;
+    size_t num_active_particles;
+    size_t num_leaves;
+    size_t leaf_capacity;
+    int needs_resize;
+} ao_batch_system_info;
+
+/* One Tree<Real, Octree>(x[s], y[s], z[s], counts[s], config) per system s
+ * (tree.hpp:25), all on `stream`.  AO_ERR_INVALID_ARGUMENT for NFCount, views,
+ * a binary kind or more than 2^32 - 1 particles in total. */
+AO_API ao_status ao_batch_create(int real_type, int num_systems, const void *const *x, const void *const *y,
+                                 const void *const *z, const size_t *counts, const ao_config *config, void *stream,
+                                 ao_batch **out);
+AO_API ao_status ao_batch_destroy(ao_batch *batch);
+/* build() of every system (octree.cu:427-457). */
+AO_API ao_status ao_batch_build(ao_batch *batch);
+/* update() of every system (octree.cu:459-496); capturable when frozen is
+ * NULL.  frozen: optional host array of num_systems bytes; a system marked
+ * non-zero keeps its tree, as if update() were not called on it (for the
+ * resize-and-retry step of the systems that needed a resize). */
+AO_API ao_status ao_batch_update(ao_batch *batch, const unsigned char *frozen);
+/* doBuffersNeedResize() of every system; *any = 1 if one of them needs it. */
+AO_API ao_status ao_batch_needs_resize(ao_batch *batch, int *any);
+/* resizeBuffers() of every system that needs a resize. */
+AO_API ao_status ao_batch_resize_buffers(ao_batch *batch);
+/* New coordinate pointers of one system (same count). */
+AO_API ao_status ao_batch_set_coordinates(ao_batch *batch, int system, const void *x, const void *y, const void *z);
+/* Getter of one system: AO_BUF_PARTICLE_KEYS, AO_BUF_PERM, AO_BUF_CORNERSTONE
+ * or AO_BUF_LEAF_COUNTS; sizes as of the last build/needs_resize. */
+AO_API ao_status ao_batch_get_buffer(ao_batch *batch, int system, int which, const void **ptr, size_t *size);
+AO_API ao_status ao_batch_get_info(ao_batch *batch, int system, ao_batch_system_info *info);
+
 /* Message of the last failed call on this thread ("" if none). */
 AO_API const char *ao_last_error(void);
 

@@ -3,6 +3,8 @@ and exports every entry point the C header declares."""
 import ctypes
 import os
 import re
+import subprocess
+import sys
 
 import pytest
 
@@ -43,8 +45,10 @@ def test_library_exports_nothing_else(lib):
 
 
 def test_last_error_is_empty_string_initially(lib):
-    lib.ao_last_error.restype = ctypes.c_char_p
-    assert lib.ao_last_error() == b""
+    """In a fresh process (other tests of this session leave messages behind)."""
+    code = ("import ctypes, sys; L = ctypes.CDLL(sys.argv[1]); L.ao_last_error.restype = ctypes.c_char_p; "
+            "assert L.ao_last_error() == b''")
+    subprocess.run([sys.executable, "-c", code, lib._name], check=True, timeout=120)
 
 
 def test_capi_validates_arguments_without_a_gpu(lib):
