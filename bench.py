@@ -240,6 +240,139 @@ def build_only(args):
     return 0
 
 
+C4_SYSTEMS = 512
+C4_METRIC = "particles/s (batched octree build, 512 systems, fp32, Morton, LeafCount 64)"
+C4_WORKLOAD = ("512 independent octrees, sizes floor(10^U(3,6)) (seed 4), fp32 uniform or Plummer (coin flip per "
+               "system), Morton keys, LeafCount 64; one batched build and 10 graph-replayed batched updates "
+               "(N(0,1e-3) jitter) against a loop of plain per-tree build()/update() on the same inputs")
+
+
+def c4_systems():
+    rng = np.random.default_rng(4)
+    sizes = np.floor(10.0 ** rng.uniform(3.0, 6.0, C4_SYSTEMS)).astype(np.int64)
+    plum = rng.random(C4_SYSTEMS) < 0.5
+    return sizes, plum
+
+
+def batched_bench(args):
+    """C4: Batch (one set of launches for all systems) against a loop of plain trees."""
+    import torch
+
+    import adaptive_trees_b200 as ab
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.Stream(device=dev)
+    sizes, plum = c4_systems()
+    total = int(sizes.sum())
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    host = [np.empty(total, np.float32) for _ in range(3)]
+    for k in range(C4_SYSTEMS):
+        n = int(sizes[k])
+        if plum[k]:
+            xyz = plummer(n, 100 + k)
+        else:
+            r = np.random.default_rng(100 + k)
+            xyz = tuple(r.random(n, dtype=np.float32) for _ in range(3))
+        for a in range(3):
+            host[a][offs[k]:offs[k + 1]] = xyz[a]
+    allc = [torch.from_numpy(h).to(dev) for h in host]
+    views = [[c[offs[k]:offs[k + 1]] for c in allc] for k in range(C4_SYSTEMS)]
+    cfg = ab.TreeConfig(maxParticlesPerLeaf=64)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn):
+        a, b = ev(), ev()
+        a.record(s)
+        fn()
+        b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    names = ("particleKeys_d", "perm_d", "cornerstone_d", "leafCounts_d")
+
+    def identical(batch, trees):
+        batch.doBuffersNeedResize()
+        for k, t in enumerate(trees):
+            t.doBuffersNeedResize()
+            for nm in names:
+                a, b = batch.get(k, nm), t.get(nm)
+                if a.numel() != b.numel() or not torch.equal(a.view(torch.uint8), b.view(torch.uint8)):
+                    return False
+        return True
+
+    with torch.cuda.stream(s):
+        batch = ab.Batch([v[0] for v in views], [v[1] for v in views], [v[2] for v in views], cfg, stream=s)
+        trees = [ab.Tree(0, *v, cfg, stream=s) for v in views]
+        launches = lambda: trees[0].info().kernel_launches  # noqa: E731  (process-wide counter)
+        for _ in range(args.warmup):
+            batch.build()
+            for t in trees:
+                t.build()
+        l0 = launches()
+        b_build = [timed(batch.build) for _ in range(args.steps)]
+        batch_launches = launches() - l0
+
+        def plain_build():
+            for t in trees:
+                t.build()
+        p_build = [timed(plain_build) for _ in range(args.steps)]
+        same = identical(batch, trees)
+
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(77)
+
+        def jitter():
+            for c in allc:
+                c.add_(torch.randn(c.shape, generator=gen, device=dev, dtype=c.dtype) * 1e-3).clamp_(0.0, 0.99999994)
+
+        def capture():
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                batch.update()
+            return g
+
+        graph = capture()
+        b_upd, p_upd, resizes = [], [], 0
+
+        def plain_update():
+            for t in trees:
+                t.update()
+        for _ in range(10):
+            jitter()
+            s.synchronize()
+            b_upd.append(timed(graph.replay))
+            p_upd.append(timed(plain_update))
+            flags = [t.doBuffersNeedResize() for t in trees]
+            if batch.doBuffersNeedResize() or any(flags):
+                resizes += 1
+                for t, f in zip(trees, flags):
+                    if f:
+                        t.resizeBuffers()
+                        t.update()
+                batch.resizeBuffers()
+                batch.update(frozen=[not f for f in flags])
+                del graph
+                graph = capture()
+            same = same and identical(batch, trees)
+        del graph
+        batch.close()
+    bb, pb = statistics.median(b_build), statistics.median(p_build)
+    bu, pu = statistics.median(b_upd), statistics.median(p_upd)
+    line = {"metric": C4_METRIC, "value": total / (bb * 1e-3), "unit": "particles/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": bb, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": C4_WORKLOAD, "systems": C4_SYSTEMS, "particles": total,
+                       "largest": int(sizes.max()), "smallest": int(sizes.min()), "parallelism": "replicas1"},
+            "batched": {"build_ms": bb, "update_ms": bu, "build_value": total / (bb * 1e-3),
+                        "update_value": total / (bu * 1e-3), "update_graph_replayed": True,
+                        "build_launches": batch_launches // max(1, args.steps)},
+            "plain_loop": {"build_ms": pb, "update_ms": pu, "build_value": total / (pb * 1e-3),
+                           "update_value": total / (pu * 1e-3)},
+            "speedup": {"build": pb / bb, "update": pu / bu}, "identical_outputs": bool(same), "resizes": resizes}
+    print(json.dumps(line), flush=True)
+    return 0 if same else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -254,6 +387,8 @@ def main():
                     help="kernels: only key generation + the 64-bit pair sort of the workload's keys; "
                          "build: one build + one update of the workload's tree (small commands for ncu)")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--config", default="c2", choices=["c2", "c4"],
+                    help="c2: the 16Mi NFCount octree (headline); c4: 512 batched octrees vs a per-tree loop")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -261,6 +396,8 @@ def main():
         return kernels_only(args)
     if args.mode == "build":
         return build_only(args)
+    if args.config == "c4":
+        return batched_bench(args)
 
     import torch
     import torch.distributed as dist
