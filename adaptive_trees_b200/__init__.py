@@ -7,8 +7,9 @@ hand-written sm_100a kernel; importing `Tree` without the built library
 raises ImportError.
 """
 from .batch import Batch  # noqa: F401
+from .serve import Server, release_cached_memory  # noqa: F401
 from .tree import (BINARY, OCTREE, SfcKind, SplitCriterion, Tree, TreeConfig, TreeType, ViewConfig,  # noqa: F401
                    compute_sfc_keys, device_tensor)
 
-__all__ = ["Tree", "Batch", "TreeConfig", "ViewConfig", "TreeType", "SplitCriterion", "SfcKind", "OCTREE", "BINARY",
+__all__ = ["Tree", "Batch", "Server", "release_cached_memory", "TreeConfig", "ViewConfig", "TreeType", "SplitCriterion", "SfcKind", "OCTREE", "BINARY",
            "compute_sfc_keys", "device_tensor"]

@@ -42,6 +42,23 @@ class AoBatchSystemInfo(ctypes.Structure):
                 ("needs_resize", ci)]
 
 
+class AoRequest(ctypes.Structure):
+    _fields_ = [("op", ci), ("tree", ctypes.c_longlong), ("kind", ci), ("real_type", ci), ("config", AoConfig),
+                ("n", sz), ("x", vp), ("y", vp), ("z", vp), ("want_digest", ci)]
+
+
+class AoRequestResult(ctypes.Structure):
+    _fields_ = [("status", ci), ("queued_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("num_leaves", sz), ("resizes", ci), ("digest", ctypes.c_ulonglong)]
+
+
+class AoServeStats(ctypes.Structure):
+    _fields_ = [("submitted", sz), ("completed", sz), ("failed", sz), ("resident_trees", sz),
+                ("resident_bytes", sz), ("peak_bytes", sz), ("particles", ctypes.c_ulonglong),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("particles_per_s", ctypes.c_double), ("span_s", ctypes.c_double)]
+
+
 PROTOTYPES = {
     "ao_tree_create": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(AoConfig), vp, ctypes.POINTER(vp)],
     "ao_tree_destroy": [vp],
@@ -66,6 +83,14 @@ PROTOTYPES = {
     "ao_batch_set_coordinates": [vp, ci, vp, vp, vp],
     "ao_batch_get_buffer": [vp, ci, ci, ctypes.POINTER(vp), ctypes.POINTER(sz)],
     "ao_batch_get_info": [vp, ci, ctypes.POINTER(AoBatchSystemInfo)],
+    "ao_serve_create": [ci, sz, ctypes.POINTER(vp)],
+    "ao_serve_destroy": [vp],
+    "ao_serve_submit": [vp, ctypes.POINTER(AoRequest), ctypes.POINTER(ctypes.c_longlong)],
+    "ao_serve_wait": [vp, ctypes.c_longlong, ctypes.POINTER(AoRequestResult)],
+    "ao_serve_drain": [vp],
+    "ao_serve_get_stats": [vp, ctypes.POINTER(AoServeStats)],
+    "ao_serve_reset_stats": [vp],
+    "ao_release_cached_memory": [],
 }
 
 # n limit of ao_sort_pairs_noalloc (AO_SORT_PAIRS_NOALLOC_MAX_ITEMS)

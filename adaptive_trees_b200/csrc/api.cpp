@@ -8,6 +8,7 @@
 #include "adaptive_trees_b200.h"
 #include "engine.hpp"
 #include "forest.hpp"
+#include "serve.hpp"
 
 namespace adaptive_octree
 {
@@ -221,6 +222,11 @@ struct ao_tree
 struct ao_batch
 {
     std::unique_ptr<aot::ForestEngine> engine;
+};
+
+struct ao_server
+{
+    std::unique_ptr<aot::Server> server;
 };
 
 namespace
@@ -518,6 +524,102 @@ ao_status ao_batch_get_info(ao_batch *batch, int system, ao_batch_system_info *i
         info->leaf_capacity = s.leafCapacity;
         info->needs_resize = s.needsResize ? 1 : 0;
     });
+}
+
+ao_status ao_serve_create(int slots, size_t memory_budget_bytes, ao_server **out)
+{
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("ao_serve_create: null argument");
+        *out = nullptr;
+        if (slots <= 0) throw std::invalid_argument("ao_serve_create: need at least one slot");
+        if (memory_budget_bytes == 0) throw std::invalid_argument("ao_serve_create: the memory budget must be positive");
+        auto s = std::make_unique<ao_server>();
+        s->server = std::make_unique<aot::Server>(slots, memory_budget_bytes);
+        *out = s.release();
+    });
+}
+
+ao_status ao_serve_destroy(ao_server *server)
+{
+    return guarded([&] { delete server; });
+}
+
+ao_status ao_serve_submit(ao_server *server, const ao_request *request, long long *ticket)
+{
+    return guarded([&] {
+        if (!server || !request || !ticket) throw std::invalid_argument("ao_serve_submit: null argument");
+        aot::ServeRequest r;
+        r.op = request->op;
+        r.tree = request->tree;
+        if (request->op == AO_REQUEST_BUILD)
+            r.cfg = engineConfig(request->kind, request->real_type, request->config, nullptr);
+        r.n = request->n;
+        r.x = request->x;
+        r.y = request->y;
+        r.z = request->z;
+        r.digest = request->want_digest != 0;
+        *ticket = server->server->submit(r);
+    });
+}
+
+ao_status ao_serve_wait(ao_server *server, long long ticket, ao_request_result *result)
+{
+    aot::ServeResult r;
+    const ao_status s = guarded([&] {
+        if (!server || !result) throw std::invalid_argument("ao_serve_wait: null argument");
+        r = server->server->wait(ticket);
+        result->status = r.status;
+        result->queued_ms = r.queuedMs;
+        result->latency_ms = r.latencyMs;
+        result->num_leaves = r.leaves;
+        result->resizes = r.resizes;
+        result->digest = r.digest;
+    });
+    if (s != AO_OK) return s;
+    if (r.status != AO_OK) return fail(static_cast<ao_status>(r.status), r.message.c_str());
+    return AO_OK;
+}
+
+ao_status ao_serve_drain(ao_server *server)
+{
+    return guarded([&] {
+        if (!server) throw std::invalid_argument("ao_serve_drain: null server");
+        server->server->drain();
+    });
+}
+
+ao_status ao_serve_get_stats(ao_server *server, ao_serve_stats *stats)
+{
+    return guarded([&] {
+        if (!server || !stats) throw std::invalid_argument("ao_serve_get_stats: null argument");
+        const aot::ServeStats s = server->server->stats();
+        stats->submitted = s.submitted;
+        stats->completed = s.completed;
+        stats->failed = s.failed;
+        stats->resident_trees = s.residentTrees;
+        stats->resident_bytes = s.residentBytes;
+        stats->peak_bytes = s.peakBytes;
+        stats->particles = s.particles;
+        stats->p50_ms = s.p50Ms;
+        stats->p99_ms = s.p99Ms;
+        stats->mean_ms = s.meanMs;
+        stats->max_ms = s.maxMs;
+        stats->particles_per_s = s.particlesPerS;
+        stats->span_s = s.spanS;
+    });
+}
+
+ao_status ao_serve_reset_stats(ao_server *server)
+{
+    return guarded([&] {
+        if (!server) throw std::invalid_argument("ao_serve_reset_stats: null server");
+        server->server->resetStats();
+    });
+}
+
+ao_status ao_release_cached_memory(void)
+{
+    return guarded([&] { aot::blockcache::trim(); });
 }
 
 ao_status ao_sort_pairs_noalloc(const unsigned long long *keys_in, unsigned long long *keys_out,

@@ -19,7 +19,11 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <stdexcept>
+#include <utility>
+#include <vector>
 
 #include "engine_util.cuh"
 #include "keygen.cuh"
@@ -29,35 +33,175 @@
 namespace aot
 {
 // --------------------------------------------------------------------------
+// block cache
+// --------------------------------------------------------------------------
+namespace blockcache
+{
+namespace
+{
+struct Cache
+{
+    std::mutex mu;
+    std::map<std::pair<int, size_t>, std::vector<void *>> dev;  // (device, class) -> blocks
+    std::map<size_t, std::vector<void *>> host;
+    size_t devBytes = 0;
+};
+Cache &cache()
+{
+    static Cache *c = new Cache();  // never destroyed: blocks may be given back during process exit
+    return *c;
+}
+// size class: b rounded up to a quarter of its power of two (>= 256 bytes)
+size_t sizeClass(size_t b)
+{
+    if (b <= 256) return 256;
+    size_t top = size_t(1) << (63 - __builtin_clzll(b));
+    const size_t step = std::max<size_t>(top / 4, 256);
+    return (b + step - 1) / step * step;
+}
+int currentDevice()
+{
+    int d = 0;
+    AOT_CHECK(cudaGetDevice(&d));
+    return d;
+}
+}  // namespace
+
+void *take(size_t bytes, size_t *classBytes)
+{
+    const size_t c = sizeClass(bytes);
+    const int d = currentDevice();
+    Cache &k = cache();
+    {
+        std::lock_guard<std::mutex> lock(k.mu);
+        auto it = k.dev.find({d, c});
+        if (it != k.dev.end() && !it->second.empty())
+        {
+            void *p = it->second.back();
+            it->second.pop_back();
+            k.devBytes -= c;
+            *classBytes = c;
+            return p;
+        }
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, c);
+    if (e == cudaErrorMemoryAllocation)
+    {
+        // give the cached blocks back and retry once
+        (void)cudaGetLastError();
+        trim();
+        e = cudaMalloc(&p, c);
+    }
+    AOT_CHECK(e);
+    *classBytes = c;
+    return p;
+}
+
+void give(void *p, size_t classBytes)
+{
+    if (!p) return;
+    int d = 0;
+    if (cudaGetDevice(&d) != cudaSuccess) return;
+    Cache &k = cache();
+    std::lock_guard<std::mutex> lock(k.mu);
+    k.dev[{d, classBytes}].push_back(p);
+    k.devBytes += classBytes;
+}
+
+void *takeHost(size_t bytes, size_t *classBytes)
+{
+    const size_t c = sizeClass(bytes);
+    Cache &k = cache();
+    {
+        std::lock_guard<std::mutex> lock(k.mu);
+        auto it = k.host.find(c);
+        if (it != k.host.end() && !it->second.empty())
+        {
+            void *p = it->second.back();
+            it->second.pop_back();
+            *classBytes = c;
+            return p;
+        }
+    }
+    void *p = nullptr;
+    AOT_CHECK(cudaMallocHost(&p, c));
+    *classBytes = c;
+    return p;
+}
+
+void giveHost(void *p, size_t classBytes)
+{
+    if (!p) return;
+    Cache &k = cache();
+    std::lock_guard<std::mutex> lock(k.mu);
+    k.host[classBytes].push_back(p);
+}
+
+size_t cachedBytes()
+{
+    Cache &k = cache();
+    std::lock_guard<std::mutex> lock(k.mu);
+    return k.devBytes;
+}
+
+void trim()
+{
+    Cache &k = cache();
+    std::lock_guard<std::mutex> lock(k.mu);
+    int cur = 0;
+    (void)cudaGetDevice(&cur);
+    for (auto &kv : k.dev)
+    {
+        (void)cudaSetDevice(kv.first.first);
+        for (void *p : kv.second) (void)cudaFree(p);
+        kv.second.clear();
+    }
+    (void)cudaSetDevice(cur);
+    k.dev.clear();
+    k.devBytes = 0;
+}
+}  // namespace blockcache
+
+// --------------------------------------------------------------------------
 // DevMem
 // --------------------------------------------------------------------------
-DevMem::~DevMem()
+DevMem::~DevMem() { release(); }
+void DevMem::release()
 {
-    if (p) cudaFree(p);
+    if (p) blockcache::give(p, bytes);
+    p = nullptr;
+    bytes = 0;
 }
 void DevMem::reserve(size_t b)
 {
     if (b <= bytes) return;
-    if (p) AOT_CHECK(cudaFree(p));
+    if (p)
+    {
+        // work queued on the old block (on any stream of its owner) must end
+        // before another buffer can be handed the block
+        AOT_CHECK(cudaDeviceSynchronize());
+        blockcache::give(p, bytes);
+    }
     p = nullptr;
     bytes = 0;
-    AOT_CHECK(cudaMalloc(&p, b));
-    bytes = b;
+    p = blockcache::take(b, &bytes);
 }
 void DevMem::grow(size_t b, size_t keep, cudaStream_t s)
 {
     if (b <= bytes) return;
-    void *q = nullptr;
-    AOT_CHECK(cudaMalloc(&q, b));
+    size_t nb = 0;
+    void *q = blockcache::take(b, &nb);
     keep = std::min(keep, bytes);
-    if (keep && p)
+    if (keep && p) AOT_CHECK(cudaMemcpyAsync(q, p, keep, cudaMemcpyDeviceToDevice, s));
+    if (p)
     {
-        AOT_CHECK(cudaMemcpyAsync(q, p, keep, cudaMemcpyDeviceToDevice, s));
+        // the owner queues its work on this block on s only
         AOT_CHECK(cudaStreamSynchronize(s));
+        blockcache::give(p, bytes);
     }
-    if (p) AOT_CHECK(cudaFree(p));
     p = q;
-    bytes = b;
+    bytes = nb;
 }
 
 namespace
@@ -322,8 +466,10 @@ struct TreeEngine::Impl
     DevMem P[2], Perm[2], sample;
     SortArena sortArena;
     // state
-    DeviceState *st = nullptr;   // device
-    DeviceState *hst = nullptr;  // pinned mirror
+    DevMem stMem;
+    DeviceState *st = nullptr;   // device (stMem)
+    DeviceState *hst = nullptr;  // pinned mirror (block cache)
+    size_t hstBytes = 0;
     cudaStream_t d2h = nullptr;
     cudaEvent_t ready = nullptr;
     DevMem history;
@@ -345,10 +491,28 @@ struct TreeEngine::Impl
 
     ~Impl()
     {
-        if (st) cudaFree(st);
-        if (hst) cudaFreeHost(hst);
+        if (hst) blockcache::giveHost(hst, hstBytes);
         if (ready) cudaEventDestroy(ready);
         if (d2h) cudaStreamDestroy(d2h);
+    }
+
+    // device bytes held by this tree
+    size_t bytes() const
+    {
+        const DevMem *all[] = {&P[0],        &P[1],        &Perm[0],        &Perm[1],      &sample,
+                               &sortArena.counters, &sortArena.status, &stMem, &history, &K[0],
+                               &K[1],        &B[0],        &B[1],           &NF[0],        &NF[1],
+                               &N[0],        &N[1],        &G[0],           &G[1],         &offs,
+                               &dirty,       &scan,        &vBox,           &vSplit,       &vDepth,
+                               &vParent,     &vChild,      &vLevelOffset,   &vPbegin,      &vPcount,
+                               &vPmap,       &vMaxDepth,   &vLeafLevel,     &vLeafToNode,  &vLevels,
+                               &vCandStart,  &vCandLevel,  &vLvKeys[0],     &vLvKeys[1],   &vLvVals[0],
+                               &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
+                               &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
+                               &viewSort.counters, &viewSort.status};
+        size_t s = 0;
+        for (const DevMem *d : all) s += d->bytes;
+        return s;
     }
 
     rb::TreeBufs bufs() const
@@ -438,9 +602,11 @@ TreeEngine::TreeEngine(const void *x, const void *y, const void *z, size_t n, co
     m_->kpd.h = hilbertTables();
     prepared_ = cfg.views;
 
-    AOT_CHECK(cudaMalloc(&m_->st, sizeof(DeviceState)));
-    AOT_CHECK(cudaMemset(m_->st, 0, sizeof(DeviceState)));
-    AOT_CHECK(cudaMallocHost(&m_->hst, sizeof(DeviceState)));
+    // stream-ordered set-up: nothing here synchronises the device
+    m_->stMem.reserve(sizeof(DeviceState));
+    m_->st = m_->stMem.as<DeviceState>();
+    AOT_CHECK(cudaMemsetAsync(m_->st, 0, sizeof(DeviceState), cfg.stream));
+    m_->hst = static_cast<DeviceState *>(blockcache::takeHost(sizeof(DeviceState), &m_->hstBytes));
     std::memset(m_->hst, 0, sizeof(DeviceState));
     AOT_CHECK(cudaStreamCreateWithFlags(&m_->d2h, cudaStreamNonBlocking));
     AOT_CHECK(cudaEventCreateWithFlags(&m_->ready, cudaEventDisableTiming));
@@ -458,11 +624,22 @@ TreeEngine::TreeEngine(const void *x, const void *y, const void *z, size_t n, co
     if (cfg.kind == 0)
     {
         const u64 root[2] = {0, kMaxKey};
-        AOT_CHECK(cudaMemcpy(m_->K[0].p, root, sizeof(root), cudaMemcpyHostToDevice));
+        AOT_CHECK(cudaMemcpyAsync(m_->K[0].p, root, sizeof(root), cudaMemcpyHostToDevice, cfg.stream));
+        AOT_CHECK(cudaStreamSynchronize(cfg.stream));
     }
 }
 
-TreeEngine::~TreeEngine() = default;
+size_t TreeEngine::deviceBytes() const { return m_->bytes(); }
+
+// The buffers go back to the block cache: no queued work may still use them.
+TreeEngine::~TreeEngine()
+{
+    if (m_)
+    {
+        (void)cudaStreamSynchronize(cfg_.stream);
+        if (m_->d2h) (void)cudaStreamSynchronize(m_->d2h);
+    }
+}
 
 void TreeEngine::setCoordinates(const void *x, const void *y, const void *z)
 {
@@ -491,7 +668,11 @@ void TreeEngine::ensurePhysical(size_t capacity)
         }
         else
         {
+            // nearFieldCounts_d of a LeafCount tree (or a binary tree) is never
+            // written: it reads as zeros, as the reference's value-initialised vector
+            const size_t before = m_->NF[k].bytes;
             m_->NF[k].grow(sizeof(u32) * (c + 1), m_->NF[k].bytes, s);
+            if (m_->NF[k].bytes != before) AOT_CHECK(cudaMemsetAsync(m_->NF[k].p, 0, m_->NF[k].bytes, s));
             m_->G[k].grow(16, m_->G[k].bytes, s);
         }
     }

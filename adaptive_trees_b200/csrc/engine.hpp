@@ -52,7 +52,27 @@ struct EngineConfig
     cudaStream_t stream = nullptr;
 };
 
-// Raw device allocation that only grows.
+// Process-wide cache of device and pinned host blocks.
+//
+// cudaMalloc, cudaFree and cudaMallocHost synchronise the whole device, so a
+// process that creates and destroys trees while other trees' work is queued
+// (a serving loop) would stall all of it at every allocation.  Freed blocks
+// are therefore kept per device and size class (quarter-octave steps) and
+// handed to the next request of that class; the driver is only asked on a
+// miss.  A block may be given back only when no queued work can still touch
+// it: engines synchronise their stream before they release their buffers.
+namespace blockcache
+{
+void *take(size_t bytes, size_t *classBytes);  // device block of >= bytes
+void give(void *p, size_t classBytes);
+void *takeHost(size_t bytes, size_t *classBytes);  // pinned host block
+void giveHost(void *p, size_t classBytes);
+size_t cachedBytes();  // device bytes held for reuse
+void trim();           // returns every cached block to the driver
+}  // namespace blockcache
+
+// Device allocation that only grows, backed by the block cache.  The owner
+// must have no queued work on the block when it is destroyed.
 struct DevMem
 {
     void *p = nullptr;
@@ -63,6 +83,7 @@ struct DevMem
     ~DevMem();
     void reserve(size_t b);                        // discard contents
     void grow(size_t b, size_t keep, cudaStream_t s);  // keep the first `keep` bytes
+    void release();                                    // back to the cache (no queued work may use it)
     template <class T> T *as() const { return static_cast<T *>(p); }
 };
 
@@ -94,6 +115,7 @@ public:
     size_t numParticles() const { return n_; }
     size_t numActiveParticles() const { return hostActive_; }
     size_t numNodes() const { return hostNodes_; }
+    size_t numLeaves() const { return hostLeaves_; }
     unsigned maxAchievedDepth() const;
     size_t leafCapacity() const { return leafCapacity_; }
     const EngineConfig &config() const { return cfg_; }
@@ -102,6 +124,8 @@ public:
     size_t physicalCapacity() const { return physCap_; }
     // kernel launches issued by the engine in this process
     static unsigned long long kernelLaunches();
+    // device memory held by this tree's buffers
+    size_t deviceBytes() const;
     // stable sort of (key, value) pairs by bits [beginBit, endBit)
     // (cub::DeviceRadixSort::SortPairs semantics; scratch == nullptr queries
     // the scratch size; valsIn == nullptr sorts the indices 0..n-1)

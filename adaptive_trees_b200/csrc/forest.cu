@@ -40,8 +40,9 @@ struct ForestEngine::Impl
     size_t scanTiles = 0;
     // state
     DevMem st, sys, history, frozen;
-    forest::State *hst = nullptr;
+    forest::State *hst = nullptr;       // pinned mirrors (block cache)
     forest::SysState *hsys = nullptr;
+    size_t hstBytes = 0, hsysBytes = 0;
     std::vector<OctreeCapacity> capModel;
     std::vector<size_t> leafCap;
     bool built = false;
@@ -50,8 +51,8 @@ struct ForestEngine::Impl
 
     ~Impl()
     {
-        if (hst) cudaFreeHost(hst);
-        if (hsys) cudaFreeHost(hsys);
+        if (hst) blockcache::giveHost(hst, hstBytes);
+        if (hsys) blockcache::giveHost(hsys, hsysBytes);
     }
 
     forest::Bufs bufs() const
@@ -163,20 +164,26 @@ ForestEngine::ForestEngine(const void *const *x, const void *const *y, const voi
     m.tileCounters.reserve(sort::kMaxPasses * 4);
     m.status.reserve(std::max<size_t>(m.numTiles, 1) * sort::kMaxPasses * sort::kRadix * 8);
     m.st.reserve(sizeof(forest::State));
-    AOT_CHECK(cudaMemset(m.st.p, 0, sizeof(forest::State)));
+    AOT_CHECK(cudaMemsetAsync(m.st.p, 0, sizeof(forest::State), cfg.stream));
     m.sys.reserve(size_t(numSystems) * sizeof(forest::SysState));
-    AOT_CHECK(cudaMemset(m.sys.p, 0, size_t(numSystems) * sizeof(forest::SysState)));
+    AOT_CHECK(cudaMemsetAsync(m.sys.p, 0, size_t(numSystems) * sizeof(forest::SysState), cfg.stream));
     m.history.reserve(size_t(std::max(cfg.maxDepth, 1u)) * numSystems * sizeof(long long));
     m.frozen.reserve(size_t(numSystems));
-    AOT_CHECK(cudaMemset(m.frozen.p, 0, size_t(numSystems)));
-    AOT_CHECK(cudaMallocHost(&m.hst, sizeof(forest::State)));
-    AOT_CHECK(cudaMallocHost(&m.hsys, size_t(numSystems) * sizeof(forest::SysState)));
+    AOT_CHECK(cudaMemsetAsync(m.frozen.p, 0, size_t(numSystems), cfg.stream));
+    AOT_CHECK(cudaStreamSynchronize(cfg.stream));
+    m.hst = static_cast<forest::State *>(blockcache::takeHost(sizeof(forest::State), &m.hstBytes));
+    m.hsys = static_cast<forest::SysState *>(
+        blockcache::takeHost(size_t(numSystems) * sizeof(forest::SysState), &m.hsysBytes));
     std::memset(m.hst, 0, sizeof(forest::State));
     std::memset(m.hsys, 0, size_t(numSystems) * sizeof(forest::SysState));
     ensurePhysical(size_t(4) * numSystems + 4096);
 }
 
-ForestEngine::~ForestEngine() = default;
+// The buffers go back to the block cache: no queued work may still use them.
+ForestEngine::~ForestEngine()
+{
+    if (m_) (void)cudaStreamSynchronize(m_->cfg.stream);
+}
 
 int ForestEngine::numSystems() const { return m_->S; }
 size_t ForestEngine::numParticles() const { return m_->total; }

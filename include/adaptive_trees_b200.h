@@ -227,6 +227,71 @@ AO_API ao_status ao_batch_set_coordinates(ao_batch *batch, int system, const voi
 AO_API ao_status ao_batch_get_buffer(ao_batch *batch, int system, int which, const void **ptr, size_t *size);
 AO_API ao_status ao_batch_get_info(ao_batch *batch, int system, ao_batch_system_info *info);
 
+/* ---------------------------------------------------------------------------
+ * Serving.  The reference has no serving layer: its callers build and update
+ * trees one at a time.  A server takes requests to build new trees and to
+ * update or release resident ones, and runs them on `slots` worker threads:
+ * every resident tree keeps its buffers and its own copy of its coordinates
+ * on the device between requests and runs on its own stream, so requests on
+ * different trees overlap on the GPU.  Builds are admitted in arrival order
+ * when their memory fits `memory_budget_bytes` next to the resident trees;
+ * updates and releases pass waiting builds; requests on one tree run in
+ * arrival order.  An update that exceeds the tree's capacity is completed by
+ * resizeBuffers() and another update(), as the reference's callers do.  Each
+ * request gives the result it gives when it runs alone.
+ * ------------------------------------------------------------------------- */
+typedef struct ao_server ao_server;
+
+enum { AO_REQUEST_BUILD = 0, AO_REQUEST_UPDATE = 1, AO_REQUEST_RELEASE = 2 };
+
+typedef struct ao_request
+{
+    int op;             /* AO_REQUEST_BUILD / _UPDATE / _RELEASE */
+    long long tree;     /* caller-chosen id, unique among resident trees */
+    int kind;           /* build: AO_OCTREE / AO_BINARY */
+    int real_type;      /* build: AO_FLOAT32 / AO_FLOAT64 */
+    ao_config config;   /* build */
+    size_t n;           /* build: particles; update: the tree's particle count */
+    const void *x, *y, *z; /* build/update: coordinates (device or pinned host), copied into the
+                            tree's own storage when the request starts: keep them valid and
+                            unchanged until the request completes */
+    int want_digest;    /* 1: hash the tree's keys, perm, cornerstone and counts when done */
+} ao_request;
+
+typedef struct ao_request_result
+{
+    int status;                /* ao_status of the request */
+    double queued_ms;          /* submit -> start */
+    double latency_ms;         /* submit -> result ready */
+    size_t num_leaves;
+    int resizes;               /* resize-and-retry steps of an update */
+    unsigned long long digest; /* with want_digest */
+} ao_request_result;
+
+typedef struct ao_serve_stats
+{
+    size_t submitted, completed, failed, resident_trees, resident_bytes, peak_bytes;
+    unsigned long long particles; /* particles of the completed builds and updates */
+    double p50_ms, p99_ms, mean_ms, max_ms; /* request latency, submit -> result ready */
+    double particles_per_s, span_s;         /* over first submit -> last completion */
+} ao_serve_stats;
+
+AO_API ao_status ao_serve_create(int slots, size_t memory_budget_bytes, ao_server **out);
+/* Requests still queued end with AO_ERR_RUNTIME; running ones complete. */
+AO_API ao_status ao_serve_destroy(ao_server *server);
+/* Queues a request; returns at once. */
+AO_API ao_status ao_serve_submit(ao_server *server, const ao_request *request, long long *ticket);
+/* Blocks until the request is done; returns its status (message in ao_last_error). */
+AO_API ao_status ao_serve_wait(ao_server *server, long long ticket, ao_request_result *result);
+/* Blocks until every submitted request is done. */
+AO_API ao_status ao_serve_drain(ao_server *server);
+AO_API ao_status ao_serve_get_stats(ao_server *server, ao_serve_stats *stats);
+AO_API ao_status ao_serve_reset_stats(ao_server *server);
+
+/* Freed device blocks are kept for reuse by later trees (cudaMalloc and
+ * cudaFree would synchronise the device); this hands them back to the driver. */
+AO_API ao_status ao_release_cached_memory(void);
+
 /* Message of the last failed call on this thread ("" if none). */
 AO_API const char *ao_last_error(void);
 
