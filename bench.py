@@ -373,6 +373,117 @@ def batched_bench(args):
     return 0 if same else 1
 
 
+C5_METRIC = "particles/s served (Poisson 2000 req/s, 30% builds / 70% updates, 120 GB budget)"
+
+
+def serving_bench(args):
+    """C5: a Server fed by an open-loop Poisson client; latency from submit to result."""
+    import torch
+
+    import adaptive_trees_b200 as ab
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    rate, budget, max_n = 2000.0, 120 << 30, 4_000_000
+    rng = np.random.default_rng(5)
+    # coordinate pools: per distribution one base set and four jittered copies
+    pools = {}
+    for dist in ("uniform", "plummer"):
+        if dist == "plummer":
+            base = plummer(max_n, 55)
+        else:
+            r = np.random.default_rng(56)
+            base = tuple(r.random(max_n, dtype=np.float32) for _ in range(3))
+        versions = [tuple(torch.from_numpy(a).to(dev) for a in base)]
+        g = torch.Generator(device=dev)
+        g.manual_seed(57)
+        for _ in range(4):
+            versions.append(tuple((t + torch.randn(t.shape, generator=g, device=dev) * 1e-3).clamp_(0.0, 0.99999994)
+                                  for t in versions[0]))
+        pools[dist] = versions
+    torch.cuda.synchronize()
+
+    def make_requests(seconds, first_id):
+        """Arrival times and requests of an open-loop client over `seconds`."""
+        reqs, live, t, tid = [], [], 0.0, first_id
+        while True:
+            t += rng.exponential(1.0 / rate)
+            if t >= seconds:
+                break
+            if not live or rng.random() < 0.3:
+                n = int(10 ** rng.uniform(4.0, np.log10(max_n)))
+                dist = "plummer" if rng.random() < 0.5 else "uniform"
+                nf = rng.random() < 0.5
+                cfg = ab.TreeConfig(maxParticlesPerLeaf=512 if nf else 64,
+                                    splitCriterion=ab.SplitCriterion.NFCount if nf else ab.SplitCriterion.LeafCount,
+                                    sfcKind=ab.SfcKind.Hilbert if rng.random() < 0.5 else ab.SfcKind.Morton)
+                off = int(rng.integers(0, max_n - n + 1))
+                if len(live) >= args.live_trees:
+                    reqs.append((t, ("release", live.pop(0))))
+                live.append((tid, dist, n, off, [0]))
+                reqs.append((t, ("build", live[-1], cfg)))
+                tid += 1
+            else:
+                tr = live[int(rng.integers(0, len(live)))]
+                tr[4][0] = tr[4][0] % 4 + 1
+                reqs.append((t, ("update", tr, tr[4][0])))
+        return reqs, live, tid
+
+    def submit(server, req):
+        kind = req[0]
+        if kind == "release":
+            return server.release(req[1][0])
+        tid, dist, n, off, _ = req[1]
+        v = 0 if kind == "build" else req[2]
+        xyz = [a[off:off + n] for a in pools[dist][v]]
+        if kind == "build":
+            return server.build(tid, *xyz, config=req[2])
+        return server.update(tid, *xyz)
+
+    def play(server, reqs):
+        t0 = time.perf_counter()
+        tickets = []
+        for at, req in reqs:
+            while True:
+                dt = at - (time.perf_counter() - t0)
+                if dt <= 0:
+                    break
+                time.sleep(min(dt, 0.002) if dt > 0.0005 else 0)
+            tickets.append(submit(server, req))
+        server.drain()
+        return tickets
+
+    server = ab.Server(slots=args.slots, memory_budget_bytes=budget)
+    warm, live, next_id = make_requests(args.warm_seconds, 0)
+    play(server, warm)
+    for tr in live:
+        server.release(tr[0])
+    server.drain()
+    server.reset_stats()
+    reqs, live, _ = make_requests(args.duration, next_id)
+    with ClockSampler(0) as clocks:
+        tickets = play(server, reqs)
+    st = server.stats()
+    failed = [server.wait(k) for k in tickets]
+    failed = [r["message"] for r in failed if r["status"] != 0]
+    offered = sum(r[1][1][2] for r in reqs if r[1][0] != "release")
+    server.close()
+    line = {"metric": C5_METRIC, "value": st["particles_per_s"], "unit": "particles/s", "n_gpus": 1,
+            "steps": len(reqs), "warmup": len(warm), "ms_per_step": st["mean_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "C5 serving: open-loop Poisson client, 2000 req/s, 30% builds of new trees / "
+                                   "70% updates of live trees, sizes floor(10^U(4, log10 4e6)), fp32 uniform or "
+                                   "Plummer, Morton or Hilbert, LeafCount 64 or NFCount 512; 120 GB budget",
+                       "duration_s": args.duration, "slots": args.slots, "live_trees": args.live_trees,
+                       "parallelism": "replicas1"},
+            "latency": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                        "max_ms": st["max_ms"]},
+            "requests": {"completed": st["completed"], "failed": st["failed"], "first_failures": failed[:3]},
+            "offered_particles_per_s": offered / args.duration, "span_s": st["span_s"],
+            "peak_bytes": st["peak_bytes"], "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0 if not failed else 1
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,8 +498,13 @@ def main():
                     help="kernels: only key generation + the 64-bit pair sort of the workload's keys; "
                          "build: one build + one update of the workload's tree (small commands for ncu)")
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--config", default="c2", choices=["c2", "c4"],
-                    help="c2: the 16Mi NFCount octree (headline); c4: 512 batched octrees vs a per-tree loop")
+    ap.add_argument("--config", default="c2", choices=["c2", "c4", "c5"],
+                    help="c2: the 16Mi NFCount octree (headline); c4: 512 batched octrees vs a per-tree loop; "
+                         "c5: serving under a Poisson request stream")
+    ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of requests")
+    ap.add_argument("--warm-seconds", type=float, default=2.0, help="c5: seconds of untimed requests first")
+    ap.add_argument("--slots", type=int, default=8, help="c5: server worker threads")
+    ap.add_argument("--live-trees", type=int, default=256, help="c5: resident trees the client keeps")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -398,6 +514,8 @@ def main():
         return build_only(args)
     if args.config == "c4":
         return batched_bench(args)
+    if args.config == "c5":
+        return serving_bench(args)
 
     import torch
     import torch.distributed as dist
