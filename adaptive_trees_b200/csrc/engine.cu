@@ -16,6 +16,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -39,11 +41,20 @@ namespace blockcache
 {
 namespace
 {
+// Misses are served by a stream-ordered pool of this library (cudaMallocAsync
+// does not synchronise the device as cudaMalloc does); blocks never go back
+// to the pool except through trim().
+struct DevicePool
+{
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;
+};
 struct Cache
 {
     std::mutex mu;
     std::map<std::pair<int, size_t>, std::vector<void *>> dev;  // (device, class) -> blocks
     std::map<size_t, std::vector<void *>> host;
+    std::map<int, DevicePool> pools;
     size_t devBytes = 0;
 };
 Cache &cache()
@@ -51,19 +62,36 @@ Cache &cache()
     static Cache *c = new Cache();  // never destroyed: blocks may be given back during process exit
     return *c;
 }
-// size class: b rounded up to a quarter of its power of two (>= 256 bytes)
+// size class: b rounded up to 2^k or 1.5 * 2^k (at most 50% above b), >= 256 bytes
 size_t sizeClass(size_t b)
 {
     if (b <= 256) return 256;
-    size_t top = size_t(1) << (63 - __builtin_clzll(b));
-    const size_t step = std::max<size_t>(top / 4, 256);
-    return (b + step - 1) / step * step;
+    const size_t top = size_t(1) << (63 - __builtin_clzll(b));
+    if (b == top) return b;
+    return b <= top + top / 2 ? top + top / 2 : 2 * top;
 }
 int currentDevice()
 {
     int d = 0;
     AOT_CHECK(cudaGetDevice(&d));
     return d;
+}
+// with k.mu held
+DevicePool &poolOf(Cache &k, int d)
+{
+    DevicePool &p = k.pools[d];
+    if (!p.pool)
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = d;
+        AOT_CHECK(cudaMemPoolCreate(&p.pool, &props));
+        unsigned long long keep = ~0ull;  // keep what it maps until trim()
+        AOT_CHECK(cudaMemPoolSetAttribute(p.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        AOT_CHECK(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+    }
+    return p;
 }
 }  // namespace
 
@@ -72,6 +100,8 @@ void *take(size_t bytes, size_t *classBytes)
     const size_t c = sizeClass(bytes);
     const int d = currentDevice();
     Cache &k = cache();
+    cudaStream_t s = nullptr;
+    cudaMemPool_t pool = nullptr;
     {
         std::lock_guard<std::mutex> lock(k.mu);
         auto it = k.dev.find({d, c});
@@ -83,17 +113,21 @@ void *take(size_t bytes, size_t *classBytes)
             *classBytes = c;
             return p;
         }
+        DevicePool &dp = poolOf(k, d);
+        s = dp.stream;
+        pool = dp.pool;
     }
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, c);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, c, pool, s);
     if (e == cudaErrorMemoryAllocation)
     {
         // give the cached blocks back and retry once
         (void)cudaGetLastError();
         trim();
-        e = cudaMalloc(&p, c);
+        e = cudaMallocFromPoolAsync(&p, c, pool, s);
     }
     AOT_CHECK(e);
+    waitStream(s);  // usable from any stream from here on
     *classBytes = c;
     return p;
 }
@@ -153,15 +187,59 @@ void trim()
     (void)cudaGetDevice(&cur);
     for (auto &kv : k.dev)
     {
-        (void)cudaSetDevice(kv.first.first);
-        for (void *p : kv.second) (void)cudaFree(p);
+        const int d = kv.first.first;
+        auto pit = k.pools.find(d);
+        if (pit == k.pools.end()) continue;
+        (void)cudaSetDevice(d);
+        for (void *p : kv.second) (void)cudaFreeAsync(p, pit->second.stream);
         kv.second.clear();
+    }
+    for (auto &kv : k.pools)
+    {
+        (void)cudaSetDevice(kv.first);
+        (void)cudaStreamSynchronize(kv.second.stream);
+        (void)cudaMemPoolTrimTo(kv.second.pool, 0);
     }
     (void)cudaSetDevice(cur);
     k.dev.clear();
     k.devBytes = 0;
 }
 }  // namespace blockcache
+
+namespace
+{
+thread_local bool t_sleepingWaits = false;
+}
+
+void sleepingWaits(bool on) { t_sleepingWaits = on; }
+
+void waitStream(cudaStream_t s)
+{
+    if (!t_sleepingWaits)
+    {
+        AOT_CHECK(cudaStreamSynchronize(s));
+        return;
+    }
+    // one blocking-sync event per host thread and device
+    thread_local std::map<int, cudaEvent_t> events;
+    int d = 0;
+    AOT_CHECK(cudaGetDevice(&d));
+    cudaEvent_t &ev = events[d];
+    if (!ev) AOT_CHECK(cudaEventCreateWithFlags(&ev, cudaEventBlockingSync | cudaEventDisableTiming));
+    AOT_CHECK(cudaEventRecord(ev, s));
+    // short waits (a tree's own round trips) are polled, yielding the core
+    // between polls; long ones sleep in the blocking synchronisation
+    const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(1000);
+    for (;;)
+    {
+        const cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return;
+        if (e != cudaErrorNotReady) AOT_CHECK(e);
+        if (std::chrono::steady_clock::now() >= until) break;
+        std::this_thread::yield();
+    }
+    AOT_CHECK(cudaEventSynchronize(ev));
+}
 
 // --------------------------------------------------------------------------
 // DevMem
@@ -173,14 +251,15 @@ void DevMem::release()
     p = nullptr;
     bytes = 0;
 }
-void DevMem::reserve(size_t b)
+void DevMem::reserve(size_t b, cudaStream_t owner)
 {
     if (b <= bytes) return;
     if (p)
     {
-        // work queued on the old block (on any stream of its owner) must end
-        // before another buffer can be handed the block
-        AOT_CHECK(cudaDeviceSynchronize());
+        // work queued on the old block must end before another buffer can be
+        // handed the block
+        if (owner) waitStream(owner);
+        else AOT_CHECK(cudaDeviceSynchronize());
         blockcache::give(p, bytes);
     }
     p = nullptr;
@@ -197,7 +276,7 @@ void DevMem::grow(size_t b, size_t keep, cudaStream_t s)
     if (p)
     {
         // the owner queues its work on this block on s only
-        AOT_CHECK(cudaStreamSynchronize(s));
+        waitStream(s);
         blockcache::give(p, bytes);
     }
     p = q;
@@ -301,13 +380,13 @@ struct SortArena
 {
     DevMem counters, status;
     size_t tilesCap = 0;
-    void ensure(size_t n)
+    void ensure(size_t n, cudaStream_t owner)
     {
         const size_t tiles = std::max<size_t>(1, (n + sort::kTile - 1) / sort::kTile);
-        counters.reserve((2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses) * sizeof(u32));
+        counters.reserve((2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses) * sizeof(u32), owner);
         if (tiles > tilesCap)
         {
-            status.reserve(size_t(sort::kMaxPasses) * tiles * sort::kRadix * sizeof(u64));
+            status.reserve(size_t(sort::kMaxPasses) * tiles * sort::kRadix * sizeof(u64), owner);
             tilesCap = tiles;
         }
     }
@@ -360,7 +439,7 @@ void clearArena(cudaStream_t s, SortArena &a, size_t n, int passes)
 int sortWithIndices(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int passes, SortArena &a, int *error)
 {
     if (n == 0) return 0;
-    a.ensure(n);
+    a.ensure(n, s);
     clearArena(s, a, n, passes);
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n, sort::kThreads), unsigned(smCount()) * 8u));
     sort::histogramKernel<<<blocks, sort::kThreads, 0, s>>>(k[0], n, 0, passes, a.hist()), noteLaunch();
@@ -618,14 +697,14 @@ TreeEngine::TreeEngine(const void *x, const void *y, const void *z, size_t n, co
             m_->Perm[k].reserve(n * sizeof(u32));
         }
         m_->sample.reserve(((n + kSampleStride - 1) >> kSampleShift) * sizeof(u64));
-        m_->sortArena.ensure(n);
+        m_->sortArena.ensure(n, cfg.stream);
     }
     ensurePhysical(16);
     if (cfg.kind == 0)
     {
         const u64 root[2] = {0, kMaxKey};
         AOT_CHECK(cudaMemcpyAsync(m_->K[0].p, root, sizeof(root), cudaMemcpyHostToDevice, cfg.stream));
-        AOT_CHECK(cudaStreamSynchronize(cfg.stream));
+        waitStream(cfg.stream);
     }
 }
 
@@ -676,11 +755,11 @@ void TreeEngine::ensurePhysical(size_t capacity)
             m_->G[k].grow(16, m_->G[k].bytes, s);
         }
     }
-    m_->offs.reserve((c + 1) * sizeof(i64));
-    m_->dirty.reserve((c + 1) * sizeof(int));
+    m_->offs.reserve((c + 1) * sizeof(i64), s);
+    m_->dirty.reserve((c + 1) * sizeof(int), s);
     // candidate group leaders are first children of distinct internal nodes: <= (L - 1) / 7
     m_->scanTiles = (c + 1 + rb::kScanTile - 1) / rb::kScanTile;
-    m_->scan.reserve((m_->scanTiles + 1) * sizeof(u64));
+    m_->scan.reserve((m_->scanTiles + 1) * sizeof(u64), s);
     physCap_ = c;
 }
 
@@ -692,7 +771,7 @@ void TreeEngine::sortParticles()
     if (n_ == 0) return;
     cudaStream_t s = cfg_.stream;
     SortArena &a = m_->sortArena;
-    a.ensure(n_);
+    a.ensure(n_, s);
     clearArena(s, a, n_, sort::kMaxPasses);
     u64 *k[2] = {m_->P[0].as<u64>(), m_->P[1].as<u64>()};
     u32 *v[2] = {m_->Perm[0].as<u32>(), m_->Perm[1].as<u32>()};
@@ -890,7 +969,7 @@ void TreeEngine::readState()
     AOT_CHECK(cudaEventRecord(m_->ready, cfg_.stream));
     AOT_CHECK(cudaStreamWaitEvent(m_->d2h, m_->ready, 0));
     AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, m_->d2h));
-    AOT_CHECK(cudaStreamSynchronize(m_->d2h));
+    waitStream(m_->d2h);
     const DeviceState &h = *m_->hst;
     if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
     hostActiveBuffer_ = h.activeBuffer;
@@ -942,7 +1021,7 @@ void TreeEngine::resizeBuffers()
     readState();
     prepareGraphBuffers(leafCapacity_ + (leafCapacity_ + 3) / 4);
     AOT_CHECK(cudaMemsetAsync(&m_->st->needsResize, 0, sizeof(int), cfg_.stream));
-    AOT_CHECK(cudaStreamSynchronize(cfg_.stream));
+    waitStream(cfg_.stream);
 }
 
 // --------------------------------------------------------------------------
@@ -957,13 +1036,13 @@ void TreeEngine::build()
 void TreeEngine::octreeBuild()
 {
     cudaStream_t s = cfg_.stream;
-    AOT_CHECK(cudaStreamSynchronize(s));
+    waitStream(s);
     capModel_.buildStart();
     sortParticles();
     // Room for the build rounds; grown on overflow.
     const size_t estimate = std::max<size_t>(4096, cfg_.nf ? n_ + 4096 : n_ / 4 + 4096);
     ensurePhysical(std::max(physCap_, estimate));
-    m_->history.reserve(std::max<size_t>(cfg_.maxDepth, 1) * sizeof(long long));
+    m_->history.reserve(std::max<size_t>(cfg_.maxDepth, 1) * sizeof(long long), cfg_.stream);
     rb::TreeBufs tb = m_->bufs();
     octInitRootKernel<<<1, 1, 0, s>>>(tb, m_->P[0].as<u64>(), n_), noteLaunch();
     AOT_LAUNCH_CHECK();
@@ -975,7 +1054,7 @@ void TreeEngine::octreeBuild()
         const int batch = std::min(4, maxRounds - done);
         for (int r = 0; r < batch; ++r) octreePass(true, (long long)physCap_);
         AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
-        AOT_CHECK(cudaStreamSynchronize(s));
+        waitStream(s);
         const DeviceState h = *m_->hst;
         if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
         done = h.rounds;
@@ -989,7 +1068,7 @@ void TreeEngine::octreeBuild()
         }
     }
     AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
-    AOT_CHECK(cudaStreamSynchronize(s));
+    waitStream(s);
     const DeviceState h = *m_->hst;
     buildRounds_ = h.iteration;
     // Replay the reference's K_d/tmpTree capacity history (octree.cu:159-180,
@@ -1025,7 +1104,7 @@ void TreeEngine::octreeBuild()
 void TreeEngine::binaryBuild()
 {
     cudaStream_t s = cfg_.stream;
-    AOT_CHECK(cudaStreamSynchronize(s));
+    waitStream(s);
     built_ = false;
     hostLeaves_ = 1;
     prepareGraphBuffers(std::max<size_t>(2, leafCapacity_));
@@ -1044,7 +1123,7 @@ void TreeEngine::binaryBuild()
         for (int r = 0; r < batch; ++r) binaryPass(true, (long long)physCap_);
         passes += batch;
         AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
-        AOT_CHECK(cudaStreamSynchronize(s));
+        waitStream(s);
         const DeviceState h = *m_->hst;
         if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
         if (h.converged) break;
@@ -1119,24 +1198,24 @@ void TreeEngine::prepareViews(size_t capacity, const adaptive_octree::ViewConfig
         m.vPcount.grow((nodes + 1) * 4, m.vPcount.bytes, s);
     }
     if (m.viewPrepared.particleMapping) m.vPmap.grow(std::max<size_t>(m.viewParticleCap, 1) * 8, m.vPmap.bytes, s);
-    m.vLeafLevel.reserve(L);
-    m.vLeafToNode.reserve(L * 4);
-    m.vLevels.reserve(4 * 66 * 4);
-    m.vCandStart.reserve(L * 8);
-    m.vCandLevel.reserve(L);
+    m.vLeafLevel.reserve(L, s);
+    m.vLeafToNode.reserve(L * 4, s);
+    m.vLevels.reserve(4 * 66 * 4, s);
+    m.vCandStart.reserve(L * 8, s);
+    m.vCandLevel.reserve(L, s);
     for (int k = 0; k < 2; ++k)
     {
-        m.vLvKeys[k].reserve(L * 8);
-        m.vLvVals[k].reserve(L * 4);
-        m.vLayKeys[k].reserve(std::max<size_t>(I, 1) * 8);
-        m.vLayVals[k].reserve(std::max<size_t>(I, 1) * 4);
+        m.vLvKeys[k].reserve(L * 8, s);
+        m.vLvVals[k].reserve(L * 4, s);
+        m.vLayKeys[k].reserve(std::max<size_t>(I, 1) * 8, s);
+        m.vLayVals[k].reserve(std::max<size_t>(I, 1) * 4, s);
     }
-    m.vIntStartSfc.reserve(std::max<size_t>(I, 1) * 8);
-    m.vIntLevelSfc.reserve(std::max<size_t>(I, 1));
-    m.vIntM.reserve(std::max<size_t>(I, 1) * 4);
-    m.vIntStartLay.reserve(std::max<size_t>(I, 1) * 8);
-    m.vIntLevelLay.reserve(std::max<size_t>(I, 1));
-    m.viewSort.ensure(L);
+    m.vIntStartSfc.reserve(std::max<size_t>(I, 1) * 8, s);
+    m.vIntLevelSfc.reserve(std::max<size_t>(I, 1), s);
+    m.vIntM.reserve(std::max<size_t>(I, 1) * 4, s);
+    m.vIntStartLay.reserve(std::max<size_t>(I, 1) * 8, s);
+    m.vIntLevelLay.reserve(std::max<size_t>(I, 1), s);
+    m.viewSort.ensure(L, s);
 }
 
 void TreeEngine::syncViewSizes()
@@ -1289,7 +1368,7 @@ unsigned TreeEngine::maxAchievedDepth() const
         // kdtree3d.cu: maxAchievedDepth from the cornerstone when no view is configured
         std::vector<u64> k(hostLeaves_ + 1);
         AOT_CHECK(cudaMemcpyAsync(k.data(), m.K[hostActiveBuffer_].p, k.size() * 8, cudaMemcpyDeviceToHost, s));
-        AOT_CHECK(cudaStreamSynchronize(s));
+        waitStream(s);
         unsigned d = 0;
         for (size_t i = 0; i + 1 < k.size(); ++i) d = std::max(d, unsigned(clz64(k[i + 1] - k[i])));
         return d;
@@ -1297,7 +1376,7 @@ unsigned TreeEngine::maxAchievedDepth() const
     if (!m.viewScratch) return 0;
     u8 v = 0;
     AOT_CHECK(cudaMemcpyAsync(&v, m.vMaxDepth.p, 1, cudaMemcpyDeviceToHost, s));
-    AOT_CHECK(cudaStreamSynchronize(s));
+    waitStream(s);
     return v;
 }
 

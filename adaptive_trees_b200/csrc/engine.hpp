@@ -71,6 +71,14 @@ size_t cachedBytes();  // device bytes held for reuse
 void trim();           // returns every cached block to the driver
 }  // namespace blockcache
 
+// Host wait for the work queued on `s` so far.  By default the thread spins
+// (cudaStreamSynchronize), the lowest latency for one tree.  A thread that
+// called sleepingWaits(true) -- one of many host threads waiting at once, as
+// in a serving loop -- polls briefly, yielding its core, then sleeps on a
+// blocking-sync event, so waiting threads do not starve the working ones.
+void waitStream(cudaStream_t s);
+void sleepingWaits(bool on);  // for the calling thread
+
 // Device allocation that only grows, backed by the block cache.  The owner
 // must have no queued work on the block when it is destroyed.
 struct DevMem
@@ -81,7 +89,9 @@ struct DevMem
     DevMem(const DevMem &) = delete;
     DevMem &operator=(const DevMem &) = delete;
     ~DevMem();
-    void reserve(size_t b);                        // discard contents
+    // discard contents; a replaced block waits for `owner` (the stream the
+    // owner queues its work on), or for the whole device without one
+    void reserve(size_t b, cudaStream_t owner = nullptr);
     void grow(size_t b, size_t keep, cudaStream_t s);  // keep the first `keep` bytes
     void release();                                    // back to the cache (no queued work may use it)
     template <class T> T *as() const { return static_cast<T *>(p); }

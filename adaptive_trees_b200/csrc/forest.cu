@@ -170,7 +170,7 @@ ForestEngine::ForestEngine(const void *const *x, const void *const *y, const voi
     m.history.reserve(size_t(std::max(cfg.maxDepth, 1u)) * numSystems * sizeof(long long));
     m.frozen.reserve(size_t(numSystems));
     AOT_CHECK(cudaMemsetAsync(m.frozen.p, 0, size_t(numSystems), cfg.stream));
-    AOT_CHECK(cudaStreamSynchronize(cfg.stream));
+    waitStream(cfg.stream);
     m.hst = static_cast<forest::State *>(blockcache::takeHost(sizeof(forest::State), &m.hstBytes));
     m.hsys = static_cast<forest::SysState *>(
         blockcache::takeHost(size_t(numSystems) * sizeof(forest::SysState), &m.hsysBytes));
@@ -199,7 +199,7 @@ void ForestEngine::setCoordinates(int s, const void *x, const void *y, const voi
     m.systems[s].z = z;
     AOT_CHECK(cudaMemcpyAsync(m.systemsD.as<forest::System>() + s, &m.systems[s], sizeof(forest::System),
                               cudaMemcpyHostToDevice, m.cfg.stream));
-    AOT_CHECK(cudaStreamSynchronize(m.cfg.stream));
+    waitStream(m.cfg.stream);
 }
 
 // Leaf arrays for `entries` entries; the active arrays keep their contents.
@@ -216,12 +216,12 @@ void ForestEngine::ensurePhysical(size_t entries)
         m.SEG[k].grow((c + 1) * 4, m.SEG[k].bytes, s);
     }
     m.N.grow((c + 1) * 4, m.N.bytes, s);
-    m.ops.reserve((c + 1) * 4);
+    m.ops.reserve((c + 1) * 4, s);
     m.offs.grow((c + 2) * 8, m.offs.bytes, s);  // a build round grows the arrays between scan and scatter
-    m.dirty.reserve((c + 1) * 4);
+    m.dirty.reserve((c + 1) * 4, s);
     m.scanTiles = (c + 2 + rb::kScanTile - 1) / rb::kScanTile;
-    m.scanStatus.reserve((m.scanTiles + 1) * 8);
-    m.scanTile.reserve(16);
+    m.scanStatus.reserve((m.scanTiles + 1) * 8, s);
+    m.scanTile.reserve(16, s);
     m.entryCap = c;
 }
 
@@ -297,7 +297,7 @@ void ForestEngine::pass(bool build, const unsigned char *frozenDevice)
     {
         // the proposal decides the room the scatter needs
         AOT_CHECK(cudaMemcpyAsync(m.hst, m.st.p, sizeof(forest::State), cudaMemcpyDeviceToHost, s));
-        AOT_CHECK(cudaStreamSynchronize(s));
+        waitStream(s);
         if (m.hst->error) throw std::runtime_error("forest: a device scan gave up waiting (bounded look-back)");
         if (!m.hst->changed) return;
         ensurePhysical(size_t(m.hst->proposal));
@@ -318,7 +318,7 @@ void ForestEngine::readState(bool model)
     cudaStream_t s = m.cfg.stream;
     AOT_CHECK(cudaMemcpyAsync(m.hst, m.st.p, sizeof(forest::State), cudaMemcpyDeviceToHost, s));
     AOT_CHECK(cudaMemcpyAsync(m.hsys, m.sys.p, size_t(m.S) * sizeof(forest::SysState), cudaMemcpyDeviceToHost, s));
-    AOT_CHECK(cudaStreamSynchronize(s));
+    waitStream(s);
     if (m.hst->error) throw std::runtime_error("forest: a device scan gave up waiting (bounded look-back)");
     if (model)
         for (int i = 0; i < m.S; ++i) m.capModel[i].stateRead(size_t(std::max(m.hsys[i].leaves, 0)));
@@ -328,7 +328,7 @@ void ForestEngine::build()
 {
     Impl &m = *m_;
     cudaStream_t s = m.cfg.stream;
-    AOT_CHECK(cudaStreamSynchronize(s));
+    waitStream(s);
     for (auto &c : m.capModel) c.buildStart();
     sortParticles();
     ensurePhysical(size_t(2) * m.S);
@@ -422,7 +422,7 @@ void ForestEngine::resizeBuffers()
     ensurePhysical(entries);
     AOT_CHECK(cudaMemcpyAsync(m.sys.p, m.hsys, size_t(m.S) * sizeof(forest::SysState), cudaMemcpyHostToDevice,
                               m.cfg.stream));
-    AOT_CHECK(cudaStreamSynchronize(m.cfg.stream));
+    waitStream(m.cfg.stream);
 }
 
 void ForestEngine::buffer(int s, int which, const void **ptr, size_t *len) const

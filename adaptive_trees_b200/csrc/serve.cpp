@@ -206,6 +206,7 @@ bool Server::admit(Job &out)
 void Server::worker()
 {
     (void)cudaSetDevice(device_);
+    sleepingWaits(true);  // many workers wait at once: do not spin
     std::unique_lock<std::mutex> lk(mu_);
     for (;;)
     {

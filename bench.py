@@ -441,30 +441,37 @@ def serving_bench(args):
 
     def play(server, reqs):
         t0 = time.perf_counter()
-        tickets = []
+        tickets, late = [], []
         for at, req in reqs:
             while True:
                 dt = at - (time.perf_counter() - t0)
                 if dt <= 0:
                     break
                 time.sleep(min(dt, 0.002) if dt > 0.0005 else 0)
+            late.append(-dt)
             tickets.append(submit(server, req))
         server.drain()
-        return tickets
+        return tickets, late
 
     server = ab.Server(slots=args.slots, memory_budget_bytes=budget)
     warm, live, next_id = make_requests(args.warm_seconds, 0)
-    play(server, warm)
+    play(server, warm)[0]
     for tr in live:
         server.release(tr[0])
     server.drain()
     server.reset_stats()
     reqs, live, _ = make_requests(args.duration, next_id)
     with ClockSampler(0) as clocks:
-        tickets = play(server, reqs)
+        tickets, late = play(server, reqs)
     st = server.stats()
-    failed = [server.wait(k) for k in tickets]
-    failed = [r["message"] for r in failed if r["status"] != 0]
+    results = [server.wait(k) for k in tickets]
+    failed = [r["message"] for r in results if r["status"] != 0]
+    # latency by second of arrival: a steady tail or bursts
+    per_second = []
+    for sec in range(int(np.ceil(args.duration))):
+        lat = [r["latency_ms"] for (at, _), r in zip(reqs, results) if sec <= at < sec + 1 and r["status"] == 0]
+        if lat:
+            per_second.append([round(float(np.percentile(lat, 50)), 2), round(float(np.percentile(lat, 99)), 2)])
     offered = sum(r[1][1][2] for r in reqs if r[1][0] != "release")
     server.close()
     line = {"metric": C5_METRIC, "value": st["particles_per_s"], "unit": "particles/s", "n_gpus": 1,
@@ -478,6 +485,9 @@ def serving_bench(args):
             "latency": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
                         "max_ms": st["max_ms"]},
             "requests": {"completed": st["completed"], "failed": st["failed"], "first_failures": failed[:3]},
+            "latency_by_second_p50_p99": per_second,
+            "client_late_ms": {"p50": float(np.percentile(late, 50)) * 1e3, "max": float(max(late)) * 1e3},
+            "host_cpus": os.cpu_count(),
             "offered_particles_per_s": offered / args.duration, "span_s": st["span_s"],
             "peak_bytes": st["peak_bytes"], "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
