@@ -60,6 +60,41 @@ def plummer(n, seed, scale=0.05, rmax=0.5):
     return tuple(np.ascontiguousarray(out[:, i].astype(np.float32)) for i in range(3))
 
 
+def rank_env():
+    """(world size, rank, local rank) of a torchrun launch; (1, 0, 0) alone."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(v, world, device):
+    """The slowest rank's value; every rank must call it (one all-reduce)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(total_units, slowest_ms):
+    """Whole-job throughput: the units of all ranks over the slowest rank's time."""
+    return total_units / (slowest_ms * 1e-3)
+
+
+def partition_by_particles(sizes, world):
+    """Owner rank of each independent system: largest first onto the least loaded rank.
+
+    Systems never exchange data, so a rank builds and updates its share alone."""
+    loads = [0] * world
+    owner = [0] * len(sizes)
+    for i in sorted(range(len(sizes)), key=lambda k: (-int(sizes[k]), k)):
+        r = min(range(world), key=lambda q: (loads[q], q))
+        owner[i] = r
+        loads[r] += int(sizes[i])
+    return owner
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -257,26 +292,36 @@ def c4_systems():
 def batched_bench(args):
     """C4: Batch (one set of launches for all systems) against a loop of plain trees."""
     import torch
+    import torch.distributed as dist
 
     import adaptive_trees_b200 as ab
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
+    world, rank, local = rank_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     s = torch.cuda.Stream(device=dev)
-    sizes, plum = c4_systems()
+    sizes_all, plum_all = c4_systems()
+    # systems never exchange data: each rank takes a particle-balanced share
+    owner = partition_by_particles(sizes_all, world)
+    mine = [k for k in range(C4_SYSTEMS) if owner[k] == rank]
+    sizes, plum = sizes_all[mine], plum_all[mine]
+    total_all = int(sizes_all.sum())
     total = int(sizes.sum())
     offs = np.concatenate([[0], np.cumsum(sizes)])
     host = [np.empty(total, np.float32) for _ in range(3)]
-    for k in range(C4_SYSTEMS):
-        n = int(sizes[k])
+    for j, k in enumerate(mine):
+        n = int(sizes[j])
         if plum[k]:
             xyz = plummer(n, 100 + k)
         else:
             r = np.random.default_rng(100 + k)
             xyz = tuple(r.random(n, dtype=np.float32) for _ in range(3))
         for a in range(3):
-            host[a][offs[k]:offs[k + 1]] = xyz[a]
+            host[a][offs[j]:offs[j + 1]] = xyz[a]
     allc = [torch.from_numpy(h).to(dev) for h in host]
-    views = [[c[offs[k]:offs[k + 1]] for c in allc] for k in range(C4_SYSTEMS)]
+    views = [[c[offs[j]:offs[j + 1]] for c in allc] for j in range(len(mine))]
     cfg = ab.TreeConfig(maxParticlesPerLeaf=64)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
@@ -356,18 +401,26 @@ def batched_bench(args):
             same = same and identical(batch, trees)
         del graph
         batch.close()
-    bb, pb = statistics.median(b_build), statistics.median(p_build)
-    bu, pu = statistics.median(b_upd), statistics.median(p_upd)
-    line = {"metric": C4_METRIC, "value": total / (bb * 1e-3), "unit": "particles/s", "n_gpus": 1,
+    bb = max_over_ranks(statistics.median(b_build), world, dev)
+    pb = max_over_ranks(statistics.median(p_build), world, dev)
+    bu = max_over_ranks(statistics.median(b_upd), world, dev)
+    pu = max_over_ranks(statistics.median(p_upd), world, dev)
+    same = max_over_ranks(0.0 if same else 1.0, world, dev) == 0.0
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0 if same else 1
+    line = {"metric": C4_METRIC, "value": job_rate(total_all, bb), "unit": "particles/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": bb, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": C4_WORKLOAD, "systems": C4_SYSTEMS, "particles": total,
-                       "largest": int(sizes.max()), "smallest": int(sizes.min()), "parallelism": "replicas1"},
-            "batched": {"build_ms": bb, "update_ms": bu, "build_value": total / (bb * 1e-3),
-                        "update_value": total / (bu * 1e-3), "update_graph_replayed": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": C4_WORKLOAD, "systems": C4_SYSTEMS, "particles": total_all,
+                       "largest": int(sizes_all.max()), "smallest": int(sizes_all.min()),
+                       "parallelism": f"systems partitioned over {world} rank(s), no collective on the path"},
+            "batched": {"build_ms": bb, "update_ms": bu, "build_value": job_rate(total_all, bb),
+                        "update_value": job_rate(total_all, bu), "update_graph_replayed": True,
                         "build_launches": batch_launches // max(1, args.steps)},
-            "plain_loop": {"build_ms": pb, "update_ms": pu, "build_value": total / (pb * 1e-3),
-                           "update_value": total / (pu * 1e-3)},
+            "plain_loop": {"build_ms": pb, "update_ms": pu, "build_value": job_rate(total_all, pb),
+                           "update_value": job_rate(total_all, pu)},
             "speedup": {"build": pb / bb, "update": pu / bu}, "identical_outputs": bool(same), "resizes": resizes}
     print(json.dumps(line), flush=True)
     return 0 if same else 1
@@ -533,9 +586,7 @@ def main():
     import adaptive_trees_b200 as ab
     from adaptive_trees_b200 import _capi as C
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = rank_env()
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -556,13 +607,6 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     with torch.cuda.stream(s):
@@ -661,9 +705,9 @@ def main():
         keygen_ms = graph_ms(lambda: ab.compute_sfc_keys(0, *xs, sfc_kind=ab.SfcKind.Hilbert, stream=s), s, 7)
     barrier()
 
-    step_ms = max_over_ranks(statistics.median(build_ms))
-    upd_ms = max_over_ranks(statistics.median(update_ms))
-    e2e = max_over_ranks(statistics.median(e2e_ms))
+    step_ms = max_over_ranks(statistics.median(build_ms), world, dev)
+    upd_ms = max_over_ranks(statistics.median(update_ms), world, dev)
+    e2e = max_over_ranks(statistics.median(e2e_ms), world, dev)
     total = n * world
     hbm, peak_kind = peaks()
     pass_bytes = 24.0 * n
