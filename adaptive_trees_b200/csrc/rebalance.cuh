@@ -652,21 +652,32 @@ __device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, c
         hint = lo;
 
         const unsigned char *pos = sPos + lane * 8;
-#pragma unroll
-        for (int o = 0; o < 8; ++o)
-            if (pos[o] != 0xff) block[pos[o]] = 0;
         const u32 n = hi - lo;
         const unsigned cShift = 3u * (kOctLevels - level);
         const u64 *P = idx.keys + lo;
         if (n <= kNFScanMax)
         {
+            // count Q's particles per child octant in registers: 16-bit fields
+            // (n <= kNFScanMax < 2^16) of two words; the child digit maps to its
+            // octant through a 3-bit-per-digit word built once for Q's state
+            u32 octOf = 0;
+            if constexpr (Hilbert)
+            {
+#pragma unroll
+                for (int d = 0; d < 8; ++d) octOf |= u32(sDec[qState * 8 + d]) << (3 * d);
+            }
+            u64 lowOcts = 0, highOcts = 0;
             for (u32 t = 0; t < n; ++t)
             {
                 const unsigned d = unsigned(__ldg(P + t) >> cShift) & 7u;
-                const unsigned o = Hilbert ? unsigned(sDec[qState * 8 + int(d)]) : d;
-                const unsigned p = pos[o];
-                if (p != 0xff) ++block[p];
+                const unsigned o = Hilbert ? (octOf >> (3 * d)) & 7u : d;
+                const u64 inc = u64(1) << (16 * (o & 3u));
+                if (o < 4) lowOcts += inc;
+                else highOcts += inc;
             }
+#pragma unroll
+            for (int o = 0; o < 8; ++o)
+                if (pos[o] != 0xff) block[pos[o]] = u32(((o < 4 ? lowOcts : highOcts) >> (16 * (o & 3))) & 0xffffu);
         }
         else
         {
