@@ -126,6 +126,9 @@ struct SharedPass
 {
     u64 keys[kTile];
     u32 vals[kTile];
+    u32 stage[kTile];              // the tile's input values, staged by one bulk copy (16-byte aligned)
+    u64 valuesReady;               // mbarrier of that copy
+    u32 staged;                    // values in `stage` (a multiple of 4)
     u32 warpHist[kWarps][kRadix];  // per-warp digit counts, then exclusive warp offsets
     u32 localStart[kRadix];
     u32 gstart[kRadix];            // global position of local index 0 of each digit (mod 2^32)
@@ -152,11 +155,50 @@ __device__ __forceinline__ unsigned peerLanes(unsigned digit, int bits, unsigned
     return peers;
 }
 
+// Shared-memory address of a pointer into shared memory.
+__device__ __forceinline__ unsigned smemAddr(const void *p) { return unsigned(__cvta_generic_to_shared(p)); }
+
+// mbarrier and bulk-copy helpers (PTX ISA: mbarrier, cp.async.bulk)
+__device__ __forceinline__ void mbarInit(u64 *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fenceMbarInit() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbarArriveExpectTx(u64 *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbarArrive(u64 *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(u64 *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Global -> shared copy of `bytes` (a multiple of 16; both addresses 16-byte
+// aligned) that completes on `bar`.  No multicast: the source is this GPU's memory.
+__device__ __forceinline__ void bulkLoad(void *dst, const void *src, unsigned bytes, u64 *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(smemAddr(bar))
+                 : "memory");
+}
+constexpr unsigned kStageSpins = 1u << 22;  // bounded wait for the staged values
+
 // Tile geometry of a pass over one contiguous key array keys[0, n).  The
 // accessors are cheap and recomputed where used, so that nothing extra stays
 // live in registers across the pass.
 struct ContiguousTiles
 {
+    static constexpr bool kStageValues = true;  // tiles start at multiples of kTile
     size_t n;
     const u32 *bins;  // [kRadix] global start of each digit
     // the tile's keys are [base(t), min(base(t) + kTile, end(t)))
@@ -176,6 +218,7 @@ struct ContiguousTiles
 // the segment.
 struct SegmentTiles
 {
+    static constexpr bool kStageValues = false;  // tiles start anywhere: plain loads
     const u32 *tileSeg, *tileBegin, *tileEnd, *segFirstTile, *segBase;
     const u32 *bins;  // [segments][kRadix] global start of each digit of this pass
     __device__ __forceinline__ size_t base(size_t tile) const { return tileBegin[tile]; }
@@ -198,12 +241,39 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
     SharedPass &sm = *reinterpret_cast<SharedPass *>(smemRaw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
+    const bool stage = Tiles::kStageValues && valsIn != nullptr;
     for (int i = tid; i < kWarps * kRadix; i += kThreads) (&sm.warpHist[0][0])[i] = 0;
-    if (tid == 0) sm.tile = atomicAdd(tileCounter, 1u);
+    if (tid == 0)
+    {
+        sm.tile = atomicAdd(tileCounter, 1u);
+        if (stage)
+        {
+            mbarInit(&sm.valuesReady, 1);
+            fenceMbarInit();
+        }
+    }
     __syncthreads();
     const size_t tile = sm.tile;
     const size_t tileBase = tiles.base(tile);
     const size_t warpBase = tileBase + size_t(warp) * (32 * kItems);
+    if (stage && tid == 0)
+    {
+        // the values travel to shared memory while the keys are ranked
+        const size_t end = tiles.end(tile);
+        const u32 count = u32((end - tileBase) < size_t(kTile) ? end - tileBase : size_t(kTile));
+        const bool aligned = (reinterpret_cast<uintptr_t>(valsIn + tileBase) & 15u) == 0;
+        const u32 bulk = aligned ? (count & ~3u) : 0u;
+        sm.staged = bulk;
+        if (bulk)
+        {
+            mbarArriveExpectTx(&sm.valuesReady, bulk * 4u);
+            bulkLoad(sm.stage, valsIn + tileBase, bulk * 4u, &sm.valuesReady);
+        }
+        else
+        {
+            mbarArrive(&sm.valuesReady);
+        }
+    }
 
     u64 key[kItems];
 #pragma unroll
@@ -273,6 +343,22 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
     }
     __syncthreads();
     // Reorder the tile in shared memory.
+    u32 staged = 0;
+    bool copyPending = false;
+    if (stage)
+    {
+        unsigned spins = 0;
+        while (!mbarTryWait(&sm.valuesReady, 0))
+        {
+            if (++spins > kStageSpins)
+            {
+                atomicExch(error, kErrLookback);
+                copyPending = true;
+                break;
+            }
+        }
+        staged = copyPending ? 0u : sm.staged;
+    }
 #pragma unroll
     for (int i = 0; i < kItems; ++i)
     {
@@ -283,7 +369,9 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
             const u32 r = (rank2[i >> 1] >> ((i & 1) * 16)) & 0xffffu;
             const u32 pos = sm.localStart[d] + sm.warpHist[warp][d] + r;
             sm.keys[pos] = key[i];
-            sm.vals[pos] = valsIn ? __ldcs(valsIn + idx) : u32(idx) - tiles.valueOffset(tile);
+            const u32 li = u32(idx - tileBase);
+            sm.vals[pos] = valsIn ? (li < staged ? sm.stage[li] : __ldcs(valsIn + idx))
+                                  : u32(idx) - tiles.valueOffset(tile);
         }
     }
     // Look-back: global start of each digit for this tile.
@@ -345,6 +433,13 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
         const u32 out = sm.gstart[d] + u32(j);
         keysOut[out] = k;
         valsOut[out] = sm.vals[j];
+    }
+    if (copyPending)
+    {
+        // the CTA does not leave with its copy still in flight (bounded again)
+        for (unsigned spins = 0; spins < kStageSpins && !mbarTryWait(&sm.valuesReady, 0); ++spins)
+        {
+        }
     }
 }
 
