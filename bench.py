@@ -275,6 +275,150 @@ def build_only(args):
     return 0
 
 
+# The two other single-tree configurations (measured on request; the default
+# line is C2).  kind 0 octree / 1 binary; updates with N(0, jitter) per step.
+SINGLE_CONFIGS = {
+    "c1": {"metric": "particles/s (octree build, 2^20 uniform fp64, Morton, LeafCount 64)",
+           "workload": "octree, 1,048,576 fp64 particles i.i.d. U[0,1)^3 (default_rng(1)), Morton, LeafCount 64; "
+                       "one build from the root",
+           "kind": 0, "n": 1 << 20, "bucket": 64, "updates": 0, "jitter": 0.0},
+    "c3": {"metric": "particles/s (binary k-d build, 8Mi Gaussian mixture fp64, LeafCount 32)",
+           "workload": "binary k-d tree, 8,388,608 fp64 particles from 8 anisotropic Gaussians (centres "
+                       "U[0.2,0.8]^3, sigma log-uniform [0.005,0.05], seed 3), LeafCount 32; build + 10 "
+                       "graph-replayed updates with N(0, 5e-4) jitter",
+           "kind": 1, "n": 1 << 23, "bucket": 32, "updates": 10, "jitter": 5e-4},
+}
+
+
+def mixture(n, seed, clusters=8):
+    """Equal-weight mixture of anisotropic Gaussians, clamped to [0, 1)."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0.2, 0.8, size=(clusters, 3))
+    sigmas = np.exp(rng.uniform(np.log(0.005), np.log(0.05), size=(clusters, 3)))
+    which = rng.integers(0, clusters, size=n)
+    pts = centres[which] + sigmas[which] * rng.normal(size=(n, 3))
+    np.clip(pts, 0.0, np.nextafter(1.0, 0.0), out=pts)
+    return tuple(np.ascontiguousarray(pts[:, i]) for i in range(3))
+
+
+def single_config_bench(args):
+    """C1 / C3: one tree of the configuration, next to the reference library on the same GPU."""
+    import torch
+
+    import adaptive_trees_b200 as ab
+    spec = SINGLE_CONFIGS[args.config]
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    s = torch.cuda.Stream(device=dev)
+    n = spec["n"]
+    if spec["kind"] == 0:
+        r = np.random.default_rng(1)
+        hx = tuple(r.random(n) for _ in range(3))
+    else:
+        hx = mixture(n, 3)
+    pinned = [torch.from_numpy(a).pin_memory() for a in hx]
+    xs = [p.to(dev) for p in pinned]
+    torch.cuda.synchronize()
+    cfg = ab.TreeConfig(maxParticlesPerLeaf=spec["bucket"])
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def timed(fn):
+        a, b = ev(), ev()
+        a.record(s)
+        fn()
+        b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    with torch.cuda.stream(s):
+        tree = ab.Tree(spec["kind"], *xs, cfg, stream=s)
+        for _ in range(args.warmup):
+            tree.build()
+        launches0 = tree.info().kernel_launches
+        with ClockSampler(0) as clocks:
+            build_ms = [timed(tree.build) for _ in range(args.steps)]
+        launches = (tree.info().kernel_launches - launches0) // max(1, args.steps)
+        info = tree.info()
+        leaves = info.num_leaves
+        # end to end: pinned host coordinates in, build, the counters out
+        host_counters = torch.zeros(3, dtype=torch.int32).pin_memory()
+        cnt = tree.counters()
+
+        def e2e_step():
+            for d, p in zip(xs, pinned):
+                d.copy_(p, non_blocking=True)
+            tree.build()
+            for k, (ptr, ts) in enumerate(zip(cnt, ("<i4", "<i4", "<u4"))):
+                host_counters[k:k + 1].copy_(ab.device_tensor(ptr, 1, ts).view(torch.int32), non_blocking=True)
+        e2e_ms = statistics.median([timed(e2e_step) for _ in range(args.steps)])
+        update_ms, resizes = [], 0
+        frame1 = None
+        if spec["updates"]:
+            gen = torch.Generator(device=dev)
+            gen.manual_seed(31)
+            upper = float(np.nextafter(1.0, 0.0))
+
+            def jitter():
+                for t in xs:
+                    t.add_(torch.randn(t.shape, generator=gen, device=dev, dtype=t.dtype) * spec["jitter"])
+                    t.clamp_(0.0, upper)
+
+            def capture():
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=s):
+                    tree.update()
+                return g
+            tree.build()
+            graph = capture()
+            for i in range(spec["updates"]):
+                jitter()
+                s.synchronize()
+                if frame1 is None:
+                    frame1 = tuple(t.cpu().numpy() for t in xs)
+                update_ms.append(timed(graph.replay))
+                if tree.doBuffersNeedResize():
+                    resizes += 1
+                    del graph
+                    tree.resizeBuffers()
+                    tree.update()
+                    graph = capture()
+            del graph
+    line = {"metric": spec["metric"], "value": n / (statistics.median(build_ms) * 1e-3), "unit": "particles/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(build_ms),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": spec["workload"], "n": n, "coords": "float64", "leaves": int(leaves),
+                       "parallelism": "replicas1"},
+            "clocks": clocks.summary(), "gpu_launches": int(launches),
+            "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "particles/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 12}}
+    if update_ms:
+        um = statistics.median(update_ms)
+        line["update"] = {"value": n / (um * 1e-3), "unit": "particles/s", "ms_per_step": um,
+                          "graph_replayed": True, "resizes": resizes, "steps": len(update_ms)}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        m = min(n, args.cpu_sample)
+        t = O.OracleTree(spec["kind"], *(a[:m] for a in hx), O.make_config(max_particles_per_leaf=spec["bucket"]))
+        t0 = time.perf_counter()
+        t.build()
+        line["cpu_baseline"] = {"value": m / (time.perf_counter() - t0), "unit": "particles/s", "cores": 1,
+                                "kind": "port", "sample": f"one build of the first {m} particles (CPU oracle port)"}
+    if not args.no_reference_gpu:
+        try:
+            from oracle import refrun
+            if refrun.available():
+                frames = [hx, frame1 if frame1 is not None else hx]
+                r = refrun.time_reference(spec["kind"], frames, reps=3, bucket=spec["bucket"],
+                                          views=(False, False, False))
+                line["reference_gpu"] = {"build_ms": r["build_ms"], "update_ms": r["update_ms"],
+                                         "build_value": n / (r["build_ms"] * 1e-3), "unit": "particles/s",
+                                         "what": "reference library compiled for sm_100a, same inputs and GPU"}
+        except Exception as e:  # informational
+            line["reference_gpu"] = {"error": str(e)[:200]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 C4_SYSTEMS = 512
 C4_METRIC = "particles/s (batched octree build, 512 systems, fp32, Morton, LeafCount 64)"
 C4_WORKLOAD = ("512 independent octrees, sizes floor(10^U(3,6)) (seed 4), fp32 uniform or Plummer (coin flip per "
@@ -561,8 +705,9 @@ def main():
                     help="kernels: only key generation + the 64-bit pair sort of the workload's keys; "
                          "build: one build + one update of the workload's tree (small commands for ncu)")
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--config", default="c2", choices=["c2", "c4", "c5"],
-                    help="c2: the 16Mi NFCount octree (headline); c4: 512 batched octrees vs a per-tree loop; "
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2: the 16Mi NFCount octree (headline); c1: 2^20 uniform fp64 LeafCount octree; "
+                         "c3: 8Mi fp64 binary k-d tree; c4: 512 batched octrees vs a per-tree loop; "
                          "c5: serving under a Poisson request stream")
     ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of requests")
     ap.add_argument("--warm-seconds", type=float, default=2.0, help="c5: seconds of untimed requests first")
@@ -575,6 +720,8 @@ def main():
         return kernels_only(args)
     if args.mode == "build":
         return build_only(args)
+    if args.config in SINGLE_CONFIGS:
+        return single_config_bench(args)
     if args.config == "c4":
         return batched_bench(args)
     if args.config == "c5":
