@@ -554,6 +554,8 @@ struct TreeEngine::Impl
     DevMem history;
     // tree
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
+    DevMem groupKeys, groupFirst;  // group table of the near-field refresh (NFCount)
+    u32 groupMask = 0;
     size_t scanTiles = 0;
     // views
     DevMem vBox, vSplit, vDepth, vParent, vChild, vLevelOffset, vPbegin, vPcount, vPmap, vMaxDepth;
@@ -588,7 +590,7 @@ struct TreeEngine::Impl
                                &vCandStart,  &vCandLevel,  &vLvKeys[0],     &vLvKeys[1],   &vLvVals[0],
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
-                               &viewSort.counters, &viewSort.status};
+                               &viewSort.counters, &viewSort.status, &groupKeys, &groupFirst};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -760,6 +762,15 @@ void TreeEngine::ensurePhysical(size_t capacity)
     // candidate group leaders are first children of distinct internal nodes: <= (L - 1) / 7
     m_->scanTiles = (c + 1 + rb::kScanTile - 1) / rb::kScanTile;
     m_->scan.reserve((m_->scanTiles + 1) * sizeof(u64), s);
+    if (cfg_.kind == 0 && cfg_.nf)
+    {
+        // complete groups <= leaves / 8; the table stays at most half full
+        size_t slots = 1024;
+        while (slots < 2 * (c / 8 + 1)) slots <<= 1;
+        m_->groupKeys.reserve(slots * sizeof(u64), s);
+        m_->groupFirst.reserve(slots * sizeof(u32), s);
+        m_->groupMask = u32(slots - 1);
+    }
     physCap_ = c;
 }
 
@@ -943,14 +954,17 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
     if (cfg_.nf)
     {
         const HilbertTables &h = m_->kpd.h;
+        const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupFirst.as<u32>(), m_->groupMask};
+        AOT_CHECK(cudaMemsetAsync(gt.keys, 0, (size_t(gt.mask) + 1) * sizeof(u64), s));
+        rb::groupTableKernel<<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
         if (all && cfg_.hilbert)
-            rb::octNearFieldKernel<true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h), noteLaunch();
+            rb::octNearFieldKernel<true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();
         else if (all)
-            rb::octNearFieldKernel<false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h), noteLaunch();
+            rb::octNearFieldKernel<false, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();
         else if (cfg_.hilbert)
-            rb::octNearFieldKernel<true, false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h), noteLaunch();
+            rb::octNearFieldKernel<true, false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();
         else
-            rb::octNearFieldKernel<false, false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h), noteLaunch();
+            rb::octNearFieldKernel<false, false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();
     }
     AOT_LAUNCH_CHECK();
 }

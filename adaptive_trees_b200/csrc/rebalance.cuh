@@ -510,21 +510,28 @@ static __global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBuf
 // around the parent, one level up) <= bucket (computeGroupCanMergeKernel,
 // octree_rebalance.cuh:636-700).  Both depend only on the particles, not on
 // the tree, so they are computed per parent cell P at level l-1 (a "unit"):
-//   * the 27 parent-level cells Q around P (P included) are found by two
-//     lower bounds each, one lane per Q;
 //   * the 8 children of P have their 27-cell stencils inside the 4 x 4 x 4
 //     block of level-l cells around P, and that block is partitioned by the
-//     children of the Q's that touch P (per axis: offset -1 gives the upper
-//     child, 0 both, +1 the lower): each lane counts its Q's particles into
-//     its block positions (a scan of a short range, or binary searches of
-//     its child boundaries when the range is long);
+//     children of the 27 parent-level cells Q around P (P included) that
+//     touch P (per axis: offset -1 gives the upper child, 0 both, +1 the
+//     lower);
+//   * a Q whose 8 children are leaves of the tree (a complete group, found
+//     in the group table) gives its child counts as differences of the begin
+//     indices, without a search; any other Q is found by two lower bounds in
+//     the sorted keys and its particles are counted per child;
 //   * each leaf of P sums its 3 x 3 x 3 sub-block, and the group flag is the
 //     sum of the 27 Q populations.
 // Periodic wrap at low levels makes several offsets name the same cell;
-// every offset is counted, as in the per-leaf stencil.  One warp per unit:
-// 54 lower bounds serve up to 8 leaves and the group flag.
+// every offset is counted, as in the per-leaf stencil.
+// A warp takes 32 list entries, cuts them into units (runs of leaves with
+// the same parent) and treats up to kUnitBatch units at once: phase A spreads
+// the (unit, Q) pairs over the lanes and resolves those found in the group
+// table; the rest are queued and phase B spreads them over the lanes for the
+// searches; phase C gives every lane its own leaf.  Lanes stay busy instead
+// of following the slowest Q of one unit.
 constexpr u32 kNFScanMax = 256;  // Q ranges up to this length are scanned
-constexpr int kNFGallop = 4;     // gallop window of the Q searches: 15 keys from the last unit's
+constexpr int kNFGallop = 4;     // gallop window of the Q searches: 15 keys
+constexpr int kUnitBatch = 8;    // units of a warp in flight
 
 // Leaf index of child 0 of the parent at `pStart` if all 8 children are
 // leaves (a complete group), else -1.
@@ -578,185 +585,194 @@ __device__ __forceinline__ CellPath decodeCell(u64 start, unsigned pl, const uns
     return c;
 }
 
-__device__ __forceinline__ CellPath shflPath(const CellPath &c, int src)
+// Complete sibling groups of the active leaves: parent cell -> first leaf.
+// Open addressing (linear probing) over a power-of-two table at most half
+// full; keys are cell codes (never 0), 0 marks an empty slot.
+struct GroupTable
 {
-    CellPath r;
-    r.x = __shfl_sync(0xffffffffu, c.x, src);
-    r.y = __shfl_sync(0xffffffffu, c.y, src);
-    r.z = __shfl_sync(0xffffffffu, c.z, src);
-    r.st0 = __shfl_sync(0xffffffffu, c.st0, src);
-    r.st1 = __shfl_sync(0xffffffffu, c.st1, src);
-    r.st2 = __shfl_sync(0xffffffffu, c.st2, src);
-    r.childState = __shfl_sync(0xffffffffu, c.childState, src);
-    return r;
+    u64 *keys;
+    u32 *first;
+    u32 mask;
+};
+
+// Cell code: the key prefix of a cell at `level` below a placeholder bit,
+// unique over all levels.
+__device__ __forceinline__ u64 cellCode(u64 start, unsigned level)
+{
+    return (start >> (3u * (kOctLevels - level))) | (u64(1) << (3u * level));
 }
 
-// One unit: the leaves h..h+run-1 (children of the parent P at level
-// level-1, decoded in `pp`) and the group flag of P's complete group.
-// sPos[q * 8 + o] is the block position of child octant o of the Q at lane q,
-// or 0xff where that child does not touch P.
-template <bool Hilbert>
-__device__ __forceinline__ void nearFieldUnit(const KeyIndex &idx, u32 *block, const u64 *K, const u32 *B, u32 *NF,
-                                              u8 *G, int L, unsigned bucket, int h, int run, unsigned level,
-                                              const CellPath &pp, u32 &hint, const unsigned char *sEnc,
-                                              const unsigned char *sNext, const unsigned char *sDec,
-                                              const unsigned char *sPos)
+__device__ __forceinline__ u32 codeSlot(u64 code, u32 mask)
 {
-    const int lane = threadIdx.x & 31;
-    const unsigned pl = level - 1;  // parent level
-    const u64 pRange = octRange(pl);
-    const u64 pStart = K[h] & ~(pRange - 1);
+    u64 z = code * 0x9E3779B97F4A7C15ull;  // splitmix64 finaliser
+    z ^= z >> 30;
+    z *= 0xBF58476D1CE4E5B9ull;
+    z ^= z >> 27;
+    z *= 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return u32(z) & mask;
+}
 
-    // lane q < 27: the parent-level cell Q at offset (q%3-1, q/3%3-1, q/9-1)
-    u32 lo = 0, hi = 0;
-    if (lane < 27)
+// First leaf of the complete group under the cell `code`, or -1.
+__device__ __forceinline__ int groupFirst(const GroupTable &gt, u64 code)
+{
+    u32 slot = codeSlot(code, gt.mask);
+    for (u32 probe = 0; probe <= gt.mask; ++probe)
     {
-        const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
-        const u32 cube = 1u << (kOctLevels - pl);
-        const u32 x = (pp.x + u32(dx) * cube) & 0x1fffffu;
-        const u32 y = (pp.y + u32(dy) * cube) & 0x1fffffu;
-        const u32 z = (pp.z + u32(dz) * cube) & 0x1fffffu;
-        u64 qKey = pStart;
-        int qState = pp.childState;  // Hilbert state of Q's children
-        const u32 diff = (x ^ pp.x) | (y ^ pp.y) | (z ^ pp.z);  // zero only when the wrap maps Q onto P
-        if (diff != 0)
-        {
-            if constexpr (Hilbert)
-            {
-                // Q agrees with P on the levels above the first differing bit:
-                // keep that key prefix and encode the suffix from P's state there
-                const unsigned m = unsigned(__clz(diff)) - (32u - kOctLevels);
-                const u64 word = m < 10 ? pp.st0 : (m < 20 ? pp.st1 : pp.st2);
-                int st = int((word >> (6 * (m < 10 ? m : (m < 20 ? m - 10 : m - 20)))) & 63u);
-                u64 suffix = 0;
-                for (unsigned k = m; k < pl; ++k)
-                {
-                    const unsigned b = kOctLevels - 1 - k;
-                    const unsigned o = (((x >> b) & 1u) << 2) | (((y >> b) & 1u) << 1) | ((z >> b) & 1u);
-                    const int e = st * 8 + int(o);
-                    suffix = (suffix << 3) | sEnc[e];
-                    st = sNext[e];
-                }
-                qState = st;
-                const unsigned keep = 3u * m;
-                const u64 prefix = keep ? (pStart >> (63u - keep)) << (63u - keep) : 0ull;
-                qKey = prefix | (suffix << (3u * (kOctLevels - pl)));
-            }
-            else
-            {
-                qKey = mortonKey(x, y, z);
-            }
-        }
-        lo = idx.lowerNear<kNFGallop>(hint, qKey);
-        hi = lowerFrom(idx, lo, qKey + pRange);
-        hint = lo;
+        const u64 k = __ldg(gt.keys + slot);
+        if (k == code) return int(__ldg(gt.first + slot));
+        if (k == 0) return -1;
+        slot = (slot + 1) & gt.mask;
+    }
+    return -1;
+}
 
-        const unsigned char *pos = sPos + lane * 8;
-        const u32 n = hi - lo;
-        const unsigned cShift = 3u * (kOctLevels - level);
-        const u64 *P = idx.keys + lo;
-        if (n <= kNFScanMax)
+// Inserts every complete group of the active leaves (the keys were zeroed).
+static __global__ void __launch_bounds__(kRefreshThreads) groupTableKernel(TreeBufs tb, GroupTable gt)
+{
+    const DeviceState *st = tb.st;
+    if (halted(st)) return;
+    const int a = st->activeBuffer;
+    const int L = st->numLeaves;
+    const u64 *K = tb.k(a);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x)
+    {
+        const u64 s = K[i];
+        const unsigned level = octLevel(K[i + 1] - s);
+        if (level == 0 || level > kOctLevels || octDigit(s, level) != 0 || i + 8 > L) continue;
+        if (K[i + 8] != s + octRange(level - 1)) continue;
+        const u64 code = cellCode(s, level - 1);
+        u32 slot = codeSlot(code, gt.mask);
+        for (u32 probe = 0; probe <= gt.mask; ++probe)
         {
-            // count Q's particles per child octant in registers: 16-bit fields
-            // (n <= kNFScanMax < 2^16) of two words; the child digit maps to its
-            // octant through a 3-bit-per-digit word built once for Q's state
-            u32 octOf = 0;
-            if constexpr (Hilbert)
+            const u64 prev = atomicCAS(reinterpret_cast<unsigned long long *>(gt.keys + slot), 0ull,
+                                       static_cast<unsigned long long>(code));
+            if (prev == 0ull || prev == code)
             {
-#pragma unroll
-                for (int d = 0; d < 8; ++d) octOf |= u32(sDec[qState * 8 + d]) << (3 * d);
+                gt.first[slot] = u32(i);
+                break;
             }
-            u64 lowOcts = 0, highOcts = 0;
-            for (u32 t = 0; t < n; ++t)
-            {
-                const unsigned d = unsigned(__ldg(P + t) >> cShift) & 7u;
-                const unsigned o = Hilbert ? (octOf >> (3 * d)) & 7u : d;
-                const u64 inc = u64(1) << (16 * (o & 3u));
-                if (o < 4) lowOcts += inc;
-                else highOcts += inc;
-            }
-#pragma unroll
-            for (int o = 0; o < 8; ++o)
-                if (pos[o] != 0xff) block[pos[o]] = u32(((o < 4 ? lowOcts : highOcts) >> (16 * (o & 3))) & 0xffffu);
+            slot = (slot + 1) & gt.mask;
         }
-        else
+    }
+}
+
+// Per-warp scratch of the units in flight.
+struct UnitScratch
+{
+    u64 pStart[kUnitBatch], st0[kUnitBatch], st1[kUnitBatch], st2[kUnitBatch];
+    unsigned long long qsum[kUnitBatch];  // population of the 27 Q's
+    u32 cx[kUnitBatch], cy[kUnitBatch], cz[kUnitBatch];
+    u32 hintB[kUnitBatch];                // begin index of the unit's first leaf
+    u32 pc[kUnitBatch];                   // population of P itself
+    int childState[kUnitBatch], level[kUnitBatch], active[kUnitBatch];
+    u32 block[kUnitBatch][64];
+    u64 slowKey[kUnitBatch * 27];
+    unsigned short slowItem[kUnitBatch * 27];  // unit * 27 + q
+    unsigned char slowState[kUnitBatch * 27];
+    int nSlow;
+};
+
+// Key and child Hilbert state of the parent-level cell at offset q around the
+// parent of unit u.
+template <bool Hilbert>
+__device__ __forceinline__ u64 neighbourCell(const UnitScratch &w, int u, int q, int &qState,
+                                             const unsigned char *sEnc, const unsigned char *sNext)
+{
+    const unsigned pl = unsigned(w.level[u]) - 1;
+    const u64 pStart = w.pStart[u];
+    const int dx = q % 3 - 1, dy = (q / 3) % 3 - 1, dz = q / 9 - 1;
+    const u32 cube = 1u << (kOctLevels - pl);
+    const u32 cx = w.cx[u], cy = w.cy[u], cz = w.cz[u];
+    const u32 x = (cx + u32(dx) * cube) & 0x1fffffu;
+    const u32 y = (cy + u32(dy) * cube) & 0x1fffffu;
+    const u32 z = (cz + u32(dz) * cube) & 0x1fffffu;
+    qState = w.childState[u];
+    const u32 diff = (x ^ cx) | (y ^ cy) | (z ^ cz);  // zero only when the wrap maps Q onto P
+    if (diff == 0) return pStart;
+    if constexpr (Hilbert)
+    {
+        // Q agrees with P on the levels above the first differing bit: keep
+        // that key prefix and encode the suffix from P's state there
+        const unsigned m = unsigned(__clz(diff)) - (32u - kOctLevels);
+        const u64 word = m < 10 ? w.st0[u] : (m < 20 ? w.st1[u] : w.st2[u]);
+        int st = int((word >> (6 * (m < 10 ? m : (m < 20 ? m - 10 : m - 20)))) & 63u);
+        u64 suffix = 0;
+        for (unsigned k = m; k < pl; ++k)
         {
-            const u64 cr = octRange(level);
+            const unsigned b = kOctLevels - 1 - k;
+            const unsigned o = (((x >> b) & 1u) << 2) | (((y >> b) & 1u) << 1) | ((z >> b) & 1u);
+            const int e = st * 8 + int(o);
+            suffix = (suffix << 3) | sEnc[e];
+            st = sNext[e];
+        }
+        qState = st;
+        const unsigned keep = 3u * m;
+        const u64 prefix = keep ? (pStart >> (63u - keep)) << (63u - keep) : 0ull;
+        return prefix | (suffix << (3u * (kOctLevels - pl)));
+    }
+    else
+    {
+        return mortonKey(x, y, z);
+    }
+}
+
+// Counts Q's particles [lo, lo + n) per child octant into the unit's block
+// positions `pos` (0xff: the child does not touch P).
+template <bool Hilbert>
+__device__ __forceinline__ void countChildren(const u64 *P, u32 n, u64 qKey, unsigned level, int qState,
+                                              const unsigned char *pos, u32 *block, const unsigned char *sEnc,
+                                              const unsigned char *sDec)
+{
+    const unsigned cShift = 3u * (kOctLevels - level);
+    if (n <= kNFScanMax)
+    {
+        // 16-bit counters per octant in two registers (n <= kNFScanMax < 2^16);
+        // the digit -> octant map of Q's state packed 3 bits per digit
+        u32 octOf = 0;
+        if constexpr (Hilbert)
+        {
+#pragma unroll
+            for (int d = 0; d < 8; ++d) octOf |= u32(sDec[qState * 8 + d]) << (3 * d);
+        }
+        u64 lowOcts = 0, highOcts = 0;
+        for (u32 t = 0; t < n; ++t)
+        {
+            const unsigned d = unsigned(__ldg(P + t) >> cShift) & 7u;
+            const unsigned o = Hilbert ? (octOf >> (3 * d)) & 7u : d;
+            const u64 inc = u64(1) << (16 * (o & 3u));
+            if (o < 4) lowOcts += inc;
+            else highOcts += inc;
+        }
+#pragma unroll
+        for (int o = 0; o < 8; ++o)
+            if (pos[o] != 0xff) block[pos[o]] = u32(((o < 4 ? lowOcts : highOcts) >> (16 * (o & 3))) & 0xffffu);
+    }
+    else
+    {
+        const u64 cr = octRange(level);
 #pragma unroll 1
-            for (int o = 0; o < 8; ++o)
-            {
-                const unsigned p = pos[o];
-                if (p == 0xff) continue;
-                const unsigned dg = Hilbert ? unsigned(sEnc[qState * 8 + o]) : unsigned(o);
-                const u64 cs = qKey + u64(dg) * cr;
-                block[p] = lowerBound32(P, n, cs + cr) - lowerBound32(P, n, cs);
-            }
-        }
-    }
-    __syncwarp();
-
-    // the unit's leaves: own count x population of the 3 x 3 x 3 sub-block
-    // (27 distinct cells, so at most n < 2^32, except at level 1 where the
-    // periodic wrap repeats cells)
-    if (lane < run)
-    {
-        const int i = h + lane;
-        const u32 c = B[i + 1] - B[i];
-        u32 out = 0;
-        if (c)
+        for (int o = 0; o < 8; ++o)
         {
-            const unsigned d = octDigit(K[i], level);
-            const unsigned o = Hilbert ? unsigned(sDec[pp.childState * 8 + int(d)]) : d;
-            const u32 *sub = block + (o >> 2) * 16 + ((o >> 1) & 1u) * 4 + (o & 1u);
-            u64 pop;
-            if (level > 1)
-            {
-                u32 p32 = 0;
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-#pragma unroll
-                    for (int b = 0; b < 3; ++b)
-#pragma unroll
-                        for (int e = 0; e < 3; ++e) p32 += sub[a * 16 + b * 4 + e];
-                pop = p32;
-            }
-            else
-            {
-                pop = 0;
-                for (int a = 0; a < 3; ++a)
-                    for (int b = 0; b < 3; ++b)
-                        for (int e = 0; e < 3; ++e) pop += sub[a * 16 + b * 4 + e];
-            }
-            const u64 v = u64(c) * pop;
-            out = v > 0xffffffffull ? 0xffffffffu : u32(v);
+            const unsigned p = pos[o];
+            if (p == 0xff) continue;
+            const unsigned dg = Hilbert ? unsigned(sEnc[qState * 8 + o]) : unsigned(o);
+            const u64 cs = qKey + u64(dg) * cr;
+            block[p] = lowerBound32(P, n, cs + cr) - lowerBound32(P, n, cs);
         }
-        NF[i] = out;
     }
-
-    // group flag of a complete group: parent count x population around the parent
-    u64 qpop = lane < 27 ? u64(hi - lo) : 0;
-    for (int off = 16; off > 0; off >>= 1) qpop += __shfl_xor_sync(0xffffffffu, qpop, off);
-    const u32 pc = __shfl_sync(0xffffffffu, hi - lo, 13);
-    if (lane == 0)
-    {
-        const int i0 = completeGroup(K, L, h, level, pStart, pRange);
-        if (i0 >= 0) G[i0] = u64(pc) * qpop <= u64(bucket) ? 1 : 0;
-    }
-    __syncwarp();
 }
 
 // Near-field counts and group flags of the new leaves (All: of every leaf),
-// after octBeginKernel.  Each warp takes 32 list entries at a time, cuts them
-// into runs of consecutive leaves with the same parent, decodes the runs'
-// parents lane-parallel and processes each run as one unit.  A run of empty
-// leaves whose group is incomplete or empty needs no search (NF 0; an empty
-// parent can always merge).
+// after octBeginKernel and groupTableKernel.  A run of empty leaves whose
+// group is incomplete or empty needs no work (NF 0; an empty parent can
+// always merge).
 template <bool Hilbert, bool All>
 static __global__ void __launch_bounds__(kRefreshThreads)
-    octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h)
+    octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h, GroupTable gt)
 {
     __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8], sPos[27 * 8];
-    __shared__ u32 sBlock[kRefreshThreads / 32][64];
+    __shared__ UnitScratch sWarp[kRefreshThreads / 32];
     DeviceState *st = tb.st;
     if (halted(st)) return;
     if constexpr (Hilbert)
@@ -770,8 +786,7 @@ static __global__ void __launch_bounds__(kRefreshThreads)
     }
     for (int k = threadIdx.x; k < 27 * 8; k += blockDim.x)
     {
-        // per axis: offset -1 touches P with its upper child, 0 with both, +1 with its lower;
-        // block coordinate 2 * offset + child bit + 1
+        // block coordinate 2 * offset + child bit + 1 per axis, where Q touches P
         const int q = k >> 3, o = k & 7;
         const int d[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
         const int bit[3] = {o >> 2, (o >> 1) & 1, o & 1};
@@ -791,12 +806,12 @@ static __global__ void __launch_bounds__(kRefreshThreads)
     const u32 *B = tb.b(a);
     u32 *NF = tb.nf(a);
     u8 *Gf = tb.g(a);
-    u32 *block = sBlock[threadIdx.x >> 5];
+    UnitScratch &w = sWarp[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
+    const unsigned ltMask = (1u << lane) - 1u;
     const int warpsTotal = gridDim.x * (blockDim.x / 32);
     const int w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     const int count = All ? L : st->dirtyCount;
-    u32 hint = 0;
     for (int base = w0 * 32; base < count; base += warpsTotal * 32)
     {
         const int j = base + lane;
@@ -810,52 +825,175 @@ static __global__ void __launch_bounds__(kRefreshThreads)
         const u64 pkPrev = __shfl_up_sync(0xffffffffu, pk, 1);
         const unsigned levPrev = __shfl_up_sync(0xffffffffu, lev, 1);
         const bool head = valid && (lane == 0 || i != iPrev + 1 || pk != pkPrev || lev != levPrev || lev == 0);
-        unsigned heads = __ballot_sync(0xffffffffu, head);
+        const unsigned heads = __ballot_sync(0xffffffffu, head);
         const unsigned validMask = __ballot_sync(0xffffffffu, valid);
         const unsigned nonEmpty = __ballot_sync(0xffffffffu, c != 0);
         const int endLane = 32 - __clz(validMask);
-        // decode the parents of all runs at once (head lanes)
+        const int nUnits = __popc(heads);
+        // this lane's unit (within the chunk) and, for heads, the unit's last lane + 1
+        const int myUnit = valid ? __popc(heads & (ltMask | (1u << lane))) - 1 : -1;
+        const unsigned later = heads & ~(ltMask | (1u << lane));
+        const int runEnd = later ? __ffs(later) - 1 : endLane;
         CellPath path{0, 0, 0, 0, 0, 0, kHilbertStart};
         if (head && lev > 0) path = decodeCell<Hilbert>(pk, lev - 1, sNext, sDec);
-        while (heads)
+
+        for (int b0 = 0; b0 < nUnits; b0 += kUnitBatch)
         {
-            const int hl = __ffs(heads) - 1;
-            heads &= heads - 1;
-            const int next = heads ? __ffs(heads) - 1 : endLane;
-            const int hIdx = __shfl_sync(0xffffffffu, i, hl);
-            const unsigned lv = __shfl_sync(0xffffffffu, lev, hl);
-            const int run = next - hl;
-            if (lv == 0)
+            const int nb = min(kUnitBatch, nUnits - b0);
+            // ---- set-up: the head lane of each unit of the batch
+            if (head && myUnit >= b0 && myUnit < b0 + nb)
             {
-                // the root leaf: all 27 periodic cells are the root itself
-                if (lane == 0)
+                const int u = myUnit - b0;
+                int act = 1;
+                if (lev == 0)
                 {
-                    const u64 cr = B[hIdx + 1] - B[hIdx];
+                    // the root leaf: all 27 periodic cells are the root itself
+                    const u64 cr = c;
                     const u64 v = cr * cr * 27ull;
-                    NF[hIdx] = v > 0xffffffffull ? 0xffffffffu : u32(v);
+                    NF[i] = v > 0xffffffffull ? 0xffffffffu : u32(v);
+                    act = 0;
                 }
-                continue;
-            }
-            const unsigned runMask = (next == 32 ? 0xffffffffu : ((1u << next) - 1u)) & ~((1u << hl) - 1u);
-            if ((nonEmpty & runMask) == 0)
-            {
-                // empty run: NF 0; the group flag needs a search only if the parent holds particles
-                const u64 pRange = octRange(lv - 1);
-                const u64 pStart = __shfl_sync(0xffffffffu, s, hl) & ~(pRange - 1);
-                int i0 = -1;
-                if (lane == 0) i0 = completeGroup(K, L, hIdx, lv, pStart, pRange);
-                i0 = __shfl_sync(0xffffffffu, i0, 0);
-                const bool parentEmpty = i0 < 0 || B[i0 + 8] == B[i0];
-                if (parentEmpty)
+                else
                 {
-                    if (lane >= hl && lane < next) NF[i] = 0;
-                    if (lane == 0 && i0 >= 0) Gf[i0] = 1;
-                    continue;
+                    const unsigned runMask =
+                        (runEnd == 32 ? 0xffffffffu : ((1u << runEnd) - 1u)) & ~((1u << lane) - 1u);
+                    if ((nonEmpty & runMask) == 0)
+                    {
+                        // empty run: NF 0; the flag needs the Q's only if the parent holds particles
+                        const u64 pRange = octRange(lev - 1);
+                        const int i0 = completeGroup(K, L, i, lev, pk, pRange);
+                        if (i0 < 0 || B[i0 + 8] == B[i0])
+                        {
+                            for (int t = 0; t < runEnd - lane; ++t) NF[i + t] = 0;
+                            if (i0 >= 0) Gf[i0] = 1;
+                            act = 0;
+                        }
+                    }
+                }
+                w.active[u] = act;
+                w.pStart[u] = pk;
+                w.level[u] = int(lev);
+                w.cx[u] = path.x;
+                w.cy[u] = path.y;
+                w.cz[u] = path.z;
+                w.st0[u] = path.st0;
+                w.st1[u] = path.st1;
+                w.st2[u] = path.st2;
+                w.childState[u] = path.childState;
+                w.hintB[u] = B[i];
+                w.qsum[u] = 0;
+                w.pc[u] = 0;
+            }
+            if (lane == 0) w.nSlow = 0;
+            __syncwarp();
+
+            // ---- phase A: (unit, Q) pairs over the lanes; complete groups from the table
+            const int items = nb * 27;
+            for (int ib = 0; ib < items; ib += 32)
+            {
+                const int it = ib + lane;
+                const int u = it / 27, q = it - (it / 27) * 27;
+                bool slow = false;
+                u64 qKey = 0;
+                int qState = 0;
+                if (it < items && w.active[u])
+                {
+                    qKey = neighbourCell<Hilbert>(w, u, q, qState, sEnc, sNext);
+                    const unsigned level = unsigned(w.level[u]);
+                    const int g0 = groupFirst(gt, cellCode(qKey, level - 1));
+                    if (g0 >= 0)
+                    {
+                        const unsigned char *pos = sPos + q * 8;
+#pragma unroll
+                        for (int o = 0; o < 8; ++o)
+                        {
+                            if (pos[o] == 0xff) continue;
+                            const int dg = Hilbert ? int(sEnc[qState * 8 + o]) : o;
+                            w.block[u][pos[o]] = __ldg(B + g0 + dg + 1) - __ldg(B + g0 + dg);
+                        }
+                        const u32 total = __ldg(B + g0 + 8) - __ldg(B + g0);
+                        atomicAdd(&w.qsum[u], (unsigned long long)total);
+                        if (q == 13) w.pc[u] = total;
+                    }
+                    else
+                    {
+                        slow = true;
+                    }
+                }
+                const unsigned slowMask = __ballot_sync(0xffffffffu, slow);
+                if (slow)
+                {
+                    const int k = w.nSlow + __popc(slowMask & ltMask);
+                    w.slowKey[k] = qKey;
+                    w.slowItem[k] = (unsigned short)it;
+                    w.slowState[k] = (unsigned char)qState;
+                }
+                __syncwarp();
+                if (lane == 0) w.nSlow += __popc(slowMask);
+                __syncwarp();
+            }
+
+            // ---- phase B: the other Q's by search, over the lanes
+            const int nSlow = w.nSlow;
+            for (int k = lane; k < nSlow; k += 32)
+            {
+                const int it = w.slowItem[k];
+                const int u = it / 27, q = it - u * 27;
+                const u64 qKey = w.slowKey[k];
+                const unsigned level = unsigned(w.level[u]);
+                const u64 pRange = octRange(level - 1);
+                const u32 lo = idx.lowerNear<kNFGallop>(w.hintB[u], qKey);
+                const u32 hi = lowerFrom(idx, lo, qKey + pRange);
+                countChildren<Hilbert>(idx.keys + lo, hi - lo, qKey, level, int(w.slowState[k]), sPos + q * 8,
+                                       w.block[u], sEnc, sDec);
+                atomicAdd(&w.qsum[u], (unsigned long long)(hi - lo));
+                if (q == 13) w.pc[u] = hi - lo;
+            }
+            __syncwarp();
+
+            // ---- phase C: every lane its own leaf; the head lane the group flag
+            if (valid && myUnit >= b0 && myUnit < b0 + nb)
+            {
+                const int u = myUnit - b0;
+                if (w.active[u])
+                {
+                    u32 out = 0;
+                    if (c)
+                    {
+                        const unsigned d = octDigit(s, lev);
+                        const unsigned o = Hilbert ? unsigned(sDec[w.childState[u] * 8 + int(d)]) : d;
+                        const u32 *sub = w.block[u] + (o >> 2) * 16 + ((o >> 1) & 1u) * 4 + (o & 1u);
+                        u64 pop = 0;
+                        if (lev > 1)
+                        {
+                            u32 p32 = 0;
+#pragma unroll
+                            for (int x = 0; x < 3; ++x)
+#pragma unroll
+                                for (int y = 0; y < 3; ++y)
+#pragma unroll
+                                    for (int z = 0; z < 3; ++z) p32 += sub[x * 16 + y * 4 + z];
+                            pop = p32;
+                        }
+                        else
+                        {
+                            // level 1: the periodic wrap repeats cells, the sum may exceed 2^32
+                            for (int x = 0; x < 3; ++x)
+                                for (int y = 0; y < 3; ++y)
+                                    for (int z = 0; z < 3; ++z) pop += sub[x * 16 + y * 4 + z];
+                        }
+                        const u64 v = u64(c) * pop;
+                        out = v > 0xffffffffull ? 0xffffffffu : u32(v);
+                    }
+                    NF[i] = out;
+                    if (head)
+                    {
+                        const int i0 = completeGroup(K, L, i, lev, pk, octRange(lev - 1));
+                        if (i0 >= 0) Gf[i0] = u64(w.pc[u]) * w.qsum[u] <= u64(bucket) ? 1 : 0;
+                    }
                 }
             }
-            const CellPath pp = shflPath(path, hl);
-            nearFieldUnit<Hilbert>(idx, block, K, B, NF, Gf, L, bucket, hIdx, run, lv, pp, hint, sEnc, sNext, sDec,
-                                   sPos);
+            __syncwarp();
         }
     }
 }
