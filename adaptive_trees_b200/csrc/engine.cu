@@ -554,7 +554,7 @@ struct TreeEngine::Impl
     DevMem history;
     // tree
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
-    DevMem groupKeys, groupFirst;  // group table of the near-field refresh (NFCount)
+    DevMem groupKeys, groupBegins;  // group table of the near-field refresh (NFCount)
     u32 groupMask = 0;
     size_t scanTiles = 0;
     // views
@@ -590,7 +590,7 @@ struct TreeEngine::Impl
                                &vCandStart,  &vCandLevel,  &vLvKeys[0],     &vLvKeys[1],   &vLvVals[0],
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
-                               &viewSort.counters, &viewSort.status, &groupKeys, &groupFirst};
+                               &viewSort.counters, &viewSort.status, &groupKeys, &groupBegins};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -768,7 +768,7 @@ void TreeEngine::ensurePhysical(size_t capacity)
         size_t slots = 1024;
         while (slots < 2 * (c / 8 + 1)) slots <<= 1;
         m_->groupKeys.reserve(slots * sizeof(u64), s);
-        m_->groupFirst.reserve(slots * sizeof(u32), s);
+        m_->groupBegins.reserve(slots * rb::kGroupBegins * sizeof(u32), s);
         m_->groupMask = u32(slots - 1);
     }
     physCap_ = c;
@@ -954,7 +954,7 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
     if (cfg_.nf)
     {
         const HilbertTables &h = m_->kpd.h;
-        const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupFirst.as<u32>(), m_->groupMask};
+        const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupBegins.as<u32>(), m_->groupMask};
         AOT_CHECK(cudaMemsetAsync(gt.keys, 0, (size_t(gt.mask) + 1) * sizeof(u64), s));
         rb::groupTableKernel<<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
         if (all && cfg_.hilbert)

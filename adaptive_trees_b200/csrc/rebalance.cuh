@@ -585,13 +585,17 @@ __device__ __forceinline__ CellPath decodeCell(u64 start, unsigned pl, const uns
     return c;
 }
 
-// Complete sibling groups of the active leaves: parent cell -> first leaf.
-// Open addressing (linear probing) over a power-of-two table at most half
-// full; keys are cell codes (never 0), 0 marks an empty slot.
+// Complete sibling groups of the active leaves: parent cell -> the begin
+// indices of its 8 children and its end (9 values; child counts and the
+// parent count are their differences).  Open addressing (linear probing)
+// over a power-of-two table at most half full; keys are cell codes (never 0),
+// 0 marks an empty slot.  A lookup loads a slot's key and begin indices
+// together, so a hit in the first slot costs one round trip.
+constexpr int kGroupBegins = 9;
 struct GroupTable
 {
     u64 *keys;
-    u32 *first;
+    u32 *begins;  // [slot][kGroupBegins]
     u32 mask;
 };
 
@@ -613,18 +617,22 @@ __device__ __forceinline__ u32 codeSlot(u64 code, u32 mask)
     return u32(z) & mask;
 }
 
-// First leaf of the complete group under the cell `code`, or -1.
-__device__ __forceinline__ int groupFirst(const GroupTable &gt, u64 code)
+// Begin indices of the complete group under the cell `code` (9 values into
+// b), or false.
+__device__ __forceinline__ bool groupBegins(const GroupTable &gt, u64 code, u32 (&b)[kGroupBegins])
 {
     u32 slot = codeSlot(code, gt.mask);
     for (u32 probe = 0; probe <= gt.mask; ++probe)
     {
-        const u64 k = __ldg(gt.keys + slot);
-        if (k == code) return int(__ldg(gt.first + slot));
-        if (k == 0) return -1;
+        const u32 *row = gt.begins + size_t(slot) * kGroupBegins;
+#pragma unroll
+        for (int k = 0; k < kGroupBegins; ++k) b[k] = __ldg(row + k);  // loaded beside the key
+        const u64 key = __ldg(gt.keys + slot);
+        if (key == code) return true;
+        if (key == 0) return false;
         slot = (slot + 1) & gt.mask;
     }
-    return -1;
+    return false;
 }
 
 // Inserts every complete group of the active leaves (the keys were zeroed).
@@ -635,6 +643,7 @@ static __global__ void __launch_bounds__(kRefreshThreads) groupTableKernel(TreeB
     const int a = st->activeBuffer;
     const int L = st->numLeaves;
     const u64 *K = tb.k(a);
+    const u32 *B = tb.b(a);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x)
     {
         const u64 s = K[i];
@@ -649,7 +658,9 @@ static __global__ void __launch_bounds__(kRefreshThreads) groupTableKernel(TreeB
                                        static_cast<unsigned long long>(code));
             if (prev == 0ull || prev == code)
             {
-                gt.first[slot] = u32(i);
+                u32 *row = gt.begins + size_t(slot) * kGroupBegins;
+#pragma unroll
+                for (int k = 0; k < kGroupBegins; ++k) row[k] = B[i + k];
                 break;
             }
             slot = (slot + 1) & gt.mask;
@@ -900,8 +911,8 @@ static __global__ void __launch_bounds__(kRefreshThreads)
                 {
                     qKey = neighbourCell<Hilbert>(w, u, q, qState, sEnc, sNext);
                     const unsigned level = unsigned(w.level[u]);
-                    const int g0 = groupFirst(gt, cellCode(qKey, level - 1));
-                    if (g0 >= 0)
+                    u32 gb[kGroupBegins];
+                    if (groupBegins(gt, cellCode(qKey, level - 1), gb))
                     {
                         const unsigned char *pos = sPos + q * 8;
 #pragma unroll
@@ -909,9 +920,18 @@ static __global__ void __launch_bounds__(kRefreshThreads)
                         {
                             if (pos[o] == 0xff) continue;
                             const int dg = Hilbert ? int(sEnc[qState * 8 + o]) : o;
-                            w.block[u][pos[o]] = __ldg(B + g0 + dg + 1) - __ldg(B + g0 + dg);
+                            // gb[dg + 1] - gb[dg] without dynamic register indexing
+                            u32 lo = 0, hi = 0;
+#pragma unroll
+                            for (int k = 0; k < 8; ++k)
+                                if (k == dg)
+                                {
+                                    lo = gb[k];
+                                    hi = gb[k + 1];
+                                }
+                            w.block[u][pos[o]] = hi - lo;
                         }
-                        const u32 total = __ldg(B + g0 + 8) - __ldg(B + g0);
+                        const u32 total = gb[8] - gb[0];
                         atomicAdd(&w.qsum[u], (unsigned long long)total);
                         if (q == 13) w.pc[u] = total;
                     }
