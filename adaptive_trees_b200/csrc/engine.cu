@@ -554,8 +554,9 @@ struct TreeEngine::Impl
     DevMem history;
     // tree
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
-    DevMem groupKeys, groupBegins;  // group table of the near-field refresh (NFCount)
-    u32 groupMask = 0;
+    DevMem groupKeys, groupBegins, memoKeys, memoBegins;  // cell tables of the near-field refresh (NFCount)
+    u32 groupMask = 0, memoMask = 0;
+    bool groupStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
     // views
     DevMem vBox, vSplit, vDepth, vParent, vChild, vLevelOffset, vPbegin, vPcount, vPmap, vMaxDepth;
@@ -590,7 +591,7 @@ struct TreeEngine::Impl
                                &vCandStart,  &vCandLevel,  &vLvKeys[0],     &vLvKeys[1],   &vLvVals[0],
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
-                               &viewSort.counters, &viewSort.status, &groupKeys, &groupBegins};
+                               &viewSort.counters, &viewSort.status, &groupKeys, &groupBegins, &memoKeys, &memoBegins};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -764,12 +765,19 @@ void TreeEngine::ensurePhysical(size_t capacity)
     m_->scan.reserve((m_->scanTiles + 1) * sizeof(u64), s);
     if (cfg_.kind == 0 && cfg_.nf)
     {
-        // complete groups <= leaves / 8; the table stays at most half full
+        // complete groups (<= leaves / 8) and memoised neighbour cells: half a
+        // slot per leaf in each table
         size_t slots = 1024;
-        while (slots < 2 * (c / 8 + 1)) slots <<= 1;
-        m_->groupKeys.reserve(slots * sizeof(u64), s);
-        m_->groupBegins.reserve(slots * rb::kGroupBegins * sizeof(u32), s);
-        m_->groupMask = u32(slots - 1);
+        while (slots < c / 2 + 1) slots <<= 1;
+        if (slots != size_t(m_->groupMask) + 1)
+        {
+            m_->groupKeys.reserve(slots * sizeof(u64), s);
+            m_->groupBegins.reserve(slots * rb::kGroupBegins * sizeof(u32), s);
+            m_->memoKeys.reserve(slots * sizeof(u64), s);
+            m_->memoBegins.reserve(slots * rb::kGroupBegins * sizeof(u32), s);
+            m_->groupMask = m_->memoMask = u32(slots - 1);
+            m_->groupStale = true;
+        }
     }
     physCap_ = c;
 }
@@ -779,6 +787,7 @@ void TreeEngine::ensurePhysical(size_t capacity)
 // --------------------------------------------------------------------------
 void TreeEngine::sortParticles()
 {
+    m_->groupStale = true;  // cell table entries hold indices into the sorted keys
     if (n_ == 0) return;
     cudaStream_t s = cfg_.stream;
     SortArena &a = m_->sortArena;
@@ -954,9 +963,16 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
     if (cfg_.nf)
     {
         const HilbertTables &h = m_->kpd.h;
-        const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupBegins.as<u32>(), m_->groupMask};
-        AOT_CHECK(cudaMemsetAsync(gt.keys, 0, (size_t(gt.mask) + 1) * sizeof(u64), s));
-        rb::groupTableKernel<<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
+        const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupBegins.as<u32>(), m_->groupMask,
+                                m_->memoKeys.as<u64>(),  m_->memoBegins.as<u32>(),  m_->memoMask};
+        if (m_->groupStale)
+        {
+            AOT_CHECK(cudaMemsetAsync(gt.keys, 0, (size_t(gt.mask) + 1) * sizeof(u64), s));
+            AOT_CHECK(cudaMemsetAsync(gt.memoKeys, 0, (size_t(gt.memoMask) + 1) * sizeof(u64), s));
+            m_->groupStale = false;
+        }
+        if (all) rb::groupTableKernel<true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
+        else rb::groupTableKernel<false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
         if (all && cfg_.hilbert)
             rb::octNearFieldKernel<true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();
         else if (all)

@@ -585,18 +585,32 @@ __device__ __forceinline__ CellPath decodeCell(u64 start, unsigned pl, const uns
     return c;
 }
 
-// Complete sibling groups of the active leaves: parent cell -> the begin
-// indices of its 8 children and its end (9 values; child counts and the
-// parent count are their differences).  Open addressing (linear probing)
-// over a power-of-two table at most half full; keys are cell codes (never 0),
-// 0 marks an empty slot.  A lookup loads a slot's key and begin indices
-// together, so a hit in the first slot costs one round trip.
+// Cell tables: cell -> the begin indices of its 8 children and its end (9
+// values; child counts and the cell's count are their differences).  The
+// values depend only on the sorted keys, so an entry stays right while the
+// tree changes: the tables are cleared when the particles are sorted again
+// and otherwise only grow.  Two tables:
+//   * groups: the parent cells of complete sibling groups, entered by
+//     groupTableKernel before the refresh and read-only during it, so a
+//     lookup may load a slot's key and values together (one round trip);
+//   * memo: the neighbour cells the refresh had to search for, entered while
+//     other warps read it -- a slot is claimed with kBusyCode, its values
+//     stored, then the key released, and readers acquire the key before they
+//     load the values.
+// A cell found in neither is searched, so the tables only save work.  Open
+// addressing with linear probing, at most kCellProbes probes; keys are cell
+// codes (never 0 or kBusyCode), 0 marks an empty slot.
 constexpr int kGroupBegins = 9;
+constexpr u32 kCellProbes = 64;
+constexpr u64 kBusyCode = ~u64(0);
 struct GroupTable
 {
     u64 *keys;
     u32 *begins;  // [slot][kGroupBegins]
     u32 mask;
+    u64 *memoKeys;
+    u32 *memoBegins;
+    u32 memoMask;
 };
 
 // Cell code: the key prefix of a cell at `level` below a placeholder bit,
@@ -617,12 +631,11 @@ __device__ __forceinline__ u32 codeSlot(u64 code, u32 mask)
     return u32(z) & mask;
 }
 
-// Begin indices of the complete group under the cell `code` (9 values into
-// b), or false.
+// Begin indices of the cell `code` (9 values into b), or false.
 __device__ __forceinline__ bool groupBegins(const GroupTable &gt, u64 code, u32 (&b)[kGroupBegins])
 {
     u32 slot = codeSlot(code, gt.mask);
-    for (u32 probe = 0; probe <= gt.mask; ++probe)
+    for (u32 probe = 0; probe < kCellProbes; ++probe)
     {
         const u32 *row = gt.begins + size_t(slot) * kGroupBegins;
 #pragma unroll
@@ -635,7 +648,89 @@ __device__ __forceinline__ bool groupBegins(const GroupTable &gt, u64 code, u32 
     return false;
 }
 
-// Inserts every complete group of the active leaves (the keys were zeroed).
+__device__ __forceinline__ u64 ldAcquire(const u64 *p)
+{
+    u64 v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ u32 ldRelaxed32(const u32 *p)
+{
+    u32 v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void stRelease(u64 *p, u64 v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Memo lookup (coherent with inserts running in the same kernel).
+__device__ __forceinline__ bool memoFind(const GroupTable &gt, u64 code, u32 (&b)[kGroupBegins])
+{
+    u32 slot = codeSlot(code, gt.memoMask);
+    for (u32 probe = 0; probe < kCellProbes; ++probe)
+    {
+        const u64 key = ldAcquire(gt.memoKeys + slot);
+        if (key == code)
+        {
+            const u32 *row = gt.memoBegins + size_t(slot) * kGroupBegins;
+#pragma unroll
+            for (int k = 0; k < kGroupBegins; ++k) b[k] = ldRelaxed32(row + k);
+            return true;
+        }
+        if (key == 0) return false;
+        slot = (slot + 1) & gt.memoMask;
+    }
+    return false;
+}
+
+// Memo insert: claim, store the values, release the key.
+__device__ __forceinline__ void memoInsert(const GroupTable &gt, u64 code, const u32 (&b)[kGroupBegins])
+{
+    u32 slot = codeSlot(code, gt.memoMask);
+    for (u32 probe = 0; probe < kCellProbes; ++probe)
+    {
+        u64 *key = gt.memoKeys + slot;
+        const u64 prev = atomicCAS(reinterpret_cast<unsigned long long *>(key), 0ull,
+                                   static_cast<unsigned long long>(kBusyCode));
+        if (prev == 0ull)
+        {
+            u32 *row = gt.memoBegins + size_t(slot) * kGroupBegins;
+#pragma unroll
+            for (int k = 0; k < kGroupBegins; ++k) row[k] = b[k];
+            __threadfence();
+            stRelease(key, code);
+            return;
+        }
+        if (prev == code) return;
+        slot = (slot + 1) & gt.memoMask;
+    }
+}
+
+// Enters a group cell (before the refresh; a racing insert of the same cell
+// writes the same values).
+__device__ __forceinline__ void cellInsert(const GroupTable &gt, u64 code, const u32 (&b)[kGroupBegins])
+{
+    u32 slot = codeSlot(code, gt.mask);
+    for (u32 probe = 0; probe < kCellProbes; ++probe)
+    {
+        const u64 prev = atomicCAS(reinterpret_cast<unsigned long long *>(gt.keys + slot), 0ull,
+                                   static_cast<unsigned long long>(code));
+        if (prev == 0ull || prev == code)
+        {
+            u32 *row = gt.begins + size_t(slot) * kGroupBegins;
+#pragma unroll
+            for (int k = 0; k < kGroupBegins; ++k) row[k] = b[k];
+            return;
+        }
+        slot = (slot + 1) & gt.mask;
+    }
+}
+
+// Enters the parent cells of complete sibling groups: of every leaf (All),
+// or of the new leaves of the last pass (the others are already in).
+template <bool All>
 static __global__ void __launch_bounds__(kRefreshThreads) groupTableKernel(TreeBufs tb, GroupTable gt)
 {
     const DeviceState *st = tb.st;
@@ -644,27 +739,23 @@ static __global__ void __launch_bounds__(kRefreshThreads) groupTableKernel(TreeB
     const int L = st->numLeaves;
     const u64 *K = tb.k(a);
     const u32 *B = tb.b(a);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x)
+    const int count = All ? L : st->dirtyCount;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
     {
+        const int i = All ? j : tb.dirty[j];
         const u64 s = K[i];
         const unsigned level = octLevel(K[i + 1] - s);
-        if (level == 0 || level > kOctLevels || octDigit(s, level) != 0 || i + 8 > L) continue;
-        if (K[i + 8] != s + octRange(level - 1)) continue;
-        const u64 code = cellCode(s, level - 1);
-        u32 slot = codeSlot(code, gt.mask);
-        for (u32 probe = 0; probe <= gt.mask; ++probe)
-        {
-            const u64 prev = atomicCAS(reinterpret_cast<unsigned long long *>(gt.keys + slot), 0ull,
-                                       static_cast<unsigned long long>(code));
-            if (prev == 0ull || prev == code)
-            {
-                u32 *row = gt.begins + size_t(slot) * kGroupBegins;
+        if (level == 0 || level > kOctLevels) continue;
+        const int i0 = i - int(octDigit(s, level));  // the group's first leaf
+        if (All && i0 != i) continue;                // one insert per group
+        if (i0 < 0 || i0 + 8 > L) continue;
+        const u64 pRange = octRange(level - 1);
+        const u64 pStart = s & ~(pRange - 1);
+        if (K[i0] != pStart || K[i0 + 8] != pStart + pRange) continue;
+        u32 b[kGroupBegins];
 #pragma unroll
-                for (int k = 0; k < kGroupBegins; ++k) row[k] = B[i + k];
-                break;
-            }
-            slot = (slot + 1) & gt.mask;
-        }
+        for (int k = 0; k < kGroupBegins; ++k) b[k] = B[i0 + k];
+        cellInsert(gt, cellCode(pStart, level - 1), b);
     }
 }
 
@@ -729,12 +820,14 @@ __device__ __forceinline__ u64 neighbourCell(const UnitScratch &w, int u, int q,
 }
 
 // Counts Q's particles [lo, lo + n) per child octant into the unit's block
-// positions `pos` (0xff: the child does not touch P).
+// positions `pos` (0xff: the child does not touch P).  A scanned range also
+// gives the begin indices of all 8 children (into `begins`, returns true).
 template <bool Hilbert>
-__device__ __forceinline__ void countChildren(const u64 *P, u32 n, u64 qKey, unsigned level, int qState,
+__device__ __forceinline__ bool countChildren(const u64 *P, u32 lo, u32 n, u64 qKey, unsigned level, int qState,
                                               const unsigned char *pos, u32 *block, const unsigned char *sEnc,
-                                              const unsigned char *sDec)
+                                              const unsigned char *sDec, u32 (&begins)[kGroupBegins])
 {
+    P += lo;
     const unsigned cShift = 3u * (kOctLevels - level);
     if (n <= kNFScanMax)
     {
@@ -758,20 +851,27 @@ __device__ __forceinline__ void countChildren(const u64 *P, u32 n, u64 qKey, uns
 #pragma unroll
         for (int o = 0; o < 8; ++o)
             if (pos[o] != 0xff) block[pos[o]] = u32(((o < 4 ? lowOcts : highOcts) >> (16 * (o & 3))) & 0xffffu);
-    }
-    else
-    {
-        const u64 cr = octRange(level);
-#pragma unroll 1
-        for (int o = 0; o < 8; ++o)
+        // children in digit order: begin indices
+        begins[0] = lo;
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
         {
-            const unsigned p = pos[o];
-            if (p == 0xff) continue;
-            const unsigned dg = Hilbert ? unsigned(sEnc[qState * 8 + o]) : unsigned(o);
-            const u64 cs = qKey + u64(dg) * cr;
-            block[p] = lowerBound32(P, n, cs + cr) - lowerBound32(P, n, cs);
+            const unsigned o = Hilbert ? (octOf >> (3 * d)) & 7u : unsigned(d);
+            begins[d + 1] = begins[d] + u32(((o < 4 ? lowOcts : highOcts) >> (16 * (o & 3u))) & 0xffffu);
         }
+        return true;
     }
+    const u64 cr = octRange(level);
+#pragma unroll 1
+    for (int o = 0; o < 8; ++o)
+    {
+        const unsigned p = pos[o];
+        if (p == 0xff) continue;
+        const unsigned dg = Hilbert ? unsigned(sEnc[qState * 8 + o]) : unsigned(o);
+        const u64 cs = qKey + u64(dg) * cr;
+        block[p] = lowerBound32(P, n, cs + cr) - lowerBound32(P, n, cs);
+    }
+    return false;
 }
 
 // Near-field counts and group flags of the new leaves (All: of every leaf),
@@ -779,7 +879,7 @@ __device__ __forceinline__ void countChildren(const u64 *P, u32 n, u64 qKey, uns
 // group is incomplete or empty needs no work (NF 0; an empty parent can
 // always merge).
 template <bool Hilbert, bool All>
-static __global__ void __launch_bounds__(kRefreshThreads)
+static __global__ void __launch_bounds__(kRefreshThreads, 4)
     octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h, GroupTable gt)
 {
     __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8], sPos[27 * 8];
@@ -962,12 +1062,42 @@ static __global__ void __launch_bounds__(kRefreshThreads)
                 const u64 qKey = w.slowKey[k];
                 const unsigned level = unsigned(w.level[u]);
                 const u64 pRange = octRange(level - 1);
-                const u32 lo = idx.lowerNear<kNFGallop>(w.hintB[u], qKey);
-                const u32 hi = lowerFrom(idx, lo, qKey + pRange);
-                countChildren<Hilbert>(idx.keys + lo, hi - lo, qKey, level, int(w.slowState[k]), sPos + q * 8,
-                                       w.block[u], sEnc, sDec);
-                atomicAdd(&w.qsum[u], (unsigned long long)(hi - lo));
-                if (q == 13) w.pc[u] = hi - lo;
+                const u64 code = cellCode(qKey, level - 1);
+                const int qState = int(w.slowState[k]);
+                u32 begins[kGroupBegins];
+                u32 total;
+                if (memoFind(gt, code, begins))
+                {
+                    // searched before by another unit
+                    const unsigned char *pos = sPos + q * 8;
+#pragma unroll
+                    for (int o = 0; o < 8; ++o)
+                    {
+                        if (pos[o] == 0xff) continue;
+                        const int dg = Hilbert ? int(sEnc[qState * 8 + o]) : o;
+                        u32 b0 = 0, b1 = 0;
+#pragma unroll
+                        for (int t = 0; t < 8; ++t)
+                            if (t == dg)
+                            {
+                                b0 = begins[t];
+                                b1 = begins[t + 1];
+                            }
+                        w.block[u][pos[o]] = b1 - b0;
+                    }
+                    total = begins[8] - begins[0];
+                }
+                else
+                {
+                    const u32 lo = idx.lowerNear<kNFGallop>(w.hintB[u], qKey);
+                    const u32 hi = lowerFrom(idx, lo, qKey + pRange);
+                    if (countChildren<Hilbert>(idx.keys, lo, hi - lo, qKey, level, qState, sPos + q * 8, w.block[u],
+                                               sEnc, sDec, begins))
+                        memoInsert(gt, code, begins);  // for the next units that need Q
+                    total = hi - lo;
+                }
+                atomicAdd(&w.qsum[u], (unsigned long long)total);
+                if (q == 13) w.pc[u] = total;
             }
             __syncwarp();
 
