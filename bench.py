@@ -37,9 +37,9 @@ N_DEFAULT = 1 << 24
 BUCKET = 512
 METRIC = "particles/s (octree build, 16Mi Plummer fp32, Hilbert, NFCount 512)"
 WORKLOAD = "octree build + graph-replayed update, 16Mi Plummer fp32 (a=0.05, r<=0.5), Hilbert keys, NFCount 512"
-# DRAM bytes of one 16Mi-key onesweep pass (key+value in and out), from the ncu
-# capture summarised in profiles/onesweep_pass_16Mi.txt; None until captured.
-ONESWEEP_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) of one 16Mi-key onesweep pass, from the ncu capture
+# summarised in profiles/onesweepKernel_pass_16Mi.md (201.7 MB + 153.4 MB).
+ONESWEEP_TRAFFIC_BYTES = 355.1e6
 
 
 def plummer(n, seed, scale=0.05, rmax=0.5):
