@@ -819,6 +819,22 @@ __device__ __forceinline__ u64 neighbourCell(const UnitScratch &w, int u, int q,
     }
 }
 
+// Child counts of Q from its 9 begin indices (children in digit order) into
+// the unit's block positions `pos` (0xff: the child does not touch P).  The
+// loop runs over digits, so the register array is indexed statically.
+template <bool Hilbert>
+__device__ __forceinline__ void childrenFromBegins(const u32 (&b)[kGroupBegins], int qState, const unsigned char *pos,
+                                                   u32 *block, const unsigned char *sDec)
+{
+#pragma unroll
+    for (int d = 0; d < 8; ++d)
+    {
+        const unsigned o = Hilbert ? unsigned(sDec[qState * 8 + d]) : unsigned(d);
+        const unsigned p = pos[o];
+        if (p != 0xff) block[p] = b[d + 1] - b[d];
+    }
+}
+
 // Counts Q's particles [lo, lo + n) per child octant into the unit's block
 // positions `pos` (0xff: the child does not touch P).  A scanned range also
 // gives the begin indices of all 8 children (into `begins`, returns true).
@@ -1014,23 +1030,7 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                     u32 gb[kGroupBegins];
                     if (groupBegins(gt, cellCode(qKey, level - 1), gb))
                     {
-                        const unsigned char *pos = sPos + q * 8;
-#pragma unroll
-                        for (int o = 0; o < 8; ++o)
-                        {
-                            if (pos[o] == 0xff) continue;
-                            const int dg = Hilbert ? int(sEnc[qState * 8 + o]) : o;
-                            // gb[dg + 1] - gb[dg] without dynamic register indexing
-                            u32 lo = 0, hi = 0;
-#pragma unroll
-                            for (int k = 0; k < 8; ++k)
-                                if (k == dg)
-                                {
-                                    lo = gb[k];
-                                    hi = gb[k + 1];
-                                }
-                            w.block[u][pos[o]] = hi - lo;
-                        }
+                        childrenFromBegins<Hilbert>(gb, qState, sPos + q * 8, w.block[u], sDec);
                         const u32 total = gb[8] - gb[0];
                         atomicAdd(&w.qsum[u], (unsigned long long)total);
                         if (q == 13) w.pc[u] = total;
@@ -1069,22 +1069,7 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                 if (memoFind(gt, code, begins))
                 {
                     // searched before by another unit
-                    const unsigned char *pos = sPos + q * 8;
-#pragma unroll
-                    for (int o = 0; o < 8; ++o)
-                    {
-                        if (pos[o] == 0xff) continue;
-                        const int dg = Hilbert ? int(sEnc[qState * 8 + o]) : o;
-                        u32 b0 = 0, b1 = 0;
-#pragma unroll
-                        for (int t = 0; t < 8; ++t)
-                            if (t == dg)
-                            {
-                                b0 = begins[t];
-                                b1 = begins[t + 1];
-                            }
-                        w.block[u][pos[o]] = b1 - b0;
-                    }
+                    childrenFromBegins<Hilbert>(begins, qState, sPos + q * 8, w.block[u], sDec);
                     total = begins[8] - begins[0];
                 }
                 else
