@@ -766,15 +766,17 @@ def main():
         # ---------------- timed builds (inputs 192 MiB > L2: no flush needed)
         barrier()
         build_ms = []
-        with ClockSampler(local) as clocks:
-            for _ in range(args.steps):
-                a, b = ev(), ev()
-                a.record(s)
-                tree.build()
-                b.record(s)
-                b.synchronize()
-                build_ms.append(a.elapsed_time(b))
-            barrier()
+        # clocks are sampled across the timed builds, updates and end-to-end steps
+        clocks = ClockSampler(local)
+        clocks.__enter__()
+        for _ in range(args.steps):
+            a, b = ev(), ev()
+            a.record(s)
+            tree.build()
+            b.record(s)
+            b.synchronize()
+            build_ms.append(a.elapsed_time(b))
+        barrier()
         launches = tree.info().kernel_launches - launches0
         info = tree.info()
         leaves = info.num_leaves
@@ -840,6 +842,8 @@ def main():
             if i >= args.warmup:
                 e2e_ms.append(a.elapsed_time(b))
         assert int(host_counters[0]) == leaves
+
+        clocks.__exit__(None, None, None)
 
         # ---------------- roofline: onesweep pass timed live via ao_sort_pairs,
         # replayed from CUDA graphs so no host launch time is inside the events
