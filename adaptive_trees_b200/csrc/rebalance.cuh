@@ -368,17 +368,19 @@ template <bool NF>
 __device__ __forceinline__ void octScatterLeaf(const TreeBufs &tb, DeviceState *st, int i, int L, int a, int b,
                                                long long total)
 {
+    const int lane = threadIdx.x & 31;
     int nDirty = 0, op = 0;
     i64 ni = 0;
+    u64 start = 0, nr = 0;
+    u64 *Kn = tb.k(b);
     if (i < L)
     {
         const u64 *K = tb.k(a);
         const i64 *offs = tb.offs;
         op = opAt(offs, i);
-        const u64 start = K[i];
+        start = K[i];
         const unsigned level = octLevel(K[i + 1] - start);
         ni = offs[i];
-        u64 *Kn = tb.k(b);
         u32 *Bn = tb.b(b);
         if (op == 1)
         {
@@ -404,29 +406,54 @@ __device__ __forceinline__ void octScatterLeaf(const TreeBufs &tb, DeviceState *
         }
         else if (op > 1)
         {
-            const u64 nr = octRange(level + splitLevels(op));
-            for (int c = 0; c < op; ++c) Kn[ni + c] = start + u64(c) * nr;
+            nr = octRange(level + splitLevels(op));
             Bn[ni] = tb.b(a)[i];  // the first child starts where the parent did
             nDirty = NF ? op : op - 1;
         }
         if (i == 0)
         {
             Kn[total] = kMaxKey;
-            Bn[total] = st->numActiveParticles;
+            tb.b(b)[total] = st->numActiveParticles;
         }
     }
     // work lists (warp-aggregated appends; list order is irrelevant)
     const int d0 = warpAppend(&st->dirtyCount, nDirty);
-    if (nDirty)
+    if (nDirty && op == 1) tb.dirty[d0] = int(ni);
+    // the children of the warp's split leaves, written by all lanes together
+    // (consecutive children in consecutive lanes): each child finds its
+    // leaf as the last lane whose exclusive child offset is <= its index
+    const int children = op > 1 ? op : 0;
+    int inc = children;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1)
     {
-        if (op > 1)
+        const int t = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += t;
+    }
+    const int excl = inc - children;
+    const int warpChildren = __shfl_sync(0xffffffffu, inc, 31);
+    const int c0 = NF ? 0 : 1;  // LeafCount: the first child needs no search
+    for (int base = 0; base < warpChildren; base += 32)
+    {
+        const int t = base + lane;
+        int owner = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
         {
-            const int c0 = NF ? 0 : 1;
-            for (int c = c0; c < op; ++c) tb.dirty[d0 + c - c0] = int(ni) + c;
+            const int cand = owner + step;
+            const int ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+            if (cand < 32 && ex <= t) owner = cand;
         }
-        else
+        const i64 niL = __shfl_sync(0xffffffffu, ni, owner);
+        const u64 startL = __shfl_sync(0xffffffffu, start, owner);
+        const u64 nrL = __shfl_sync(0xffffffffu, nr, owner);
+        const int d0L = __shfl_sync(0xffffffffu, d0, owner);
+        const int exL = __shfl_sync(0xffffffffu, excl, owner);
+        if (t < warpChildren)
         {
-            tb.dirty[d0] = int(ni);
+            const int c = t - exL;
+            Kn[niL + c] = startL + u64(c) * nrL;
+            if (c >= c0) tb.dirty[d0L + c - c0] = int(niL) + c;
         }
     }
 }
