@@ -91,6 +91,7 @@ PROTOTYPES = {
     "ao_serve_get_stats": [vp, ctypes.POINTER(AoServeStats)],
     "ao_serve_reset_stats": [vp],
     "ao_release_cached_memory": [],
+    "ao_tree_gather": [vp, vp, vp, sz],
 }
 
 # n limit of ao_sort_pairs_noalloc (AO_SORT_PAIRS_NOALLOC_MAX_ITEMS)

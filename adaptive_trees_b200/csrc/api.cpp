@@ -444,6 +444,14 @@ ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsigned lon
     });
 }
 
+ao_status ao_tree_gather(ao_tree *tree, const void *src, void *dst, size_t elem_bytes)
+{
+    return guarded([&] {
+        if (!tree) throw std::invalid_argument("ao_tree_gather: null tree");
+        tree->engine->gather(src, dst, elem_bytes);
+    });
+}
+
 ao_status ao_batch_create(int real_type, int num_systems, const void *const *x, const void *const *y,
                           const void *const *z, const size_t *counts, const ao_config *config, void *stream,
                           ao_batch **out)

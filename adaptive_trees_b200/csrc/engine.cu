@@ -713,6 +713,48 @@ TreeEngine::TreeEngine(const void *x, const void *y, const void *z, size_t n, co
 
 size_t TreeEngine::deviceBytes() const { return m_->bytes(); }
 
+namespace
+{
+// dst[i] = src[perm[i]], W-byte words
+template <class W>
+__global__ void gatherKernel(const W *__restrict__ src, W *__restrict__ dst, const u32 *__restrict__ perm, size_t n)
+{
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        dst[i] = src[perm[i]];
+}
+__global__ void gatherBytesKernel(const unsigned char *__restrict__ src, unsigned char *__restrict__ dst,
+                                  const u32 *__restrict__ perm, size_t n, size_t e)
+{
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    {
+        const unsigned char *s = src + size_t(perm[i]) * e;
+        for (size_t b = 0; b < e; ++b) dst[i * e + b] = s[b];
+    }
+}
+}  // namespace
+
+void TreeEngine::gather(const void *src, void *dst, size_t elemBytes) const
+{
+    if (n_ == 0) return;
+    if (!src || !dst) throw std::invalid_argument("adaptive_octree: gather needs device source and destination");
+    if (elemBytes == 0) throw std::invalid_argument("adaptive_octree: gather element size must be positive");
+    if (src == dst) throw std::invalid_argument("adaptive_octree: gather cannot work in place");
+    cudaStream_t s = cfg_.stream;
+    const u32 *perm = m_->Perm[0].as<u32>();
+    const unsigned blocks = std::min<unsigned>(gridFor(n_, 256), unsigned(smCount()) * 16u);
+    const uintptr_t align = reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst);
+    if (elemBytes == 4 && align % 4 == 0)
+        gatherKernel<u32><<<blocks, 256, 0, s>>>(static_cast<const u32 *>(src), static_cast<u32 *>(dst), perm, n_), noteLaunch();
+    else if (elemBytes == 8 && align % 8 == 0)
+        gatherKernel<u64><<<blocks, 256, 0, s>>>(static_cast<const u64 *>(src), static_cast<u64 *>(dst), perm, n_), noteLaunch();
+    else if (elemBytes == 16 && align % 16 == 0)
+        gatherKernel<uint4><<<blocks, 256, 0, s>>>(static_cast<const uint4 *>(src), static_cast<uint4 *>(dst), perm, n_), noteLaunch();
+    else
+        gatherBytesKernel<<<blocks, 256, 0, s>>>(static_cast<const unsigned char *>(src), static_cast<unsigned char *>(dst),
+                                                 perm, n_, elemBytes), noteLaunch();
+    AOT_LAUNCH_CHECK();
+}
+
 // The buffers go back to the block cache: no queued work may still use them.
 TreeEngine::~TreeEngine()
 {
@@ -1371,6 +1413,7 @@ void TreeEngine::buffer(int which, const void **ptr, size_t *len, size_t *cap, s
         c = m.vPcount.bytes / 4;
         e = 4;
         break;
+    case LeafBegins: p = m.B[a].p; l = hostLeaves_ + 1; c = physCap_ + 1; e = 4; break;
     case SfcParticleIndex:
         p = m.vPmap.p;
         l = (m.viewScratch && m.viewPrepared.particleMapping) ? m.mappingLogical : 0;

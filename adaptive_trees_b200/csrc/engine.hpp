@@ -116,7 +116,8 @@ public:
     enum Buffer
     {
         ParticleKeys = 0, Perm, Cornerstone, LeafCounts, NearFieldCounts, SfcBoxIndex, HasBoxSplit, BoxDepth,
-        ParentIndex, ChildIndex, LevelOffset, ParticleBeginIndex, ParticleCounts, SfcParticleIndex, NumBuffers
+        ParentIndex, ChildIndex, LevelOffset, ParticleBeginIndex, ParticleCounts, SfcParticleIndex, LeafBegins,
+        NumBuffers
     };
     void buffer(int which, const void **ptr, size_t *len, size_t *cap, size_t *elemBytes) const;
     const int *numLeavesDevice() const;
@@ -142,6 +143,9 @@ public:
     static void sortPairs(void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
                           unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
                           int beginBit, int endBit, cudaStream_t s);
+    // dst[i] = src[perm[i]] for the numParticles() elements of elemBytes
+    // each: per-particle data in key order (device pointers, the tree's stream)
+    void gather(const void *src, void *dst, size_t elemBytes) const;
     // one-shot key generation without a sort (computeSfcKeys semantics)
     static void computeKeys(int kind, int real, const void *x, const void *y, const void *z, size_t n,
                             const double *box, bool hilbert, unsigned maxDepth, unsigned long long *keys,

@@ -73,7 +73,7 @@ BUFFERS = {
     "nearFieldCounts_d": (4, "<u4"), "sfcBoxIndex_d": (5, "<u8"), "hasBoxSplit_d": (6, "|u1"),
     "boxDepth_d": (7, "|u1"), "parentIndex_d": (8, "<i4"), "childIndex_d": (9, "<i4"),
     "levelOffset_d": (10, "<i4"), "particleBeginIndex_d": (11, "<u4"), "particleCounts_d": (12, "<u4"),
-    "sfcParticleIndex_d": (13, "<u8"),
+    "sfcParticleIndex_d": (13, "<u8"), "leafBegins_d": (14, "<u4"),
 }
 
 
@@ -174,6 +174,17 @@ class Tree:
     def get(self, name: str):
         p, n, _, typestr = self.buffer_info(name)
         return device_tensor(p, n, typestr)
+
+    def gather(self, t):
+        """Per-particle data in key order: out[i] = t[perm[i]] (device tensor, first dim numParticles)."""
+        torch = _torch()
+        if not t.is_cuda or t.shape[0] != self.numParticles():
+            raise ValueError("gather needs a CUDA tensor with numParticles rows")
+        t = t.contiguous()
+        out = torch.empty_like(t)
+        if t.numel():
+            C.check(C.load().ao_tree_gather(self._h, t.data_ptr(), out.data_ptr(), t.element_size() * t[0].numel()))
+        return out
 
     def info(self) -> C.AoTreeInfo:
         i = C.AoTreeInfo()

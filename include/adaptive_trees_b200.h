@@ -59,7 +59,10 @@ enum
     AO_BUF_LEVEL_OFFSET = 10,        /* levelOffset_d       i32, 23 (octree) / 65 (binary) */
     AO_BUF_PARTICLE_BEGIN_INDEX = 11,/* particleBeginIndex_d u32, numNodes                */
     AO_BUF_PARTICLE_COUNTS = 12,     /* particleCounts_d    u32, numNodes + 1             */
-    AO_BUF_SFC_PARTICLE_INDEX = 13   /* sfcParticleIndex_d  u64, numActiveParticles       */
+    AO_BUF_SFC_PARTICLE_INDEX = 13,  /* sfcParticleIndex_d  u64, numActiveParticles       */
+    AO_BUF_LEAF_BEGINS = 14          /* first particle (index into P) of every leaf and the active end,
+                                        u32, numLeaves + 1; no getter in the reference (its counts'
+                                        prefix sum), kept by this engine for the near field of an FMM */
 };
 
 /* TreeConfig<Real> (config.hpp:147-160); the box is given in double and
@@ -291,6 +294,12 @@ AO_API ao_status ao_serve_reset_stats(ao_server *server);
 /* Freed device blocks are kept for reuse by later trees (cudaMalloc and
  * cudaFree would synchronise the device); this hands them back to the driver. */
 AO_API ao_status ao_release_cached_memory(void);
+
+/* Per-particle data in key order, the gather an FMM does after the tree is
+ * built (no entry point in the reference; its callers index with perm_d):
+ * dst[i] = src[perm[i]] for the tree's numParticles() elements of
+ * elem_bytes each.  Device pointers, not overlapping; on the tree's stream. */
+AO_API ao_status ao_tree_gather(ao_tree *tree, const void *src, void *dst, size_t elem_bytes);
 
 /* Message of the last failed call on this thread ("" if none). */
 AO_API const char *ao_last_error(void);
