@@ -92,6 +92,15 @@ PROTOTYPES = {
     "ao_serve_reset_stats": [vp],
     "ao_release_cached_memory": [],
     "ao_tree_gather": [vp, vp, vp, sz],
+    "ao_read_particles": [ctypes.c_char_p, ci, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                          ctypes.POINTER(sz)],
+    "ao_free": [vp],
+    "ao_read_manifest": [ctypes.c_char_p, ctypes.POINTER(vp)],
+    "ao_manifest_info": [vp, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(sz), ctypes.POINTER(ctypes.c_double),
+                         ctypes.POINTER(sz)],
+    "ao_manifest_frame": [vp, sz, ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ci),
+                          ctypes.POINTER(ctypes.c_char_p)],
+    "ao_manifest_destroy": [vp],
 }
 
 # n limit of ao_sort_pairs_noalloc (AO_SORT_PAIRS_NOALLOC_MAX_ITEMS)

@@ -1,5 +1,9 @@
 // api.cpp -- adaptive_octree::Octree<Real> / KDTree3D<Real> and the C ABI over TreeEngine.
+#include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <vector>
 #include <new>
 #include <ostream>
 #include <string>
@@ -8,6 +12,7 @@
 #include "adaptive_trees_b200.h"
 #include "engine.hpp"
 #include "forest.hpp"
+#include "particle_io.hpp"
 #include "serve.hpp"
 
 namespace adaptive_octree
@@ -227,6 +232,11 @@ struct ao_batch
 struct ao_server
 {
     std::unique_ptr<aot::Server> server;
+};
+
+struct ao_manifest
+{
+    aot::io::Manifest m;
 };
 
 namespace
@@ -628,6 +638,86 @@ ao_status ao_serve_reset_stats(ao_server *server)
 ao_status ao_release_cached_memory(void)
 {
     return guarded([&] { aot::blockcache::trim(); });
+}
+
+ao_status ao_read_particles(const char *path, int layout, double **x, double **y, double **z, size_t *n)
+{
+    return guarded([&] {
+        if (!path || !x || !y || !z || !n) throw std::invalid_argument("ao_read_particles: null argument");
+        *x = *y = *z = nullptr;
+        *n = 0;
+        std::vector<double> vx, vy, vz;
+        if (layout == AO_LAYOUT_BINARY_XYZ) aot::io::readBinary(path, vx, vy, vz);
+        else if (layout == AO_LAYOUT_CHARGE_XYZ) aot::io::readText(path, 1, vx, vy, vz);
+        else if (layout == AO_LAYOUT_XYZ_CHARGE) aot::io::readText(path, 0, vx, vy, vz);
+        else throw std::invalid_argument("ao_read_particles: unknown layout");
+        const size_t bytes = std::max<size_t>(vx.size(), 1) * sizeof(double);
+        double *px = static_cast<double *>(std::malloc(bytes));
+        double *py = static_cast<double *>(std::malloc(bytes));
+        double *pz = static_cast<double *>(std::malloc(bytes));
+        if (!px || !py || !pz)
+        {
+            std::free(px);
+            std::free(py);
+            std::free(pz);
+            throw std::bad_alloc();
+        }
+        std::memcpy(px, vx.data(), vx.size() * sizeof(double));
+        std::memcpy(py, vy.data(), vy.size() * sizeof(double));
+        std::memcpy(pz, vz.data(), vz.size() * sizeof(double));
+        *x = px;
+        *y = py;
+        *z = pz;
+        *n = vx.size();
+    });
+}
+
+ao_status ao_free(void *p)
+{
+    std::free(p);
+    return AO_OK;
+}
+
+ao_status ao_read_manifest(const char *path, ao_manifest **out)
+{
+    return guarded([&] {
+        if (!path || !out) throw std::invalid_argument("ao_read_manifest: null argument");
+        *out = nullptr;
+        auto m = std::make_unique<ao_manifest>();
+        m->m = aot::io::readManifest(path);
+        *out = m.release();
+    });
+}
+
+ao_status ao_manifest_info(const ao_manifest *manifest, const char **dataset, size_t *slots, double *box6,
+                           size_t *frames)
+{
+    return guarded([&] {
+        if (!manifest) throw std::invalid_argument("ao_manifest_info: null manifest");
+        if (dataset) *dataset = manifest->m.dataset.c_str();
+        if (slots) *slots = manifest->m.slots;
+        if (box6) std::memcpy(box6, manifest->m.box, sizeof(manifest->m.box));
+        if (frames) *frames = manifest->m.frames.size();
+    });
+}
+
+ao_status ao_manifest_frame(const ao_manifest *manifest, size_t i, int *index, long long *id, int *layout,
+                            const char **path)
+{
+    return guarded([&] {
+        if (!manifest) throw std::invalid_argument("ao_manifest_frame: null manifest");
+        if (i >= manifest->m.frames.size()) throw std::invalid_argument("ao_manifest_frame: no such frame");
+        const auto &f = manifest->m.frames[i];
+        if (index) *index = f.index;
+        if (id) *id = f.id;
+        if (layout) *layout = f.layout;
+        if (path) *path = f.path.c_str();
+    });
+}
+
+ao_status ao_manifest_destroy(ao_manifest *manifest)
+{
+    return guarded([&] { delete manifest; });
 }
 
 ao_status ao_sort_pairs_noalloc(const unsigned long long *keys_in, unsigned long long *keys_out,

@@ -301,6 +301,31 @@ AO_API ao_status ao_release_cached_memory(void);
  * elem_bytes each.  Device pointers, not overlapping; on the tree's stream. */
 AO_API ao_status ao_tree_gather(ao_tree *tree, const void *src, void *dst, size_t elem_bytes);
 
+/* ---------------------------------------------------------------------------
+ * Particle files and dataset manifests of the reference's tests and benchmarks
+ * (tests/particle_io.hpp; benchmarks/drivers/common.hpp:62-175), so the same
+ * inputs feed this engine.  Text rows: four numbers in charge-x-y-z or
+ * x-y-z-charge order, or ESC for an escaped particle that keeps its slot
+ * (blank and '#' rows skipped).  Binary frames: x y z doubles, NaN x = escaped.
+ * Escaped particles read as the escape coordinate (DBL_MAX) on every axis.
+ * ------------------------------------------------------------------------- */
+enum { AO_LAYOUT_CHARGE_XYZ = 0, AO_LAYOUT_XYZ_CHARGE = 1, AO_LAYOUT_BINARY_XYZ = 2 };
+
+/* *x, *y, *z receive malloc'ed host arrays of *n doubles; release them with ao_free. */
+AO_API ao_status ao_read_particles(const char *path, int layout, double **x, double **y, double **z, size_t *n);
+AO_API ao_status ao_free(void *p);
+
+typedef struct ao_manifest ao_manifest;
+AO_API ao_status ao_read_manifest(const char *path, ao_manifest **out);
+/* dataset name, particle slots of every frame, the shared box, frame count */
+AO_API ao_status ao_manifest_info(const ao_manifest *manifest, const char **dataset, size_t *slots, double *box6,
+                                  size_t *frames);
+/* frame i: its index and id, layout (AO_LAYOUT_*), and file path (relative
+ * paths resolved against the manifest's directory) */
+AO_API ao_status ao_manifest_frame(const ao_manifest *manifest, size_t i, int *index, long long *id, int *layout,
+                                   const char **path);
+AO_API ao_status ao_manifest_destroy(ao_manifest *manifest);
+
 /* Message of the last failed call on this thread ("" if none). */
 AO_API const char *ao_last_error(void);
 
