@@ -64,6 +64,7 @@ PROTOTYPES = {
     "ao_tree_destroy": [vp],
     "ao_tree_build": [vp],
     "ao_tree_update": [vp],
+    "ao_tree_update_until_converged": [vp, ci, ctypes.POINTER(ci)],
     "ao_tree_compute_views": [vp, ctypes.POINTER(AoViewConfig)],
     "ao_tree_needs_resize": [vp, ctypes.POINTER(ci)],
     "ao_tree_resize_buffers": [vp],
@@ -78,6 +79,7 @@ PROTOTYPES = {
     "ao_batch_destroy": [vp],
     "ao_batch_build": [vp],
     "ao_batch_update": [vp, vp],
+    "ao_batch_update_until_converged": [vp, vp, ci, ctypes.POINTER(ci)],
     "ao_batch_needs_resize": [vp, ctypes.POINTER(ci)],
     "ao_batch_resize_buffers": [vp],
     "ao_batch_set_coordinates": [vp, ci, vp, vp, vp],

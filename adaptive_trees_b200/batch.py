@@ -73,6 +73,17 @@ class Batch:
             arr = (ctypes.c_ubyte * self.num_systems)(*[1 if f else 0 for f in frozen])
             C.check(C.load().ao_batch_update(self._h, arr))
 
+    def updateUntilConverged(self, max_passes: int = 64, frozen=None) -> int:
+        """Opt-in: update passes until one changes no system, at most
+        `max_passes`; returns the passes that changed some system.  Every
+        system's tree equals update() with updateIterations = max_passes."""
+        arr = None
+        if frozen is not None:
+            arr = (ctypes.c_ubyte * self.num_systems)(*[1 if f else 0 for f in frozen])
+        out = ctypes.c_int()
+        C.check(C.load().ao_batch_update_until_converged(self._h, arr, int(max_passes), ctypes.byref(out)))
+        return out.value
+
     def doBuffersNeedResize(self) -> bool:
         out = ctypes.c_int()
         C.check(C.load().ao_batch_needs_resize(self._h, ctypes.byref(out)))

@@ -358,6 +358,17 @@ ao_status ao_tree_update(ao_tree *tree)
     });
 }
 
+ao_status ao_tree_update_until_converged(ao_tree *tree, int max_passes, int *changed_passes)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        if (max_passes < 1) throw std::invalid_argument("ao_tree_update_until_converged: max_passes must be >= 1");
+        unsigned changed = 0;
+        tree->engine->updateUntilConverged(unsigned(max_passes), changed_passes ? &changed : nullptr);
+        if (changed_passes) *changed_passes = int(changed);
+    });
+}
+
 ao_status ao_tree_compute_views(ao_tree *tree, const ao_view_config *views)
 {
     return guarded([&] {
@@ -494,6 +505,18 @@ ao_status ao_batch_update(ao_batch *batch, const unsigned char *frozen)
     return guarded([&] {
         if (!batch) throw std::invalid_argument("ao_batch_update: null batch");
         batch->engine->update(frozen);
+    });
+}
+
+ao_status ao_batch_update_until_converged(ao_batch *batch, const unsigned char *frozen, int max_passes,
+                                          int *changed_passes)
+{
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("ao_batch_update_until_converged: null batch");
+        if (max_passes < 1) throw std::invalid_argument("ao_batch_update_until_converged: max_passes must be >= 1");
+        unsigned changed = 0;
+        batch->engine->updateUntilConverged(frozen, unsigned(max_passes), changed_passes ? &changed : nullptr);
+        if (changed_passes) *changed_passes = int(changed);
     });
 }
 

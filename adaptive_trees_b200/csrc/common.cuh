@@ -44,7 +44,7 @@ struct DeviceState
     int error;           // a bounded device wait gave up (see kErrLookback)
     int iteration;       // build rounds that changed the tree
     int dirtyCount;      // dirty-leaf list length of the last materialisation
-    int pad1;
+    int updatePasses;    // update passes that changed the tree since the last update() began
     int doneBlocks;      // completion counter of the scatter kernel
     int rounds;          // build rounds completed (changed or found converged)
     int pad;

@@ -1233,6 +1233,51 @@ void TreeEngine::update()
     buildViews(cfg_.views);
 }
 
+// update() runs a fixed number of passes (octree.cu:471-481,
+// kdtree3d.cu:259-270), so fast-moving particles can leave overfull or
+// mergeable leaves behind.  This variant keeps passing until a pass finds
+// nothing to change: passes are launched in groups of cfg.iterations and the
+// device state is read between groups.  A pass launched after convergence
+// returns at once in every kernel (halted state), so a group may overshoot at
+// no cost.  The passes themselves are update()'s, so the result equals
+// update() with iterations = maxPasses.
+void TreeEngine::updateUntilConverged(unsigned maxPasses, unsigned *changedPasses)
+{
+    if (!built_) throw std::logic_error("adaptive_octree: call build() before update()");
+    if (maxPasses == 0) throw std::invalid_argument("adaptive_octree: updateUntilConverged needs maxPasses >= 1");
+    cudaStream_t s = cfg_.stream;
+    sortParticles();
+    refreshAll();
+    const unsigned group = std::max(1u, cfg_.iterations);
+    unsigned launched = 0;
+    while (launched < maxPasses)
+    {
+        const unsigned k = std::min(group, maxPasses - launched);
+        for (unsigned i = 0; i < k; ++i)
+        {
+            if (cfg_.kind == 0) octreePass(false, (long long)leafCapacity_);
+            else binaryPass(false, (long long)leafCapacity_);
+        }
+        launched += k;
+        if (launched == maxPasses) break;
+        // the raw state only: host-side sizes and the capacity model follow
+        // the reference's readbacks, which happen in doBuffersNeedResize()
+        AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
+        waitStream(s);
+        if (m_->hst->error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
+        if (m_->hst->converged) break;
+    }
+    materializeCounts();
+    buildViews(cfg_.views);
+    if (changedPasses)
+    {
+        AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
+        waitStream(s);
+        if (m_->hst->error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
+        *changedPasses = unsigned(m_->hst->updatePasses);
+    }
+}
+
 void TreeEngine::computeViews(const adaptive_octree::ViewConfig &v)
 {
     if (!built_) throw std::logic_error("adaptive_octree: call build() before computeViews()");

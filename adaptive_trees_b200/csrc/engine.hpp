@@ -107,6 +107,10 @@ public:
 
     void build();
     void update();
+    // Opt-in: update passes until one changes nothing (or would exceed the
+    // leaf capacity), at most maxPasses; returns the passes that changed the
+    // tree when `changedPasses` is set (a host wait at the end).
+    void updateUntilConverged(unsigned maxPasses, unsigned *changedPasses);
     void computeViews(const adaptive_octree::ViewConfig &v);
     bool doBuffersNeedResize();
     void resizeBuffers();

@@ -368,7 +368,7 @@ void ForestEngine::build()
     readState(true);
 }
 
-void ForestEngine::update(const unsigned char *frozen)
+void ForestEngine::beginUpdate(const unsigned char *frozen)
 {
     Impl &m = *m_;
     if (!m.built) throw std::logic_error("adaptive_octree: call build() before update()");
@@ -377,14 +377,57 @@ void ForestEngine::update(const unsigned char *frozen)
         AOT_CHECK(cudaMemcpyAsync(m.frozen.p, frozen, size_t(m.S), cudaMemcpyHostToDevice, s));
     else
         AOT_CHECK(cudaMemsetAsync(m.frozen.p, 0, size_t(m.S), s));
+    AOT_CHECK(cudaMemsetAsync(&m.st.as<forest::State>()->changedPasses, 0, sizeof(int), s));
     sortParticles();
     const forest::Bufs f = m.bufs();
-    const unsigned wide = unsigned(smCount()) * 8u;
-    forest::refreshKernel<true><<<wide, forest::kThreads, 0, s>>>(f), noteLaunch();
+    forest::refreshKernel<true><<<unsigned(smCount()) * 8u, forest::kThreads, 0, s>>>(f), noteLaunch();
     AOT_LAUNCH_CHECK();
-    for (unsigned i = 0; i < m.cfg.iterations; ++i) pass(false, m.frozen.as<unsigned char>());
-    forest::materializeKernel<<<wide, 256, 0, s>>>(f), noteLaunch();
+}
+
+void ForestEngine::endUpdate()
+{
+    Impl &m = *m_;
+    forest::materializeKernel<<<unsigned(smCount()) * 8u, 256, 0, m.cfg.stream>>>(m.bufs()), noteLaunch();
     AOT_LAUNCH_CHECK();
+}
+
+void ForestEngine::update(const unsigned char *frozen)
+{
+    beginUpdate(frozen);
+    for (unsigned i = 0; i < m_->cfg.iterations; ++i) pass(false, m_->frozen.as<unsigned char>());
+    endUpdate();
+}
+
+// A pass after every system converged finds nothing to change, and its
+// scatter, commit and refresh return at once (State::changed = 0), so a group
+// of passes may overshoot convergence at the cost of its decisions only.
+void ForestEngine::updateUntilConverged(const unsigned char *frozen, unsigned maxPasses, unsigned *changedPasses)
+{
+    if (maxPasses == 0) throw std::invalid_argument("forest: updateUntilConverged needs maxPasses >= 1");
+    beginUpdate(frozen);
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    const unsigned group = std::max(1u, m.cfg.iterations);
+    unsigned launched = 0;
+    while (launched < maxPasses)
+    {
+        const unsigned k = std::min(group, maxPasses - launched);
+        for (unsigned i = 0; i < k; ++i) pass(false, m.frozen.as<unsigned char>());
+        launched += k;
+        if (launched == maxPasses) break;
+        AOT_CHECK(cudaMemcpyAsync(m.hst, m.st.p, sizeof(forest::State), cudaMemcpyDeviceToHost, s));
+        waitStream(s);
+        if (m.hst->error) throw std::runtime_error("forest: a device scan gave up waiting (bounded look-back)");
+        if (!m.hst->changed) break;
+    }
+    endUpdate();
+    if (changedPasses)
+    {
+        AOT_CHECK(cudaMemcpyAsync(m.hst, m.st.p, sizeof(forest::State), cudaMemcpyDeviceToHost, s));
+        waitStream(s);
+        if (m.hst->error) throw std::runtime_error("forest: a device scan gave up waiting (bounded look-back)");
+        *changedPasses = unsigned(m.hst->changedPasses);
+    }
 }
 
 bool ForestEngine::needsResize()

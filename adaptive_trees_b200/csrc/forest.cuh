@@ -63,7 +63,7 @@ struct State
     int changed;       // some system applies changes in this pass
     int dirtyCount;
     int error;
-    int pad;
+    int changedPasses;   // update passes that changed some system since update began
     long long proposal;  // entries after this pass
 };
 
@@ -465,6 +465,7 @@ static __global__ void commitKernel(Bufs f)
     {
         st->activeBuffer ^= 1;
         st->entries = int(st->proposal);
+        if (!Build) st->changedPasses += 1;
     }
 }
 

@@ -32,6 +32,11 @@ public:
     // frozen: host array of numSystems bytes; systems marked non-zero keep
     // their tree (their keys are still re-sorted).  nullptr: update all.
     void update(const unsigned char *frozen);
+    // Opt-in: update passes until a pass changes no system (or every change
+    // is rejected for capacity), at most maxPasses; the state is read between
+    // groups of cfg.iterations passes.  changedPasses (optional, one host
+    // wait) receives the passes that changed some system.
+    void updateUntilConverged(const unsigned char *frozen, unsigned maxPasses, unsigned *changedPasses);
     bool needsResize();                  // any system (reads the device state)
     void resizeBuffers();                // grows the systems that need it
     void setCoordinates(int s, const void *x, const void *y, const void *z);
@@ -53,6 +58,8 @@ private:
     std::unique_ptr<Impl> m_;
     void sortParticles();
     void pass(bool build, const unsigned char *frozenDevice);
+    void beginUpdate(const unsigned char *frozen);
+    void endUpdate();
     void readState(bool model);
     void ensurePhysical(size_t entries);
 };

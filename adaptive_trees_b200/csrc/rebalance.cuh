@@ -286,6 +286,10 @@ __device__ __forceinline__ void commitIfLast(DeviceState *st, long long limit, i
         st->iteration += 1;
         st->rounds += 1;
     }
+    else
+    {
+        st->updatePasses += 1;
+    }
 }
 
 // --------------------------------------------------------------------------
@@ -1275,6 +1279,7 @@ static __global__ void resetForUpdateKernel(DeviceState *st, const u64 *P, size_
     st->converged = 0;
     st->numActiveParticles = n ? u32(lowerBoundDev(P, n, kMaxKey)) : 0u;
     st->dirtyCount = 0;
+    st->updatePasses = 0;
 }
 
 // Per-pass reset of the flags the decision accumulates.

@@ -150,6 +150,16 @@ class Tree:
     def update(self):
         C.check(C.load().ao_tree_update(self._h))
 
+    def updateUntilConverged(self, max_passes: int = 64) -> int:
+        """Opt-in: update passes until one changes nothing, at most
+        `max_passes`; returns the passes that changed the tree.  The result
+        equals update() with updateIterations = max_passes; the reference's
+        update() runs a fixed pass count (octree.cu:471-481,
+        kdtree3d.cu:259-270)."""
+        out = ctypes.c_int()
+        C.check(C.load().ao_tree_update_until_converged(self._h, int(max_passes), ctypes.byref(out)))
+        return out.value
+
     def computeViews(self, views: ViewConfig | None = None):
         if views is None:
             C.check(C.load().ao_tree_compute_views(self._h, None))

@@ -119,6 +119,18 @@ AO_API ao_status ao_tree_build(ao_tree *tree);
  * Capturable into a CUDA graph on the tree's stream. */
 AO_API ao_status ao_tree_update(ao_tree *tree);
 
+/* Opt-in extension with no reference counterpart: update() that keeps
+ * passing until a pass changes nothing or would exceed the leaf capacity
+ * (then doBuffersNeedResize() reports it, as after update()), at most
+ * max_passes (>= 1).  The reference's update() runs a fixed pass count
+ * (octree.cu:471-481, kdtree3d.cu:259-270), which can leave overfull or
+ * mergeable leaves on fast-moving particles.  The tree equals update() with
+ * update_iterations = max_passes.  Reads the device state between groups of
+ * update_iterations passes, so it is not capturable.  changed_passes (may be
+ * NULL; setting it adds one host wait) receives the passes that changed the
+ * tree. */
+AO_API ao_status ao_tree_update_until_converged(ao_tree *tree, int max_passes, int *changed_passes);
+
 /* Tree::computeViews() / computeViews(ViewConfig) -- tree.hpp:49-53.
  * views == NULL uses the configured views. */
 AO_API ao_status ao_tree_compute_views(ao_tree *tree, const ao_view_config *views);
@@ -219,6 +231,12 @@ AO_API ao_status ao_batch_build(ao_batch *batch);
  * non-zero keeps its tree, as if update() were not called on it (for the
  * resize-and-retry step of the systems that needed a resize). */
 AO_API ao_status ao_batch_update(ao_batch *batch, const unsigned char *frozen);
+/* Opt-in extension (see ao_tree_update_until_converged): update passes until
+ * a pass changes no system, at most max_passes (>= 1); every system's tree
+ * equals update() with update_iterations = max_passes.  Not capturable.
+ * changed_passes (may be NULL) receives the passes that changed some system. */
+AO_API ao_status ao_batch_update_until_converged(ao_batch *batch, const unsigned char *frozen, int max_passes,
+                                                 int *changed_passes);
 /* doBuffersNeedResize() of every system; *any = 1 if one of them needs it. */
 AO_API ao_status ao_batch_needs_resize(ao_batch *batch, int *any);
 /* resizeBuffers() of every system that needs a resize. */
