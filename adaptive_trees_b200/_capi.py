@@ -37,6 +37,13 @@ class AoTreeInfo(ctypes.Structure):
                 ("kernel_launches", ctypes.c_ulonglong)]
 
 
+class AoStageTimes(ctypes.Structure):
+    _fields_ = [("keys_and_sort_ms", ctypes.c_double), ("refresh_ms", ctypes.c_double),
+                ("passes_ms", ctypes.c_double), ("finish_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("near_field_ms", ctypes.c_double), ("near_field_first_ms", ctypes.c_double),
+                ("near_field_launches", ci), ("call", ci), ("valid", ci)]
+
+
 class AoBatchSystemInfo(ctypes.Structure):
     _fields_ = [("num_particles", sz), ("num_active_particles", sz), ("num_leaves", sz), ("leaf_capacity", sz),
                 ("needs_resize", ci)]
@@ -65,6 +72,8 @@ PROTOTYPES = {
     "ao_tree_build": [vp],
     "ao_tree_update": [vp],
     "ao_tree_update_until_converged": [vp, ci, ctypes.POINTER(ci)],
+    "ao_tree_set_profiling": [vp, ci],
+    "ao_tree_stage_times": [vp, vp],
     "ao_tree_compute_views": [vp, ctypes.POINTER(AoViewConfig)],
     "ao_tree_needs_resize": [vp, ctypes.POINTER(ci)],
     "ao_tree_resize_buffers": [vp],

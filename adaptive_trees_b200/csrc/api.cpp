@@ -358,6 +358,33 @@ ao_status ao_tree_update(ao_tree *tree)
     });
 }
 
+ao_status ao_tree_set_profiling(ao_tree *tree, int on)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        tree->engine->setProfiling(on != 0);
+    });
+}
+
+ao_status ao_tree_stage_times(ao_tree *tree, ao_stage_times *out)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        if (!out) throw std::invalid_argument("ao_tree_stage_times: null output");
+        const aot::TreeEngine::StageTimes t = tree->engine->stageTimes();
+        out->keys_and_sort_ms = t.keysAndSortMs;
+        out->refresh_ms = t.refreshMs;
+        out->passes_ms = t.passesMs;
+        out->finish_ms = t.finishMs;
+        out->total_ms = t.totalMs;
+        out->near_field_ms = t.nearFieldMs;
+        out->near_field_first_ms = t.nearFieldFirstMs;
+        out->near_field_launches = t.nearFieldLaunches;
+        out->call = t.call;
+        out->valid = t.valid ? 1 : 0;
+    });
+}
+
 ao_status ao_tree_update_until_converged(ao_tree *tree, int max_passes, int *changed_passes)
 {
     return guarded([&] {

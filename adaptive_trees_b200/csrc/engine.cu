@@ -27,6 +27,8 @@
 #include <utility>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "engine_util.cuh"
 #include "keygen.cuh"
 #include "rebalance.cuh"
@@ -551,6 +553,8 @@ struct TreeEngine::Impl
     size_t hstBytes = 0;
     cudaStream_t d2h = nullptr;
     cudaEvent_t ready = nullptr;
+    cudaEvent_t marks[8] = {};              // stage events (profiling)
+    std::vector<cudaEvent_t> nfMarks;       // begin/end pairs around near-field launches
     DevMem history;
     // tree
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
@@ -575,6 +579,9 @@ struct TreeEngine::Impl
     {
         if (hst) blockcache::giveHost(hst, hstBytes);
         if (ready) cudaEventDestroy(ready);
+        for (cudaEvent_t e : marks)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : nfMarks) cudaEventDestroy(e);
         if (d2h) cudaStreamDestroy(d2h);
     }
 
@@ -1015,6 +1022,7 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
         }
         if (all) rb::groupTableKernel<true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
         else rb::groupTableKernel<false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
+        markNearField(true);
         if (all && cfg_.hilbert)
             rb::octNearFieldKernel<true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();
         else if (all)
@@ -1023,6 +1031,7 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
             rb::octNearFieldKernel<true, false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();
         else
             rb::octNearFieldKernel<false, false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();
+        markNearField(false);
     }
     AOT_LAUNCH_CHECK();
 }
@@ -1109,8 +1118,10 @@ void TreeEngine::octreeBuild()
 {
     cudaStream_t s = cfg_.stream;
     waitStream(s);
+    mark(MarkStart, 1);
     capModel_.buildStart();
     sortParticles();
+    mark(MarkSorted);
     // Room for the build rounds; grown on overflow.
     const size_t estimate = std::max<size_t>(4096, cfg_.nf ? n_ + 4096 : n_ / 4 + 4096);
     ensurePhysical(std::max(physCap_, estimate));
@@ -1139,6 +1150,7 @@ void TreeEngine::octreeBuild()
             AOT_LAUNCH_CHECK();
         }
     }
+    mark(MarkPassed);
     AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
     waitStream(s);
     const DeviceState h = *m_->hst;
@@ -1170,6 +1182,7 @@ void TreeEngine::octreeBuild()
     built_ = true;
     materializeCounts();
     buildViews(cfg_.views);
+    mark(MarkEnd);
     (void)doBuffersNeedResize();
 }
 
@@ -1222,15 +1235,119 @@ void TreeEngine::binaryBuild()
 void TreeEngine::update()
 {
     if (!built_) throw std::logic_error("adaptive_octree: call build() before update()");
+    mark(MarkStart, 2);
     sortParticles();
+    mark(MarkSorted);
     refreshAll();
+    mark(MarkRefreshed);
     for (unsigned i = 0; i < cfg_.iterations; ++i)
     {
         if (cfg_.kind == 0) octreePass(false, (long long)leafCapacity_);
         else binaryPass(false, (long long)leafCapacity_);
     }
+    mark(MarkPassed);
     materializeCounts();
     buildViews(cfg_.views);
+    mark(MarkEnd);
+}
+
+// --------------------------------------------------------------------------
+// stage timing
+// --------------------------------------------------------------------------
+static const char *const kMarkNames[] = {"keys + sort", "refresh", "passes", "counts + views"};
+
+void TreeEngine::setProfiling(bool on)
+{
+    if (on)
+        for (cudaEvent_t &e : m_->marks)
+            if (!e) AOT_CHECK(cudaEventCreate(&e));
+    profiling_ = on;
+    marksRecorded_ = false;
+}
+
+// Records stage mark m on the tree's stream and moves the NVTX range on
+// (call: 1 build, 2 update, given with MarkStart).  Nothing is recorded while
+// the stream is captured: the events would become graph nodes and time the
+// capture, not the work.
+void TreeEngine::mark(Mark m, int call)
+{
+    if (!profiling_) return;
+    if (m == MarkStart)
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        AOT_CHECK(cudaStreamIsCapturing(cfg_.stream, &cs));
+        marking_ = cs == cudaStreamCaptureStatusNone;
+        marksRecorded_ = false;
+        markCall_ = call;
+        nfMarks_ = 0;
+        if (!marking_) return;
+        nvtxRangePushA(call == 1 ? "build" : "update");
+        nvtxRangePushA(kMarkNames[0]);
+    }
+    if (!marking_) return;
+    AOT_CHECK(cudaEventRecord(m_->marks[m], cfg_.stream));
+    if (m == MarkSorted && markCall_ == 1)
+        AOT_CHECK(cudaEventRecord(m_->marks[MarkRefreshed], cfg_.stream));  // a build has no full refresh
+    if (m != MarkStart)
+    {
+        nvtxRangePop();
+        if (m != MarkEnd) nvtxRangePushA(kMarkNames[m]);
+    }
+    if (m == MarkEnd)
+    {
+        nvtxRangePop();
+        marking_ = false;
+        marksRecorded_ = true;
+    }
+}
+
+// Events around one near-field launch.
+void TreeEngine::markNearField(bool begin)
+{
+    if (!marking_) return;
+    std::vector<cudaEvent_t> &ev = m_->nfMarks;
+    const size_t k = size_t(nfMarks_) * 2 + (begin ? 0 : 1);
+    if (k >= ev.size())
+    {
+        cudaEvent_t e;
+        AOT_CHECK(cudaEventCreate(&e));
+        ev.push_back(e);
+    }
+    AOT_CHECK(cudaEventRecord(ev[k], cfg_.stream));
+    if (begin) nvtxRangePushA("near field");
+    else
+    {
+        nvtxRangePop();
+        ++nfMarks_;
+    }
+}
+
+TreeEngine::StageTimes TreeEngine::stageTimes()
+{
+    StageTimes t;
+    if (!marksRecorded_) return t;
+    AOT_CHECK(cudaEventSynchronize(m_->marks[MarkEnd]));
+    auto ms = [&](cudaEvent_t a, cudaEvent_t b) {
+        float v = 0;
+        AOT_CHECK(cudaEventElapsedTime(&v, a, b));
+        return double(v);
+    };
+    const cudaEvent_t *e = m_->marks;
+    t.keysAndSortMs = ms(e[MarkStart], e[MarkSorted]);
+    t.refreshMs = ms(e[MarkSorted], e[MarkRefreshed]);
+    t.passesMs = ms(e[MarkRefreshed], e[MarkPassed]);
+    t.finishMs = ms(e[MarkPassed], e[MarkEnd]);
+    t.totalMs = ms(e[MarkStart], e[MarkEnd]);
+    for (int k = 0; k < nfMarks_; ++k)
+    {
+        const double v = ms(m_->nfMarks[2 * k], m_->nfMarks[2 * k + 1]);
+        t.nearFieldMs += v;
+        if (k == 0) t.nearFieldFirstMs = v;
+    }
+    t.nearFieldLaunches = nfMarks_;
+    t.call = markCall_;
+    t.valid = true;
+    return t;
 }
 
 // update() runs a fixed number of passes (octree.cu:471-481,
@@ -1246,8 +1363,11 @@ void TreeEngine::updateUntilConverged(unsigned maxPasses, unsigned *changedPasse
     if (!built_) throw std::logic_error("adaptive_octree: call build() before update()");
     if (maxPasses == 0) throw std::invalid_argument("adaptive_octree: updateUntilConverged needs maxPasses >= 1");
     cudaStream_t s = cfg_.stream;
+    mark(MarkStart, 2);
     sortParticles();
+    mark(MarkSorted);
     refreshAll();
+    mark(MarkRefreshed);
     const unsigned group = std::max(1u, cfg_.iterations);
     unsigned launched = 0;
     while (launched < maxPasses)
@@ -1267,8 +1387,10 @@ void TreeEngine::updateUntilConverged(unsigned maxPasses, unsigned *changedPasse
         if (m_->hst->error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
         if (m_->hst->converged) break;
     }
+    mark(MarkPassed);
     materializeCounts();
     buildViews(cfg_.views);
+    mark(MarkEnd);
     if (changedPasses)
     {
         AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));

@@ -150,6 +150,22 @@ public:
     // dst[i] = src[perm[i]] for the numParticles() elements of elemBytes
     // each: per-particle data in key order (device pointers, the tree's stream)
     void gather(const void *src, void *dst, size_t elemBytes) const;
+    // Stage timing of build() and update() (the CUDA-event counterpart of the
+    // reference's NVTX ranges behind ADAPTIVE_OCTREE_PROFILING,
+    // config.hpp:20-28): when on, they record events at their stage
+    // boundaries and around every near-field launch, and push NVTX ranges;
+    // calls made while the stream is being captured record nothing.
+    struct StageTimes
+    {
+        double keysAndSortMs = 0, refreshMs = 0, passesMs = 0, finishMs = 0, totalMs = 0;
+        double nearFieldMs = 0;       // all near-field launches of the call
+        double nearFieldFirstMs = 0;  // the first one (update(): the full refresh of every leaf)
+        int nearFieldLaunches = 0;
+        int call = 0;  // 1 build, 2 update
+        bool valid = false;
+    };
+    void setProfiling(bool on);
+    StageTimes stageTimes();  // of the last profiled build() or update(); waits for it
     // one-shot key generation without a sort (computeSfcKeys semantics)
     static void computeKeys(int kind, int real, const void *x, const void *y, const void *z, size_t n,
                             const double *box, bool hilbert, unsigned maxDepth, unsigned long long *keys,
@@ -169,6 +185,13 @@ private:
     // thrust capacity model of K_d / tmpTree (octree.cu:453-457)
     OctreeCapacity capModel_;  // reference K_d / tmpTree capacities (octree)
     adaptive_octree::ViewConfig prepared_{};
+    // stage events of build()/update(): start, sorted, refreshed (update),
+    // passes done, end; near-field launches are bracketed by their own pairs
+    enum Mark { MarkStart = 0, MarkSorted, MarkRefreshed, MarkPassed, MarkEnd, NumMarks };
+    bool profiling_ = false, marking_ = false, marksRecorded_ = false;
+    int markCall_ = 0, nfMarks_ = 0;
+    void mark(Mark m, int call = 0);
+    void markNearField(bool begin);
 
     void sortParticles();
     void octreeBuild();

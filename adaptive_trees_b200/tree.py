@@ -160,6 +160,22 @@ class Tree:
         C.check(C.load().ao_tree_update_until_converged(self._h, int(max_passes), ctypes.byref(out)))
         return out.value
 
+    def setProfiling(self, on: bool = True):
+        """Stage timing of octree build() and update() with CUDA events and
+        NVTX ranges (the reference's ADAPTIVE_OCTREE_PROFILING ranges,
+        config.hpp:20-28)."""
+        C.check(C.load().ao_tree_set_profiling(self._h, 1 if on else 0))
+
+    def stageTimes(self) -> dict | None:
+        """Stage times (ms) of the last profiled build() or update(), or None."""
+        t = C.AoStageTimes()
+        C.check(C.load().ao_tree_stage_times(self._h, ctypes.byref(t)))
+        if not t.valid:
+            return None
+        out = {k: getattr(t, k) for k, _ in C.AoStageTimes._fields_ if k != "valid"}
+        out["call"] = {1: "build", 2: "update"}.get(t.call, "?")
+        return out
+
     def computeViews(self, views: ViewConfig | None = None):
         if views is None:
             C.check(C.load().ao_tree_compute_views(self._h, None))

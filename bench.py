@@ -40,6 +40,14 @@ WORKLOAD = "octree build + graph-replayed update, 16Mi Plummer fp32 (a=0.05, r<=
 # DRAM bytes (read + write) of one 16Mi-key onesweep pass, from the ncu capture
 # summarised in profiles/onesweepKernel_pass_16Mi.md (201.7 MB + 153.4 MB).
 ONESWEEP_TRAFFIC_BYTES = 355.1e6
+# Algorithmic bytes of the near-field refresh per leaf: K[i] read (8), the
+# begin index B[i] read (4), NF[i] written (4), and the group flag, one byte
+# per sibling group (1/8).
+NF_BYTES_PER_LEAF = 16.125
+# DRAM bytes (read + write) per leaf of the full near-field refresh, from the
+# ncu capture summarised in profiles/octNearFieldKernel_full_refresh_8Mi.md
+# (8 Mi particles); the traffic of the 16 Mi launch is this times its leaves.
+NF_TRAFFIC_BYTES_PER_LEAF = (763019776 + 101103360) / 6681970
 
 
 def plummer(n, seed, scale=0.05, rmax=0.5):
@@ -845,6 +853,25 @@ def main():
 
         clocks.__exit__(None, None, None)
 
+        # ---------------- stage times and the near-field kernel, timed with
+        # the tree's own CUDA events on its stream (direct calls, not graphs)
+        tree.setProfiling(True)
+        build_stages, update_stages = [], []
+        for i in range(args.warmup + args.steps):
+            tree.build()
+            bst = tree.stageTimes()
+            jitter()
+            tree.update()
+            ust = tree.stageTimes()
+            if tree.doBuffersNeedResize():
+                tree.resizeBuffers()
+                tree.update()
+            if i >= args.warmup:
+                build_stages.append(bst)
+                update_stages.append(ust)
+        tree.setProfiling(False)
+        nf_leaves = tree.info().num_leaves
+
         # ---------------- roofline: onesweep pass timed live via ao_sort_pairs,
         # replayed from CUDA graphs so no host launch time is inside the events
         keys_ptr = tree.buffer_info("particleKeys_d")[0]
@@ -863,11 +890,34 @@ def main():
     hbm, peak_kind = peaks()
     pass_bytes = 24.0 * n
     achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
-    roof = {"bound": "hbm", "kernel": "onesweepKernel (one 8-bit pass of the 64-bit key + 32-bit value sort)",
-            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-            "traffic": ONESWEEP_TRAFFIC_BYTES, "algorithmic_bytes_per_launch": pass_bytes,
-            "launch_ms": pass_ms, "sort_64bit_ms": t64,
-            "keygen": {"ms": keygen_ms, "achieved_gbs": (20.0 * n) / (keygen_ms * 1e-3) / 1e9}}
+    roof_sort = {"bound": "hbm", "kernel": "onesweepKernel (one 8-bit pass of the 64-bit key + 32-bit value sort)",
+                 "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                 "traffic": ONESWEEP_TRAFFIC_BYTES, "algorithmic_bytes_per_launch": pass_bytes,
+                 "launch_ms": pass_ms, "sort_64bit_ms": t64,
+                 "keygen": {"ms": keygen_ms, "achieved_gbs": (20.0 * n) / (keygen_ms * 1e-3) / 1e9}}
+
+    def med(rows, key):
+        return statistics.median(r[key] for r in rows)
+
+    # the dominant kernel: the near-field refresh.  Its full launch in update()
+    # covers every leaf, so its algorithmic bytes are known exactly.
+    nf_ms = max_over_ranks(med(update_stages, "near_field_first_ms"), world, dev)
+    nf_bytes = NF_BYTES_PER_LEAF * nf_leaves
+    nf_achieved = nf_bytes / (nf_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": "octNearFieldKernel<Hilbert, All> (the full near-field refresh of update())",
+            "achieved": nf_achieved, "peak": hbm, "unit": "GB/s", "frac": nf_achieved / hbm, "peak_kind": peak_kind,
+            "traffic": (NF_TRAFFIC_BYTES_PER_LEAF * nf_leaves) if NF_TRAFFIC_BYTES_PER_LEAF else None,
+            "algorithmic_bytes_per_launch": nf_bytes, "launch_ms": nf_ms, "leaves": nf_leaves,
+            "note": "search-bound: 27 neighbour-cell populations per parent cell come from hash tables or "
+                    "searches of the sorted keys; HBM is the roof, not the limit"}
+    stages = {
+        "build": {k: med(build_stages, k) for k in ("keys_and_sort_ms", "passes_ms", "finish_ms", "total_ms",
+                                                     "near_field_ms")},
+        "update": {k: med(update_stages, k) for k in ("keys_and_sort_ms", "refresh_ms", "passes_ms", "finish_ms",
+                                                      "total_ms", "near_field_ms", "near_field_first_ms")},
+        "build_near_field_launches": build_stages[-1]["near_field_launches"],
+        "update_near_field_launches": update_stages[-1]["near_field_launches"],
+        "how": "CUDA events on the tree's stream around each stage (ao_tree_set_profiling), direct calls"}
     line = {"metric": METRIC, "value": total / (step_ms * 1e-3), "unit": "particles/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
@@ -879,7 +929,7 @@ def main():
                        "graph_replayed": True, "resizes": resizes},
             "e2e": {"value": total / (e2e * 1e-3), "unit": "particles/s", "ms_per_step": e2e,
                     "h2d_bytes_per_step": 3 * 4 * n, "d2h_bytes_per_step": 12},
-            "roofline": roof}
+            "roofline": roof, "roofline_sort": roof_sort, "stages": stages}
     if rank == 0 and not args.no_cpu_baseline:
         v, dt = cpu_oracle_build(args.cpu_sample)
         line["cpu_baseline"] = {"value": v, "unit": "particles/s", "cores": 1, "kind": "port",

@@ -119,6 +119,28 @@ AO_API ao_status ao_tree_build(ao_tree *tree);
  * Capturable into a CUDA graph on the tree's stream. */
 AO_API ao_status ao_tree_update(ao_tree *tree);
 
+/* Stage timing of build() and update(): the CUDA-event counterpart of the
+ * reference's NVTX ranges behind ADAPTIVE_OCTREE_PROFILING (config.hpp:20-28,
+ * octree.cu:287-306).  With profiling on, each octree build() and update()
+ * not made under stream capture records events at its stage boundaries and
+ * around every near-field launch on the tree's stream, and pushes one NVTX
+ * range per stage. */
+typedef struct ao_stage_times {
+    double keys_and_sort_ms; /* key generation, the 8 sort passes and the key sample */
+    double refresh_ms;       /* update: the full per-leaf refresh (begin indices, cell table, near field) */
+    double passes_ms;        /* the rebalance passes (build: its rounds, with the host's checks between them) */
+    double finish_ms;        /* leaf counts and views (build: and the final copies) */
+    double total_ms;
+    double near_field_ms;    /* all near-field kernel launches of the call (0 without NFCount) */
+    double near_field_first_ms; /* the first of them (update(): the full refresh of every leaf) */
+    int near_field_launches;
+    int call;                /* 1 build, 2 update */
+    int valid;               /* 0: no profiled call since profiling was switched on */
+} ao_stage_times;
+AO_API ao_status ao_tree_set_profiling(ao_tree *tree, int on);
+/* Waits for the last profiled build() or update() and reads its stage times. */
+AO_API ao_status ao_tree_stage_times(ao_tree *tree, ao_stage_times *out);
+
 /* Opt-in extension with no reference counterpart: update() that keeps
  * passing until a pass changes nothing or would exceed the leaf capacity
  * (then doBuffersNeedResize() reports it, as after update()), at most
