@@ -36,6 +36,7 @@
 
 namespace aot
 {
+static_assert(sort::kTile == int(kSortTileItems), "kSortTileItems must match the onesweep tile");
 // --------------------------------------------------------------------------
 // block cache
 // --------------------------------------------------------------------------
@@ -821,7 +822,7 @@ void TreeEngine::ensurePhysical(size_t capacity)
         if (slots != size_t(m_->groupMask) + 1)
         {
             m_->groupKeys.reserve(slots * sizeof(u64), s);
-            m_->groupBegins.reserve(slots * rb::kGroupBegins * sizeof(u32), s);
+            m_->groupBegins.reserve(slots * rb::kGroupRow * sizeof(u32), s);
             m_->memoKeys.reserve(slots * sizeof(u64), s);
             m_->memoBegins.reserve(slots * rb::kGroupBegins * sizeof(u32), s);
             m_->groupMask = m_->memoMask = u32(slots - 1);
@@ -999,6 +1000,43 @@ void TreeEngine::refreshAll()
     }
 }
 
+// The digit -> block position table of the near-field kernel, once per device.
+static void ensureDigitPos()
+{
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    AOT_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64 || done[dev]) return;
+    const HilbertTables h = makeHilbertTables();
+    std::vector<unsigned long long> t(2 * 27 * 48);
+    for (int hil = 0; hil < 2; ++hil)
+        for (int q = 0; q < 27; ++q)
+            for (int st = 0; st < 48; ++st)
+            {
+                unsigned long long packed = 0;
+                for (int d = 0; d < 8; ++d)
+                {
+                    // block coordinate 2 * offset + child bit + 1 per axis, where Q touches P
+                    const int o = hil ? h.decOct[st * 8 + d] : d;
+                    const int dq[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+                    const int bit[3] = {o >> 2, (o >> 1) & 1, o & 1};
+                    bool ok = true;
+                    int p = 0;
+                    for (int ax = 0; ax < 3; ++ax)
+                    {
+                        if ((dq[ax] < 0 && bit[ax] == 0) || (dq[ax] > 0 && bit[ax] == 1)) ok = false;
+                        p = p * 4 + (2 * dq[ax] + bit[ax] + 1);
+                    }
+                    packed |= (unsigned long long)(ok ? p : 0xff) << (8 * d);
+                }
+                t[(hil * 27 + q) * 48 + st] = packed;
+            }
+    AOT_CHECK(cudaMemcpyToSymbol(rb::gDigitPos, t.data(), t.size() * sizeof(unsigned long long)));
+    done[dev] = true;
+}
+
 // Per-leaf quantities of the active octree: begin indices, then (NFCount)
 // near-field counts and group-merge flags.  all = every leaf, else the work
 // lists of the last materialisation.
@@ -1014,6 +1052,7 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
         const HilbertTables &h = m_->kpd.h;
         const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupBegins.as<u32>(), m_->groupMask,
                                 m_->memoKeys.as<u64>(),  m_->memoBegins.as<u32>(),  m_->memoMask};
+        ensureDigitPos();
         if (m_->groupStale)
         {
             AOT_CHECK(cudaMemsetAsync(gt.keys, 0, (size_t(gt.mask) + 1) * sizeof(u64), s));

@@ -23,6 +23,9 @@ namespace aot
 {
 struct DeviceState;
 
+// Keys per tile of the onesweep radix sort (threads x items per thread).
+constexpr size_t kSortTileItems = 2560;
+
 // A CUDA runtime failure inside the engine.
 struct CudaError : std::runtime_error
 {

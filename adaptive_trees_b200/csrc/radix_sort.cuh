@@ -29,7 +29,7 @@ constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kItems = 16;
+constexpr int kItems = 10;
 constexpr int kTile = kThreads * kItems;
 constexpr int kMaxPasses = 8;
 constexpr u64 kFlagAgg = u64(1) << 62;
@@ -445,7 +445,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
 
 // One onesweep pass over keys[0, n): digit at bit `shift` (`bits` wide).
 // valsIn == nullptr means values are the input indices (first pass).
-static __global__ void __launch_bounds__(kThreads, 3)
+static __global__ void __launch_bounds__(kThreads, 4)
     onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
                    u32 *__restrict__ valsOut, size_t n, int shift, const u32 *__restrict__ bins, u32 *tileCounter,
                    u64 *status, int *error, int bits = kRadixBits)

@@ -632,12 +632,13 @@ __device__ __forceinline__ CellPath decodeCell(u64 start, unsigned pl, const uns
 // addressing with linear probing, at most kCellProbes probes; keys are cell
 // codes (never 0 or kBusyCode), 0 marks an empty slot.
 constexpr int kGroupBegins = 9;
+constexpr int kGroupRow = 12;  // words per group-table row (48 B, 16-byte aligned)
 constexpr u32 kCellProbes = 64;
 constexpr u64 kBusyCode = ~u64(0);
 struct GroupTable
 {
     u64 *keys;
-    u32 *begins;  // [slot][kGroupBegins]
+    u32 *begins;  // [slot][kGroupRow]
     u32 mask;
     u64 *memoKeys;
     u32 *memoBegins;
@@ -653,13 +654,8 @@ __device__ __forceinline__ u64 cellCode(u64 start, unsigned level)
 
 __device__ __forceinline__ u32 codeSlot(u64 code, u32 mask)
 {
-    u64 z = code * 0x9E3779B97F4A7C15ull;  // splitmix64 finaliser
-    z ^= z >> 30;
-    z *= 0xBF58476D1CE4E5B9ull;
-    z ^= z >> 27;
-    z *= 0x94D049BB133111EBull;
-    z ^= z >> 31;
-    return u32(z) & mask;
+    // Fibonacci hashing: the high bits of one 64-bit product
+    return u32((code * 0x9E3779B97F4A7C15ull) >> 32) & mask;
 }
 
 // Begin indices of the cell `code` (9 values into b), or false.
@@ -668,9 +664,11 @@ __device__ __forceinline__ bool groupBegins(const GroupTable &gt, u64 code, u32 
     u32 slot = codeSlot(code, gt.mask);
     for (u32 probe = 0; probe < kCellProbes; ++probe)
     {
-        const u32 *row = gt.begins + size_t(slot) * kGroupBegins;
-#pragma unroll
-        for (int k = 0; k < kGroupBegins; ++k) b[k] = __ldg(row + k);  // loaded beside the key
+        const uint4 *row = reinterpret_cast<const uint4 *>(gt.begins + size_t(slot) * kGroupRow);
+        const uint4 r0 = __ldg(row), r1 = __ldg(row + 1), r2 = __ldg(row + 2);  // loaded beside the key
+        b[0] = r0.x; b[1] = r0.y; b[2] = r0.z; b[3] = r0.w;
+        b[4] = r1.x; b[5] = r1.y; b[6] = r1.z; b[7] = r1.w;
+        b[8] = r2.x;
         const u64 key = __ldg(gt.keys + slot);
         if (key == code) return true;
         if (key == 0) return false;
@@ -750,7 +748,7 @@ __device__ __forceinline__ void cellInsert(const GroupTable &gt, u64 code, const
                                    static_cast<unsigned long long>(code));
         if (prev == 0ull || prev == code)
         {
-            u32 *row = gt.begins + size_t(slot) * kGroupBegins;
+            u32 *row = gt.begins + size_t(slot) * kGroupRow;
 #pragma unroll
             for (int k = 0; k < kGroupBegins; ++k) row[k] = b[k];
             return;
@@ -794,10 +792,9 @@ static __global__ void __launch_bounds__(kRefreshThreads) groupTableKernel(TreeB
 struct UnitScratch
 {
     u64 pStart[kUnitBatch], st0[kUnitBatch], st1[kUnitBatch], st2[kUnitBatch];
-    unsigned long long qsum[kUnitBatch];  // population of the 27 Q's
+    u32 qtot[kUnitBatch][27];             // population of each Q
     u32 cx[kUnitBatch], cy[kUnitBatch], cz[kUnitBatch];
     u32 hintB[kUnitBatch];                // begin index of the unit's first leaf
-    u32 pc[kUnitBatch];                   // population of P itself
     int childState[kUnitBatch], level[kUnitBatch], active[kUnitBatch];
     u32 block[kUnitBatch][64];
     u64 slowKey[kUnitBatch * 27];
@@ -850,18 +847,22 @@ __device__ __forceinline__ u64 neighbourCell(const UnitScratch &w, int u, int q,
     }
 }
 
+// Where the children of the neighbour cell at offset q land in the unit's
+// 4 x 4 x 4 block, per child state and digit: [Morton, Hilbert][q][state],
+// 8 bits per digit (the block position, or 0xff for a child that does not
+// touch P).  Filled once per device from the host.
+__device__ u64 gDigitPos[2 * 27 * 48];
+
 // Child counts of Q from its 9 begin indices (children in digit order) into
-// the unit's block positions `pos` (0xff: the child does not touch P).  The
-// loop runs over digits, so the register array is indexed statically.
+// the unit's block.
 template <bool Hilbert>
-__device__ __forceinline__ void childrenFromBegins(const u32 (&b)[kGroupBegins], int qState, const unsigned char *pos,
-                                                   u32 *block, const unsigned char *sDec)
+__device__ __forceinline__ void childrenFromPacked(const u32 (&b)[kGroupBegins], int q, int qState, u32 *block)
 {
+    const u64 packed = gDigitPos[(Hilbert ? 27 * 48 : 0) + q * 48 + qState];
 #pragma unroll
     for (int d = 0; d < 8; ++d)
     {
-        const unsigned o = Hilbert ? unsigned(sDec[qState * 8 + d]) : unsigned(d);
-        const unsigned p = pos[o];
+        const unsigned p = unsigned(packed >> (8 * d)) & 0xffu;
         if (p != 0xff) block[p] = b[d + 1] - b[d];
     }
 }
@@ -1039,8 +1040,6 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                 w.st2[u] = path.st2;
                 w.childState[u] = path.childState;
                 w.hintB[u] = B[i];
-                w.qsum[u] = 0;
-                w.pc[u] = 0;
             }
             if (lane == 0) w.nSlow = 0;
             __syncwarp();
@@ -1061,10 +1060,9 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                     u32 gb[kGroupBegins];
                     if (groupBegins(gt, cellCode(qKey, level - 1), gb))
                     {
-                        childrenFromBegins<Hilbert>(gb, qState, sPos + q * 8, w.block[u], sDec);
+                        childrenFromPacked<Hilbert>(gb, q, qState, w.block[u]);
                         const u32 total = gb[8] - gb[0];
-                        atomicAdd(&w.qsum[u], (unsigned long long)total);
-                        if (q == 13) w.pc[u] = total;
+                        w.qtot[u][q] = total;
                     }
                     else
                     {
@@ -1100,7 +1098,7 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                 if (memoFind(gt, code, begins))
                 {
                     // searched before by another unit
-                    childrenFromBegins<Hilbert>(begins, qState, sPos + q * 8, w.block[u], sDec);
+                    childrenFromPacked<Hilbert>(begins, q, qState, w.block[u]);
                     total = begins[8] - begins[0];
                 }
                 else
@@ -1112,8 +1110,7 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                         memoInsert(gt, code, begins);  // for the next units that need Q
                     total = hi - lo;
                 }
-                atomicAdd(&w.qsum[u], (unsigned long long)total);
-                if (q == 13) w.pc[u] = total;
+                w.qtot[u][q] = total;
             }
             __syncwarp();
 
@@ -1155,7 +1152,12 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                     if (head)
                     {
                         const int i0 = completeGroup(K, L, i, lev, pk, octRange(lev - 1));
-                        if (i0 >= 0) Gf[i0] = u64(w.pc[u]) * w.qsum[u] <= u64(bucket) ? 1 : 0;
+                        if (i0 >= 0)
+                        {
+                            u64 qsum = 0;
+                            for (int q = 0; q < 27; ++q) qsum += w.qtot[u][q];
+                            Gf[i0] = u64(w.qtot[u][13]) * qsum <= u64(bucket) ? 1 : 0;
+                        }
                     }
                 }
             }

@@ -34,15 +34,15 @@ namespace
 {
 // Scratch layout of the pair sort for kNoAllocMaxItems items: alternate keys
 // (8 B/item), alternate values (4 B/item), counters (2 x 8 passes x 256
-// digits + 8 + 2 words), look-back status (8 passes x tiles of 4096 items x
-// 256 digits x 8 B), each part rounded up to 256 bytes.  The call checks the
+// digits + 8 + 2 words), look-back status (8 passes x tiles of
+// kSortTileItems items x 256 digits x 8 B), each part rounded up to 256 bytes.  The call checks the
 // sort's own size query against this before using the array.
 constexpr size_t kNoAllocMaxItems = size_t(1) << 20;
 constexpr size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
-constexpr size_t kNoAllocTiles = (kNoAllocMaxItems + 4095) / 4096;
+constexpr size_t kNoAllocTiles = (kNoAllocMaxItems + kSortTileItems - 1) / kSortTileItems;
 constexpr size_t kNoAllocScratchBytes =
     up256(up256(up256(up256(kNoAllocMaxItems * 8) + kNoAllocMaxItems * 4) + (2 * 8 * 256 + 8 + 2) * 4) +
-          size_t(8) * kNoAllocTiles * 256 * 8);  // 16,793,600 bytes
+          size_t(8) * kNoAllocTiles * 256 * 8);  // 19,316,992 bytes
 
 static __device__ __align__(256) unsigned char g_noAllocScratch[kNoAllocScratchBytes];
 
