@@ -38,8 +38,8 @@ BUCKET = 512
 METRIC = "particles/s (octree build, 16Mi Plummer fp32, Hilbert, NFCount 512)"
 WORKLOAD = "octree build + graph-replayed update, 16Mi Plummer fp32 (a=0.05, r<=0.5), Hilbert keys, NFCount 512"
 # DRAM bytes (read + write) of one 16Mi-key onesweep pass, from the ncu capture
-# summarised in profiles/onesweepKernel_pass_16Mi.md (201.7 MB + 153.4 MB).
-ONESWEEP_TRAFFIC_BYTES = 355.1e6
+# summarised in profiles/onesweepKernel_pass_16Mi.md (204.9 MB + 162.7 MB).
+ONESWEEP_TRAFFIC_BYTES = 367.6e6
 # Algorithmic bytes of the near-field refresh per leaf: K[i] read (8), the
 # begin index B[i] read (4), NF[i] written (4), and the group flag, one byte
 # per sibling group (1/8).
@@ -47,7 +47,7 @@ NF_BYTES_PER_LEAF = 16.125
 # DRAM bytes (read + write) per leaf of the full near-field refresh, from the
 # ncu capture summarised in profiles/octNearFieldKernel_full_refresh_8Mi.md
 # (8 Mi particles); the traffic of the 16 Mi launch is this times its leaves.
-NF_TRAFFIC_BYTES_PER_LEAF = (763019776 + 101103360) / 6681970
+NF_TRAFFIC_BYTES_PER_LEAF = (780793856 + 101675776) / 6677490
 
 
 def plummer(n, seed, scale=0.05, rmax=0.5):
