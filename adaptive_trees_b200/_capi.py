@@ -83,6 +83,12 @@ PROTOTYPES = {
     "ao_compute_sfc_keys": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_double), ci, cu, vp, vp, vp],
     "ao_sort_pairs": [vp, ctypes.POINTER(sz), vp, vp, vp, vp, sz, ci, ci, vp],
     "ao_sort_pairs_noalloc": [vp, vp, vp, vp, sz, ci, ci, vp],
+    "ao_sort_config_count": [ctypes.POINTER(ci)],
+    "ao_sort_config_info": [ci, ctypes.POINTER(ci), ctypes.POINTER(ci)],
+    "ao_sort_tuning": [ci, sz, ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci)],
+    "ao_sort_set_autotune": [ci],
+    "ao_sort_force_config": [ci],
+    "ao_sort_forget_tuning": [],
     "ao_batch_create": [ci, ci, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(sz),
                         ctypes.POINTER(AoConfig), vp, ctypes.POINTER(vp)],
     "ao_batch_destroy": [vp],

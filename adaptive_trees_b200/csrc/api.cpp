@@ -492,6 +492,52 @@ ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsigned lon
     });
 }
 
+ao_status ao_sort_config_count(int *count)
+{
+    return guarded([&] {
+        if (!count) throw std::invalid_argument("ao_sort_config_count: null output");
+        *count = aot::sortConfigCount();
+    });
+}
+
+ao_status ao_sort_config_info(int config, int *digit_bits, int *items_per_thread)
+{
+    return guarded([&] {
+        if (!digit_bits || !items_per_thread) throw std::invalid_argument("ao_sort_config_info: null output");
+        const aot::SortTuning t = aot::sortConfigInfo(config);
+        *digit_bits = t.digitBits;
+        *items_per_thread = t.itemsPerThread;
+    });
+}
+
+ao_status ao_sort_tuning(int segmented, size_t n, int *config, int *digit_bits, int *items_per_thread, int *tuned)
+{
+    return guarded([&] {
+        if (!config || !digit_bits || !items_per_thread || !tuned)
+            throw std::invalid_argument("ao_sort_tuning: null output");
+        const aot::SortTuning t = aot::sortTuning(segmented != 0, n);
+        *config = t.config;
+        *digit_bits = t.digitBits;
+        *items_per_thread = t.itemsPerThread;
+        *tuned = t.tuned ? 1 : 0;
+    });
+}
+
+ao_status ao_sort_set_autotune(int on)
+{
+    return guarded([&] { aot::sortSetAutotune(on != 0); });
+}
+
+ao_status ao_sort_force_config(int config)
+{
+    return guarded([&] { aot::sortForceConfig(config); });
+}
+
+ao_status ao_sort_forget_tuning(void)
+{
+    return guarded([&] { aot::sortForgetTuning(); });
+}
+
 ao_status ao_tree_gather(ao_tree *tree, const void *src, void *dst, size_t elem_bytes)
 {
     return guarded([&] {

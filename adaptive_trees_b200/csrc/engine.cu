@@ -22,6 +22,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <stdexcept>
 #include <utility>
@@ -377,77 +378,75 @@ __global__ void iotaKernel(u32 *perm, size_t n)
         perm[i] = u32(i);
 }
 
-// Sort scratch layout: hist[8][256] | bins[8][256] | tileCounters[8] (u32),
-// then status words (u64) for `passes` passes.
+// Sort scratch layout: hist[kPassSlots][256] | bins[kPassSlots][256] |
+// tileCounters[kPassSlots] (u32), then look-back status words (u64), room for
+// every configuration: kPassSlots passes of the smallest tiles.
 struct SortArena
 {
     DevMem counters, status;
     size_t tilesCap = 0;
     void ensure(size_t n, cudaStream_t owner)
     {
-        const size_t tiles = std::max<size_t>(1, (n + sort::kTile - 1) / sort::kTile);
-        counters.reserve((2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses) * sizeof(u32), owner);
+        const size_t tiles = std::max<size_t>(1, (n + sort::kMinTile - 1) / sort::kMinTile);
+        counters.reserve((2 * sort::kPassSlots * sort::kRadix + sort::kPassSlots) * sizeof(u32), owner);
         if (tiles > tilesCap)
         {
-            status.reserve(size_t(sort::kMaxPasses) * tiles * sort::kRadix * sizeof(u64), owner);
+            status.reserve(size_t(sort::kPassSlots) * tiles * sort::kRadix * sizeof(u64), owner);
             tilesCap = tiles;
         }
     }
     u32 *hist() const { return counters.as<u32>(); }
-    u32 *bins() const { return counters.as<u32>() + sort::kMaxPasses * sort::kRadix; }
-    u32 *tileCounters() const { return counters.as<u32>() + 2 * sort::kMaxPasses * sort::kRadix; }
+    u32 *bins() const { return counters.as<u32>() + sort::kPassSlots * sort::kRadix; }
+    u32 *tileCounters() const { return counters.as<u32>() + 2 * sort::kPassSlots * sort::kRadix; }
 };
 
-void setPassSmem()
-{
-    static bool done = false;
-    if (!done)
-    {
-        AOT_CHECK(cudaFuncSetAttribute(sort::onesweepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(sort::passSmem())));
-        done = true;
-    }
-}
+size_t configTiles(int cfg, size_t n) { return std::max<size_t>(1, (n + sort::configTile(cfg) - 1) / sort::configTile(cfg)); }
 
-// Onesweep passes over (k[0], v[0]) -> ... ; counts must already be in
-// hist.  valsAreIndices: the first pass generates the values.  Returns the
-// index (0/1) of the buffers holding the result.
-int runPasses(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int beginBit, int passes, bool valsAreIndices,
+// Onesweep passes of configuration `cfg` over (k[0], v[0]) -> ... for bits
+// [beginBit, endBit); the counts must already be in hist.  valsAreIndices:
+// the first pass generates the values.  Returns the index (0/1) of the
+// buffers holding the result.
+int runPasses(int cfg, cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int beginBit, int endBit, bool valsAreIndices,
               SortArena &a, int *error)
 {
-    setPassSmem();
-    const size_t tiles = (n + sort::kTile - 1) / sort::kTile;
+    sort::setPassSmemAll();
+    const int bitsPer = sort::kSortConfigs[cfg].bits;
+    const int passes = (endBit - beginBit + bitsPer - 1) / bitsPer;
+    const size_t tiles = configTiles(cfg, n);
     sort::binsKernel<<<1, sort::kRadix, 0, s>>>(a.hist(), a.bins(), passes), noteLaunch();
     AOT_LAUNCH_CHECK();
     for (int p = 0; p < passes; ++p)
     {
         const int in = p & 1, out = in ^ 1;
-        sort::onesweepKernel<<<unsigned(tiles), sort::kThreads, sort::passSmem(), s>>>(
-            k[in], (p == 0 && valsAreIndices) ? nullptr : v[in], k[out], v[out], n, beginBit + p * sort::kRadixBits,
-            a.bins() + p * sort::kRadix, a.tileCounters() + p, a.status.as<u64>() + size_t(p) * tiles * sort::kRadix,
-            error), noteLaunch();
+        const int shift = beginBit + p * bitsPer;
+        sort::launchPass(cfg, s, k[in], (p == 0 && valsAreIndices) ? nullptr : v[in], k[out], v[out], n, shift,
+                         a.bins() + p * sort::kRadix, a.tileCounters() + p,
+                         a.status.as<u64>() + size_t(p) * tiles * sort::kRadix, error, std::min(bitsPer, endBit - shift)),
+            noteLaunch();
         AOT_LAUNCH_CHECK();
     }
     return passes & 1;
 }
 
-void clearArena(cudaStream_t s, SortArena &a, size_t n, int passes)
+// Zeroes the counters and the status words configuration `cfg` reads.
+void clearArena(int cfg, cudaStream_t s, SortArena &a, size_t n, int passes)
 {
-    const size_t tiles = std::max<size_t>(1, (n + sort::kTile - 1) / sort::kTile);
     AOT_CHECK(cudaMemsetAsync(a.counters.p, 0, a.counters.bytes, s));
-    AOT_CHECK(cudaMemsetAsync(a.status.p, 0, size_t(passes) * tiles * sort::kRadix * sizeof(u64), s));
+    AOT_CHECK(cudaMemsetAsync(a.status.p, 0, size_t(passes) * configTiles(cfg, n) * sort::kRadix * sizeof(u64), s));
 }
 
-// Generic stable sort of (keys, identity indices) by bits [0, 8*passes).
+// Generic stable sort of (keys, identity indices) by bits [0, 8*passes),
+// default configuration.
 int sortWithIndices(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int passes, SortArena &a, int *error)
 {
     if (n == 0) return 0;
+    const int cfg = sort::kDefaultSortConfig;
     a.ensure(n, s);
-    clearArena(s, a, n, passes);
+    clearArena(cfg, s, a, n, passes);
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n, sort::kThreads), unsigned(smCount()) * 8u));
-    sort::histogramKernel<<<blocks, sort::kThreads, 0, s>>>(k[0], n, 0, passes, a.hist()), noteLaunch();
+    sort::launchHistogram(cfg, s, blocks, k[0], n, 0, passes, a.hist(), 8 * passes), noteLaunch();
     AOT_LAUNCH_CHECK();
-    return runPasses(s, k, v, n, 0, passes, true, a, error);
+    return runPasses(cfg, s, k, v, n, 0, 8 * passes, true, a, error);
 }
 
 }  // namespace
@@ -457,6 +456,120 @@ unsigned gridFor(size_t n, unsigned threads) { return std::max(1u, ceilDiv(std::
 unsigned long long TreeEngine::kernelLaunches() { return g_launches.load(std::memory_order_relaxed); }
 
 // --------------------------------------------------------------------------
+// sort tuner
+// --------------------------------------------------------------------------
+namespace
+{
+struct TunerState
+{
+    std::mutex mu;
+    std::map<std::tuple<int, int, int>, int> chosen;  // (device, segmented, size class) -> configuration
+    std::map<std::tuple<int, int, int>, int> timing;  // classes being timed by some thread
+    bool autotune = true;
+    int forced = -1;
+};
+TunerState &tuner()
+{
+    static TunerState t;
+    return t;
+}
+std::tuple<int, int, int> tuneKey(bool segmented, size_t n)
+{
+    int dev = 0;
+    AOT_CHECK(cudaGetDevice(&dev));
+    int cls = 0;
+    while (cls < 63 && (size_t(1) << (cls + 1)) <= std::max<size_t>(n, 1)) ++cls;
+    return {dev, segmented ? 1 : 0, cls};
+}
+}  // namespace
+
+int sortConfigCount() { return sort::kNumSortConfigs; }
+
+SortTuning sortConfigInfo(int config)
+{
+    if (config < 0 || config >= sort::kNumSortConfigs) throw std::invalid_argument("sort: unknown configuration");
+    return {config, sort::kSortConfigs[config].bits, sort::kSortConfigs[config].items, false};
+}
+
+SortTuning sortTuning(bool segmented, size_t n)
+{
+    TunerState &t = tuner();
+    const auto key = tuneKey(segmented, n);
+    std::lock_guard<std::mutex> lock(t.mu);
+    if (t.forced >= 0) return sortConfigInfo(t.forced);
+    const auto it = t.chosen.find(key);
+    if (it != t.chosen.end())
+    {
+        SortTuning r = sortConfigInfo(it->second);
+        r.tuned = true;
+        return r;
+    }
+    return sortConfigInfo(sort::kDefaultSortConfig);
+}
+
+bool sortNeedsTuning(bool segmented, size_t n)
+{
+    TunerState &t = tuner();
+    const auto key = tuneKey(segmented, n);
+    std::lock_guard<std::mutex> lock(t.mu);
+    return t.autotune && t.forced < 0 && t.chosen.find(key) == t.chosen.end() && t.timing.find(key) == t.timing.end();
+}
+
+int sortTune(bool segmented, size_t n, float (*time)(int, void *), void *ctx)
+{
+    TunerState &t = tuner();
+    const auto key = tuneKey(segmented, n);
+    {
+        std::lock_guard<std::mutex> lock(t.mu);
+        t.timing[key] = 1;  // other threads sort this class with the default meanwhile
+    }
+    struct Done
+    {
+        TunerState &t;
+        std::tuple<int, int, int> key;
+        ~Done()
+        {
+            std::lock_guard<std::mutex> lock(t.mu);
+            t.timing.erase(key);
+        }
+    } done{t, key};
+    int best = sort::kDefaultSortConfig;
+    float bestMs = 0.f;
+    for (int c = 0; c < sort::kNumSortConfigs; ++c)
+    {
+        time(c, ctx);  // first launches of a configuration load and set up its kernels
+        const float ms = time(c, ctx);
+        if (c == 0 || ms < bestMs)
+        {
+            best = c;
+            bestMs = ms;
+        }
+    }
+    std::lock_guard<std::mutex> lock(t.mu);
+    t.chosen[key] = best;
+    return best;
+}
+
+void sortSetAutotune(bool on)
+{
+    std::lock_guard<std::mutex> lock(tuner().mu);
+    tuner().autotune = on;
+}
+
+void sortForceConfig(int config)
+{
+    if (config >= sort::kNumSortConfigs) throw std::invalid_argument("sort: unknown configuration");
+    std::lock_guard<std::mutex> lock(tuner().mu);
+    tuner().forced = config < 0 ? -1 : config;
+}
+
+void sortForgetTuning()
+{
+    std::lock_guard<std::mutex> lock(tuner().mu);
+    tuner().chosen.clear();
+}
+
+// --------------------------------------------------------------------------
 // stand-alone stable pair sort (cub::DeviceRadixSort::SortPairs semantics)
 // --------------------------------------------------------------------------
 namespace
@@ -464,29 +577,55 @@ namespace
 struct PairSortLayout
 {
     size_t altKeys = 0, altVals = 0, counters = 0, status = 0, total = 0, tiles = 0;
-    explicit PairSortLayout(size_t n)
+    int passes = 0;
+    PairSortLayout(size_t n, int cfg)
     {
         auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-        tiles = std::max<size_t>(1, (n + sort::kTile - 1) / sort::kTile);
+        tiles = configTiles(cfg, n);
+        passes = sort::configPasses(cfg);
         altKeys = 0;
         altVals = up(altKeys + n * sizeof(u64));
         counters = up(altVals + n * sizeof(u32));
-        status = up(counters + (2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses + 2) * sizeof(u32));
-        total = up(status + size_t(sort::kMaxPasses) * tiles * sort::kRadix * sizeof(u64));
+        status = up(counters + (2 * size_t(passes) * sort::kRadix + passes + 2) * sizeof(u32));
+        total = up(status + size_t(passes) * tiles * sort::kRadix * sizeof(u64));
     }
 };
 }  // namespace
 
+// The scratch a caller sizes must fit whichever configuration the tuner
+// later picks, so the size query answers the largest.
 void TreeEngine::sortPairs(void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
                            unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
                            int beginBit, int endBit, cudaStream_t s)
+{
+    if (!scratchBytes) throw std::invalid_argument("ao_sort_pairs: scratch_bytes must not be null");
+    if (!scratch)
+    {
+        size_t most = 0;
+        for (int c = 0; c < sort::kNumSortConfigs; ++c)
+        {
+            size_t b = 0;
+            sortPairsWith(c, nullptr, &b, keysIn, keysOut, valsIn, valsOut, n, beginBit, endBit, s);
+            most = std::max(most, b);
+        }
+        *scratchBytes = most;
+        return;
+    }
+    sortPairsWith(sortTuning(false, n).config, scratch, scratchBytes, keysIn, keysOut, valsIn, valsOut, n, beginBit,
+                  endBit, s);
+}
+
+void TreeEngine::sortPairsWith(int cfg, void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
+                               unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
+                               int beginBit, int endBit, cudaStream_t s)
 {
     if (!scratchBytes) throw std::invalid_argument("ao_sort_pairs: scratch_bytes must not be null");
     if (beginBit < 0 || endBit > 64 || beginBit > endBit)
         throw std::invalid_argument("ao_sort_pairs: need 0 <= begin_bit <= end_bit <= 64");
     if (n > size_t(std::numeric_limits<std::uint32_t>::max()))
         throw std::invalid_argument("ao_sort_pairs: more than 2^32 - 1 items");
-    const PairSortLayout lay(n);
+    if (cfg < 0 || cfg >= sort::kNumSortConfigs) throw std::invalid_argument("ao_sort_pairs: unknown configuration");
+    const PairSortLayout lay(n, cfg);
     if (!scratch)
     {
         *scratchBytes = lay.total;
@@ -501,8 +640,12 @@ void TreeEngine::sortPairs(void *scratch, size_t *scratchBytes, const unsigned l
     u32 *altV = reinterpret_cast<u32 *>(base + lay.altVals);
     u32 *ctr = reinterpret_cast<u32 *>(base + lay.counters);
     u64 *status = reinterpret_cast<u64 *>(base + lay.status);
-    int *error = reinterpret_cast<int *>(ctr + 2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses);
-    const int passes = (endBit - beginBit + sort::kRadixBits - 1) / sort::kRadixBits;
+    const int slots = lay.passes;  // rows of hist and bins
+    u32 *bins = ctr + size_t(slots) * sort::kRadix;
+    u32 *tileCounters = ctr + 2 * size_t(slots) * sort::kRadix;
+    int *error = reinterpret_cast<int *>(tileCounters + slots);
+    const int bitsPer = sort::kSortConfigs[cfg].bits;
+    const int passes = (endBit - beginBit + bitsPer - 1) / bitsPer;
     if (passes == 0)
     {
         AOT_CHECK(cudaMemcpyAsync(keysOut, keysIn, n * sizeof(u64), cudaMemcpyDeviceToDevice, s));
@@ -511,14 +654,14 @@ void TreeEngine::sortPairs(void *scratch, size_t *scratchBytes, const unsigned l
         AOT_LAUNCH_CHECK();
         return;
     }
-    AOT_CHECK(cudaMemsetAsync(ctr, 0, (2 * sort::kMaxPasses * sort::kRadix + sort::kMaxPasses + 2) * sizeof(u32), s));
+    AOT_CHECK(cudaMemsetAsync(ctr, 0, (2 * size_t(slots) * sort::kRadix + slots + 2) * sizeof(u32), s));
     AOT_CHECK(cudaMemsetAsync(status, 0, size_t(passes) * lay.tiles * sort::kRadix * sizeof(u64), s));
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n, sort::kThreads), unsigned(smCount()) * 8u));
-    sort::histogramKernel<<<blocks, sort::kThreads, 0, s>>>(reinterpret_cast<const u64 *>(keysIn), n, beginBit, passes,
-                                                             ctr, endBit), noteLaunch();
-    sort::binsKernel<<<1, sort::kRadix, 0, s>>>(ctr, ctr + sort::kMaxPasses * sort::kRadix, passes), noteLaunch();
+    sort::launchHistogram(cfg, s, blocks, reinterpret_cast<const u64 *>(keysIn), n, beginBit, passes, ctr, endBit),
+        noteLaunch();
+    sort::binsKernel<<<1, sort::kRadix, 0, s>>>(ctr, bins, passes), noteLaunch();
     AOT_LAUNCH_CHECK();
-    setPassSmem();
+    sort::setPassSmemAll();
     const u64 *kin = reinterpret_cast<const u64 *>(keysIn);
     const u32 *vin = valsIn;
     for (int p = 0; p < passes; ++p)
@@ -527,12 +670,11 @@ void TreeEngine::sortPairs(void *scratch, size_t *scratchBytes, const unsigned l
         const bool toOut = ((passes - 1 - p) & 1) == 0;
         u64 *kout = toOut ? reinterpret_cast<u64 *>(keysOut) : altK;
         u32 *vout = toOut ? valsOut : altV;
-        const int shift = beginBit + p * sort::kRadixBits;
-        const int bits = std::min(sort::kRadixBits, endBit - shift);
-        sort::onesweepKernel<<<unsigned(lay.tiles), sort::kThreads, sort::passSmem(), s>>>(
-            kin, vin, kout, vout, n, shift, ctr + sort::kMaxPasses * sort::kRadix + p * sort::kRadix,
-            ctr + 2 * sort::kMaxPasses * sort::kRadix + p, status + size_t(p) * lay.tiles * sort::kRadix, error,
-            bits), noteLaunch();
+        const int shift = beginBit + p * bitsPer;
+        const int bits = std::min(bitsPer, endBit - shift);
+        sort::launchPass(cfg, s, kin, vin, kout, vout, n, shift, bins + p * sort::kRadix, tileCounters + p,
+                         status + size_t(p) * lay.tiles * sort::kRadix, error, bits),
+            noteLaunch();
         AOT_LAUNCH_CHECK();
         kin = kout;
         vin = vout;
@@ -555,6 +697,7 @@ struct TreeEngine::Impl
     cudaStream_t d2h = nullptr;
     cudaEvent_t ready = nullptr;
     cudaEvent_t marks[8] = {};              // stage events (profiling)
+    cudaEvent_t tuneStart = nullptr, tuneEnd = nullptr;  // sort tuner timing
     std::vector<cudaEvent_t> nfMarks;       // begin/end pairs around near-field launches
     DevMem history;
     // tree
@@ -582,6 +725,8 @@ struct TreeEngine::Impl
         if (ready) cudaEventDestroy(ready);
         for (cudaEvent_t e : marks)
             if (e) cudaEventDestroy(e);
+        if (tuneStart) cudaEventDestroy(tuneStart);
+        if (tuneEnd) cudaEventDestroy(tuneEnd);
         for (cudaEvent_t e : nfMarks) cudaEventDestroy(e);
         if (d2h) cudaStreamDestroy(d2h);
     }
@@ -840,22 +985,64 @@ void TreeEngine::sortParticles()
     m_->groupStale = true;  // cell table entries hold indices into the sorted keys
     if (n_ == 0) return;
     cudaStream_t s = cfg_.stream;
+    m_->sortArena.ensure(n_, s);
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    AOT_CHECK(cudaStreamIsCapturing(s, &capture));
+    if (capture == cudaStreamCaptureStatusNone && cfg_.tuneSort && sortNeedsTuning(false, n_))
+    {
+        // every configuration sorts identically, so the keys of the last
+        // timed run are the sorted keys
+        if (!m_->tuneStart) AOT_CHECK(cudaEventCreate(&m_->tuneStart));
+        if (!m_->tuneEnd) AOT_CHECK(cudaEventCreate(&m_->tuneEnd));
+        auto time = [](int c, void *ctx) -> float {
+            TreeEngine &e = *static_cast<TreeEngine *>(ctx);
+            AOT_CHECK(cudaEventRecord(e.m_->tuneStart, e.cfg_.stream));
+            e.sortKeys(c);
+            AOT_CHECK(cudaEventRecord(e.m_->tuneEnd, e.cfg_.stream));
+            AOT_CHECK(cudaEventSynchronize(e.m_->tuneEnd));
+            float ms = 0.f;
+            AOT_CHECK(cudaEventElapsedTime(&ms, e.m_->tuneStart, e.m_->tuneEnd));
+            return ms;
+        };
+        sortTune(false, n_, time, this);
+    }
+    else
+    {
+        sortKeys(sortTuning(false, n_).config);
+    }
+    const KeyIndex idx = m_->keyIndex(n_);
+    rb::sampleKeysKernel<<<gridFor(idx.ns, 256), 256, 0, s>>>(m_->P[0].as<u64>(), n_, m_->sample.as<u64>(), idx.ns),
+        noteLaunch();
+    AOT_LAUNCH_CHECK();
+}
+
+// Keys of every particle, then the stable (key, slot) sort with sort
+// configuration `config`; the result lands in P[0] / Perm[0].
+void TreeEngine::sortKeys(int config)
+{
+    cudaStream_t s = cfg_.stream;
     SortArena &a = m_->sortArena;
-    a.ensure(n_, s);
-    clearArena(s, a, n_, sort::kMaxPasses);
+    const int passes = sort::configPasses(config);
+    if (passes & 1) throw std::logic_error("adaptive_octree: sort configurations must have an even pass count");
+    clearArena(config, s, a, n_, passes);
     u64 *k[2] = {m_->P[0].as<u64>(), m_->P[1].as<u64>()};
     u32 *v[2] = {m_->Perm[0].as<u32>(), m_->Perm[1].as<u32>()};
+    // 8-bit digits: the histogram comes with the keys; otherwise a pass of its own
+    const bool fused = sort::kSortConfigs[config].bits == sort::kRadixBits;
+    const int histPasses = fused ? sort::kMaxPasses : 0;
     if (cfg_.real == 0)
         launchKeygen<float>(cfg_.kind, cfg_.hilbert, static_cast<const float *>(x_), static_cast<const float *>(y_),
-                            static_cast<const float *>(z_), n_, m_->kpf, k[0], a.hist(), sort::kMaxPasses, s);
+                            static_cast<const float *>(z_), n_, m_->kpf, k[0], a.hist(), histPasses, s);
     else
         launchKeygen<double>(cfg_.kind, cfg_.hilbert, static_cast<const double *>(x_), static_cast<const double *>(y_),
-                             static_cast<const double *>(z_), n_, m_->kpd, k[0], a.hist(), sort::kMaxPasses, s);
-    const int where = runPasses(s, k, v, n_, 0, sort::kMaxPasses, true, a, &m_->st->error);
-    (void)where;  // eight passes end in buffer 0
-    const size_t ns = (n_ + kSampleStride - 1) >> kSampleShift;
-    rb::sampleKeysKernel<<<gridFor(ns, 256), 256, 0, s>>>(k[0], n_, m_->sample.as<u64>(), ns), noteLaunch();
-    AOT_LAUNCH_CHECK();
+                             static_cast<const double *>(z_), n_, m_->kpd, k[0], a.hist(), histPasses, s);
+    if (!fused)
+    {
+        const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n_, sort::kThreads), unsigned(smCount()) * 8u));
+        sort::launchHistogram(config, s, blocks, k[0], n_, 0, passes, a.hist(), 64), noteLaunch();
+        AOT_LAUNCH_CHECK();
+    }
+    runPasses(config, s, k, v, n_, 0, 64, true, a, &m_->st->error);  // an even pass count ends in buffer 0
 }
 
 void TreeEngine::computeKeys(int kind, int real, const void *x, const void *y, const void *z, size_t n,

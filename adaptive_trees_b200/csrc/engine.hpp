@@ -53,6 +53,9 @@ struct EngineConfig
     double box[6] = {0, 1, 0, 1, 0, 1};
     adaptive_octree::ViewConfig views{};
     cudaStream_t stream = nullptr;
+    // a build may time the sort configurations for the sort tuner (off for
+    // latency-bound callers: they use the tuned choice or the default)
+    bool tuneSort = true;
 };
 
 // Process-wide cache of device and pinned host blocks.
@@ -150,6 +153,10 @@ public:
     static void sortPairs(void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
                           unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
                           int beginBit, int endBit, cudaStream_t s);
+    // the same with sort configuration `config` (its own scratch size)
+    static void sortPairsWith(int config, void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
+                              unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
+                              int beginBit, int endBit, cudaStream_t s);
     // dst[i] = src[perm[i]] for the numParticles() elements of elemBytes
     // each: per-particle data in key order (device pointers, the tree's stream)
     void gather(const void *src, void *dst, size_t elemBytes) const;
@@ -197,6 +204,7 @@ private:
     void markNearField(bool begin);
 
     void sortParticles();
+    void sortKeys(int config);
     void octreeBuild();
     void binaryBuild();
     void octreePass(bool buildMode, long long limit);
@@ -211,6 +219,29 @@ private:
     void readState();
     void materializeCounts();
 };
+
+// The radix sort tuner: which compiled sort configuration (digit width, keys
+// per thread) a sort of n keys uses on the current device, for contiguous
+// (tree, pair) or segmented (forest) sorts.  Sizes are grouped by bit length.
+// The first tree or forest build of a size class times every configuration
+// on its own keys and keeps the fastest; later sorts of that class reuse it.
+struct SortTuning
+{
+    int config;          // index into the compiled configurations
+    int digitBits;
+    int itemsPerThread;  // tile = 256 threads x itemsPerThread keys
+    bool tuned;          // chosen by timing (else the default or a forced one)
+};
+int sortConfigCount();
+SortTuning sortConfigInfo(int config);
+SortTuning sortTuning(bool segmented, size_t n);
+bool sortNeedsTuning(bool segmented, size_t n);
+// time(c) sorts with configuration c and returns its duration in ms; each
+// configuration is timed twice and the second time counts.
+int sortTune(bool segmented, size_t n, float (*time)(int, void *), void *ctx);
+void sortSetAutotune(bool on);
+void sortForceConfig(int config);  // -1 lifts the force
+void sortForgetTuning();
 
 // TreeEngine::sortPairs with its scratch in a fixed device array of
 // sort_noalloc.cu (no allocation; at most sortPairsNoAllocMaxItems() items;

@@ -30,8 +30,10 @@ struct ForestEngine::Impl
     int S = 0;
     size_t total = 0;
     std::vector<forest::System> systems;
-    // segmented sort
+    // segmented sort: tiles of the sort configuration `tileConfig`
     u32 numTiles = 0;
+    int tileConfig = -1;
+    cudaEvent_t tuneStart = nullptr, tuneEnd = nullptr;  // sort tuner timing
     DevMem systemsD, tileSys, tileBegin, tileEnd, segFirstTile, segBase;
     DevMem P[2], Perm[2], hist, bins, tileCounters, status;
     // leaf arrays (entries = all systems' leaves + sentinels)
@@ -53,6 +55,45 @@ struct ForestEngine::Impl
     {
         if (hst) blockcache::giveHost(hst, hstBytes);
         if (hsys) blockcache::giveHost(hsys, hsysBytes);
+        if (tuneStart) cudaEventDestroy(tuneStart);
+        if (tuneEnd) cudaEventDestroy(tuneEnd);
+    }
+
+    // Tile table of the segmented sort for configuration `config`: every
+    // system in tiles of that configuration's size (a host build and upload,
+    // done when the configuration changes).
+    void buildTiles(int config, cudaStream_t stream)
+    {
+        if (config == tileConfig) return;
+        const u32 tile = u32(sort::configTile(config));
+        std::vector<u32> tSys, tBeg, tEnd;
+        std::vector<u32> first(static_cast<size_t>(S), 0xffffffffu);
+        std::vector<u32> base(static_cast<size_t>(S), 0u);
+        for (int s = 0; s < S; ++s)
+        {
+            const forest::System &sy = systems[s];
+            base[s] = sy.base;
+            if (sy.n) first[s] = u32(tSys.size());
+            for (u32 b = 0; b < sy.n; b += tile)
+            {
+                tSys.push_back(u32(s));
+                tBeg.push_back(sy.base + b);
+                tEnd.push_back(sy.base + std::min<u32>(sy.n, b + tile));
+            }
+        }
+        waitStream(stream);  // the old tables may still be read
+        numTiles = u32(tSys.size());
+        auto upload = [](DevMem &d, const void *src, size_t bytes) {
+            d.reserve(std::max<size_t>(bytes, 16));
+            if (bytes) AOT_CHECK(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice));
+        };
+        upload(tileSys, tSys.data(), tSys.size() * 4);
+        upload(tileBegin, tBeg.data(), tBeg.size() * 4);
+        upload(tileEnd, tEnd.data(), tEnd.size() * 4);
+        upload(segFirstTile, first.data(), first.size() * 4);
+        upload(segBase, base.data(), base.size() * 4);
+        status.reserve(std::max<size_t>(numTiles, 1) * sort::kPassSlots * sort::kRadix * 8);
+        tileConfig = config;
     }
 
     forest::Bufs bufs() const
@@ -79,20 +120,6 @@ struct ForestEngine::Impl
         return f;
     }
 };
-
-namespace
-{
-bool forestPassSmemSet = false;
-void setForestPassSmem()
-{
-    if (!forestPassSmemSet)
-    {
-        AOT_CHECK(cudaFuncSetAttribute(sort::segmentOnesweepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(sort::passSmem())));
-        forestPassSmemSet = true;
-    }
-}
-}  // namespace
 
 ForestEngine::ForestEngine(const void *const *x, const void *const *y, const void *const *z, const size_t *n,
                            int numSystems, const EngineConfig &cfg)
@@ -127,42 +154,20 @@ ForestEngine::ForestEngine(const void *const *x, const void *const *y, const voi
     m.capModel.assign(size_t(numSystems), OctreeCapacity{});
     m.leafCap.assign(size_t(numSystems), 0);
 
-    // tile table of the segmented sort: every system in tiles of sort::kTile
-    std::vector<u32> tSys, tBeg, tEnd;
-    std::vector<u32> first(static_cast<size_t>(numSystems), 0xffffffffu);
-    std::vector<u32> base(static_cast<size_t>(numSystems), 0u);
-    for (int s = 0; s < numSystems; ++s)
     {
-        const forest::System &sy = m.systems[s];
-        base[s] = sy.base;
-        if (sy.n) first[s] = u32(tSys.size());
-        for (u32 b = 0; b < sy.n; b += u32(sort::kTile))
-        {
-            tSys.push_back(u32(s));
-            tBeg.push_back(sy.base + b);
-            tEnd.push_back(sy.base + std::min<u32>(sy.n, b + u32(sort::kTile)));
-        }
+        const size_t bytes = m.systems.size() * sizeof(forest::System);
+        m.systemsD.reserve(std::max<size_t>(bytes, 16));
+        if (bytes) AOT_CHECK(cudaMemcpy(m.systemsD.p, m.systems.data(), bytes, cudaMemcpyHostToDevice));
     }
-    m.numTiles = u32(tSys.size());
-    auto upload = [](DevMem &d, const void *src, size_t bytes) {
-        d.reserve(std::max<size_t>(bytes, 16));
-        if (bytes) AOT_CHECK(cudaMemcpy(d.p, src, bytes, cudaMemcpyHostToDevice));
-    };
-    upload(m.systemsD, m.systems.data(), m.systems.size() * sizeof(forest::System));
-    upload(m.tileSys, tSys.data(), tSys.size() * 4);
-    upload(m.tileBegin, tBeg.data(), tBeg.size() * 4);
-    upload(m.tileEnd, tEnd.data(), tEnd.size() * 4);
-    upload(m.segFirstTile, first.data(), first.size() * 4);
-    upload(m.segBase, base.data(), base.size() * 4);
+    m.buildTiles(sortTuning(true, total).config, cfg.stream);
     for (int k = 0; k < 2; ++k)
     {
         m.P[k].reserve(std::max<size_t>(total, 1) * 8);
         m.Perm[k].reserve(std::max<size_t>(total, 1) * 4);
     }
-    m.hist.reserve(size_t(numSystems) * sort::kMaxPasses * sort::kRadix * 4);
-    m.bins.reserve(size_t(numSystems) * sort::kMaxPasses * sort::kRadix * 4);
-    m.tileCounters.reserve(sort::kMaxPasses * 4);
-    m.status.reserve(std::max<size_t>(m.numTiles, 1) * sort::kMaxPasses * sort::kRadix * 8);
+    m.hist.reserve(size_t(numSystems) * sort::kPassSlots * sort::kRadix * 4);
+    m.bins.reserve(size_t(numSystems) * sort::kPassSlots * sort::kRadix * 4);
+    m.tileCounters.reserve(sort::kPassSlots * 4);
     m.st.reserve(sizeof(forest::State));
     AOT_CHECK(cudaMemsetAsync(m.st.p, 0, sizeof(forest::State), cfg.stream));
     m.sys.reserve(size_t(numSystems) * sizeof(forest::SysState));
@@ -231,51 +236,106 @@ void ForestEngine::sortParticles()
     cudaStream_t s = m.cfg.stream;
     if (m.total)
     {
-        AOT_CHECK(cudaMemsetAsync(m.hist.p, 0, size_t(m.S) * sort::kMaxPasses * sort::kRadix * 4, s));
-        AOT_CHECK(cudaMemsetAsync(m.tileCounters.p, 0, sort::kMaxPasses * 4, s));
-        AOT_CHECK(cudaMemsetAsync(m.status.p, 0, size_t(m.numTiles) * sort::kMaxPasses * sort::kRadix * 8, s));
-        const unsigned grid = std::max(1u, std::min<unsigned>(m.numTiles, unsigned(smCount()) * 8u));
-        u64 *keys = m.P[0].as<u64>();
-        const Impl &cm = m;
-        auto launch = [&](auto real) {
-            using Real = decltype(real);
-            const KeygenParams<Real> &prm = [&]() -> const KeygenParams<Real> & {
-                if constexpr (sizeof(Real) == 4) return cm.kpf;
-                else return cm.kpd;
-            }();
-            if (m.cfg.hilbert)
-                forest::keygenKernel<Real, Curve::Hilbert><<<grid, forest::kThreads, 0, s>>>(
-                    m.systemsD.as<forest::System>(), m.tileSys.as<u32>(), m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
-                    m.numTiles, prm, keys, m.hist.as<u32>()), noteLaunch();
-            else
-                forest::keygenKernel<Real, Curve::Morton><<<grid, forest::kThreads, 0, s>>>(
-                    m.systemsD.as<forest::System>(), m.tileSys.as<u32>(), m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
-                    m.numTiles, prm, keys, m.hist.as<u32>()), noteLaunch();
-        };
-        if (m.cfg.real == 0) launch(float{});
-        else launch(double{});
-        forest::binsKernel<<<unsigned(m.S), sort::kRadix, 0, s>>>(m.systemsD.as<forest::System>(), m.S,
-                                                                  m.hist.as<u32>(), m.bins.as<u32>()), noteLaunch();
-        AOT_LAUNCH_CHECK();
-        setForestPassSmem();
-        u64 *k[2] = {m.P[0].as<u64>(), m.P[1].as<u64>()};
-        u32 *v[2] = {m.Perm[0].as<u32>(), m.Perm[1].as<u32>()};
-        for (int p = 0; p < sort::kMaxPasses; ++p)
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        AOT_CHECK(cudaStreamIsCapturing(s, &capture));
+        if (capture != cudaStreamCaptureStatusNone)
         {
-            const int in = p & 1, out = in ^ 1;
-            const sort::SegmentTiles tiles{m.tileSys.as<u32>(),      m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
-                                           m.segFirstTile.as<u32>(), m.segBase.as<u32>(),
-                                           m.bins.as<u32>() + size_t(p) * m.S * sort::kRadix};
-            sort::segmentOnesweepKernel<<<m.numTiles, sort::kThreads, sort::passSmem(), s>>>(
-                tiles, k[in], p == 0 ? nullptr : v[in], k[out], v[out], p * sort::kRadixBits,
-                m.tileCounters.as<u32>() + p, m.status.as<u64>() + size_t(p) * m.numTiles * sort::kRadix,
-                &m.st.as<forest::State>()->error), noteLaunch();
-            AOT_LAUNCH_CHECK();
+            sortKeys(m.tileConfig);  // under capture the tables stay as they are
         }
-        // eight passes end in buffer 0
+        else if (m.cfg.tuneSort && sortNeedsTuning(true, m.total))
+        {
+            // every configuration sorts identically: the keys of the last timed
+            // run stand, and the tables follow the chosen configuration
+            if (!m.tuneStart) AOT_CHECK(cudaEventCreate(&m.tuneStart));
+            if (!m.tuneEnd) AOT_CHECK(cudaEventCreate(&m.tuneEnd));
+            auto time = [](int c, void *ctx) -> float {
+                ForestEngine &e = *static_cast<ForestEngine *>(ctx);
+                Impl &im = *e.m_;
+                im.buildTiles(c, im.cfg.stream);
+                AOT_CHECK(cudaEventRecord(im.tuneStart, im.cfg.stream));
+                e.sortKeys(c);
+                AOT_CHECK(cudaEventRecord(im.tuneEnd, im.cfg.stream));
+                AOT_CHECK(cudaEventSynchronize(im.tuneEnd));
+                float ms = 0.f;
+                AOT_CHECK(cudaEventElapsedTime(&ms, im.tuneStart, im.tuneEnd));
+                return ms;
+            };
+            const int best = sortTune(true, m.total, time, this);
+            m.buildTiles(best, s);
+        }
+        else
+        {
+            const int config = sortTuning(true, m.total).config;
+            m.buildTiles(config, s);
+            sortKeys(config);
+        }
     }
     forest::activeKernel<<<gridFor(size_t(m.S), 256), 256, 0, s>>>(m.bufs()), noteLaunch();
     AOT_LAUNCH_CHECK();
+}
+
+// Keys of every system and the segmented sort with sort configuration
+// `config`, whose tile table must be in place; the result lands in P[0] /
+// Perm[0] (an even pass count).
+void ForestEngine::sortKeys(int config)
+{
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    if (config != m.tileConfig) throw std::logic_error("forest: the tile table is not the sort configuration's");
+    const int bitsPer = sort::kSortConfigs[config].bits;
+    const int passes = sort::configPasses(config);
+    if (passes & 1) throw std::logic_error("forest: sort configurations must have an even pass count");
+    AOT_CHECK(cudaMemsetAsync(m.hist.p, 0, size_t(m.S) * sort::kPassSlots * sort::kRadix * 4, s));
+    AOT_CHECK(cudaMemsetAsync(m.tileCounters.p, 0, sort::kPassSlots * 4, s));
+    AOT_CHECK(cudaMemsetAsync(m.status.p, 0, size_t(m.numTiles) * passes * sort::kRadix * 8, s));
+    const unsigned grid = std::max(1u, std::min<unsigned>(m.numTiles, unsigned(smCount()) * 8u));
+    u64 *keys = m.P[0].as<u64>();
+    // 8-bit digits: the histograms come with the keys; otherwise a pass of their own
+    const bool fused = bitsPer == sort::kRadixBits;
+    u32 *keygenHist = fused ? m.hist.as<u32>() : nullptr;
+    const Impl &cm = m;
+    auto launch = [&](auto real) {
+        using Real = decltype(real);
+        const KeygenParams<Real> &prm = [&]() -> const KeygenParams<Real> & {
+            if constexpr (sizeof(Real) == 4) return cm.kpf;
+            else return cm.kpd;
+        }();
+        if (m.cfg.hilbert)
+            forest::keygenKernel<Real, Curve::Hilbert><<<grid, forest::kThreads, 0, s>>>(
+                m.systemsD.as<forest::System>(), m.tileSys.as<u32>(), m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
+                m.numTiles, prm, keys, keygenHist), noteLaunch();
+        else
+            forest::keygenKernel<Real, Curve::Morton><<<grid, forest::kThreads, 0, s>>>(
+                m.systemsD.as<forest::System>(), m.tileSys.as<u32>(), m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
+                m.numTiles, prm, keys, keygenHist), noteLaunch();
+    };
+    if (m.cfg.real == 0) launch(float{});
+    else launch(double{});
+    if (!fused)
+        forest::segHistKernel<7><<<m.numTiles, forest::kThreads, 0, s>>>(m.tileSys.as<u32>(), m.tileBegin.as<u32>(),
+                                                                      m.tileEnd.as<u32>(), keys, passes,
+                                                                      m.hist.as<u32>()),
+            noteLaunch();
+    forest::binsKernel<<<unsigned(m.S), sort::kRadix, 0, s>>>(m.systemsD.as<forest::System>(), m.S, m.hist.as<u32>(),
+                                                              m.bins.as<u32>(), passes),
+        noteLaunch();
+    AOT_LAUNCH_CHECK();
+    sort::setPassSmemAll();
+    u64 *k[2] = {m.P[0].as<u64>(), m.P[1].as<u64>()};
+    u32 *v[2] = {m.Perm[0].as<u32>(), m.Perm[1].as<u32>()};
+    for (int p = 0; p < passes; ++p)
+    {
+        const int in = p & 1, out = in ^ 1;
+        const int shift = p * bitsPer;
+        const sort::SegmentTiles tiles{m.tileSys.as<u32>(),      m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
+                                       m.segFirstTile.as<u32>(), m.segBase.as<u32>(),
+                                       m.bins.as<u32>() + size_t(p) * m.S * sort::kRadix};
+        sort::launchSegmentPass(config, s, m.numTiles, tiles, k[in], p == 0 ? nullptr : v[in], k[out], v[out], shift,
+                                m.tileCounters.as<u32>() + p, m.status.as<u64>() + size_t(p) * m.numTiles * sort::kRadix,
+                                &m.st.as<forest::State>()->error, std::min(bitsPer, 64 - shift)),
+            noteLaunch();
+        AOT_LAUNCH_CHECK();
+    }
 }
 
 // One decision round (build) or fixed pass (update) over all systems.

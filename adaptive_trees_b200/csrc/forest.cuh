@@ -92,9 +92,10 @@ struct Bufs
 // --------------------------------------------------------------------------
 // keys and the segmented sort
 // --------------------------------------------------------------------------
-// Keys of every system's particles and the per-system digit histograms of
-// all eight passes.  Each CTA takes a contiguous range of tiles, so its
-// shared histogram is flushed only where the system changes.
+// Keys of every system's particles and (hist != nullptr) the per-system
+// histograms of the eight 8-bit digits, hist[system][pass slot][digit].  Each
+// CTA takes a contiguous range of tiles, so its shared histogram is flushed
+// only where the system changes.
 template <class Real, Curve C>
 static __global__ void __launch_bounds__(kThreads)
     keygenKernel(const System *__restrict__ systems, const u32 *__restrict__ tileSys,
@@ -116,9 +117,9 @@ static __global__ void __launch_bounds__(kThreads)
     int cur = -1;
     auto flush = [&]() {
         __syncthreads();
-        if (cur >= 0)
+        if (cur >= 0 && hist)
         {
-            u32 *h = hist + size_t(cur) * sort::kMaxPasses * sort::kRadix;
+            u32 *h = hist + size_t(cur) * sort::kPassSlots * sort::kRadix;
             for (int i = threadIdx.x; i < sort::kMaxPasses * sort::kRadix; i += blockDim.x)
             {
                 const u32 v = sh[i];
@@ -149,26 +150,61 @@ static __global__ void __launch_bounds__(kThreads)
             const u32 l = g - sy.base;
             const u64 k = particleKey<Real, C>(x[l], y[l], z[l], prm, sEnc, sNext);
             keys[g] = k;
+            if (hist)
+            {
 #pragma unroll
-            for (int p = 0; p < sort::kMaxPasses; ++p)
-                atomicAdd(&sh[p * sort::kRadix + int((k >> (p * sort::kRadixBits)) & (sort::kRadix - 1))], 1u);
+                for (int p = 0; p < sort::kMaxPasses; ++p)
+                    atomicAdd(&sh[p * sort::kRadix + int((k >> (p * sort::kRadixBits)) & (sort::kRadix - 1))], 1u);
+            }
         }
     }
     flush();
+}
+
+// Per-system histograms of Bits-wide digits for `passes` passes, one CTA per
+// tile of the segmented sort (the sort configurations whose digits are not
+// the 8 bits key generation counts).  hist[system][pass slot][digit].
+template <int Bits>
+static __global__ void __launch_bounds__(kThreads)
+    segHistKernel(const u32 *__restrict__ tileSys, const u32 *__restrict__ tileBegin, const u32 *__restrict__ tileEnd,
+                  const u64 *__restrict__ keys, int passes, u32 *__restrict__ hist)
+{
+    constexpr int R = 1 << Bits;
+    __shared__ u32 sh[sort::kPassSlots * R];
+    for (int i = threadIdx.x; i < sort::kPassSlots * R; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const u32 t = blockIdx.x;
+    for (u32 g = tileBegin[t] + threadIdx.x; g < tileEnd[t]; g += blockDim.x)
+    {
+        const u64 k = __ldg(keys + g);
+        for (int p = 0; p < passes; ++p)
+        {
+            const int shift = p * Bits;
+            const int bits = 64 - shift < Bits ? 64 - shift : Bits;
+            atomicAdd(&sh[p * R + int((k >> shift) & ((1u << bits) - 1))], 1u);
+        }
+    }
+    __syncthreads();
+    u32 *h = hist + size_t(tileSys[t]) * sort::kPassSlots * sort::kRadix;
+    for (int i = threadIdx.x; i < passes * R; i += blockDim.x)
+    {
+        const u32 v = sh[i];
+        if (v) atomicAdd(h + (i / R) * sort::kRadix + (i % R), v);
+    }
 }
 
 // Per system and pass: global start of each digit = base + exclusive scan of
 // the system's digit counts.  bins[pass][system][digit].
 static __global__ void __launch_bounds__(sort::kRadix)
     binsKernel(const System *__restrict__ systems, int numSystems, const u32 *__restrict__ hist,
-               u32 *__restrict__ bins)
+               u32 *__restrict__ bins, int passes)
 {
     __shared__ u32 s[sort::kRadix];
     const int sys = blockIdx.x, d = threadIdx.x;
     const u32 base = systems[sys].base;
-    for (int p = 0; p < sort::kMaxPasses; ++p)
+    for (int p = 0; p < passes; ++p)
     {
-        const u32 v = hist[(size_t(sys) * sort::kMaxPasses + p) * sort::kRadix + d];
+        const u32 v = hist[(size_t(sys) * sort::kPassSlots + p) * sort::kRadix + d];
         s[d] = v;
         __syncthreads();
         for (int off = 1; off < sort::kRadix; off <<= 1)

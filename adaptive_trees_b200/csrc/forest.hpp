@@ -57,6 +57,7 @@ private:
     struct Impl;
     std::unique_ptr<Impl> m_;
     void sortParticles();
+    void sortKeys(int config);
     void pass(bool build, const unsigned char *frozenDevice);
     void beginUpdate(const unsigned char *frozen);
     void endUpdate();

@@ -5,15 +5,19 @@
 // (tree_view.cu:664-689).  Stable: equal keys keep their input order, which
 // for the particle sort makes Perm ascend within runs of equal keys.
 //
-// Structure (one read of the keys per 8-bit digit):
+// Structure (one read of the keys per digit):
 //   1. a histogram kernel counts all digit positions at once (fused into key
-//      generation for the particle sort, so the keys are never re-read);
+//      generation for the particle sort with 8-bit digits, so the keys are
+//      never re-read);
 //   2. a tiny kernel turns the counts into per-digit global start offsets;
-//   3. one onesweep kernel per digit: each CTA takes a tile of 4096 keys in
-//      arrival order (atomic tile counter), ranks them per warp with
-//      __match_any_sync, publishes its per-digit counts, resolves its global
-//      offsets by decoupled look-back over earlier tiles, reorders the tile in
-//      shared memory and writes digit runs out contiguously.
+//   3. one onesweep kernel per digit: each CTA takes a tile of keys in
+//      arrival order (atomic tile counter), ranks them per warp with ballots,
+//      publishes its per-digit counts, resolves its global offsets by
+//      decoupled look-back over earlier tiles, reorders the tile in shared
+//      memory and writes digit runs out contiguously.
+// The digit width and the keys per thread are template parameters; the
+// configurations compiled in are listed in kSortConfigs, and the sort tuner
+// (sort_tuner.hpp) picks one per device and problem size by timing them.
 // The look-back wait is bounded: after kLookbackSpins polls it records
 // kErrLookback in the device error word and proceeds, so a broken invariant
 // surfaces as an error status instead of a hung GPU.
@@ -25,13 +29,15 @@ namespace aot
 {
 namespace sort
 {
-constexpr int kRadixBits = 8;
-constexpr int kRadix = 1 << kRadixBits;
+constexpr int kRadixBits = 8;              // digit width of the default configuration
+constexpr int kRadix = 1 << kRadixBits;     // largest radix: stride of every per-pass digit array
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kItems = 10;
+constexpr int kItems = 10;                  // keys per thread of the default configuration
 constexpr int kTile = kThreads * kItems;
-constexpr int kMaxPasses = 8;
+constexpr int kMaxPasses = 8;               // passes of 8-bit digits over 64-bit keys
+constexpr int kPassSlots = 10;              // most passes of any configuration (7-bit digits)
+constexpr int kMinTile = kThreads * 8;      // smallest tile of any configuration
 constexpr u64 kFlagAgg = u64(1) << 62;
 constexpr u64 kFlagPrefix = u64(2) << 62;
 constexpr u64 kValueMask = (u64(1) << 62) - 1;
@@ -68,38 +74,36 @@ struct Scratch
     size_t tiles;
 };
 
-inline size_t scratchBytes(size_t n)
-{
-    const size_t tiles = (n + kTile - 1) / kTile;
-    return size_t(kMaxPasses) * kRadix * 4 * 2 + 64 + size_t(kMaxPasses) * (tiles ? tiles : 1) * kRadix * 8;
-}
-
-// Histogram of the digits of keys[0, n) for passes covering [beginBit, endBit).
+// Histogram of the Bits-wide digits of keys[0, n) for passes covering
+// [beginBit, endBit); pass p's counts go to hist[p * kRadix + digit].
+template <int Bits = kRadixBits>
 static __global__ void __launch_bounds__(kThreads) histogramKernel(const u64 *__restrict__ keys, size_t n, int beginBit,
                                                              int passes, u32 *__restrict__ hist, int endBit = 64)
 {
-    __shared__ u32 sh[kMaxPasses][kRadix];
-    for (int i = threadIdx.x; i < kMaxPasses * kRadix; i += kThreads) (&sh[0][0])[i] = 0;
+    constexpr int R = 1 << Bits;
+    __shared__ u32 sh[kPassSlots][R];
+    for (int i = threadIdx.x; i < kPassSlots * R; i += kThreads) (&sh[0][0])[i] = 0;
     __syncthreads();
     for (size_t i = blockIdx.x * size_t(kThreads) + threadIdx.x; i < n; i += size_t(gridDim.x) * kThreads)
     {
         const u64 k = __ldg(keys + i);
         for (int p = 0; p < passes; ++p)
         {
-            const int shift = beginBit + p * kRadixBits;
-            const int bits = endBit - shift < kRadixBits ? endBit - shift : kRadixBits;
+            const int shift = beginBit + p * Bits;
+            const int bits = endBit - shift < Bits ? endBit - shift : Bits;
             atomicAdd(&sh[p][(k >> shift) & ((1u << bits) - 1)], 1u);
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < passes * kRadix; i += kThreads)
+    for (int i = threadIdx.x; i < passes * R; i += kThreads)
     {
         const u32 v = (&sh[0][0])[i];
-        if (v) atomicAdd(hist + i, v);
+        if (v) atomicAdd(hist + (i / R) * kRadix + (i % R), v);
     }
 }
 
-// Exclusive scan of each pass' 256 digit counts.
+// Exclusive scan of each pass' 256 digit counts (a narrower radix leaves the
+// upper counts zero, so their starts are unused).
 static __global__ void __launch_bounds__(kRadix) binsKernel(const u32 *__restrict__ hist, u32 *__restrict__ bins, int passes)
 {
     __shared__ u32 s[kRadix];
@@ -122,20 +126,40 @@ static __global__ void __launch_bounds__(kRadix) binsKernel(const u32 *__restric
     }
 }
 
+template <int Bits, int Items>
 struct SharedPass
 {
-    u64 keys[kTile];
-    u32 vals[kTile];
-    u32 stage[kTile];              // the tile's input values, staged by one bulk copy (16-byte aligned)
-    u64 valuesReady;               // mbarrier of that copy
-    u32 staged;                    // values in `stage` (a multiple of 4)
-    u32 warpHist[kWarps][kRadix];  // per-warp digit counts, then exclusive warp offsets
-    u32 localStart[kRadix];
-    u32 gstart[kRadix];            // global position of local index 0 of each digit (mod 2^32)
-    u32 count[kRadix];
+    static constexpr int R = 1 << Bits;
+    static constexpr int T = kThreads * Items;
+    u64 keys[T];
+    u32 vals[T];
+    u32 stage[T];              // the tile's input values, staged by one bulk copy (16-byte aligned)
+    u64 valuesReady;           // mbarrier of that copy
+    u32 staged;                // values in `stage` (a multiple of 4)
+    u32 warpHist[kWarps][R];   // per-warp digit counts, then exclusive warp offsets
+    u32 localStart[R];
+    u32 gstart[R];             // global position of local index 0 of each digit (mod 2^32)
+    u32 count[R];
     u32 warpSums[kWarps];
     u32 tile;
 };
+
+// The compiled configurations: digit width, keys per thread and the CTAs per
+// SM they are built for (their shared memory and a 64-register budget allow
+// 4 CTAs for tiles of up to 3072 keys).  Each gives an even number of passes
+// over 64-bit keys (8 or 10), so the sorted data ends where it started.
+struct SortConfig
+{
+    int bits, items;
+};
+constexpr SortConfig kSortConfigs[] = {{8, 10}, {8, 16}, {8, 8}, {7, 12}, {7, 16}};
+constexpr int kNumSortConfigs = int(sizeof(kSortConfigs) / sizeof(kSortConfigs[0]));
+constexpr int kDefaultSortConfig = 0;
+constexpr int configTile(int c) { return kThreads * kSortConfigs[c].items; }
+constexpr int configPasses(int c, int bits = 64)
+{
+    return (bits + kSortConfigs[c].bits - 1) / kSortConfigs[c].bits;
+}
 
 // Lanes of the warp whose (valid) digit equals this lane's: eight ballots, one
 // per digit bit, instead of __match_any_sync.
@@ -196,13 +220,14 @@ constexpr unsigned kStageSpins = 1u << 22;  // bounded wait for the staged value
 // Tile geometry of a pass over one contiguous key array keys[0, n).  The
 // accessors are cheap and recomputed where used, so that nothing extra stays
 // live in registers across the pass.
+template <int Tile>
 struct ContiguousTiles
 {
-    static constexpr bool kStageValues = true;  // tiles start at multiples of kTile
+    static constexpr bool kStageValues = true;  // tiles start at multiples of Tile (16-byte aligned values)
     size_t n;
-    const u32 *bins;  // [kRadix] global start of each digit
-    // the tile's keys are [base(t), min(base(t) + kTile, end(t)))
-    __device__ __forceinline__ size_t base(size_t tile) const { return tile * kTile; }
+    const u32 *bins;  // [radix] global start of each digit
+    // the tile's keys are [base(t), min(base(t) + Tile, end(t)))
+    __device__ __forceinline__ size_t base(size_t tile) const { return tile * size_t(Tile); }
     __device__ __forceinline__ size_t end(size_t) const { return n; }
     // the tile publishes an inclusive prefix without look-back
     __device__ __forceinline__ bool chainStart(size_t tile) const { return tile == 0; }
@@ -212,7 +237,7 @@ struct ContiguousTiles
 };
 
 // Tile geometry of a segmented pass (the systems of a forest): tile t holds
-// the keys [tileBegin[t], tileEnd[t]) of segment tileSeg[t] (at most kTile,
+// the keys [tileBegin[t], tileEnd[t]) of segment tileSeg[t] (at most one tile,
 // never straddling segments); a look-back chain ends at the segment's first
 // tile; digit starts are per segment, and generated values are indices within
 // the segment.
@@ -228,21 +253,28 @@ struct SegmentTiles
     __device__ __forceinline__ u32 valueOffset(size_t tile) const { return segBase[tileSeg[tile]]; }
 };
 
-// One onesweep pass: digit at bit `shift` (`bits` wide) of the tiles of
-// `tiles`.  valsIn == nullptr means values are generated (first pass).
-template <class Tiles>
+// One onesweep pass: the Bits-wide digit at bit `shift` (`bits` <= Bits
+// wide) of the tiles of `tiles`, Items keys per thread.  valsIn == nullptr
+// means values are generated (first pass).  Threads below the radix own one
+// digit each in the per-digit steps.
+template <int Bits, int Items, class Tiles>
 __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__restrict__ keysIn,
                                              const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
                                              u32 *__restrict__ valsOut, int shift, u32 *tileCounter, u64 *status,
                                              int *error, int bits)
 {
+    using Smem = SharedPass<Bits, Items>;
+    constexpr int R = Smem::R;
+    constexpr int T = Smem::T;
+    static_assert(R <= kThreads && R <= kRadix, "one digit per thread");
+    static_assert(Items % 2 == 0, "ranks are packed in pairs");
     const unsigned dmask = (1u << bits) - 1;
     extern __shared__ __align__(16) unsigned char smemRaw[];
-    SharedPass &sm = *reinterpret_cast<SharedPass *>(smemRaw);
+    Smem &sm = *reinterpret_cast<Smem *>(smemRaw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
     const bool stage = Tiles::kStageValues && valsIn != nullptr;
-    for (int i = tid; i < kWarps * kRadix; i += kThreads) (&sm.warpHist[0][0])[i] = 0;
+    for (int i = tid; i < kWarps * R; i += kThreads) (&sm.warpHist[0][0])[i] = 0;
     if (tid == 0)
     {
         sm.tile = atomicAdd(tileCounter, 1u);
@@ -255,12 +287,12 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
     __syncthreads();
     const size_t tile = sm.tile;
     const size_t tileBase = tiles.base(tile);
-    const size_t warpBase = tileBase + size_t(warp) * (32 * kItems);
+    const size_t warpBase = tileBase + size_t(warp) * (32 * Items);
     if (stage && tid == 0)
     {
         // the values travel to shared memory while the keys are ranked
         const size_t end = tiles.end(tile);
-        const u32 count = u32((end - tileBase) < size_t(kTile) ? end - tileBase : size_t(kTile));
+        const u32 count = u32((end - tileBase) < size_t(T) ? end - tileBase : size_t(T));
         const bool aligned = (reinterpret_cast<uintptr_t>(valsIn + tileBase) & 15u) == 0;
         const u32 bulk = aligned ? (count & ~3u) : 0u;
         sm.staged = bulk;
@@ -275,9 +307,9 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
         }
     }
 
-    u64 key[kItems];
+    u64 key[Items];
 #pragma unroll
-    for (int i = 0; i < kItems; ++i)
+    for (int i = 0; i < Items; ++i)
     {
         const size_t idx = warpBase + size_t(i) * 32 + lane;
         key[i] = idx < tiles.end(tile) ? __ldcs(keysIn + idx) : 0ull;
@@ -287,9 +319,9 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
     // counter and broadcasts the old value.
     u32 *wh = sm.warpHist[warp];
     const unsigned ltMask = laneMaskLt();
-    u32 rank2[kItems / 2];
+    u32 rank2[Items / 2];
 #pragma unroll
-    for (int i = 0; i < kItems; ++i)
+    for (int i = 0; i < Items; ++i)
     {
         const size_t idx = warpBase + size_t(i) * 32 + lane;
         const bool valid = idx < tiles.end(tile);
@@ -307,6 +339,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
     }
     __syncthreads();
     // Per digit: warp exclusive offsets and tile total (thread = digit).
+    if (tid < R)
     {
         const int d = tid;
         u32 acc = 0;
@@ -319,14 +352,16 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
         }
         sm.count[d] = acc;
     }
+    __syncthreads();
     // Publish this tile's digit counts early (a chain's first tile publishes
     // final prefixes), then build the tile-local order; the look-back comes
     // last so earlier tiles have had time to publish inclusive prefixes.
     {
         const int d = tid;
-        stRelaxed(status + tile * kRadix + d, (tiles.chainStart(tile) ? kFlagPrefix : kFlagAgg) | u64(sm.count[d]));
+        const u32 cnt = d < R ? sm.count[d] : 0u;
+        if (d < R) stRelaxed(status + tile * R + d, (tiles.chainStart(tile) ? kFlagPrefix : kFlagAgg) | u64(cnt));
         // exclusive scan of the tile's digit counts -> local starts
-        u32 v = sm.count[d];
+        u32 v = cnt;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1)
         {
@@ -339,7 +374,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
 #pragma unroll
         for (int w = 0; w < kWarps; ++w)
             if (w < warp) wOff += sm.warpSums[w];
-        sm.localStart[d] = wOff + v - sm.count[d];
+        if (d < R) sm.localStart[d] = wOff + v - cnt;
     }
     __syncthreads();
     // Reorder the tile in shared memory.
@@ -360,7 +395,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
         staged = copyPending ? 0u : sm.staged;
     }
 #pragma unroll
-    for (int i = 0; i < kItems; ++i)
+    for (int i = 0; i < Items; ++i)
     {
         const size_t idx = warpBase + size_t(i) * 32 + lane;
         if (idx < tiles.end(tile))
@@ -375,6 +410,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
         }
     }
     // Look-back: global start of each digit for this tile.
+    if (tid < R)
     {
         const int d = tid;
         const u64 total = sm.count[d];
@@ -391,7 +427,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
                 u64 w8[kLookbackWindow];
 #pragma unroll
                 for (int k = 0; k < kLookbackWindow; ++k)
-                    w8[k] = j - k >= 0 ? ldRelaxed(status + size_t(j - k) * kRadix + d) : kFlagPrefix;
+                    w8[k] = j - k >= 0 ? ldRelaxed(status + size_t(j - k) * R + d) : kFlagPrefix;
                 int k = 0;
                 bool done = false;
                 for (; k < kLookbackWindow; ++k)
@@ -417,14 +453,14 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
                     if (spins > 64) __nanosleep(64);
                 }
             }
-            stRelaxed(status + tile * kRadix + d, kFlagPrefix | (excl + total));
+            stRelaxed(status + tile * R + d, kFlagPrefix | (excl + total));
         }
         // modulo 2^32: gstart + j is exact for every key of digit d
         sm.gstart[d] = tiles.digitBase(tile)[d] + u32(excl) - sm.localStart[d];
     }
     __syncthreads();
     const size_t remain = tiles.end(tile) - tileBase;
-    const int valid = remain < size_t(kTile) ? int(remain) : kTile;
+    const int valid = remain < size_t(T) ? int(remain) : T;
 #pragma unroll 4
     for (int j = tid; j < valid; j += kThreads)
     {
@@ -443,27 +479,118 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
     }
 }
 
+// CTAs per SM each configuration is built for.
+template <int Bits, int Items>
+constexpr int passMinBlocks()
+{
+    return Items <= 12 ? 4 : 3;
+}
+
 // One onesweep pass over keys[0, n): digit at bit `shift` (`bits` wide).
-// valsIn == nullptr means values are the input indices (first pass).
-static __global__ void __launch_bounds__(kThreads, 4)
+// valsIn == nullptr means values are the input indices (first pass).  The
+// look-back status holds one word per tile and digit of the radix.
+template <int Bits, int Items>
+static __global__ void __launch_bounds__(kThreads, passMinBlocks<Bits, Items>())
     onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
                    u32 *__restrict__ valsOut, size_t n, int shift, const u32 *__restrict__ bins, u32 *tileCounter,
-                   u64 *status, int *error, int bits = kRadixBits)
+                   u64 *status, int *error, int bits)
 {
-    onesweepTile(ContiguousTiles{n, bins}, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);
+    onesweepTile<Bits, Items>(ContiguousTiles<kThreads * Items>{n, bins}, keysIn, valsIn, keysOut, valsOut, shift,
+                              tileCounter, status, error, bits);
 }
 
 // One onesweep pass over the segments of a forest: every segment is sorted
 // on its own (stable within the segment), in place in the global arrays.
-static __global__ void __launch_bounds__(kThreads, 3)
+template <int Bits, int Items>
+static __global__ void __launch_bounds__(kThreads, passMinBlocks<Bits, Items>())
     segmentOnesweepKernel(SegmentTiles tiles, const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn,
                           u64 *__restrict__ keysOut, u32 *__restrict__ valsOut, int shift, u32 *tileCounter,
-                          u64 *status, int *error)
+                          u64 *status, int *error, int bits)
 {
-    onesweepTile(tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, kRadixBits);
+    onesweepTile<Bits, Items>(tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);
 }
 
-inline size_t passSmem() { return sizeof(SharedPass); }
+// ---------------------------------------------------------------------------
+// Host-side dispatch over kSortConfigs (one instantiation per configuration):
+// X(index, digit bits, keys per thread), in the order of kSortConfigs.
+// ---------------------------------------------------------------------------
+#define AOT_SORT_CONFIGS(X) X(0, 8, 10) X(1, 8, 16) X(2, 8, 8) X(3, 7, 12) X(4, 7, 16)
+
+inline size_t passSmem(int c)
+{
+    switch (c)
+    {
+#define AOT_CASE(i, B, I) \
+    case i: return sizeof(SharedPass<B, I>);
+        AOT_SORT_CONFIGS(AOT_CASE)
+#undef AOT_CASE
+    default: throw std::invalid_argument("sort: unknown configuration");
+    }
+}
+
+// Opts every pass kernel of this translation unit into its dynamic shared
+// memory, once per device.
+static void setPassSmemAll()
+{
+    static bool done[64] = {};
+    int dev = 0;
+    AOT_CHECK(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && done[dev]) return;
+#define AOT_CASE(i, B, I)                                                                                        \
+    AOT_CHECK(cudaFuncSetAttribute(onesweepKernel<B, I>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                                   int(sizeof(SharedPass<B, I>))));                                              \
+    AOT_CHECK(cudaFuncSetAttribute(segmentOnesweepKernel<B, I>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                   int(sizeof(SharedPass<B, I>))));
+    AOT_SORT_CONFIGS(AOT_CASE)
+#undef AOT_CASE
+    if (dev >= 0 && dev < 64) done[dev] = true;
+}
+
+// One contiguous pass of configuration c over n keys.
+static void launchPass(int c, cudaStream_t s, const u64 *keysIn, const u32 *valsIn, u64 *keysOut, u32 *valsOut,
+                       size_t n, int shift, const u32 *bins, u32 *tileCounter, u64 *status, int *error, int bits)
+{
+    const unsigned tiles = unsigned((n + size_t(configTile(c)) - 1) / size_t(configTile(c)));
+    switch (c)
+    {
+#define AOT_CASE(i, B, I)                                                                                        \
+    case i:                                                                                                      \
+        onesweepKernel<B, I><<<tiles, kThreads, sizeof(SharedPass<B, I>), s>>>(                                  \
+            keysIn, valsIn, keysOut, valsOut, n, shift, bins, tileCounter, status, error, bits);                 \
+        break;
+        AOT_SORT_CONFIGS(AOT_CASE)
+#undef AOT_CASE
+    default: throw std::invalid_argument("sort: unknown configuration");
+    }
+}
+
+// One segmented pass of configuration c over `numTiles` tiles.
+static void launchSegmentPass(int c, cudaStream_t s, unsigned numTiles, const SegmentTiles &tiles, const u64 *keysIn,
+                              const u32 *valsIn, u64 *keysOut, u32 *valsOut, int shift, u32 *tileCounter,
+                              u64 *status, int *error, int bits)
+{
+    switch (c)
+    {
+#define AOT_CASE(i, B, I)                                                                                        \
+    case i:                                                                                                      \
+        segmentOnesweepKernel<B, I><<<numTiles, kThreads, sizeof(SharedPass<B, I>), s>>>(                       \
+            tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);                   \
+        break;
+        AOT_SORT_CONFIGS(AOT_CASE)
+#undef AOT_CASE
+    default: throw std::invalid_argument("sort: unknown configuration");
+    }
+}
+
+// Histogram of configuration c's digits.
+static void launchHistogram(int c, cudaStream_t s, unsigned blocks, const u64 *keys, size_t n, int beginBit, int passes,
+                            u32 *hist, int endBit)
+{
+    if (kSortConfigs[c].bits == 8)
+        histogramKernel<8><<<blocks, kThreads, 0, s>>>(keys, n, beginBit, passes, hist, endBit);
+    else
+        histogramKernel<7><<<blocks, kThreads, 0, s>>>(keys, n, beginBit, passes, hist, endBit);
+}
 
 }  // namespace sort
 }  // namespace aot

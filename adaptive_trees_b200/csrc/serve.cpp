@@ -22,12 +22,16 @@ using Clock = std::chrono::steady_clock;
 
 double ms(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); }
 
-// device bytes a build of n particles may need before it is measured
+// device bytes a build of n particles may need before it is measured: its
+// coordinates, keys and permutation (both halves), the key sample, the sort's
+// look-back status (room for every sort configuration the tuner may time:
+// 10 passes of 2048-key tiles, 256 digits of 8 B, 10 B per particle), and
+// the leaf arrays
 size_t buildEstimate(const ServeRequest &r)
 {
     const size_t n = r.n, rb = r.cfg.real ? 8 : 4;
     const size_t leaves = r.cfg.nf ? n + 4096 : n / std::max(1u, r.cfg.bucket) * 8 + 4096;
-    return n * (3 * rb + 24 + 8) + leaves * 64 + (size_t(1) << 20);
+    return n * (3 * rb + 24 + 8 + 11) + leaves * 64 + (size_t(1) << 20);
 }
 
 // exception -> ao_status (as the C ABI maps them)
@@ -267,6 +271,7 @@ void Server::run(Job &job, ServeResult &res)
             }
             AOT_CHECK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
             EngineConfig cfg = r.cfg;
+            cfg.tuneSort = false;  // no timing runs inside a request
             cfg.stream = t->stream;
             t->n = r.n;
             t->realBytes = cfg.real ? 8 : 4;

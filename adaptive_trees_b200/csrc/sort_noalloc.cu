@@ -79,12 +79,13 @@ void sortPairsNoAlloc(const unsigned long long *keysIn, unsigned long long *keys
         throw std::invalid_argument("ao_sort_pairs_noalloc: n = " + std::to_string(n) +
                                     " exceeds the fixed scratch limit of " + std::to_string(kNoAllocMaxItems) +
                                     " items; use ao_sort_pairs with caller scratch");
+    // always the default sort configuration, whose scratch the array is sized for
     size_t need = 0;
-    TreeEngine::sortPairs(nullptr, &need, keysIn, keysOut, valsIn, valsOut, n, beginBit, endBit, s);
+    TreeEngine::sortPairsWith(0, nullptr, &need, keysIn, keysOut, valsIn, valsOut, n, beginBit, endBit, s);
     if (need > kNoAllocScratchBytes)
         throw std::logic_error("ao_sort_pairs_noalloc: the sort needs " + std::to_string(need) +
                                " scratch bytes, more than the fixed " + std::to_string(kNoAllocScratchBytes));
     size_t have = kNoAllocScratchBytes;
-    TreeEngine::sortPairs(noAllocScratch(), &have, keysIn, keysOut, valsIn, valsOut, n, beginBit, endBit, s);
+    TreeEngine::sortPairsWith(0, noAllocScratch(), &have, keysIn, keysOut, valsIn, valsOut, n, beginBit, endBit, s);
 }
 }  // namespace aot

@@ -395,7 +395,7 @@ def single_config_bench(args):
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(build_ms),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": spec["workload"], "n": n, "coords": "float64", "leaves": int(leaves),
-                       "parallelism": "replicas1"},
+                       "parallelism": "replicas1", "sort": ab.sort_tuning(n)},
             "clocks": clocks.summary(), "gpu_launches": int(launches),
             "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "particles/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 12}}
@@ -558,6 +558,7 @@ def batched_bench(args):
     bu = max_over_ranks(statistics.median(b_upd), world, dev)
     pu = max_over_ranks(statistics.median(p_upd), world, dev)
     same = max_over_ranks(0.0 if same else 1.0, world, dev) == 0.0
+    sort_choice = ab.sort_tuning(total, segmented=True)
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -567,7 +568,8 @@ def batched_bench(args):
             "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": C4_WORKLOAD, "systems": C4_SYSTEMS, "particles": total_all,
                        "largest": int(sizes_all.max()), "smallest": int(sizes_all.min()),
-                       "parallelism": f"systems partitioned over {world} rank(s), no collective on the path"},
+                       "parallelism": f"systems partitioned over {world} rank(s), no collective on the path",
+                       "sort": sort_choice},
             "batched": {"build_ms": bb, "update_ms": bu, "build_value": job_rate(total_all, bb),
                         "update_value": job_rate(total_all, bu), "update_graph_replayed": True,
                         "build_launches": batch_launches // max(1, args.steps)},
@@ -871,6 +873,7 @@ def main():
                 update_stages.append(ust)
         tree.setProfiling(False)
         nf_leaves = tree.info().num_leaves
+        sort_choice = ab.sort_tuning(n)
 
         # ---------------- roofline: onesweep pass timed live via ao_sort_pairs,
         # replayed from CUDA graphs so no host launch time is inside the events
@@ -923,7 +926,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n_per_gpu": n, "coords": "float32", "leaves": leaves,
                        "l2": "inputs 192 MiB > 126 MB L2; no flush", "views": "off",
-                       "parallelism": f"replicas{world}"},
+                       "parallelism": f"replicas{world}", "sort": sort_choice},
             "clocks": clocks.summary(), "gpu_launches": int(launches),
             "update": {"value": total / (upd_ms * 1e-3), "unit": "particles/s", "ms_per_step": upd_ms,
                        "graph_replayed": True, "resizes": resizes},

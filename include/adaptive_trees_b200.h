@@ -193,10 +193,33 @@ AO_API ao_status ao_compute_sfc_keys(int kind, int real_type, const void *x, con
  * [begin_bit, end_bit), onesweep with decoupled look-back.  With scratch ==
  * NULL only *scratch_bytes is set.  values_in == NULL sorts the indices
  * 0..n-1 (the identity permutation).  keys_in/values_in are not modified and
- * must not alias the outputs.  No allocation; capturable. */
+ * must not alias the outputs.  No allocation; capturable.  The sort uses
+ * the configuration the sort tuner holds for n (below); the size query
+ * answers for the largest configuration, so the scratch fits any of them. */
 AO_API ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsigned long long *keys_in,
                                unsigned long long *keys_out, const unsigned *values_in, unsigned *values_out,
                                size_t n, int begin_bit, int end_bit, void *stream);
+
+/* The sort tuner (no counterpart in the reference; it picks what the
+ * reference leaves to CUB's fixed policy).  The radix sort is compiled in a
+ * few configurations of digit width (7 or 8 bits) and keys per thread (8 to
+ * 16; a tile is 256 threads times that).  The first octree or forest build
+ * of a size class (sizes grouped by bit length) on a device times every
+ * configuration on its own keys and keeps the fastest for that device, size
+ * class and kind (contiguous: trees and ao_sort_pairs; segmented: batches).
+ * Every configuration gives the same sorted output. */
+AO_API ao_status ao_sort_config_count(int *count);
+AO_API ao_status ao_sort_config_info(int config, int *digit_bits, int *items_per_thread);
+/* The configuration the next sort of n keys uses on the current device;
+ * *tuned = 1 when it was chosen by timing. */
+AO_API ao_status ao_sort_tuning(int segmented, size_t n, int *config, int *digit_bits, int *items_per_thread,
+                                int *tuned);
+/* on = 0: no timing; untuned sizes use the default configuration. */
+AO_API ao_status ao_sort_set_autotune(int on);
+/* Every sort uses `config` (-1 lifts this). */
+AO_API ao_status ao_sort_force_config(int config);
+/* Forgets the tuned choices of every device. */
+AO_API ao_status ao_sort_forget_tuning(void);
 
 /* Allocation-free variant of ao_sort_pairs; it has no counterpart in the
  * reference.  The same sort, with its scratch in a fixed device array inside
