@@ -379,21 +379,20 @@ __global__ void iotaKernel(u32 *perm, size_t n)
 }
 
 // Sort scratch layout: hist[kPassSlots][256] | bins[kPassSlots][256] |
-// tileCounters[kPassSlots] (u32), then look-back status words (u64), room for
-// every configuration: kPassSlots passes of the smallest tiles.
+// tileCounters[kPassSlots] (u32), then look-back status words (u64): passes x
+// tiles x 256 of configuration `config`, or room for every configuration
+// (config < 0: kPassSlots passes of the smallest tiles).
 struct SortArena
 {
     DevMem counters, status;
-    size_t tilesCap = 0;
-    void ensure(size_t n, cudaStream_t owner)
+    void ensure(size_t n, int config, cudaStream_t owner)
     {
-        const size_t tiles = std::max<size_t>(1, (n + sort::kMinTile - 1) / sort::kMinTile);
         counters.reserve((2 * sort::kPassSlots * sort::kRadix + sort::kPassSlots) * sizeof(u32), owner);
-        if (tiles > tilesCap)
-        {
-            status.reserve(size_t(sort::kPassSlots) * tiles * sort::kRadix * sizeof(u64), owner);
-            tilesCap = tiles;
-        }
+        const size_t words = config < 0
+                                 ? size_t(sort::kPassSlots) * std::max<size_t>(1, (n + sort::kMinTile - 1) / sort::kMinTile)
+                                 : size_t(sort::configPasses(config)) *
+                                       std::max<size_t>(1, (n + sort::configTile(config) - 1) / sort::configTile(config));
+        status.reserve(words * sort::kRadix * sizeof(u64), owner);
     }
     u32 *hist() const { return counters.as<u32>(); }
     u32 *bins() const { return counters.as<u32>() + sort::kPassSlots * sort::kRadix; }
@@ -441,7 +440,7 @@ int sortWithIndices(cudaStream_t s, u64 *k[2], u32 *v[2], size_t n, int passes, 
 {
     if (n == 0) return 0;
     const int cfg = sort::kDefaultSortConfig;
-    a.ensure(n, s);
+    a.ensure(n, cfg, s);
     clearArena(cfg, s, a, n, passes);
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n, sort::kThreads), unsigned(smCount()) * 8u));
     sort::launchHistogram(cfg, s, blocks, k[0], n, 0, passes, a.hist(), 8 * passes), noteLaunch();
@@ -853,7 +852,7 @@ TreeEngine::TreeEngine(const void *x, const void *y, const void *z, size_t n, co
             m_->Perm[k].reserve(n * sizeof(u32));
         }
         m_->sample.reserve(((n + kSampleStride - 1) >> kSampleShift) * sizeof(u64));
-        m_->sortArena.ensure(n, cfg.stream);
+        m_->sortArena.ensure(n, sort::kDefaultSortConfig, cfg.stream);
     }
     ensurePhysical(16);
     if (cfg.kind == 0)
@@ -985,7 +984,6 @@ void TreeEngine::sortParticles()
     m_->groupStale = true;  // cell table entries hold indices into the sorted keys
     if (n_ == 0) return;
     cudaStream_t s = cfg_.stream;
-    m_->sortArena.ensure(n_, s);
     cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
     AOT_CHECK(cudaStreamIsCapturing(s, &capture));
     if (capture == cudaStreamCaptureStatusNone && cfg_.tuneSort && sortNeedsTuning(false, n_))
@@ -994,6 +992,7 @@ void TreeEngine::sortParticles()
         // timed run are the sorted keys
         if (!m_->tuneStart) AOT_CHECK(cudaEventCreate(&m_->tuneStart));
         if (!m_->tuneEnd) AOT_CHECK(cudaEventCreate(&m_->tuneEnd));
+        m_->sortArena.ensure(n_, -1, s);
         auto time = [](int c, void *ctx) -> float {
             TreeEngine &e = *static_cast<TreeEngine *>(ctx);
             AOT_CHECK(cudaEventRecord(e.m_->tuneStart, e.cfg_.stream));
@@ -1004,11 +1003,17 @@ void TreeEngine::sortParticles()
             AOT_CHECK(cudaEventElapsedTime(&ms, e.m_->tuneStart, e.m_->tuneEnd));
             return ms;
         };
-        sortTune(false, n_, time, this);
+        const int best = sortTune(false, n_, time, this);
+        // keep only the chosen configuration's status words
+        waitStream(s);
+        m_->sortArena.status.release();
+        m_->sortArena.ensure(n_, best, s);
     }
     else
     {
-        sortKeys(sortTuning(false, n_).config);
+        const int config = sortTuning(false, n_).config;
+        m_->sortArena.ensure(n_, config, s);
+        sortKeys(config);
     }
     const KeyIndex idx = m_->keyIndex(n_);
     rb::sampleKeysKernel<<<gridFor(idx.ns, 256), 256, 0, s>>>(m_->P[0].as<u64>(), n_, m_->sample.as<u64>(), idx.ns),
@@ -1680,7 +1685,7 @@ void TreeEngine::prepareViews(size_t capacity, const adaptive_octree::ViewConfig
     m.vIntM.reserve(std::max<size_t>(I, 1) * 4, s);
     m.vIntStartLay.reserve(std::max<size_t>(I, 1) * 8, s);
     m.vIntLevelLay.reserve(std::max<size_t>(I, 1), s);
-    m.viewSort.ensure(L, s);
+    m.viewSort.ensure(L, sort::kDefaultSortConfig, s);
 }
 
 void TreeEngine::syncViewSizes()

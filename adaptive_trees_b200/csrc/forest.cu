@@ -92,7 +92,8 @@ struct ForestEngine::Impl
         upload(tileEnd, tEnd.data(), tEnd.size() * 4);
         upload(segFirstTile, first.data(), first.size() * 4);
         upload(segBase, base.data(), base.size() * 4);
-        status.reserve(std::max<size_t>(numTiles, 1) * sort::kPassSlots * sort::kRadix * 8);
+        status.release();
+        status.reserve(std::max<size_t>(numTiles, 1) * sort::configPasses(config) * sort::kRadix * 8);
         tileConfig = config;
     }
 
