@@ -701,8 +701,8 @@ struct TreeEngine::Impl
     DevMem history;
     // tree
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
-    DevMem groupKeys, groupBegins, memoKeys, memoBegins;  // cell tables of the near-field refresh (NFCount)
-    u32 groupMask = 0, memoMask = 0;
+    DevMem groupKeys, groupBegins;  // node table of the near-field refresh (NFCount)
+    u32 groupSlots = 0;
     bool groupStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
     // views
@@ -743,7 +743,7 @@ struct TreeEngine::Impl
                                &vCandStart,  &vCandLevel,  &vLvKeys[0],     &vLvKeys[1],   &vLvVals[0],
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
-                               &viewSort.counters, &viewSort.status, &groupKeys, &groupBegins, &memoKeys, &memoBegins};
+                               &viewSort.counters, &viewSort.status, &groupKeys, &groupBegins};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -959,17 +959,15 @@ void TreeEngine::ensurePhysical(size_t capacity)
     m_->scan.reserve((m_->scanTiles + 1) * sizeof(u64), s);
     if (cfg_.kind == 0 && cfg_.nf)
     {
-        // complete groups (<= leaves / 8) and memoised neighbour cells: half a
-        // slot per leaf in each table
-        size_t slots = 1024;
-        while (slots < c / 2 + 1) slots <<= 1;
-        if (slots != size_t(m_->groupMask) + 1)
+        // every internal node of the tree (about a seventh of the leaves) and
+        // cells that were internal nodes since the last sort, with room to
+        // spare: linear probing stays short
+        const size_t slots = std::min<size_t>(c / 2 + 1024, 0xffffffffu);
+        if (slots > m_->groupSlots)
         {
             m_->groupKeys.reserve(slots * sizeof(u64), s);
             m_->groupBegins.reserve(slots * rb::kGroupRow * sizeof(u32), s);
-            m_->memoKeys.reserve(slots * sizeof(u64), s);
-            m_->memoBegins.reserve(slots * rb::kGroupBegins * sizeof(u32), s);
-            m_->groupMask = m_->memoMask = u32(slots - 1);
+            m_->groupSlots = u32(slots);
             m_->groupStale = true;
         }
     }
@@ -1008,6 +1006,10 @@ void TreeEngine::sortParticles()
         waitStream(s);
         m_->sortArena.status.release();
         m_->sortArena.ensure(n_, best, s);
+    }
+    else if (capture != cudaStreamCaptureStatusNone && sortConfig_ >= 0)
+    {
+        sortKeys(sortConfig_);  // under capture: the last sort's configuration and scratch
     }
     else
     {
@@ -1048,6 +1050,7 @@ void TreeEngine::sortKeys(int config)
         AOT_LAUNCH_CHECK();
     }
     runPasses(config, s, k, v, n_, 0, 64, true, a, &m_->st->error);  // an even pass count ends in buffer 0
+    sortConfig_ = config;
 }
 
 void TreeEngine::computeKeys(int kind, int real, const void *x, const void *y, const void *z, size_t n,
@@ -1242,17 +1245,17 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
     if (cfg_.nf)
     {
         const HilbertTables &h = m_->kpd.h;
-        const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupBegins.as<u32>(), m_->groupMask,
-                                m_->memoKeys.as<u64>(),  m_->memoBegins.as<u32>(),  m_->memoMask};
+        const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupBegins.as<u32>(), m_->groupSlots};
         ensureDigitPos();
+        // a cleared table takes the nodes of every leaf, else those of the new leaves
+        const bool fill = all || m_->groupStale;
         if (m_->groupStale)
         {
-            AOT_CHECK(cudaMemsetAsync(gt.keys, 0, (size_t(gt.mask) + 1) * sizeof(u64), s));
-            AOT_CHECK(cudaMemsetAsync(gt.memoKeys, 0, (size_t(gt.memoMask) + 1) * sizeof(u64), s));
+            AOT_CHECK(cudaMemsetAsync(gt.keys, 0, size_t(gt.slots) * sizeof(u64), s));
             m_->groupStale = false;
         }
-        if (all) rb::groupTableKernel<true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
-        else rb::groupTableKernel<false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
+        if (fill) rb::nodeTableKernel<true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
+        else rb::nodeTableKernel<false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
         markNearField(true);
         if (all && cfg_.hilbert)
             rb::octNearFieldKernel<true, true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx, cfg_.bucket, h, gt), noteLaunch();

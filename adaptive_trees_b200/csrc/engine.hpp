@@ -200,6 +200,7 @@ private:
     enum Mark { MarkStart = 0, MarkSorted, MarkRefreshed, MarkPassed, MarkEnd, NumMarks };
     bool profiling_ = false, marking_ = false, marksRecorded_ = false;
     int markCall_ = 0, nfMarks_ = 0;
+    int sortConfig_ = -1;  // sort configuration of the last sort (kept under stream capture)
     void mark(Mark m, int call = 0);
     void markNearField(bool begin);
 

@@ -616,33 +616,26 @@ __device__ __forceinline__ CellPath decodeCell(u64 start, unsigned pl, const uns
     return c;
 }
 
-// Cell tables: cell -> the begin indices of its 8 children and its end (9
-// values; child counts and the cell's count are their differences).  The
-// values depend only on the sorted keys, so an entry stays right while the
-// tree changes: the tables are cleared when the particles are sorted again
-// and otherwise only grow.  Two tables:
-//   * groups: the parent cells of complete sibling groups, entered by
-//     groupTableKernel before the refresh and read-only during it, so a
-//     lookup may load a slot's key and values together (one round trip);
-//   * memo: the neighbour cells the refresh had to search for, entered while
-//     other warps read it -- a slot is claimed with kBusyCode, its values
-//     stored, then the key released, and readers acquire the key before they
-//     load the values.
-// A cell found in neither is searched, so the tables only save work.  Open
+// Node table: internal node -> the begin indices of its 8 children in the
+// sorted keys and its end (9 values; child counts and the node's count are
+// their differences).  It holds every cell that has been an internal node
+// of the tree since the keys were last sorted: nodeTableKernel enters the
+// ancestors of new leaves before each near-field refresh, and the refresh
+// only reads it.  The values depend only on the sorted keys, so an entry
+// stays right while the tree changes; the table is cleared when the
+// particles are sorted again and otherwise only grows.  A cell that is not
+// in the table is a leaf or lies inside one: the child of its deepest entered
+// ancestor that holds it has few keys, which the refresh counts.  Open
 // addressing with linear probing, at most kCellProbes probes; keys are cell
-// codes (never 0 or kBusyCode), 0 marks an empty slot.
+// codes (never 0), 0 marks an empty slot.
 constexpr int kGroupBegins = 9;
-constexpr int kGroupRow = 12;  // words per group-table row (48 B, 16-byte aligned)
+constexpr int kGroupRow = 12;  // words per table row (48 B, 16-byte aligned)
 constexpr u32 kCellProbes = 64;
-constexpr u64 kBusyCode = ~u64(0);
 struct GroupTable
 {
     u64 *keys;
     u32 *begins;  // [slot][kGroupRow]
-    u32 mask;
-    u64 *memoKeys;
-    u32 *memoBegins;
-    u32 memoMask;
+    u32 slots;
 };
 
 // Cell code: the key prefix of a cell at `level` below a placeholder bit,
@@ -652,16 +645,20 @@ __device__ __forceinline__ u64 cellCode(u64 start, unsigned level)
     return (start >> (3u * (kOctLevels - level))) | (u64(1) << (3u * level));
 }
 
-__device__ __forceinline__ u32 codeSlot(u64 code, u32 mask)
+// Home slot of a code among `slots`: Fibonacci hashing (the high bits of one
+// 64-bit product), then a multiply-shift into [0, slots).
+__device__ __forceinline__ u32 codeSlot(u64 code, u32 slots)
 {
-    // Fibonacci hashing: the high bits of one 64-bit product
-    return u32((code * 0x9E3779B97F4A7C15ull) >> 32) & mask;
+    const u32 h = u32((code * 0x9E3779B97F4A7C15ull) >> 32);
+    return u32((u64(h) * slots) >> 32);
 }
+
+__device__ __forceinline__ u32 nextSlot(u32 slot, u32 slots) { return slot + 1 < slots ? slot + 1 : 0u; }
 
 // Begin indices of the cell `code` (9 values into b), or false.
 __device__ __forceinline__ bool groupBegins(const GroupTable &gt, u64 code, u32 (&b)[kGroupBegins])
 {
-    u32 slot = codeSlot(code, gt.mask);
+    u32 slot = codeSlot(code, gt.slots);
     for (u32 probe = 0; probe < kCellProbes; ++probe)
     {
         const uint4 *row = reinterpret_cast<const uint4 *>(gt.begins + size_t(slot) * kGroupRow);
@@ -672,95 +669,73 @@ __device__ __forceinline__ bool groupBegins(const GroupTable &gt, u64 code, u32 
         const u64 key = __ldg(gt.keys + slot);
         if (key == code) return true;
         if (key == 0) return false;
-        slot = (slot + 1) & gt.mask;
+        slot = nextSlot(slot, gt.slots);
     }
     return false;
 }
 
-__device__ __forceinline__ u64 ldAcquire(const u64 *p)
+// The row of cell `code`, entered if absent (nullptr if the probes run out;
+// the table is sized so they do not).  Writers of one cell store the same
+// values, so racing writers are harmless.
+__device__ __forceinline__ u32 *nodeRow(const GroupTable &gt, u64 code)
 {
-    u64 v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ u32 ldRelaxed32(const u32 *p)
-{
-    u32 v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void stRelease(u64 *p, u64 v)
-{
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-// Memo lookup (coherent with inserts running in the same kernel).
-__device__ __forceinline__ bool memoFind(const GroupTable &gt, u64 code, u32 (&b)[kGroupBegins])
-{
-    u32 slot = codeSlot(code, gt.memoMask);
-    for (u32 probe = 0; probe < kCellProbes; ++probe)
-    {
-        const u64 key = ldAcquire(gt.memoKeys + slot);
-        if (key == code)
-        {
-            const u32 *row = gt.memoBegins + size_t(slot) * kGroupBegins;
-#pragma unroll
-            for (int k = 0; k < kGroupBegins; ++k) b[k] = ldRelaxed32(row + k);
-            return true;
-        }
-        if (key == 0) return false;
-        slot = (slot + 1) & gt.memoMask;
-    }
-    return false;
-}
-
-// Memo insert: claim, store the values, release the key.
-__device__ __forceinline__ void memoInsert(const GroupTable &gt, u64 code, const u32 (&b)[kGroupBegins])
-{
-    u32 slot = codeSlot(code, gt.memoMask);
-    for (u32 probe = 0; probe < kCellProbes; ++probe)
-    {
-        u64 *key = gt.memoKeys + slot;
-        const u64 prev = atomicCAS(reinterpret_cast<unsigned long long *>(key), 0ull,
-                                   static_cast<unsigned long long>(kBusyCode));
-        if (prev == 0ull)
-        {
-            u32 *row = gt.memoBegins + size_t(slot) * kGroupBegins;
-#pragma unroll
-            for (int k = 0; k < kGroupBegins; ++k) row[k] = b[k];
-            __threadfence();
-            stRelease(key, code);
-            return;
-        }
-        if (prev == code) return;
-        slot = (slot + 1) & gt.memoMask;
-    }
-}
-
-// Enters a group cell (before the refresh; a racing insert of the same cell
-// writes the same values).
-__device__ __forceinline__ void cellInsert(const GroupTable &gt, u64 code, const u32 (&b)[kGroupBegins])
-{
-    u32 slot = codeSlot(code, gt.mask);
+    u32 slot = codeSlot(code, gt.slots);
     for (u32 probe = 0; probe < kCellProbes; ++probe)
     {
         const u64 prev = atomicCAS(reinterpret_cast<unsigned long long *>(gt.keys + slot), 0ull,
                                    static_cast<unsigned long long>(code));
-        if (prev == 0ull || prev == code)
-        {
-            u32 *row = gt.begins + size_t(slot) * kGroupRow;
-#pragma unroll
-            for (int k = 0; k < kGroupBegins; ++k) row[k] = b[k];
-            return;
-        }
-        slot = (slot + 1) & gt.mask;
+        if (prev == 0ull || prev == code) return gt.begins + size_t(slot) * kGroupRow;
+        slot = nextSlot(slot, gt.slots);
     }
+    return nullptr;
 }
 
-// Enters the parent cells of complete sibling groups: of every leaf (All),
-// or of the new leaves of the last pass (the others are already in).
+// Begin indices of the 8 children of the cell [qKey, qKey + 8 * cr) (children
+// at `level`, cr their range) among the keys P[lo, hi) of an enclosing cell:
+// a count by digit for short ranges, lower bounds otherwise.
+__device__ __forceinline__ void childBeginsWithin(const u64 *P, u32 lo, u32 hi, u64 qKey, unsigned level,
+                                                  u32 (&b)[kGroupBegins])
+{
+    const u64 cr = octRange(level);
+    const u64 qEnd = qKey + 8 * cr;
+    const unsigned cShift = 3u * (kOctLevels - level);
+    if (hi - lo <= kNFScanMax)
+    {
+        // 16-bit counters per digit in two registers (hi - lo <= kNFScanMax < 2^16)
+        u32 below = 0;
+        u64 lowDigits = 0, highDigits = 0;
+        for (u32 t = lo; t < hi; ++t)
+        {
+            const u64 k = __ldg(P + t);
+            if (k < qKey) ++below;
+            else if (k < qEnd)
+            {
+                const unsigned d = unsigned(k >> cShift) & 7u;
+                const u64 inc = u64(1) << (16 * (d & 3u));
+                if (d < 4) lowDigits += inc;
+                else highDigits += inc;
+            }
+        }
+        b[0] = lo + below;
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
+            b[d + 1] = b[d] + u32(((d < 4 ? lowDigits : highDigits) >> (16 * (d & 3))) & 0xffffu);
+        return;
+    }
+    const u32 n = hi - lo;
+#pragma unroll
+    for (int d = 0; d <= 8; ++d) b[d] = lo + lowerBound32(P + lo, n, qKey + u64(d) * cr);
+}
+
+// Enters the internal nodes above every leaf (All) or above the new leaves of
+// the last pass: the child begin of each ancestor whose child the leaf
+// starts (up the levels while the leaf is a first child), and the end of each
+// ancestor the leaf ends (up the levels while it is a last child).  Every
+// child of an internal node starts with some leaf and its last child ends
+// with one, so all 9 values of every internal node are entered; one random
+// write per entered value, about two per leaf.
 template <bool All>
-static __global__ void __launch_bounds__(kRefreshThreads) groupTableKernel(TreeBufs tb, GroupTable gt)
+static __global__ void __launch_bounds__(kRefreshThreads) nodeTableKernel(TreeBufs tb, GroupTable gt)
 {
     const DeviceState *st = tb.st;
     if (halted(st)) return;
@@ -773,19 +748,54 @@ static __global__ void __launch_bounds__(kRefreshThreads) groupTableKernel(TreeB
     {
         const int i = All ? j : tb.dirty[j];
         const u64 s = K[i];
-        const unsigned level = octLevel(K[i + 1] - s);
-        if (level == 0 || level > kOctLevels) continue;
-        const int i0 = i - int(octDigit(s, level));  // the group's first leaf
-        if (All && i0 != i) continue;                // one insert per group
-        if (i0 < 0 || i0 + 8 > L) continue;
-        const u64 pRange = octRange(level - 1);
-        const u64 pStart = s & ~(pRange - 1);
-        if (K[i0] != pStart || K[i0 + 8] != pStart + pRange) continue;
-        u32 b[kGroupBegins];
-#pragma unroll
-        for (int k = 0; k < kGroupBegins; ++k) b[k] = B[i0 + k];
-        cellInsert(gt, cellCode(pStart, level - 1), b);
+        const unsigned lev = octLevel(K[i + 1] - s);
+        if (lev > kOctLevels) continue;
+        const u32 b0 = B[i], b1 = B[i + 1];
+        for (unsigned l = lev; l >= 1; --l)
+        {
+            const unsigned d = octDigit(s, l);
+            u32 *row = nodeRow(gt, cellCode(s & ~(octRange(l - 1) - 1), l - 1));
+            if (row) row[d] = b0;
+            if (d != 0) break;
+        }
+        for (unsigned l = lev; l >= 1; --l)
+        {
+            const unsigned d = octDigit(s, l);
+            if (d != 7) break;
+            u32 *row = nodeRow(gt, cellCode(s & ~(octRange(l - 1) - 1), l - 1));
+            if (row) row[8] = b1;
+        }
     }
+}
+
+// Begin indices of the parent-level cell Q at qKey (children at `level`)
+// that is not an internal node: the child of its deepest entered ancestor
+// that holds Q (Q itself, or the leaf Q lies in; or a cell that was one of
+// them earlier) gives a short key range, in which Q's keys are counted.
+// False if no ancestor is entered or its values are not a key range.
+__device__ __forceinline__ bool beginsInside(const GroupTable &gt, const u64 *P, u32 n, u64 qKey, unsigned level,
+                                             u32 (&b)[kGroupBegins])
+{
+    for (int l = int(level) - 2; l >= 0; --l)
+    {
+        u32 e[kGroupBegins];
+        if (groupBegins(gt, cellCode(qKey & ~(octRange(unsigned(l)) - 1), unsigned(l)), e))
+        {
+            const unsigned d = octDigit(qKey, unsigned(l) + 1);  // the child that holds Q
+            u32 lo = e[0], hi = e[1];
+#pragma unroll
+            for (int k = 1; k < 8; ++k)
+                if (unsigned(k) == d)
+                {
+                    lo = e[k];
+                    hi = e[k + 1];
+                }
+            if (lo > hi || hi > n) return false;
+            childBeginsWithin(P, lo, hi, qKey, level, b);
+            return true;
+        }
+    }
+    return false;
 }
 
 // Per-warp scratch of the units in flight.
@@ -867,63 +877,8 @@ __device__ __forceinline__ void childrenFromPacked(const u32 (&b)[kGroupBegins],
     }
 }
 
-// Counts Q's particles [lo, lo + n) per child octant into the unit's block
-// positions `pos` (0xff: the child does not touch P).  A scanned range also
-// gives the begin indices of all 8 children (into `begins`, returns true).
-template <bool Hilbert>
-__device__ __forceinline__ bool countChildren(const u64 *P, u32 lo, u32 n, u64 qKey, unsigned level, int qState,
-                                              const unsigned char *pos, u32 *block, const unsigned char *sEnc,
-                                              const unsigned char *sDec, u32 (&begins)[kGroupBegins])
-{
-    P += lo;
-    const unsigned cShift = 3u * (kOctLevels - level);
-    if (n <= kNFScanMax)
-    {
-        // 16-bit counters per octant in two registers (n <= kNFScanMax < 2^16);
-        // the digit -> octant map of Q's state packed 3 bits per digit
-        u32 octOf = 0;
-        if constexpr (Hilbert)
-        {
-#pragma unroll
-            for (int d = 0; d < 8; ++d) octOf |= u32(sDec[qState * 8 + d]) << (3 * d);
-        }
-        u64 lowOcts = 0, highOcts = 0;
-        for (u32 t = 0; t < n; ++t)
-        {
-            const unsigned d = unsigned(__ldg(P + t) >> cShift) & 7u;
-            const unsigned o = Hilbert ? (octOf >> (3 * d)) & 7u : d;
-            const u64 inc = u64(1) << (16 * (o & 3u));
-            if (o < 4) lowOcts += inc;
-            else highOcts += inc;
-        }
-#pragma unroll
-        for (int o = 0; o < 8; ++o)
-            if (pos[o] != 0xff) block[pos[o]] = u32(((o < 4 ? lowOcts : highOcts) >> (16 * (o & 3))) & 0xffffu);
-        // children in digit order: begin indices
-        begins[0] = lo;
-#pragma unroll
-        for (int d = 0; d < 8; ++d)
-        {
-            const unsigned o = Hilbert ? (octOf >> (3 * d)) & 7u : unsigned(d);
-            begins[d + 1] = begins[d] + u32(((o < 4 ? lowOcts : highOcts) >> (16 * (o & 3u))) & 0xffffu);
-        }
-        return true;
-    }
-    const u64 cr = octRange(level);
-#pragma unroll 1
-    for (int o = 0; o < 8; ++o)
-    {
-        const unsigned p = pos[o];
-        if (p == 0xff) continue;
-        const unsigned dg = Hilbert ? unsigned(sEnc[qState * 8 + o]) : unsigned(o);
-        const u64 cs = qKey + u64(dg) * cr;
-        block[p] = lowerBound32(P, n, cs + cr) - lowerBound32(P, n, cs);
-    }
-    return false;
-}
-
 // Near-field counts and group flags of the new leaves (All: of every leaf),
-// after octBeginKernel and groupTableKernel.  A run of empty leaves whose
+// after octBeginKernel and nodeTableKernel.  A run of empty leaves whose
 // group is incomplete or empty needs no work (NF 0; an empty parent can
 // always merge).
 template <bool Hilbert, bool All>
@@ -1082,7 +1037,8 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                 __syncwarp();
             }
 
-            // ---- phase B: the other Q's by search, over the lanes
+            // ---- phase B: the Q's that are not nodes, over the lanes: counted
+            // inside the leaf that holds them
             const int nSlow = w.nSlow;
             for (int k = lane; k < nSlow; k += 32)
             {
@@ -1090,27 +1046,17 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                 const int u = it / 27, q = it - u * 27;
                 const u64 qKey = w.slowKey[k];
                 const unsigned level = unsigned(w.level[u]);
-                const u64 pRange = octRange(level - 1);
-                const u64 code = cellCode(qKey, level - 1);
                 const int qState = int(w.slowState[k]);
                 u32 begins[kGroupBegins];
-                u32 total;
-                if (memoFind(gt, code, begins))
+                if (!beginsInside(gt, idx.keys, u32(idx.n), qKey, level, begins))
                 {
-                    // searched before by another unit
-                    childrenFromPacked<Hilbert>(begins, q, qState, w.block[u]);
-                    total = begins[8] - begins[0];
-                }
-                else
-                {
+                    // no enclosing cell entered (not expected): search the keys
                     const u32 lo = idx.lowerNear<kNFGallop>(w.hintB[u], qKey);
-                    const u32 hi = lowerFrom(idx, lo, qKey + pRange);
-                    if (countChildren<Hilbert>(idx.keys, lo, hi - lo, qKey, level, qState, sPos + q * 8, w.block[u],
-                                               sEnc, sDec, begins))
-                        memoInsert(gt, code, begins);  // for the next units that need Q
-                    total = hi - lo;
+                    const u32 hi = lowerFrom(idx, lo, qKey + octRange(level - 1));
+                    childBeginsWithin(idx.keys, lo, hi, qKey, level, begins);
                 }
-                w.qtot[u][q] = total;
+                childrenFromPacked<Hilbert>(begins, q, qState, w.block[u]);
+                w.qtot[u][q] = begins[8] - begins[0];
             }
             __syncwarp();
 

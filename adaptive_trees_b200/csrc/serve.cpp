@@ -25,13 +25,14 @@ double ms(Clock::time_point a, Clock::time_point b) { return std::chrono::durati
 // device bytes a build of n particles may need before it is measured: its
 // coordinates, keys and permutation (both halves), the key sample, the sort's
 // look-back status (room for every sort configuration the tuner may time:
-// 10 passes of 2048-key tiles, 256 digits of 8 B, 10 B per particle), and
-// the leaf arrays
+// 10 passes of 2048-key tiles, 256 digits of 8 B, 10 B per particle), the
+// leaf arrays and (NFCount) the node table
 size_t buildEstimate(const ServeRequest &r)
 {
     const size_t n = r.n, rb = r.cfg.real ? 8 : 4;
     const size_t leaves = r.cfg.nf ? n + 4096 : n / std::max(1u, r.cfg.bucket) * 8 + 4096;
-    return n * (3 * rb + 24 + 8 + 11) + leaves * 64 + (size_t(1) << 20);
+    // NFCount trees add the node table: half a slot of 56 B per leaf of capacity
+    return n * (3 * rb + 24 + 8 + 11) + leaves * (r.cfg.nf ? 64 + 28 : 64) + (size_t(1) << 20);
 }
 
 // exception -> ao_status (as the C ABI maps them)
