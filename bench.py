@@ -47,7 +47,7 @@ NF_BYTES_PER_LEAF = 16.125
 # DRAM bytes (read + write) per leaf of the full near-field refresh, from the
 # ncu capture summarised in profiles/octNearFieldKernel_full_refresh_8Mi.md
 # (8 Mi particles); the traffic of the 16 Mi launch is this times its leaves.
-NF_TRAFFIC_BYTES_PER_LEAF = (780793856 + 101675776) / 6677490
+NF_TRAFFIC_BYTES_PER_LEAF = (454174464 + 29304576) / 6674641
 
 
 def plummer(n, seed, scale=0.05, rmax=0.5):
@@ -263,10 +263,12 @@ def kernels_only(args):
 
 
 def build_only(args):
-    """One build and one update of the workload's tree at size --n."""
+    """One build and one update of the workload's tree at size --n (the
+    default sort configuration, no tuning runs, so a profile sees only them)."""
     import torch
     import adaptive_trees_b200 as ab
     torch.cuda.set_device(0)
+    ab.set_sort_autotune(False)
     s = torch.cuda.Stream()
     xs = [torch.from_numpy(a).cuda() for a in plummer(args.n, seed=1234)]
     cfg = ab.TreeConfig(maxParticlesPerLeaf=BUCKET, splitCriterion=ab.SplitCriterion.NFCount,
