@@ -701,9 +701,9 @@ struct TreeEngine::Impl
     DevMem history;
     // tree
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
-    DevMem groupKeys, groupBegins;  // node table of the near-field refresh (NFCount)
-    u32 groupSlots = 0;
-    bool groupStale = true;         // the keys changed or the table moved: clear before use
+    DevMem nodeKeys, nodeRows;  // node table of the near-field refresh (NFCount)
+    u32 nodeSlots = 0;
+    bool nodeStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
     // views
     DevMem vBox, vSplit, vDepth, vParent, vChild, vLevelOffset, vPbegin, vPcount, vPmap, vMaxDepth;
@@ -743,7 +743,7 @@ struct TreeEngine::Impl
                                &vCandStart,  &vCandLevel,  &vLvKeys[0],     &vLvKeys[1],   &vLvVals[0],
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
-                               &viewSort.counters, &viewSort.status, &groupKeys, &groupBegins};
+                               &viewSort.counters, &viewSort.status, &nodeKeys, &nodeRows};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -963,12 +963,12 @@ void TreeEngine::ensurePhysical(size_t capacity)
         // cells that were internal nodes since the last sort, with room to
         // spare: linear probing stays short
         const size_t slots = std::min<size_t>(c / 2 + 1024, 0xffffffffu);
-        if (slots > m_->groupSlots)
+        if (slots > m_->nodeSlots)
         {
-            m_->groupKeys.reserve(slots * sizeof(u64), s);
-            m_->groupBegins.reserve(slots * rb::kGroupRow * sizeof(u32), s);
-            m_->groupSlots = u32(slots);
-            m_->groupStale = true;
+            m_->nodeKeys.reserve(slots * sizeof(u64), s);
+            m_->nodeRows.reserve(slots * rb::kGroupRow * sizeof(u32), s);
+            m_->nodeSlots = u32(slots);
+            m_->nodeStale = true;
         }
     }
     physCap_ = c;
@@ -979,7 +979,7 @@ void TreeEngine::ensurePhysical(size_t capacity)
 // --------------------------------------------------------------------------
 void TreeEngine::sortParticles()
 {
-    m_->groupStale = true;  // cell table entries hold indices into the sorted keys
+    m_->nodeStale = true;  // cell table entries hold indices into the sorted keys
     if (n_ == 0) return;
     cudaStream_t s = cfg_.stream;
     cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
@@ -1245,14 +1245,14 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
     if (cfg_.nf)
     {
         const HilbertTables &h = m_->kpd.h;
-        const rb::GroupTable gt{m_->groupKeys.as<u64>(), m_->groupBegins.as<u32>(), m_->groupSlots};
+        const rb::NodeTable gt{m_->nodeKeys.as<u64>(), m_->nodeRows.as<u32>(), m_->nodeSlots};
         ensureDigitPos();
         // a cleared table takes the nodes of every leaf, else those of the new leaves
-        const bool fill = all || m_->groupStale;
-        if (m_->groupStale)
+        const bool fill = all || m_->nodeStale;
+        if (m_->nodeStale)
         {
             AOT_CHECK(cudaMemsetAsync(gt.keys, 0, size_t(gt.slots) * sizeof(u64), s));
-            m_->groupStale = false;
+            m_->nodeStale = false;
         }
         if (fill) rb::nodeTableKernel<true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();
         else rb::nodeTableKernel<false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();

@@ -546,22 +546,22 @@ static __global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBuf
 //     children of the 27 parent-level cells Q around P (P included) that
 //     touch P (per axis: offset -1 gives the upper child, 0 both, +1 the
 //     lower);
-//   * a Q whose 8 children are leaves of the tree (a complete group, found
-//     in the group table) gives its child counts as differences of the begin
-//     indices, without a search; any other Q is found by two lower bounds in
-//     the sorted keys and its particles are counted per child;
+//   * a Q that is an internal node of the tree (found in the node table)
+//     gives its child counts as differences of its children's begin indices;
+//     any other Q is a leaf or lies inside one, and its particles are counted
+//     per child within that leaf's few keys, found through the table too;
 //   * each leaf of P sums its 3 x 3 x 3 sub-block, and the group flag is the
 //     sum of the 27 Q populations.
 // Periodic wrap at low levels makes several offsets name the same cell;
 // every offset is counted, as in the per-leaf stencil.
 // A warp takes 32 list entries, cuts them into units (runs of leaves with
 // the same parent) and treats up to kUnitBatch units at once: phase A spreads
-// the (unit, Q) pairs over the lanes and resolves those found in the group
+// the (unit, Q) pairs over the lanes and resolves those found in the node
 // table; the rest are queued and phase B spreads them over the lanes for the
-// searches; phase C gives every lane its own leaf.  Lanes stay busy instead
-// of following the slowest Q of one unit.
-constexpr u32 kNFScanMax = 256;  // Q ranges up to this length are scanned
-constexpr int kNFGallop = 4;     // gallop window of the Q searches: 15 keys
+// counts inside leaves; phase C gives every lane its own leaf.  Lanes stay
+// busy instead of following the slowest Q of one unit.
+constexpr u32 kNFScanMax = 256;  // key ranges up to this length are scanned, longer ones searched
+constexpr int kNFGallop = 4;     // gallop window of the fallback search: 15 keys
 constexpr int kUnitBatch = 8;    // units of a warp in flight
 
 // Leaf index of child 0 of the parent at `pStart` if all 8 children are
@@ -631,7 +631,7 @@ __device__ __forceinline__ CellPath decodeCell(u64 start, unsigned pl, const uns
 constexpr int kGroupBegins = 9;
 constexpr int kGroupRow = 12;  // words per table row (48 B, 16-byte aligned)
 constexpr u32 kCellProbes = 64;
-struct GroupTable
+struct NodeTable
 {
     u64 *keys;
     u32 *begins;  // [slot][kGroupRow]
@@ -656,7 +656,7 @@ __device__ __forceinline__ u32 codeSlot(u64 code, u32 slots)
 __device__ __forceinline__ u32 nextSlot(u32 slot, u32 slots) { return slot + 1 < slots ? slot + 1 : 0u; }
 
 // Begin indices of the cell `code` (9 values into b), or false.
-__device__ __forceinline__ bool groupBegins(const GroupTable &gt, u64 code, u32 (&b)[kGroupBegins])
+__device__ __forceinline__ bool nodeBegins(const NodeTable &gt, u64 code, u32 (&b)[kGroupBegins])
 {
     u32 slot = codeSlot(code, gt.slots);
     for (u32 probe = 0; probe < kCellProbes; ++probe)
@@ -677,7 +677,7 @@ __device__ __forceinline__ bool groupBegins(const GroupTable &gt, u64 code, u32 
 // The row of cell `code`, entered if absent (nullptr if the probes run out;
 // the table is sized so they do not).  Writers of one cell store the same
 // values, so racing writers are harmless.
-__device__ __forceinline__ u32 *nodeRow(const GroupTable &gt, u64 code)
+__device__ __forceinline__ u32 *nodeRow(const NodeTable &gt, u64 code)
 {
     u32 slot = codeSlot(code, gt.slots);
     for (u32 probe = 0; probe < kCellProbes; ++probe)
@@ -735,7 +735,7 @@ __device__ __forceinline__ void childBeginsWithin(const u64 *P, u32 lo, u32 hi, 
 // with one, so all 9 values of every internal node are entered; one random
 // write per entered value, about two per leaf.
 template <bool All>
-static __global__ void __launch_bounds__(kRefreshThreads) nodeTableKernel(TreeBufs tb, GroupTable gt)
+static __global__ void __launch_bounds__(kRefreshThreads) nodeTableKernel(TreeBufs tb, NodeTable gt)
 {
     const DeviceState *st = tb.st;
     if (halted(st)) return;
@@ -773,13 +773,13 @@ static __global__ void __launch_bounds__(kRefreshThreads) nodeTableKernel(TreeBu
 // that holds Q (Q itself, or the leaf Q lies in; or a cell that was one of
 // them earlier) gives a short key range, in which Q's keys are counted.
 // False if no ancestor is entered or its values are not a key range.
-__device__ __forceinline__ bool beginsInside(const GroupTable &gt, const u64 *P, u32 n, u64 qKey, unsigned level,
+__device__ __forceinline__ bool beginsInside(const NodeTable &gt, const u64 *P, u32 n, u64 qKey, unsigned level,
                                              u32 (&b)[kGroupBegins])
 {
     for (int l = int(level) - 2; l >= 0; --l)
     {
         u32 e[kGroupBegins];
-        if (groupBegins(gt, cellCode(qKey & ~(octRange(unsigned(l)) - 1), unsigned(l)), e))
+        if (nodeBegins(gt, cellCode(qKey & ~(octRange(unsigned(l)) - 1), unsigned(l)), e))
         {
             const unsigned d = octDigit(qKey, unsigned(l) + 1);  // the child that holds Q
             u32 lo = e[0], hi = e[1];
@@ -883,9 +883,9 @@ __device__ __forceinline__ void childrenFromPacked(const u32 (&b)[kGroupBegins],
 // always merge).
 template <bool Hilbert, bool All>
 static __global__ void __launch_bounds__(kRefreshThreads, 4)
-    octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h, GroupTable gt)
+    octNearFieldKernel(TreeBufs tb, KeyIndex idx, unsigned bucket, HilbertTables h, NodeTable gt)
 {
-    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8], sPos[27 * 8];
+    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
     __shared__ UnitScratch sWarp[kRefreshThreads / 32];
     DeviceState *st = tb.st;
     if (halted(st)) return;
@@ -897,21 +897,6 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
             sNext[k] = h.encNext[k];
             sDec[k] = h.decOct[k];
         }
-    }
-    for (int k = threadIdx.x; k < 27 * 8; k += blockDim.x)
-    {
-        // block coordinate 2 * offset + child bit + 1 per axis, where Q touches P
-        const int q = k >> 3, o = k & 7;
-        const int d[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
-        const int bit[3] = {o >> 2, (o >> 1) & 1, o & 1};
-        bool ok = true;
-        int p = 0;
-        for (int ax = 0; ax < 3; ++ax)
-        {
-            if ((d[ax] < 0 && bit[ax] == 0) || (d[ax] > 0 && bit[ax] == 1)) ok = false;
-            p = p * 4 + (2 * d[ax] + bit[ax] + 1);
-        }
-        sPos[k] = ok ? (unsigned char)p : (unsigned char)0xff;
     }
     __syncthreads();
     const int a = st->activeBuffer;
@@ -1013,7 +998,7 @@ static __global__ void __launch_bounds__(kRefreshThreads, 4)
                     qKey = neighbourCell<Hilbert>(w, u, q, qState, sEnc, sNext);
                     const unsigned level = unsigned(w.level[u]);
                     u32 gb[kGroupBegins];
-                    if (groupBegins(gt, cellCode(qKey, level - 1), gb))
+                    if (nodeBegins(gt, cellCode(qKey, level - 1), gb))
                     {
                         childrenFromPacked<Hilbert>(gb, q, qState, w.block[u]);
                         const u32 total = gb[8] - gb[0];
