@@ -701,7 +701,7 @@ struct TreeEngine::Impl
     DevMem history;
     // tree
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
-    DevMem nodeKeys, nodeRows;  // node table of the near-field refresh (NFCount)
+    DevMem nodeRows;  // node table of the near-field refresh (NFCount)
     u32 nodeSlots = 0;
     bool nodeStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
@@ -743,7 +743,7 @@ struct TreeEngine::Impl
                                &vCandStart,  &vCandLevel,  &vLvKeys[0],     &vLvKeys[1],   &vLvVals[0],
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
-                               &viewSort.counters, &viewSort.status, &nodeKeys, &nodeRows};
+                               &viewSort.counters, &viewSort.status, &nodeRows};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -962,10 +962,9 @@ void TreeEngine::ensurePhysical(size_t capacity)
         // every internal node of the tree (about a seventh of the leaves) and
         // cells that were internal nodes since the last sort, with room to
         // spare: linear probing stays short
-        const size_t slots = std::min<size_t>(c / 2 + 1024, 0xffffffffu);
+        const size_t slots = std::min<size_t>(c / 4 + 1024, 0xffffffffu);
         if (slots > m_->nodeSlots)
         {
-            m_->nodeKeys.reserve(slots * sizeof(u64), s);
             m_->nodeRows.reserve(slots * rb::kGroupRow * sizeof(u32), s);
             m_->nodeSlots = u32(slots);
             m_->nodeStale = true;
@@ -1245,13 +1244,13 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
     if (cfg_.nf)
     {
         const HilbertTables &h = m_->kpd.h;
-        const rb::NodeTable gt{m_->nodeKeys.as<u64>(), m_->nodeRows.as<u32>(), m_->nodeSlots};
+        const rb::NodeTable gt{m_->nodeRows.as<u32>(), m_->nodeSlots};
         ensureDigitPos();
         // a cleared table takes the nodes of every leaf, else those of the new leaves
         const bool fill = all || m_->nodeStale;
         if (m_->nodeStale)
         {
-            AOT_CHECK(cudaMemsetAsync(gt.keys, 0, size_t(gt.slots) * sizeof(u64), s));
+            AOT_CHECK(cudaMemsetAsync(gt.rows, 0, size_t(gt.slots) * rb::kGroupRow * sizeof(u32), s));
             m_->nodeStale = false;
         }
         if (fill) rb::nodeTableKernel<true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, gt), noteLaunch();

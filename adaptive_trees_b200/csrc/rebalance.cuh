@@ -629,12 +629,11 @@ __device__ __forceinline__ CellPath decodeCell(u64 start, unsigned pl, const uns
 // addressing with linear probing, at most kCellProbes probes; keys are cell
 // codes (never 0), 0 marks an empty slot.
 constexpr int kGroupBegins = 9;
-constexpr int kGroupRow = 12;  // words per table row (48 B, 16-byte aligned)
+constexpr int kGroupRow = 12;  // words per slot: the key (2), the 9 values, 1 spare (48 B, 16-byte aligned)
 constexpr u32 kCellProbes = 64;
 struct NodeTable
 {
-    u64 *keys;
-    u32 *begins;  // [slot][kGroupRow]
+    u32 *rows;  // [slot][kGroupRow]
     u32 slots;
 };
 
@@ -661,12 +660,13 @@ __device__ __forceinline__ bool nodeBegins(const NodeTable &gt, u64 code, u32 (&
     u32 slot = codeSlot(code, gt.slots);
     for (u32 probe = 0; probe < kCellProbes; ++probe)
     {
-        const uint4 *row = reinterpret_cast<const uint4 *>(gt.begins + size_t(slot) * kGroupRow);
-        const uint4 r0 = __ldg(row), r1 = __ldg(row + 1), r2 = __ldg(row + 2);  // loaded beside the key
-        b[0] = r0.x; b[1] = r0.y; b[2] = r0.z; b[3] = r0.w;
-        b[4] = r1.x; b[5] = r1.y; b[6] = r1.z; b[7] = r1.w;
-        b[8] = r2.x;
-        const u64 key = __ldg(gt.keys + slot);
+        // the key and the values in one 48-byte record: three 16-byte loads
+        const uint4 *row = reinterpret_cast<const uint4 *>(gt.rows + size_t(slot) * kGroupRow);
+        const uint4 r0 = __ldg(row), r1 = __ldg(row + 1), r2 = __ldg(row + 2);
+        const u64 key = (u64(r0.y) << 32) | r0.x;
+        b[0] = r0.z; b[1] = r0.w;
+        b[2] = r1.x; b[3] = r1.y; b[4] = r1.z; b[5] = r1.w;
+        b[6] = r2.x; b[7] = r2.y; b[8] = r2.z;
         if (key == code) return true;
         if (key == 0) return false;
         slot = nextSlot(slot, gt.slots);
@@ -682,9 +682,10 @@ __device__ __forceinline__ u32 *nodeRow(const NodeTable &gt, u64 code)
     u32 slot = codeSlot(code, gt.slots);
     for (u32 probe = 0; probe < kCellProbes; ++probe)
     {
-        const u64 prev = atomicCAS(reinterpret_cast<unsigned long long *>(gt.keys + slot), 0ull,
+        u32 *row = gt.rows + size_t(slot) * kGroupRow;
+        const u64 prev = atomicCAS(reinterpret_cast<unsigned long long *>(row), 0ull,
                                    static_cast<unsigned long long>(code));
-        if (prev == 0ull || prev == code) return gt.begins + size_t(slot) * kGroupRow;
+        if (prev == 0ull || prev == code) return row + 2;  // the values follow the key
         slot = nextSlot(slot, gt.slots);
     }
     return nullptr;

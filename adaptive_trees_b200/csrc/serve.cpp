@@ -31,8 +31,8 @@ size_t buildEstimate(const ServeRequest &r)
 {
     const size_t n = r.n, rb = r.cfg.real ? 8 : 4;
     const size_t leaves = r.cfg.nf ? n + 4096 : n / std::max(1u, r.cfg.bucket) * 8 + 4096;
-    // NFCount trees add the node table: half a slot of 56 B per leaf of capacity
-    return n * (3 * rb + 24 + 8 + 11) + leaves * (r.cfg.nf ? 64 + 28 : 64) + (size_t(1) << 20);
+    // NFCount trees add the node table: a quarter slot of 48 B per leaf of capacity
+    return n * (3 * rb + 24 + 8 + 11) + leaves * (r.cfg.nf ? 64 + 12 : 64) + (size_t(1) << 20);
 }
 
 // exception -> ao_status (as the C ABI maps them)
