@@ -47,7 +47,7 @@ NF_BYTES_PER_LEAF = 16.125
 # DRAM bytes (read + write) per leaf of the full near-field refresh, from the
 # ncu capture summarised in profiles/octNearFieldKernel_full_refresh_8Mi.md
 # (8 Mi particles); the traffic of the 16 Mi launch is this times its leaves.
-NF_TRAFFIC_BYTES_PER_LEAF = (454174464 + 29304576) / 6674641
+NF_TRAFFIC_BYTES_PER_LEAF = (292337664 + 30597888) / 6678211
 
 
 def plummer(n, seed, scale=0.05, rmax=0.5):
