@@ -733,8 +733,10 @@ __device__ __forceinline__ void childBeginsWithin(const u64 *P, u32 lo, u32 hi, 
 // starts (up the levels while the leaf is a first child), and the end of each
 // ancestor the leaf ends (up the levels while it is a last child).  Every
 // child of an internal node starts with some leaf and its last child ends
-// with one, so all 9 values of every internal node are entered; one random
-// write per entered value, about two per leaf.
+// with one, so all 9 values of every internal node are entered.  A complete
+// sibling group (a parent whose 8 children are leaves, most internal nodes)
+// is entered whole by its first leaf, which also walks on from the parent;
+// its other leaves add nothing.
 template <bool All>
 static __global__ void __launch_bounds__(kRefreshThreads) nodeTableKernel(TreeBufs tb, NodeTable gt)
 {
@@ -750,19 +752,39 @@ static __global__ void __launch_bounds__(kRefreshThreads) nodeTableKernel(TreeBu
         const int i = All ? j : tb.dirty[j];
         const u64 s = K[i];
         const unsigned lev = octLevel(K[i + 1] - s);
-        if (lev > kOctLevels) continue;
-        const u32 b0 = B[i], b1 = B[i + 1];
-        for (unsigned l = lev; l >= 1; --l)
+        if (lev < 1 || lev > kOctLevels) continue;
+        unsigned first = lev, last = lev;  // levels the two walks start from
+        u32 b1 = B[i + 1];
+        // complete sibling group around the leaf?
+        const unsigned d = octDigit(s, lev);
+        const int i0 = i - int(d);
+        const u64 pRange = octRange(lev - 1);
+        const u64 pStart = s & ~(pRange - 1);
+        if (i0 >= 0 && i0 + 8 <= L && K[i0] == pStart && K[i0 + 8] == pStart + pRange)
         {
-            const unsigned d = octDigit(s, l);
-            u32 *row = nodeRow(gt, cellCode(s & ~(octRange(l - 1) - 1), l - 1));
-            if (row) row[d] = b0;
-            if (d != 0) break;
+            if (d != 0) continue;  // the first leaf enters the group
+            u32 *row = nodeRow(gt, cellCode(pStart, lev - 1));
+            if (row)
+            {
+#pragma unroll
+                for (int k = 0; k < kGroupBegins; ++k) row[k] = B[i + k];
+            }
+            // the walks go on from the parent, which the first leaf starts and ends
+            first = last = lev - 1;
+            b1 = B[i + 8];
         }
-        for (unsigned l = lev; l >= 1; --l)
+        const u32 b0 = B[i];
+        for (unsigned l = first; l >= 1; --l)
         {
-            const unsigned d = octDigit(s, l);
-            if (d != 7) break;
+            const unsigned dd = octDigit(s, l);
+            u32 *row = nodeRow(gt, cellCode(s & ~(octRange(l - 1) - 1), l - 1));
+            if (row) row[dd] = b0;
+            if (dd != 0) break;
+        }
+        for (unsigned l = last; l >= 1; --l)
+        {
+            const unsigned dd = octDigit(s, l);
+            if (dd != 7) break;
             u32 *row = nodeRow(gt, cellCode(s & ~(octRange(l - 1) - 1), l - 1));
             if (row) row[8] = b1;
         }
