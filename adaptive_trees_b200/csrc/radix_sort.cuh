@@ -17,7 +17,7 @@
 //      memory and writes digit runs out contiguously.
 // The digit width and the keys per thread are template parameters; the
 // configurations compiled in are listed in kSortConfigs, and the sort tuner
-// (sort_tuner.hpp) picks one per device and problem size by timing them.
+// (sortTune in engine.cu) picks one per device and problem size by timing them.
 // The look-back wait is bounded: after kLookbackSpins polls it records
 // kErrLookback in the device error word and proceeds, so a broken invariant
 // surfaces as an error status instead of a hung GPU.
