@@ -100,3 +100,22 @@ def test_capi_validates_arguments_without_a_gpu(lib):
     assert L.ao_tree_update(None) == 1
     out = ctypes.c_int()
     assert L.ao_tree_needs_resize(None, ctypes.byref(out)) == 1
+
+
+def test_sort_configurations_are_listed_without_a_gpu():
+    """The compiled sort configurations and the tuner's argument checks need no device."""
+    from adaptive_trees_b200 import _capi as C
+    from adaptive_trees_b200 import sort_configs
+    configs = sort_configs()
+    assert configs[0] == (8, 10)  # the default configuration
+    assert len(configs) == len(set(configs)) >= 4
+    for bits, items in configs:
+        assert bits in (7, 8) and items % 2 == 0 and 8 <= items <= 16
+        assert (64 + bits - 1) // bits % 2 == 0  # an even pass count: results stay in the first buffers
+    lib = C.load()
+    b, i = ctypes.c_int(), ctypes.c_int()
+    assert lib.ao_sort_config_info(len(configs), ctypes.byref(b), ctypes.byref(i)) == 1
+    assert lib.ao_sort_config_info(0, None, None) == 1
+    assert lib.ao_sort_force_config(len(configs)) == 1
+    assert lib.ao_sort_force_config(-1) == 0
+    assert lib.ao_sort_set_autotune(1) == 0
