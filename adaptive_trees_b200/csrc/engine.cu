@@ -1137,7 +1137,6 @@ void TreeEngine::octreePass(bool buildMode, long long limit)
     const size_t tiles = (cap + 1 + rb::kScanTile - 1) / rb::kScanTile;
     rb::beginPassKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
     AOT_CHECK(cudaMemsetAsync(m_->scan.p, 0, (m_->scanTiles + 1) * sizeof(u64), s));
-    const KeyIndex idx = m_->keyIndex(n_);
     const int mode = buildMode ? kModeOctreeBuild : kModeUpdate;
     long long *hist = buildMode ? m_->history.as<long long>() : nullptr;
     const unsigned scatterBlocks = std::min(gridFor(cap, rb::kScatterThreads), unsigned(smCount()) * 8u);

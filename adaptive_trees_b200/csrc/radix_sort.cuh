@@ -530,7 +530,7 @@ inline size_t passSmem(int c)
 
 // Opts every pass kernel of this translation unit into its dynamic shared
 // memory, once per device.
-static void setPassSmemAll()
+static inline void setPassSmemAll()
 {
     static bool done[64] = {};
     int dev = 0;
@@ -547,7 +547,7 @@ static void setPassSmemAll()
 }
 
 // One contiguous pass of configuration c over n keys.
-static void launchPass(int c, cudaStream_t s, const u64 *keysIn, const u32 *valsIn, u64 *keysOut, u32 *valsOut,
+static inline void launchPass(int c, cudaStream_t s, const u64 *keysIn, const u32 *valsIn, u64 *keysOut, u32 *valsOut,
                        size_t n, int shift, const u32 *bins, u32 *tileCounter, u64 *status, int *error, int bits)
 {
     const unsigned tiles = unsigned((n + size_t(configTile(c)) - 1) / size_t(configTile(c)));
@@ -565,7 +565,7 @@ static void launchPass(int c, cudaStream_t s, const u64 *keysIn, const u32 *vals
 }
 
 // One segmented pass of configuration c over `numTiles` tiles.
-static void launchSegmentPass(int c, cudaStream_t s, unsigned numTiles, const SegmentTiles &tiles, const u64 *keysIn,
+static inline void launchSegmentPass(int c, cudaStream_t s, unsigned numTiles, const SegmentTiles &tiles, const u64 *keysIn,
                               const u32 *valsIn, u64 *keysOut, u32 *valsOut, int shift, u32 *tileCounter,
                               u64 *status, int *error, int bits)
 {
@@ -583,7 +583,7 @@ static void launchSegmentPass(int c, cudaStream_t s, unsigned numTiles, const Se
 }
 
 // Histogram of configuration c's digits.
-static void launchHistogram(int c, cudaStream_t s, unsigned blocks, const u64 *keys, size_t n, int beginBit, int passes,
+static inline void launchHistogram(int c, cudaStream_t s, unsigned blocks, const u64 *keys, size_t n, int beginBit, int passes,
                             u32 *hist, int endBit)
 {
     if (kSortConfigs[c].bits == 8)
