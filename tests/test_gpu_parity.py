@@ -432,3 +432,38 @@ def test_late_view_request_flags_resize(oracle_mod):
             assert not g.doBuffersNeedResize()
             assert not o.needs_resize()
             compare(g, o)
+
+
+# --------------------------------------------------------------------------
+# near-field counts on degenerate inputs
+# --------------------------------------------------------------------------
+@pytest.mark.parametrize("hilbert", [False, True])
+@pytest.mark.parametrize("scene", ["stacked", "cluster-in-void"])
+def test_near_field_degenerate_inputs_match_oracle(oracle_mod, hilbert, scene):
+    """NFCount trees whose leaves stop at the deepest level with hundreds of equal keys
+    (stacked points), or whose neighbour cells lie inside much coarser leaves (a tight
+    cluster in a sparse background); build and two jittered updates."""
+    O = oracle_mod
+    rng = np.random.default_rng(17)
+    if scene == "stacked":
+        spots = rng.random((5, 3))
+        stacked = spots[rng.integers(0, 5, size=20_000)]
+        pts = np.concatenate([stacked, rng.random((30_000, 3))])
+        bucket = 512
+    else:
+        cluster = np.clip(np.array([0.3, 0.6, 0.2]) + 1e-4 * rng.normal(size=(30_000, 3)), 0, 0.999999)
+        pts = np.concatenate([cluster, rng.random((3_000, 3))])
+        bucket = 64
+    xyz = tuple(np.ascontiguousarray(pts[:, i]) for i in range(3))
+    g, o, xs = make_pair(O, 0, xyz, bucket=bucket, nf=True, hilbert=hilbert, views=(1, 1, 1))
+    g.build()
+    o.build()
+    compare(g, o)
+    for step in range(2):
+        moved = pts.copy()
+        mask = rng.random(len(pts)) < 0.5  # half the points move, the rest keep their (stacked) keys
+        moved[mask] = np.clip(moved[mask] + 1e-4 * rng.normal(size=(mask.sum(), 3)), 0, 0.999999)
+        xyz = tuple(np.ascontiguousarray(moved[:, i]) for i in range(3))
+        set_coords(xs, o, xyz)
+        update_both(g, o)
+        compare(g, o)
