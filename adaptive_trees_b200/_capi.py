@@ -83,6 +83,9 @@ PROTOTYPES = {
     "ao_compute_sfc_keys": [ci, ci, vp, vp, vp, sz, ctypes.POINTER(ctypes.c_double), ci, cu, vp, vp, vp],
     "ao_sort_pairs": [vp, ctypes.POINTER(sz), vp, vp, vp, vp, sz, ci, ci, vp],
     "ao_sort_pairs_noalloc": [vp, vp, vp, vp, sz, ci, ci, vp],
+    "ao_sort_pairs_check": [vp, sz, vp],
+    "ao_sort_pairs_noalloc_check": [sz, vp],
+    "ao_selftest_bounded_wait": [ci, cu, ctypes.POINTER(ci)],
     "ao_sort_config_count": [ctypes.POINTER(ci)],
     "ao_sort_config_info": [ci, ctypes.POINTER(ci), ctypes.POINTER(ci)],
     "ao_sort_tuning": [ci, sz, ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci)],

@@ -492,6 +492,26 @@ ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsigned lon
     });
 }
 
+ao_status ao_sort_pairs_check(const void *scratch, size_t n, void *stream)
+{
+    return guarded([&] {
+        if (n > 0 && aot::TreeEngine::sortPairsFailed(scratch, n, static_cast<cudaStream_t>(stream)))
+            throw std::runtime_error("ao_sort_pairs: a bounded look-back wait gave up; the output is not sorted");
+    });
+}
+
+ao_status ao_selftest_bounded_wait(int which, unsigned spin_limit, int *error_word)
+{
+    return guarded([&] {
+        const int e = aot::TreeEngine::boundedWaitProbe(which, spin_limit);
+        if (error_word) *error_word = e;
+        if (e != 0)
+            throw std::runtime_error(std::string("ao_selftest_bounded_wait: the ") +
+                                     (which == 0 ? "radix sort" : "decide+scan") +
+                                     " look-back wait gave up after its limit and the kernel returned");
+    });
+}
+
 ao_status ao_sort_config_count(int *count)
 {
     return guarded([&] {
@@ -823,6 +843,15 @@ ao_status ao_sort_pairs_noalloc(const unsigned long long *keys_in, unsigned long
     return guarded([&] {
         aot::sortPairsNoAlloc(keys_in, keys_out, values_in, values_out, n, begin_bit, end_bit,
                               static_cast<cudaStream_t>(stream));
+    });
+}
+
+ao_status ao_sort_pairs_noalloc_check(size_t n, void *stream)
+{
+    return guarded([&] {
+        if (aot::sortPairsNoAllocFailed(n, static_cast<cudaStream_t>(stream)))
+            throw std::runtime_error(
+                "ao_sort_pairs_noalloc: a bounded look-back wait gave up; the output is not sorted");
     });
 }
 

@@ -575,19 +575,27 @@ namespace
 {
 struct PairSortLayout
 {
+    // altKeys | altVals | counters | status, each part 256-byte aligned.  The
+    // counters part starts with the error word (and 3 pad words), so its
+    // offset depends on n only and ao_sort_pairs_check can find it whatever
+    // configuration ran; then hist[passes][256], bins[passes][256] and the
+    // passes' tile counters.
     size_t altKeys = 0, altVals = 0, counters = 0, status = 0, total = 0, tiles = 0;
     int passes = 0;
+    static constexpr size_t kCounterHead = 4;  // error word + padding (u32 words)
+    static size_t up(size_t b) { return (b + 255) & ~size_t(255); }
+    static size_t countersOffset(size_t n) { return up(up(n * sizeof(u64)) + n * sizeof(u32)); }
     PairSortLayout(size_t n, int cfg)
     {
-        auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
         tiles = configTiles(cfg, n);
         passes = sort::configPasses(cfg);
         altKeys = 0;
         altVals = up(altKeys + n * sizeof(u64));
-        counters = up(altVals + n * sizeof(u32));
-        status = up(counters + (2 * size_t(passes) * sort::kRadix + passes + 2) * sizeof(u32));
+        counters = countersOffset(n);
+        status = up(counters + counterWords() * sizeof(u32));
         total = up(status + size_t(passes) * tiles * sort::kRadix * sizeof(u64));
     }
+    size_t counterWords() const { return kCounterHead + 2 * size_t(passes) * sort::kRadix + passes; }
 };
 }  // namespace
 
@@ -637,23 +645,25 @@ void TreeEngine::sortPairsWith(int cfg, void *scratch, size_t *scratchBytes, con
     char *base = static_cast<char *>(scratch);
     u64 *altK = reinterpret_cast<u64 *>(base + lay.altKeys);
     u32 *altV = reinterpret_cast<u32 *>(base + lay.altVals);
-    u32 *ctr = reinterpret_cast<u32 *>(base + lay.counters);
+    u32 *head = reinterpret_cast<u32 *>(base + lay.counters);
+    int *error = reinterpret_cast<int *>(head);
+    u32 *ctr = head + PairSortLayout::kCounterHead;  // hist
     u64 *status = reinterpret_cast<u64 *>(base + lay.status);
     const int slots = lay.passes;  // rows of hist and bins
     u32 *bins = ctr + size_t(slots) * sort::kRadix;
     u32 *tileCounters = ctr + 2 * size_t(slots) * sort::kRadix;
-    int *error = reinterpret_cast<int *>(tileCounters + slots);
     const int bitsPer = sort::kSortConfigs[cfg].bits;
     const int passes = (endBit - beginBit + bitsPer - 1) / bitsPer;
     if (passes == 0)
     {
+        AOT_CHECK(cudaMemsetAsync(error, 0, sizeof(int), s));  // ao_sort_pairs_check reads it
         AOT_CHECK(cudaMemcpyAsync(keysOut, keysIn, n * sizeof(u64), cudaMemcpyDeviceToDevice, s));
         if (valsIn) AOT_CHECK(cudaMemcpyAsync(valsOut, valsIn, n * sizeof(u32), cudaMemcpyDeviceToDevice, s));
         else iotaKernel<<<gridFor(n, 256), 256, 0, s>>>(valsOut, n), noteLaunch();
         AOT_LAUNCH_CHECK();
         return;
     }
-    AOT_CHECK(cudaMemsetAsync(ctr, 0, (2 * size_t(slots) * sort::kRadix + slots + 2) * sizeof(u32), s));
+    AOT_CHECK(cudaMemsetAsync(head, 0, lay.counterWords() * sizeof(u32), s));
     AOT_CHECK(cudaMemsetAsync(status, 0, size_t(passes) * lay.tiles * sort::kRadix * sizeof(u64), s));
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceilDiv(n, sort::kThreads), unsigned(smCount()) * 8u));
     sort::launchHistogram(cfg, s, blocks, reinterpret_cast<const u64 *>(keysIn), n, beginBit, passes, ctr, endBit),
@@ -678,6 +688,34 @@ void TreeEngine::sortPairsWith(int cfg, void *scratch, size_t *scratchBytes, con
         kin = kout;
         vin = vout;
     }
+}
+
+// Waits for `stream` and reads the error word of a pair sort of n items
+// that ran in `scratch` (the bounded look-back of some pass gave up, so its
+// output is not a sorted permutation).
+bool TreeEngine::sortPairsFailed(const void *scratch, size_t n, cudaStream_t s)
+{
+    if (!scratch) throw std::invalid_argument("ao_sort_pairs_check: null scratch");
+    int error = 0;
+    AOT_CHECK(cudaMemcpyAsync(&error, static_cast<const char *>(scratch) + PairSortLayout::countersOffset(n),
+                              sizeof(int), cudaMemcpyDeviceToHost, s));
+    AOT_CHECK(cudaStreamSynchronize(s));
+    return error != 0;
+}
+
+// Loads every kernel a pair sort with the default configuration can launch
+// (lazy module loading would otherwise load one at its first launch).
+void TreeEngine::sortPairsPreload()
+{
+    cudaFuncAttributes a;
+    AOT_CHECK(cudaFuncGetAttributes(&a, iotaKernel));
+    AOT_CHECK(cudaFuncGetAttributes(&a, sort::binsKernel));
+    AOT_CHECK(cudaFuncGetAttributes(&a, sort::histogramKernel<8>));
+    AOT_CHECK(cudaFuncGetAttributes(&a, sort::histogramKernel<7>));
+#define AOT_CASE(i, B, I) AOT_CHECK(cudaFuncGetAttributes(&a, sort::onesweepKernel<B, I>));
+    AOT_SORT_CONFIGS(AOT_CASE)
+#undef AOT_CASE
+    sort::setPassSmemAll();
 }
 
 // --------------------------------------------------------------------------

@@ -153,6 +153,16 @@ public:
     static void sortPairs(void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
                           unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
                           int beginBit, int endBit, cudaStream_t s);
+    // true when a pair sort of n items that ran in `scratch` on `s` had a
+    // bounded look-back wait give up (waits for `s`)
+    static bool sortPairsFailed(const void *scratch, size_t n, cudaStream_t s);
+    // loads every kernel the pair sort can launch on the current device
+    static void sortPairsPreload();
+    // self-test of the bounded device waits (selftest.cu): runs a look-back
+    // (0: radix sort pass, 1: decide+scan) whose predecessor tile never
+    // publishes, with `spinLimit` polls allowed; returns the kernel's error
+    // word (kErrLookback when the wait ran out and the kernel returned)
+    static int boundedWaitProbe(int which, unsigned spinLimit);
     // the same with sort configuration `config` (its own scratch size)
     static void sortPairsWith(int config, void *scratch, size_t *scratchBytes, const unsigned long long *keysIn,
                               unsigned long long *keysOut, const unsigned *valsIn, unsigned *valsOut, size_t n,
@@ -250,5 +260,8 @@ void sortForgetTuning();
 void sortPairsNoAlloc(const unsigned long long *keysIn, unsigned long long *keysOut, const unsigned *valsIn,
                       unsigned *valsOut, size_t n, int beginBit, int endBit, cudaStream_t s);
 size_t sortPairsNoAllocMaxItems();
+// true when the last sortPairsNoAlloc of n items on this device had a bounded
+// look-back wait give up (waits for `s`)
+bool sortPairsNoAllocFailed(size_t n, cudaStream_t s);
 
 }  // namespace aot

@@ -256,12 +256,15 @@ struct SegmentTiles
 // One onesweep pass: the Bits-wide digit at bit `shift` (`bits` <= Bits
 // wide) of the tiles of `tiles`, Items keys per thread.  valsIn == nullptr
 // means values are generated (first pass).  Threads below the radix own one
-// digit each in the per-digit steps.
+// digit each in the per-digit steps.  A look-back that polls an unpublished
+// tile more than spinLimit times records kErrLookback and goes on with the
+// prefix it has: every write stays inside the output, the result is wrong
+// and the host reports the error.
 template <int Bits, int Items, class Tiles>
 __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__restrict__ keysIn,
                                              const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
                                              u32 *__restrict__ valsOut, int shift, u32 *tileCounter, u64 *status,
-                                             int *error, int bits)
+                                             int *error, int bits, unsigned spinLimit = kLookbackSpins)
 {
     using Smem = SharedPass<Bits, Items>;
     constexpr int R = Smem::R;
@@ -445,7 +448,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
                 j -= k;
                 if (k < kLookbackWindow)  // tile j has not published yet
                 {
-                    if (++spins > kLookbackSpins)
+                    if (++spins > spinLimit)
                     {
                         atomicExch(error, kErrLookback);
                         break;

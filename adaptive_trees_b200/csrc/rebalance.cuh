@@ -99,8 +99,10 @@ __device__ __forceinline__ i64 blockExclusiveScan(i64 v, i64 *sWarp, i64 &total)
 }
 
 // Decoupled look-back: returns the exclusive prefix of `tile` given its
-// aggregate.  Called by one thread.
-__device__ __forceinline__ i64 lookback(u64 *status, u32 tile, i64 aggregate, int *error)
+// aggregate.  Called by one thread.  Polling an unpublished tile more than
+// spinLimit times records kErrLookback and returns the prefix summed so far.
+__device__ __forceinline__ i64 lookback(u64 *status, u32 tile, i64 aggregate, int *error,
+                                        unsigned spinLimit = kLookbackSpins)
 {
     if (tile == 0)
     {
@@ -133,7 +135,7 @@ __device__ __forceinline__ i64 lookback(u64 *status, u32 tile, i64 aggregate, in
         j -= k;
         if (k < 8)
         {
-            if (++spins > kLookbackSpins)
+            if (++spins > spinLimit)
             {
                 atomicExch(error, kErrLookback);
                 break;

@@ -37,17 +37,20 @@ N_DEFAULT = 1 << 24
 BUCKET = 512
 METRIC = "particles/s (octree build, 16Mi Plummer fp32, Hilbert, NFCount 512)"
 WORKLOAD = "octree build + graph-replayed update, 16Mi Plummer fp32 (a=0.05, r<=0.5), Hilbert keys, NFCount 512"
-# DRAM bytes (read + write) of one 16Mi-key onesweep pass, from the ncu capture
-# summarised in profiles/onesweepKernel_pass_16Mi.md (204.9 MB + 162.7 MB).
+# DRAM bytes (read + write) of one 16Mi-key onesweep pass, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on that pass: 204.9 MB + 162.7 MB.
 ONESWEEP_TRAFFIC_BYTES = 367.6e6
 # Algorithmic bytes of the near-field refresh per leaf: K[i] read (8), the
 # begin index B[i] read (4), NF[i] written (4), and the group flag, one byte
 # per sibling group (1/8).
 NF_BYTES_PER_LEAF = 16.125
-# DRAM bytes (read + write) per leaf of the full near-field refresh, from the
-# ncu capture summarised in profiles/octNearFieldKernel_full_refresh_8Mi.md
-# (8 Mi particles); the traffic of the 16 Mi launch is this times its leaves.
+# DRAM bytes (read + write) per leaf of the full near-field refresh, measured
+# by ncu on that launch at 8 Mi particles (6,678,211 leaves); the traffic
+# reported for the 16 Mi launch is this times its leaves (scaled, not
+# re-measured in the run).
 NF_TRAFFIC_BYTES_PER_LEAF = (292337664 + 30597888) / 6678211
+# The arrays compared with the reference library in the line's parity record.
+PARITY_ARRAYS = ("particleKeys", "perm", "cornerstone", "leafCounts", "nearFieldCounts")
 
 
 def plummer(n, seed, scale=0.05, rmax=0.5):
@@ -703,6 +706,57 @@ def serving_bench(args):
     return 0 if not failed else 1
 
 
+def reference_parity(tree, xs, frames, stream):
+    """Bit-exact check of the timed tree against the reference library.
+
+    The timed tree is built again from frame 0 (the benchmark's coordinates)
+    and updated on frame 1 with the callers' resize loop; the reference
+    library (oracle/_ref/ref_driver, compiled from the reference's sources)
+    runs build + update on the same frames.  Every array of PARITY_ARRAYS is
+    compared through its 64-bit content digest after each frame, with the
+    tree's scalars and the resize count."""
+    import torch
+
+    from oracle import refrun
+    ours, resizes = [], 0
+    for f, fr in enumerate(frames):
+        for d, a in zip(xs, fr):
+            d.copy_(torch.from_numpy(a), non_blocking=False)
+        if f == 0:
+            tree.build()
+        else:
+            tree.update()
+            while tree.doBuffersNeedResize():
+                resizes += 1
+                tree.resizeBuffers()
+                tree.update()
+        tree.doBuffersNeedResize()
+        stream.synchronize()
+        row = {}
+        for name in PARITY_ARRAYS:
+            t = tree.get(name + "_d")
+            wide = {torch.uint64: torch.int64, torch.uint32: torch.int32}.get(t.dtype)
+            a = t.view(wide).cpu().numpy() if wide is not None else t.cpu().numpy()
+            row[name] = (int(a.size), refrun.digest(a))
+        info = tree.info()
+        row["scalars"] = (info.num_particles, info.num_active_particles, info.num_nodes, info.max_achieved_depth,
+                          resizes)
+        ours.append(row)
+    ref = refrun.run(0, frames, digests=True, bucket=BUCKET, nf=True, hilbert=True, views=(False, False, False),
+                     timeout=1800)
+    mismatches = []
+    for f, (o, r) in enumerate(zip(ours, ref)):
+        for name in PARITY_ARRAYS:
+            if o[name] != tuple(r[name]):
+                mismatches.append(f"frame {f} {name}")
+        if tuple(o["scalars"]) != tuple(r["scalars"][:5]):
+            mismatches.append(f"frame {f} scalars {o['scalars']} vs {tuple(r['scalars'][:5])}")
+    return {"ref_lib_bit_exact": not mismatches and len(ref) == len(ours), "frames": ["build", "update"],
+            "buffers": list(PARITY_ARRAYS), "mismatches": mismatches[:8],
+            "how": "64-bit content digests of the timed tree's arrays vs the reference library compiled for "
+                   "sm_100a (oracle/_ref/ref_driver), same coordinates, build then update(N(0,1e-3) jitter)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -946,13 +1000,20 @@ def main():
                 rng = np.random.default_rng(5)
                 frame1 = tuple(np.clip(a + rng.normal(0, 1e-3, a.size).astype(np.float32), 0, upper).astype(
                     np.float32) for a in hx)
-                r = refrun.time_reference(0, [hx, frame1], reps=3, bucket=BUCKET, nf=True, hilbert=True,
+                with torch.cuda.stream(s):
+                    line["parity"] = reference_parity(tree, xs, [hx, frame1], s)
+                r = refrun.time_reference(0, [hx, frame1], reps=10, bucket=BUCKET, nf=True, hilbert=True,
                                           views=(False, False, False))
                 line["reference_gpu"] = {"build_ms": r["build_ms"], "update_ms": r["update_ms"],
+                                         "build_min_ms": r["build_min_ms"], "build_max_ms": r["build_max_ms"],
+                                         "cold_build_ms": r["cold_build_ms"], "reps": r["reps"],
                                          "build_value": n / (r["build_ms"] * 1e-3),
                                          "update_value": n / (r["update_ms"] * 1e-3), "unit": "particles/s",
-                                         "what": "reference library compiled for sm_100a, same inputs and GPU"}
+                                         "what": "reference library compiled for sm_100a, same inputs and GPU; "
+                                                 "build_ms: median of warm builds of one tree (its buffers "
+                                                 "already grown), cold_build_ms: the first build of a fresh tree"}
         except Exception as e:  # the reference run is informational
+            line.setdefault("parity", {"ref_lib_bit_exact": None, "error": str(e)[:200]})
             line["reference_gpu"] = {"error": str(e)[:200]}
     if world > 1:
         dist.destroy_process_group()

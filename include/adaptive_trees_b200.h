@@ -200,6 +200,22 @@ AO_API ao_status ao_sort_pairs(void *scratch, size_t *scratch_bytes, const unsig
                                unsigned long long *keys_out, const unsigned *values_in, unsigned *values_out,
                                size_t n, int begin_bit, int end_bit, void *stream);
 
+/* Waits for `stream` and checks the last ao_sort_pairs of n items that ran
+ * in `scratch`: AO_ERR_RUNTIME when a look-back wait of the sort gave up
+ * after its bounded number of polls (the output is then not sorted; CUB's
+ * SortPairs has no such failure, its waits are unbounded), AO_OK otherwise.
+ * No counterpart in the reference.  n = 0 returns AO_OK. */
+AO_API ao_status ao_sort_pairs_check(const void *scratch, size_t n, void *stream);
+
+/* Self-test of the bounded device waits (no counterpart in the reference).
+ * Runs one look-back -- which 0: a radix sort pass, 1: the rebalance
+ * decide+scan -- whose predecessor tile is never processed, so its wait can
+ * only end by its limit of spin_limit polls (1..65536).  Returns
+ * AO_ERR_RUNTIME with *error_word (may be NULL) set to the kernel's error
+ * code when the wait gave up and the kernel returned, the designed outcome;
+ * the device stays usable.  Uses its own small allocations and stream. */
+AO_API ao_status ao_selftest_bounded_wait(int which, unsigned spin_limit, int *error_word);
+
 /* The sort tuner (no counterpart in the reference; it picks what the
  * reference leaves to CUB's fixed policy).  The radix sort is compiled in a
  * few configurations of digit width (7 or 8 bits) and keys per thread (8 to
@@ -228,8 +244,10 @@ AO_API ao_status ao_sort_forget_tuning(void);
  * budget at start-up and must not grow it, or a plain C / FFI host without a
  * device allocator of its own.
  *  - n <= AO_SORT_PAIRS_NOALLOC_MAX_ITEMS, else AO_ERR_INVALID_ARGUMENT.
- *  - The first call on a device does the set-up (it looks up the array's
- *    address on that device); make it before any stream capture.
+ *  - The first call on a device does the set-up (it loads every kernel the
+ *    sort can launch there); make it before any stream capture.  Every call
+ *    looks up the array's address on the current device, so a device whose
+ *    context was torn down and created again is handled.
  *  - One array per device: calls that overlap in time on the same device
  *    (other streams, other threads) race and corrupt each other's results.
  *    Serialise them.
@@ -238,6 +256,9 @@ AO_API ao_status ao_sort_forget_tuning(void);
 AO_API ao_status ao_sort_pairs_noalloc(const unsigned long long *keys_in, unsigned long long *keys_out,
                                        const unsigned *values_in, unsigned *values_out, size_t n, int begin_bit,
                                        int end_bit, void *stream);
+/* Waits for `stream` and checks the last ao_sort_pairs_noalloc of n items on
+ * the current device, as ao_sort_pairs_check does for caller scratch. */
+AO_API ao_status ao_sort_pairs_noalloc_check(size_t n, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Batched octrees ("forest").  The reference has no batch API: its callers

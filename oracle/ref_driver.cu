@@ -15,9 +15,14 @@
 // Output file: per frame, for each of 14 arrays: u32 id, u64 count,
 //   u64 elemBytes, bytes; then u32 0xFFFFFFFF, u64 scalars[6]
 //   (numParticles, numActive, numNodes, maxAchievedDepth, resizes, 0).
+//   With a third argument `--digest` each array's bytes are replaced by one
+//   u64 digest (arrayDigest below), so large trees are compared without
+//   writing them out.
 // With timingReps > 0 it instead prints one JSON line of timings:
-//   build_ms (median of reps, each a fresh tree), update_ms (median of
-//   captured-graph replays of update() over frame 1).
+//   cold_build_ms (the first build of a fresh tree, with its allocations),
+//   build_ms (median of `reps` later builds of the same tree, its buffers
+//   already grown), update_ms (median of captured-graph replays of update()
+//   over frame 1).
 #include <cuda_runtime.h>
 #include <thrust/device_vector.h>
 #include <thrust/host_vector.h>
@@ -30,6 +35,7 @@
 #include <fstream>
 #include <iostream>
 #include <stdexcept>
+#include <type_traits>
 #include <vector>
 
 #include "adaptive_octree/tree.hpp"
@@ -52,15 +58,48 @@ void check(cudaError_t e, const char *w)
     if (e != cudaSuccess) throw std::runtime_error(std::string(w) + ": " + cudaGetErrorString(e));
 }
 
+bool g_digest = false;
+
+// Order-sensitive digest of an integer array: the sum over i of
+// splitmix64(a[i] + i * 0x9E3779B97F4A7C15) modulo 2^64, each element taken as
+// its unsigned bit pattern widened to 64 bits.  oracle/refrun.py computes the
+// same function with numpy.
+template <class T>
+std::uint64_t arrayDigest(const T *a, std::size_t n)
+{
+    using U = std::conditional_t<sizeof(T) == 1, std::uint8_t,
+                                 std::conditional_t<sizeof(T) == 4, std::uint32_t, std::uint64_t>>;
+    std::uint64_t sum = 0;
+    for (std::size_t i = 0; i < n; ++i)
+    {
+        U u;
+        std::memcpy(&u, a + i, sizeof(U));
+        std::uint64_t z = std::uint64_t(u) + std::uint64_t(i) * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        sum += z ^ (z >> 31);
+    }
+    return sum;
+}
+
 template <class T>
 void dump(std::ofstream &out, std::uint32_t id, const thrust::device_vector<T> &v)
 {
+    static_assert(sizeof(T) == 1 || sizeof(T) == 4 || sizeof(T) == 8, "array element width");
     thrust::host_vector<T> h = v;
     const std::uint64_t count = h.size(), eb = sizeof(T);
     out.write(reinterpret_cast<const char *>(&id), 4);
     out.write(reinterpret_cast<const char *>(&count), 8);
     out.write(reinterpret_cast<const char *>(&eb), 8);
-    if (count) out.write(reinterpret_cast<const char *>(h.data()), std::streamsize(count * eb));
+    if (g_digest)
+    {
+        const std::uint64_t d = arrayDigest(h.data(), h.size());
+        out.write(reinterpret_cast<const char *>(&d), 8);
+    }
+    else if (count)
+    {
+        out.write(reinterpret_cast<const char *>(h.data()), std::streamsize(count * eb));
+    }
 }
 
 template <class Real, adaptive_octree::TreeType Kind>
@@ -104,9 +143,7 @@ int run(const Header &h, const std::vector<char> &payload, const char *outPath)
         std::vector<double> builds, updates;
         load(0);
         check(cudaDeviceSynchronize(), "sync");
-        for (unsigned r = 0; r < h.timingReps + 1; ++r)
-        {
-            Tree tree(xp, yp, zp, n, c);
+        auto timedBuild = [&](Tree &tree) {
             check(cudaStreamSynchronize(stream), "sync");
             check(cudaEventRecord(a, stream), "rec");
             tree.build();
@@ -114,10 +151,16 @@ int run(const Header &h, const std::vector<char> &payload, const char *outPath)
             check(cudaEventSynchronize(b), "sync");
             float ms = 0;
             check(cudaEventElapsedTime(&ms, a, b), "elapsed");
-            if (r > 0) builds.push_back(ms);  // first build warms the process up
+            return double(ms);
+        };
+        {
+            Tree warm(xp, yp, zp, n, c);  // loads the process's kernels
+            warm.build();
         }
         Tree tree(xp, yp, zp, n, c);
-        tree.build();
+        const double coldMs = timedBuild(tree);  // a fresh tree: its buffers grow during the build
+        timedBuild(tree);
+        for (unsigned r = 0; r < h.timingReps; ++r) builds.push_back(timedBuild(tree));
         if (h.frames > 1) load(1);
         check(cudaDeviceSynchronize(), "sync");
         cudaGraph_t graph;
@@ -148,8 +191,10 @@ int run(const Header &h, const std::vector<char> &payload, const char *outPath)
         }
         std::sort(builds.begin(), builds.end());
         std::sort(updates.begin(), updates.end());
-        std::printf("{\"build_ms\": %.6f, \"update_ms\": %.6f, \"build_min_ms\": %.6f, \"update_min_ms\": %.6f}\n",
-                    builds[builds.size() / 2], updates[updates.size() / 2], builds.front(), updates.front());
+        std::printf("{\"build_ms\": %.6f, \"update_ms\": %.6f, \"build_min_ms\": %.6f, \"update_min_ms\": %.6f, "
+                    "\"build_max_ms\": %.6f, \"update_max_ms\": %.6f, \"cold_build_ms\": %.6f, \"reps\": %u}\n",
+                    builds[builds.size() / 2], updates[updates.size() / 2], builds.front(), updates.front(),
+                    builds.back(), updates.back(), coldMs, h.timingReps);
         cudaGraphExecDestroy(exec);
         cudaGraphDestroy(graph);
         return 0;
@@ -204,11 +249,12 @@ int run(const Header &h, const std::vector<char> &payload, const char *outPath)
 
 int main(int argc, char **argv)
 {
-    if (argc < 3)
+    if (argc < 3 || (argc > 3 && std::strcmp(argv[3], "--digest") != 0))
     {
-        std::fprintf(stderr, "usage: ref_driver scenario.bin out.bin\n");
+        std::fprintf(stderr, "usage: ref_driver scenario.bin out.bin [--digest]\n");
         return 2;
     }
+    g_digest = argc > 3;
     try
     {
         std::ifstream in(argv[1], std::ios::binary);

@@ -44,8 +44,24 @@ def write_scenario(path, kind, frames, max_depth=-1, bucket=64, update_iteration
                 f.write(np.ascontiguousarray(a).tobytes())
 
 
-def read_output(path):
-    """List of per-frame dicts: name -> array, plus 'scalars'."""
+def digest(a) -> int:
+    """Order-sensitive digest of an integer array, as ref_driver --digest writes
+    it: sum over i of splitmix64(a[i] + i * 0x9E3779B97F4A7C15) mod 2^64, each
+    element taken as its unsigned bit pattern widened to 64 bits."""
+    a = np.ascontiguousarray(a)
+    u = a.view({1: np.uint8, 4: np.uint32, 8: np.uint64}[a.dtype.itemsize]).astype(np.uint64)
+    z = u + np.arange(u.size, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+    z ^= z >> np.uint64(30)
+    z *= np.uint64(0xBF58476D1CE4E5B9)
+    z ^= z >> np.uint64(27)
+    z *= np.uint64(0x94D049BB133111EB)
+    z ^= z >> np.uint64(31)
+    return int(z.sum(dtype=np.uint64))
+
+
+def read_output(path, digests=False):
+    """List of per-frame dicts: name -> array (digests: name -> (count, digest)),
+    plus 'scalars'."""
     out, cur = [], {}
     with open(path, "rb") as f:
         data = f.read()
@@ -61,25 +77,35 @@ def read_output(path):
             continue
         count, eb = struct.unpack_from("<QQ", data, pos)
         pos += 16
+        if digests:
+            (d,) = struct.unpack_from("<Q", data, pos)
+            pos += 8
+            cur[ARRAY_NAMES[ident]] = (count, d)
+            continue
         arr = np.frombuffer(data, dtype=DTYPES[ident], count=count, offset=pos).copy()
         pos += count * eb
         cur[ARRAY_NAMES[ident]] = arr
     return out
 
 
-def run(kind, frames, timeout=1800, **cfg):
-    """Run the reference on build(frame 0) + update(frame k) with its resize loop."""
+def run(kind, frames, timeout=1800, digests=False, **cfg):
+    """Run the reference on build(frame 0) + update(frame k) with its resize loop.
+
+    digests: return (count, digest) per array instead of the arrays."""
     with tempfile.TemporaryDirectory() as d:
         sc, res = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
         write_scenario(sc, kind, frames, **cfg)
-        r = subprocess.run([DRIVER, sc, res], capture_output=True, text=True, timeout=timeout)
+        cmd = [DRIVER, sc, res] + (["--digest"] if digests else [])
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError(f"ref_driver failed ({r.returncode}): {r.stderr.strip()}")
-        return read_output(res)
+        return read_output(res, digests=digests)
 
 
-def time_reference(kind, frames, reps=5, timeout=1800, **cfg):
-    """Median build and captured-update times (ms) of the reference on this GPU."""
+def time_reference(kind, frames, reps=10, timeout=1800, **cfg):
+    """Build and captured-update times (ms) of the reference on this GPU: the
+    median of `reps` warm builds of one tree (and its cold first build), and of
+    `reps` graph replays of update() on frame 1."""
     with tempfile.TemporaryDirectory() as d:
         sc = os.path.join(d, "in.bin")
         write_scenario(sc, kind, frames, timing_reps=reps, **cfg)

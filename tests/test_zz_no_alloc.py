@@ -36,6 +36,7 @@ def _reference_sort(lib, keys, vals, n, begin, end, stream):
     scratch = torch.empty(max(1, nbytes.value), dtype=torch.uint8, device=keys.device)
     C.check(lib.ao_sort_pairs(_p(scratch), ctypes.byref(nbytes), _p(keys), _p(out_k), _p(vals), _p(out_v), n,
                               begin, end, ctypes.c_void_p(stream.cuda_stream)))
+    C.check(lib.ao_sort_pairs_check(_p(scratch), n, ctypes.c_void_p(stream.cuda_stream)))
     return out_k, out_v
 
 
@@ -67,6 +68,8 @@ def test_matches_ao_sort_pairs_on_two_calls_in_a_row():
             ov = torch.empty(n, dtype=torch.uint32, device="cuda")
             C.check(lib.ao_sort_pairs_noalloc(_p(keys), _p(ok), _p(vals), _p(ov), n, begin, end,
                                               ctypes.c_void_p(s.cuda_stream)))
+            # no bounded look-back wait of this call gave up
+            C.check(lib.ao_sort_pairs_noalloc_check(n, ctypes.c_void_p(s.cuda_stream)))
             outs.append((ok, ov))
         refs = [_reference_sort(lib, keys, vals, n, begin, end, s)
                 for (n, begin, end, _), (keys, vals) in zip(cases, inputs)]
@@ -86,13 +89,18 @@ def test_matches_ao_sort_pairs_on_two_calls_in_a_row():
 
 @pytest.mark.gpu
 def test_repeated_calls_leave_device_memory_unchanged():
-    """After the set-up call, further calls do not change the device's free memory."""
+    """After the set-up call, further calls do not change the device's free
+    memory: full 64-bit sorts, sorts that carry given values, and sorts of an
+    empty bit range (which copy the keys and write the identity permutation
+    without a radix pass)."""
     import torch
     lib = C.load()
     torch.cuda.set_device(0)
     n = 300_000
     rng = np.random.default_rng(7)
     keys = torch.from_numpy(rng.integers(0, 2 ** 63, size=n, dtype=np.int64)).cuda().view(torch.uint64)
+    vals = torch.from_numpy(rng.integers(0, 2 ** 31, size=n, dtype=np.int64).astype(np.int32)).cuda()
+    vals = vals.view(torch.uint32)
     ok = torch.empty_like(keys)
     ov = torch.empty(n, dtype=torch.uint32, device="cuda")
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -100,9 +108,14 @@ def test_repeated_calls_leave_device_memory_unchanged():
     torch.cuda.synchronize()
     free0, _ = torch.cuda.mem_get_info()
     for _ in range(3):
+        C.check(lib.ao_sort_pairs_noalloc(_p(keys), _p(ok), _p(vals), _p(ov), n, 0, 64, stream))
+        C.check(lib.ao_sort_pairs_noalloc(_p(keys), _p(ok), None, _p(ov), n, 17, 17, stream))
+        C.check(lib.ao_sort_pairs_noalloc_check(n, stream))
         C.check(lib.ao_sort_pairs_noalloc(_p(keys), _p(ok), None, _p(ov), n, 0, 64, stream))
+        C.check(lib.ao_sort_pairs_noalloc_check(n, stream))
     torch.cuda.synchronize()
     free1, _ = torch.cuda.mem_get_info()
     assert free1 == free0
     k = keys.view(torch.int64).cpu().numpy()
     assert np.array_equal(ok.view(torch.int64).cpu().numpy(), np.sort(k, kind="stable"))
+    assert np.array_equal(ov.view(torch.int32).cpu().numpy(), np.argsort(k, kind="stable").astype(np.int32))
