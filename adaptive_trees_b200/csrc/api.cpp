@@ -54,12 +54,13 @@ aot::EngineConfig binaryEngineConfig(const KDTree3DConfig<Real> &c)
     return e;
 }
 template <class T>
-DeviceVector<T> view(const aot::TreeEngine &e, int which)
+const DeviceVector<T> &view(const aot::TreeEngine &e, int which, DeviceVector<T> &slot)
 {
     const void *p = nullptr;
     size_t len = 0, cap = 0, elem = 0;
     e.buffer(which, &p, &len, &cap, &elem);
-    return DeviceVector<T>(static_cast<const T *>(p), len, cap);
+    slot = DeviceVector<T>(static_cast<const T *>(p), len, cap);
+    return slot;
 }
 void printSummary(std::ostream &out, const aot::TreeEngine &e, const char *name)
 {
@@ -90,47 +91,62 @@ template <class Real> const unsigned *Octree<Real>::numActiveParticles_d() const
 {
     return engine_->numActiveParticlesDevice();
 }
-template <class Real> DeviceVector<KeyType> Octree<Real>::particleKeys_d() const { return view<KeyType>(*engine_, 0); }
-template <class Real> DeviceVector<PermIndex> Octree<Real>::perm_d() const { return view<PermIndex>(*engine_, 1); }
-template <class Real> DeviceVector<KeyType> Octree<Real>::cornerstone_d() const { return view<KeyType>(*engine_, 2); }
-template <class Real> DeviceVector<unsigned> Octree<Real>::leafCounts_d() const { return view<unsigned>(*engine_, 3); }
-template <class Real> DeviceVector<unsigned> Octree<Real>::nearFieldCounts_d() const
+template <class Real> const DeviceVector<KeyType> &Octree<Real>::particleKeys_d() const
 {
-    return view<unsigned>(*engine_, 4);
+    return view<KeyType>(*engine_, 0, views_.particleKeys);
 }
-template <class Real> DeviceVector<KeyType> Octree<Real>::sfcBoxIndex_d() const { return view<KeyType>(*engine_, 5); }
-template <class Real> DeviceVector<std::uint8_t> Octree<Real>::hasBoxSplit_d() const
+template <class Real> const DeviceVector<PermIndex> &Octree<Real>::perm_d() const
 {
-    return view<std::uint8_t>(*engine_, 6);
+    return view<PermIndex>(*engine_, 1, views_.perm);
 }
-template <class Real> DeviceVector<std::uint8_t> Octree<Real>::boxDepth_d() const
+template <class Real> const DeviceVector<KeyType> &Octree<Real>::cornerstone_d() const
 {
-    return view<std::uint8_t>(*engine_, 7);
+    return view<KeyType>(*engine_, 2, views_.cornerstone);
 }
-template <class Real> DeviceVector<NodeIndex> Octree<Real>::parentIndex_d() const
+template <class Real> const DeviceVector<unsigned> &Octree<Real>::leafCounts_d() const
 {
-    return view<NodeIndex>(*engine_, 8);
+    return view<unsigned>(*engine_, 3, views_.leafCounts);
 }
-template <class Real> DeviceVector<NodeIndex> Octree<Real>::childIndex_d() const
+template <class Real> const DeviceVector<unsigned> &Octree<Real>::nearFieldCounts_d() const
 {
-    return view<NodeIndex>(*engine_, 9);
+    return view<unsigned>(*engine_, 4, views_.nearFieldCounts);
 }
-template <class Real> DeviceVector<NodeIndex> Octree<Real>::levelOffset_d() const
+template <class Real> const DeviceVector<KeyType> &Octree<Real>::sfcBoxIndex_d() const
 {
-    return view<NodeIndex>(*engine_, 10);
+    return view<KeyType>(*engine_, 5, views_.sfcBoxIndex);
+}
+template <class Real> const DeviceVector<std::uint8_t> &Octree<Real>::hasBoxSplit_d() const
+{
+    return view<std::uint8_t>(*engine_, 6, views_.hasBoxSplit);
+}
+template <class Real> const DeviceVector<std::uint8_t> &Octree<Real>::boxDepth_d() const
+{
+    return view<std::uint8_t>(*engine_, 7, views_.boxDepth);
+}
+template <class Real> const DeviceVector<NodeIndex> &Octree<Real>::parentIndex_d() const
+{
+    return view<NodeIndex>(*engine_, 8, views_.parentIndex);
+}
+template <class Real> const DeviceVector<NodeIndex> &Octree<Real>::childIndex_d() const
+{
+    return view<NodeIndex>(*engine_, 9, views_.childIndex);
+}
+template <class Real> const DeviceVector<NodeIndex> &Octree<Real>::levelOffset_d() const
+{
+    return view<NodeIndex>(*engine_, 10, views_.levelOffset);
 }
 template <class Real> unsigned Octree<Real>::maxAchievedDepth() const { return engine_->maxAchievedDepth(); }
-template <class Real> DeviceVector<unsigned> Octree<Real>::particleBeginIndex_d() const
+template <class Real> const DeviceVector<unsigned> &Octree<Real>::particleBeginIndex_d() const
 {
-    return view<unsigned>(*engine_, 11);
+    return view<unsigned>(*engine_, 11, views_.particleBeginIndex);
 }
-template <class Real> DeviceVector<unsigned> Octree<Real>::particleCounts_d() const
+template <class Real> const DeviceVector<unsigned> &Octree<Real>::particleCounts_d() const
 {
-    return view<unsigned>(*engine_, 12);
+    return view<unsigned>(*engine_, 12, views_.particleCounts);
 }
-template <class Real> DeviceVector<KeyType> Octree<Real>::sfcParticleIndex_d() const
+template <class Real> const DeviceVector<KeyType> &Octree<Real>::sfcParticleIndex_d() const
 {
-    return view<KeyType>(*engine_, 13);
+    return view<KeyType>(*engine_, 13, views_.sfcParticleIndex);
 }
 template <class Real> std::size_t Octree<Real>::numParticles() const { return engine_->numParticles(); }
 template <class Real> std::size_t Octree<Real>::numActiveParticles() const { return engine_->numActiveParticles(); }
@@ -168,46 +184,58 @@ template <class Real> const unsigned *KDTree3D<Real>::numActiveParticles_d() con
 {
     return engine_->numActiveParticlesDevice();
 }
-template <class Real> DeviceVector<KeyType> KDTree3D<Real>::particleKeys_d() const { return view<KeyType>(*engine_, 0); }
-template <class Real> DeviceVector<PermIndex> KDTree3D<Real>::perm_d() const { return view<PermIndex>(*engine_, 1); }
-template <class Real> DeviceVector<KeyType> KDTree3D<Real>::cornerstone_d() const { return view<KeyType>(*engine_, 2); }
-template <class Real> DeviceVector<unsigned> KDTree3D<Real>::leafCounts_d() const
+template <class Real> const DeviceVector<KeyType> &KDTree3D<Real>::particleKeys_d() const
 {
-    return view<unsigned>(*engine_, 3);
+    return view<KeyType>(*engine_, 0, views_.particleKeys);
 }
-template <class Real> DeviceVector<KeyType> KDTree3D<Real>::sfcBoxIndex_d() const { return view<KeyType>(*engine_, 5); }
-template <class Real> DeviceVector<std::uint8_t> KDTree3D<Real>::hasBoxSplit_d() const
+template <class Real> const DeviceVector<PermIndex> &KDTree3D<Real>::perm_d() const
 {
-    return view<std::uint8_t>(*engine_, 6);
+    return view<PermIndex>(*engine_, 1, views_.perm);
 }
-template <class Real> DeviceVector<std::uint8_t> KDTree3D<Real>::boxDepth_d() const
+template <class Real> const DeviceVector<KeyType> &KDTree3D<Real>::cornerstone_d() const
 {
-    return view<std::uint8_t>(*engine_, 7);
+    return view<KeyType>(*engine_, 2, views_.cornerstone);
 }
-template <class Real> DeviceVector<NodeIndex> KDTree3D<Real>::parentIndex_d() const
+template <class Real> const DeviceVector<unsigned> &KDTree3D<Real>::leafCounts_d() const
 {
-    return view<NodeIndex>(*engine_, 8);
+    return view<unsigned>(*engine_, 3, views_.leafCounts);
 }
-template <class Real> DeviceVector<NodeIndex> KDTree3D<Real>::childIndex_d() const
+template <class Real> const DeviceVector<KeyType> &KDTree3D<Real>::sfcBoxIndex_d() const
 {
-    return view<NodeIndex>(*engine_, 9);
+    return view<KeyType>(*engine_, 5, views_.sfcBoxIndex);
 }
-template <class Real> DeviceVector<NodeIndex> KDTree3D<Real>::levelOffset_d() const
+template <class Real> const DeviceVector<std::uint8_t> &KDTree3D<Real>::hasBoxSplit_d() const
 {
-    return view<NodeIndex>(*engine_, 10);
+    return view<std::uint8_t>(*engine_, 6, views_.hasBoxSplit);
+}
+template <class Real> const DeviceVector<std::uint8_t> &KDTree3D<Real>::boxDepth_d() const
+{
+    return view<std::uint8_t>(*engine_, 7, views_.boxDepth);
+}
+template <class Real> const DeviceVector<NodeIndex> &KDTree3D<Real>::parentIndex_d() const
+{
+    return view<NodeIndex>(*engine_, 8, views_.parentIndex);
+}
+template <class Real> const DeviceVector<NodeIndex> &KDTree3D<Real>::childIndex_d() const
+{
+    return view<NodeIndex>(*engine_, 9, views_.childIndex);
+}
+template <class Real> const DeviceVector<NodeIndex> &KDTree3D<Real>::levelOffset_d() const
+{
+    return view<NodeIndex>(*engine_, 10, views_.levelOffset);
 }
 template <class Real> unsigned KDTree3D<Real>::maxAchievedDepth() const { return engine_->maxAchievedDepth(); }
-template <class Real> DeviceVector<unsigned> KDTree3D<Real>::particleBeginIndex_d() const
+template <class Real> const DeviceVector<unsigned> &KDTree3D<Real>::particleBeginIndex_d() const
 {
-    return view<unsigned>(*engine_, 11);
+    return view<unsigned>(*engine_, 11, views_.particleBeginIndex);
 }
-template <class Real> DeviceVector<unsigned> KDTree3D<Real>::particleCounts_d() const
+template <class Real> const DeviceVector<unsigned> &KDTree3D<Real>::particleCounts_d() const
 {
-    return view<unsigned>(*engine_, 12);
+    return view<unsigned>(*engine_, 12, views_.particleCounts);
 }
-template <class Real> DeviceVector<KeyType> KDTree3D<Real>::sfcParticleIndex_d() const
+template <class Real> const DeviceVector<KeyType> &KDTree3D<Real>::sfcParticleIndex_d() const
 {
-    return view<KeyType>(*engine_, 13);
+    return view<KeyType>(*engine_, 13, views_.sfcParticleIndex);
 }
 template <class Real> std::size_t KDTree3D<Real>::numParticles() const { return engine_->numParticles(); }
 template <class Real> std::size_t KDTree3D<Real>::numActiveParticles() const { return engine_->numActiveParticles(); }

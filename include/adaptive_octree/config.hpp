@@ -1,21 +1,28 @@
-// config.hpp -- public types and configuration of the B200 adaptive-tree engine.
+// config.hpp -- public types, configuration and macros of the B200 adaptive-tree engine.
 //
 // Mirrors the public surface of nrottstegge/Adaptive_Trees
-// (include/adaptive_octree/config.hpp:36-160): the same type aliases,
+// (include/adaptive_octree/config.hpp:14-180): the same macros, type aliases,
 // sentinels, enums, defaults, Box, ViewConfig and the per-backend configs.
 // Differences at this boundary:
-//   * device buffers are returned as adaptive_octree::DeviceVector<T> (a
-//     read-only view: data/size/capacity/empty/to_host), not as
-//     thrust::device_vector<T>;
-//   * CUDA failures throw adaptive_octree::CudaError instead of exiting the
-//     process (config.hpp:164-172 of the reference calls std::exit).
+//   * device buffers are returned as const adaptive_octree::DeviceVector<T>&
+//     (engine-owned storage with size/capacity/empty/data and conversions to
+//     host and device containers such as thrust::host_vector<T> and
+//     thrust::device_vector<T>), not as const thrust::device_vector<T>&;
+//   * CUDA failures inside the library throw adaptive_octree::CudaError
+//     instead of exiting the process (the reference's library code calls
+//     std::exit through checkGpuErrors).  The checkGpuErrors macro itself
+//     keeps its meaning for callers' code: report and exit.
 #pragma once
 
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime_api.h>
@@ -25,6 +32,27 @@
 #else
 #define AO_HOST_DEVICE
 #endif
+
+// The reference's public macros (config.hpp:14-33), for callers' code.
+#ifndef HOST_DEVICE_FUN
+#define HOST_DEVICE_FUN AO_HOST_DEVICE
+#endif
+
+// NVTX ranges around callers' phases when ADAPTIVE_OCTREE_PROFILING is
+// defined; no-ops otherwise.
+#ifdef ADAPTIVE_OCTREE_PROFILING
+#include <nvtx3/nvToolsExt.h>
+#define ADAPTIVE_OCTREE_NVTX_RANGE_PUSH(name) nvtxRangePushA(name)
+#define ADAPTIVE_OCTREE_NVTX_RANGE_POP() nvtxRangePop()
+#else
+#define ADAPTIVE_OCTREE_NVTX_RANGE_PUSH(name) ((void)0)
+#define ADAPTIVE_OCTREE_NVTX_RANGE_POP() ((void)0)
+#endif
+
+// checkGpuErrors(call): on failure prints the call, file and line and exits.
+// ADAPTIVE_OCTREE_CHECK_CUDA(call): on failure throws std::runtime_error.
+#define checkGpuErrors(errcode) ::adaptive_octree::detail::checkErr((errcode), __FILE__, __LINE__, #errcode)
+#define ADAPTIVE_OCTREE_CHECK_CUDA(operation) ::adaptive_octree::detail::checkCudaResult((operation), #operation)
 
 // Symbols of the C++ classes exported by the shared library.
 #if defined(__GNUC__)
@@ -141,35 +169,119 @@ private:
     int code_;
 };
 
-// Read-only view of an engine-owned device array.  size() is the logical
-// length reported by the last host synchronisation (build() or
+namespace detail
+{
+inline void checkErr(cudaError_t error, const char *file, int line, const char *expression)
+{
+    if (error == cudaSuccess) return;
+    std::fprintf(stderr, "CUDA error: %s failed at %s:%d with %s (%s)\n", expression, file, line,
+                 cudaGetErrorName(error), cudaGetErrorString(error));
+    std::exit(EXIT_FAILURE);
+}
+
+inline void checkCudaResult(cudaError_t error, const char *operation)
+{
+    if (error != cudaSuccess) throw std::runtime_error(std::string(operation) + ": " + cudaGetErrorString(error));
+}
+
+// A host container of T with contiguous storage: value_type T, resize(n),
+// data() -> T* (std::vector<T>, thrust::host_vector<T>).
+template <class C, class T, class = void>
+struct IsHostContainer : std::false_type
+{
+};
+template <class C, class T>
+struct IsHostContainer<C, T,
+                       std::void_t<typename C::value_type, decltype(std::declval<C &>().resize(std::size_t(0))),
+                                   decltype(std::declval<C &>().data())>>
+    : std::bool_constant<std::is_same_v<typename C::value_type, T> &&
+                         std::is_same_v<decltype(std::declval<C &>().data()), T *>>
+{
+};
+
+// A device container of T whose data() is a fancy pointer with get() -> T*
+// (thrust::device_vector<T>); constructible with a size.
+template <class C, class T, class = void>
+struct IsDeviceContainer : std::false_type
+{
+};
+template <class C, class T>
+struct IsDeviceContainer<C, T, std::void_t<typename C::value_type, decltype(std::declval<C &>().data().get())>>
+    : std::bool_constant<std::is_same_v<typename C::value_type, T> &&
+                         std::is_same_v<decltype(std::declval<C &>().data().get()), T *> &&
+                         std::is_constructible_v<C, std::size_t>>
+{
+};
+
+inline void copyOrThrow(void *dst, const void *src, std::size_t bytes, cudaMemcpyKind kind)
+{
+    if (!bytes) return;
+    const cudaError_t e = cudaMemcpy(dst, src, bytes, kind);
+    if (e != cudaSuccess) throw CudaError(int(e), std::string("DeviceVector copy: ") + cudaGetErrorString(e));
+}
+}  // namespace detail
+
+// An engine-owned device array as the getters return it.  size() is the
+// logical length reported by the last host synchronisation (build() or
 // doBuffersNeedResize()), capacity() the allocation; data() is a device
-// pointer that stays valid until the next build() or resizeBuffers().
+// pointer that stays valid until the next build() or resizeBuffers() (so
+// thrust::raw_pointer_cast(tree.perm_d().data()) works as with the
+// reference).  Like the reference's const thrust::device_vector<T>&, a getter
+// returns a reference to storage held by the tree; the tree refreshes it at
+// each getter call, so reacquire it after update().
+//
+// Copies (all synchronous, cudaMemcpy on the legacy stream):
+//   thrust::host_vector<T> h = tree.particleKeys_d();   // or std::vector<T>
+//   thrust::device_vector<T> d = tree.particleKeys_d(); // a device copy
+// so callers written against the reference's getters, which assign them to
+// host vectors (tests/tree_test.cu:313-317), compile unchanged.
 template <class T>
 class DeviceVector
 {
 public:
     using value_type = T;
+    using size_type = std::size_t;
     DeviceVector() = default;
     DeviceVector(const T *data, std::size_t size, std::size_t capacity) : data_(data), size_(size), cap_(capacity) {}
     const T *data() const { return data_; }
     std::size_t size() const { return size_; }
     std::size_t capacity() const { return cap_; }
     bool empty() const { return size_ == 0; }
-    // Synchronous copy to the host (cudaMemcpy on the legacy stream).
+
     std::vector<T> to_host() const
     {
         std::vector<T> out(size_);
-        if (size_)
-        {
-            const cudaError_t e = cudaMemcpy(out.data(), data_, size_ * sizeof(T), cudaMemcpyDeviceToHost);
-            if (e != cudaSuccess) throw CudaError(int(e), cudaGetErrorString(e));
-        }
+        detail::copyOrThrow(out.data(), data_, size_ * sizeof(T), cudaMemcpyDeviceToHost);
+        return out;
+    }
+    template <class C, std::enable_if_t<detail::IsHostContainer<C, T>::value, int> = 0>
+    operator C() const
+    {
+        C out;
+        out.resize(size_);
+        detail::copyOrThrow(out.data(), data_, size_ * sizeof(T), cudaMemcpyDeviceToHost);
+        return out;
+    }
+    template <class C, std::enable_if_t<detail::IsDeviceContainer<C, T>::value, long> = 0>
+    operator C() const
+    {
+        C out(size_);
+        detail::copyOrThrow(out.data().get(), data_, size_ * sizeof(T), cudaMemcpyDeviceToDevice);
         return out;
     }
 
 private:
     const T *data_ = nullptr;
     std::size_t size_ = 0, cap_ = 0;
+};
+
+// The arrays a tree's getters return references to.
+struct GetterViews
+{
+    DeviceVector<KeyType> particleKeys, cornerstone, sfcBoxIndex, sfcParticleIndex;
+    DeviceVector<PermIndex> perm;
+    DeviceVector<unsigned> leafCounts, nearFieldCounts, particleBeginIndex, particleCounts;
+    DeviceVector<std::uint8_t> hasBoxSplit, boxDepth;
+    DeviceVector<NodeIndex> parentIndex, childIndex, levelOffset;
 };
 }  // namespace adaptive_octree

@@ -3,8 +3,8 @@
 // Same interface as nrottstegge/Adaptive_Trees include/adaptive_octree/
 // octree.hpp:24-135: borrowed device coordinates, build()/update()/
 // computeViews(), doBuffersNeedResize()/resizeBuffers(), device counters and
-// the P/Perm/K/N/NF and view getters.  Getters return DeviceVector<T> views
-// (see config.hpp) of engine-owned device arrays.
+// the P/Perm/K/N/NF and view getters.  Getters return const DeviceVector<T>&
+// (see config.hpp) over engine-owned device arrays.
 #pragma once
 
 #include <cstddef>
@@ -54,21 +54,21 @@ public:
     [[nodiscard]] const NodeIndex *numNodes_d() const;
     [[nodiscard]] const unsigned *numActiveParticles_d() const;
 
-    [[nodiscard]] DeviceVector<KeyType> particleKeys_d() const;
-    [[nodiscard]] DeviceVector<PermIndex> perm_d() const;
-    [[nodiscard]] DeviceVector<KeyType> cornerstone_d() const;
-    [[nodiscard]] DeviceVector<unsigned> leafCounts_d() const;
-    [[nodiscard]] DeviceVector<unsigned> nearFieldCounts_d() const;
-    [[nodiscard]] DeviceVector<KeyType> sfcBoxIndex_d() const;
-    [[nodiscard]] DeviceVector<std::uint8_t> hasBoxSplit_d() const;
-    [[nodiscard]] DeviceVector<std::uint8_t> boxDepth_d() const;
-    [[nodiscard]] DeviceVector<NodeIndex> parentIndex_d() const;
-    [[nodiscard]] DeviceVector<NodeIndex> childIndex_d() const;
-    [[nodiscard]] DeviceVector<NodeIndex> levelOffset_d() const;
+    [[nodiscard]] const DeviceVector<KeyType> &particleKeys_d() const;
+    [[nodiscard]] const DeviceVector<PermIndex> &perm_d() const;
+    [[nodiscard]] const DeviceVector<KeyType> &cornerstone_d() const;
+    [[nodiscard]] const DeviceVector<unsigned> &leafCounts_d() const;
+    [[nodiscard]] const DeviceVector<unsigned> &nearFieldCounts_d() const;
+    [[nodiscard]] const DeviceVector<KeyType> &sfcBoxIndex_d() const;
+    [[nodiscard]] const DeviceVector<std::uint8_t> &hasBoxSplit_d() const;
+    [[nodiscard]] const DeviceVector<std::uint8_t> &boxDepth_d() const;
+    [[nodiscard]] const DeviceVector<NodeIndex> &parentIndex_d() const;
+    [[nodiscard]] const DeviceVector<NodeIndex> &childIndex_d() const;
+    [[nodiscard]] const DeviceVector<NodeIndex> &levelOffset_d() const;
     [[nodiscard]] unsigned maxAchievedDepth() const;
-    [[nodiscard]] DeviceVector<unsigned> particleBeginIndex_d() const;
-    [[nodiscard]] DeviceVector<unsigned> particleCounts_d() const;
-    [[nodiscard]] DeviceVector<KeyType> sfcParticleIndex_d() const;
+    [[nodiscard]] const DeviceVector<unsigned> &particleBeginIndex_d() const;
+    [[nodiscard]] const DeviceVector<unsigned> &particleCounts_d() const;
+    [[nodiscard]] const DeviceVector<KeyType> &sfcParticleIndex_d() const;
 
     [[nodiscard]] std::size_t numParticles() const;
     [[nodiscard]] std::size_t numActiveParticles() const;
@@ -80,5 +80,8 @@ public:
 
 private:
     std::unique_ptr<aot::TreeEngine> engine_;
+    // what the getters return: refreshed from the engine at each getter call
+    // (one tree object is used from one host thread, as in the reference)
+    mutable GetterViews views_;
 };
 }  // namespace adaptive_octree

@@ -49,19 +49,19 @@ public:
     std::size_t numActiveParticles() const { return backend_.numActiveParticles(); }
     std::size_t numNodes() const { return backend_.numNodes(); }
     unsigned maxAchievedDepth() const { return backend_.maxAchievedDepth(); }
-    DeviceVector<KeyType> particleKeys_d() const { return backend_.particleKeys_d(); }
-    DeviceVector<PermIndex> perm_d() const { return backend_.perm_d(); }
-    DeviceVector<KeyType> cornerstone_d() const { return backend_.cornerstone_d(); }
-    DeviceVector<unsigned> leafCounts_d() const { return backend_.leafCounts_d(); }
-    DeviceVector<KeyType> sfcBoxIndex_d() const { return backend_.sfcBoxIndex_d(); }
-    DeviceVector<std::uint8_t> hasBoxSplit_d() const { return backend_.hasBoxSplit_d(); }
-    DeviceVector<std::uint8_t> boxDepth_d() const { return backend_.boxDepth_d(); }
-    DeviceVector<NodeIndex> parentIndex_d() const { return backend_.parentIndex_d(); }
-    DeviceVector<NodeIndex> childIndex_d() const { return backend_.childIndex_d(); }
-    DeviceVector<NodeIndex> levelOffset_d() const { return backend_.levelOffset_d(); }
-    DeviceVector<unsigned> particleBeginIndex_d() const { return backend_.particleBeginIndex_d(); }
-    DeviceVector<unsigned> particleCounts_d() const { return backend_.particleCounts_d(); }
-    DeviceVector<KeyType> sfcParticleIndex_d() const { return backend_.sfcParticleIndex_d(); }
+    const DeviceVector<KeyType> &particleKeys_d() const { return backend_.particleKeys_d(); }
+    const DeviceVector<PermIndex> &perm_d() const { return backend_.perm_d(); }
+    const DeviceVector<KeyType> &cornerstone_d() const { return backend_.cornerstone_d(); }
+    const DeviceVector<unsigned> &leafCounts_d() const { return backend_.leafCounts_d(); }
+    const DeviceVector<KeyType> &sfcBoxIndex_d() const { return backend_.sfcBoxIndex_d(); }
+    const DeviceVector<std::uint8_t> &hasBoxSplit_d() const { return backend_.hasBoxSplit_d(); }
+    const DeviceVector<std::uint8_t> &boxDepth_d() const { return backend_.boxDepth_d(); }
+    const DeviceVector<NodeIndex> &parentIndex_d() const { return backend_.parentIndex_d(); }
+    const DeviceVector<NodeIndex> &childIndex_d() const { return backend_.childIndex_d(); }
+    const DeviceVector<NodeIndex> &levelOffset_d() const { return backend_.levelOffset_d(); }
+    const DeviceVector<unsigned> &particleBeginIndex_d() const { return backend_.particleBeginIndex_d(); }
+    const DeviceVector<unsigned> &particleCounts_d() const { return backend_.particleCounts_d(); }
+    const DeviceVector<KeyType> &sfcParticleIndex_d() const { return backend_.sfcParticleIndex_d(); }
 
     SplitCriterion splitCriterion() const
     {
@@ -73,7 +73,7 @@ public:
         if constexpr (Kind == TreeType::Octree) return backend_.sfcKind();
         else throw std::logic_error("Tree: SFC selection requires Octree mode");
     }
-    DeviceVector<unsigned> nearFieldCounts_d() const
+    const DeviceVector<unsigned> &nearFieldCounts_d() const
     {
         if constexpr (Kind == TreeType::Octree) return backend_.nearFieldCounts_d();
         else throw std::logic_error("Tree: Binary NFCount is not implemented yet");
