@@ -73,6 +73,8 @@ PROTOTYPES = {
     "ao_tree_update": [vp],
     "ao_tree_update_until_converged": [vp, ci, ctypes.POINTER(ci)],
     "ao_tree_set_profiling": [vp, ci],
+    "ao_tree_set_build_mode": [vp, ci],
+    "ao_tree_build_path": [vp, ctypes.POINTER(ci), ctypes.POINTER(ci)],
     "ao_tree_stage_times": [vp, vp],
     "ao_tree_compute_views": [vp, ctypes.POINTER(AoViewConfig)],
     "ao_tree_needs_resize": [vp, ctypes.POINTER(ci)],

@@ -394,6 +394,23 @@ ao_status ao_tree_set_profiling(ao_tree *tree, int on)
     });
 }
 
+ao_status ao_tree_set_build_mode(ao_tree *tree, int mode)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        tree->engine->setBuildMode(mode);
+    });
+}
+
+ao_status ao_tree_build_path(ao_tree *tree, int *by_levels, int *rounds)
+{
+    return guarded([&] {
+        AO_NEED_TREE();
+        if (by_levels) *by_levels = tree->engine->lastBuildByLevels() ? 1 : 0;
+        if (rounds) *rounds = tree->engine->buildRounds();
+    });
+}
+
 ao_status ao_tree_stage_times(ao_tree *tree, ao_stage_times *out)
 {
     return guarded([&] {

@@ -32,6 +32,7 @@
 
 #include "engine_util.cuh"
 #include "keygen.cuh"
+#include "levelbuild.cuh"
 #include "rebalance.cuh"
 #include "tree_view.cuh"
 
@@ -740,6 +741,9 @@ struct TreeEngine::Impl
     // tree
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
     DevMem nodeRows;  // node table of the near-field refresh (NFCount)
+    // converged build by levels (levelbuild.cuh): unit arena and its control
+    DevMem lvRows, lvVal, lvChild, lvLeaves, lvOffset, lvScan, lvCtl;
+    size_t lvCap = 0;
     u32 nodeSlots = 0;
     bool nodeStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
@@ -781,7 +785,8 @@ struct TreeEngine::Impl
                                &vCandStart,  &vCandLevel,  &vLvKeys[0],     &vLvKeys[1],   &vLvVals[0],
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
-                               &viewSort.counters, &viewSort.status, &nodeRows};
+                               &viewSort.counters, &viewSort.status, &nodeRows, &lvRows, &lvVal, &lvChild,
+                               &lvLeaves, &lvOffset, &lvScan, &lvCtl};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -1392,68 +1397,222 @@ void TreeEngine::octreeBuild()
     capModel_.buildStart();
     sortParticles();
     mark(MarkSorted);
-    // Room for the build rounds; grown on overflow.
+    // Room for the build; grown on overflow.
     const size_t estimate = std::max<size_t>(4096, cfg_.nf ? n_ + 4096 : n_ / 4 + 4096);
     ensurePhysical(std::max(physCap_, estimate));
-    m_->history.reserve(std::max<size_t>(cfg_.maxDepth, 1) * sizeof(long long), cfg_.stream);
-    rb::TreeBufs tb = m_->bufs();
-    octInitRootKernel<<<1, 1, 0, s>>>(tb, m_->P[0].as<u64>(), n_), noteLaunch();
-    AOT_LAUNCH_CHECK();
-    // rebalanceBuild (octree.cu:159-180): at most maxDepth decision rounds
-    int done = 0;
-    const int maxRounds = int(cfg_.maxDepth);
-    while (done < maxRounds)
+    std::vector<long long> proposals;
+    lastBuildByLevels_ = buildMode_ == 0 && octreeLevelBuild(proposals);
+    size_t leaves = 0;
+    if (lastBuildByLevels_)
     {
-        const int batch = std::min(4, maxRounds - done);
-        for (int r = 0; r < batch; ++r) octreePass(true, (long long)physCap_);
+        leaves = hostLeaves_;
+    }
+    else
+    {
+        m_->history.reserve(std::max<size_t>(cfg_.maxDepth, 1) * sizeof(long long), cfg_.stream);
+        rb::TreeBufs tb = m_->bufs();
+        octInitRootKernel<<<1, 1, 0, s>>>(tb, m_->P[0].as<u64>(), n_), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        // rebalanceBuild (octree.cu:159-180): at most maxDepth decision rounds
+        int done = 0;
+        const int maxRounds = int(cfg_.maxDepth);
+        while (done < maxRounds)
+        {
+            const int batch = std::min(4, maxRounds - done);
+            for (int r = 0; r < batch; ++r) octreePass(true, (long long)physCap_);
+            AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
+            waitStream(s);
+            const DeviceState h = *m_->hst;
+            if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
+            done = h.rounds;
+            if (h.converged) break;
+            if (h.overflow)
+            {
+                const size_t need = size_t(h.proposal);
+                ensurePhysical(std::max(need + need / 4, 2 * physCap_));
+                clearOverflowKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
+                AOT_LAUNCH_CHECK();
+            }
+        }
         AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
         waitStream(s);
         const DeviceState h = *m_->hst;
-        if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
-        done = h.rounds;
-        if (h.converged) break;
-        if (h.overflow)
+        proposals.resize(size_t(h.iteration));
+        if (h.iteration)
+            AOT_CHECK(cudaMemcpy(proposals.data(), m_->history.p, proposals.size() * sizeof(long long),
+                                 cudaMemcpyDeviceToHost));
+        leaves = size_t(h.numLeaves);
+        // The final tree must sit in buffer 0 (finishBuildStateKernel resets the
+        // active buffer).
+        if (h.activeBuffer == 1)
         {
-            const size_t need = size_t(h.proposal);
-            ensurePhysical(std::max(need + need / 4, 2 * physCap_));
-            clearOverflowKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
-            AOT_LAUNCH_CHECK();
+            AOT_CHECK(cudaMemcpyAsync(m_->K[0].p, m_->K[1].p, (leaves + 1) * sizeof(u64), cudaMemcpyDeviceToDevice, s));
+            AOT_CHECK(cudaMemcpyAsync(m_->B[0].p, m_->B[1].p, (leaves + 1) * sizeof(u32), cudaMemcpyDeviceToDevice, s));
+            if (cfg_.nf)
+            {
+                AOT_CHECK(cudaMemcpyAsync(m_->NF[0].p, m_->NF[1].p, leaves * sizeof(u32), cudaMemcpyDeviceToDevice, s));
+                AOT_CHECK(cudaMemcpyAsync(m_->G[0].p, m_->G[1].p, leaves * sizeof(u8), cudaMemcpyDeviceToDevice, s));
+            }
         }
+        octFinishBuildKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
+        AOT_LAUNCH_CHECK();
     }
     mark(MarkPassed);
-    AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
-    waitStream(s);
-    const DeviceState h = *m_->hst;
-    buildRounds_ = h.iteration;
+    buildRounds_ = int(proposals.size());
+    hostLeaves_ = leaves;
     // Replay the reference's K_d/tmpTree capacity history (octree.cu:159-180,
     // 453-457; resizeWithHeadroom, helpers.cuh:122-141).
-    std::vector<long long> proposals(size_t(h.iteration));
-    if (h.iteration)
-        AOT_CHECK(cudaMemcpy(proposals.data(), m_->history.p, proposals.size() * sizeof(long long),
-                             cudaMemcpyDeviceToHost));
-    const size_t leaves = size_t(h.numLeaves);
-    hostLeaves_ = leaves;
     const size_t cap = capModel_.finishBuild(proposals.data(), proposals.size(), leaves);
-    // The final tree must sit in buffer 0 (finishBuildStateKernel resets the
-    // active buffer).
-    if (h.activeBuffer == 1)
-    {
-        AOT_CHECK(cudaMemcpyAsync(m_->K[0].p, m_->K[1].p, (leaves + 1) * sizeof(u64), cudaMemcpyDeviceToDevice, s));
-        AOT_CHECK(cudaMemcpyAsync(m_->B[0].p, m_->B[1].p, (leaves + 1) * sizeof(u32), cudaMemcpyDeviceToDevice, s));
-        if (cfg_.nf)
-        {
-            AOT_CHECK(cudaMemcpyAsync(m_->NF[0].p, m_->NF[1].p, leaves * sizeof(u32), cudaMemcpyDeviceToDevice, s));
-            AOT_CHECK(cudaMemcpyAsync(m_->G[0].p, m_->G[1].p, leaves * sizeof(u8), cudaMemcpyDeviceToDevice, s));
-        }
-    }
-    octFinishBuildKernel<<<1, 1, 0, s>>>(m_->st), noteLaunch();
-    AOT_LAUNCH_CHECK();
     prepareGraphBuffers(cap);
     built_ = true;
     materializeCounts();
     buildViews(cfg_.views);
     mark(MarkEnd);
     (void)doBuffersNeedResize();
+}
+
+void TreeEngine::setBuildMode(int mode)
+{
+    if (mode != 0 && mode != 1) throw std::invalid_argument("adaptive_octree: build mode must be 0 (levels) or 1 (rounds)");
+    buildMode_ = mode;
+}
+
+// The converged octree, level by level (levelbuild.cuh).  The tree is the
+// one the reference's build rounds converge to; the round history (leaves
+// after each round that changed the tree) comes from the per-region counts.
+bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
+{
+    if (!cfg_.nf && u64(cfg_.bucket) * 512u > 0xffffffffull) return false;  // wrapping split thresholds
+    cudaStream_t s = cfg_.stream;
+    Impl &m = *m_;
+    const bool nf = cfg_.nf;
+    const unsigned blocks = unsigned(smCount()) * 4u;
+    const KeyIndex idx = m.keyIndex(n_);
+    const u64 *P = m.P[0].as<u64>();
+    size_t cap = std::max<size_t>(m.lvCap, n_ / 4 + 4096);
+    constexpr size_t kHeadBytes = (sizeof(lb::Control) + 255) & ~size_t(255);
+    constexpr size_t kCtlBytes = kHeadBytes + (lb::kContribBins + lb::kArrivals) * sizeof(unsigned long long);
+    std::vector<unsigned char> host(kCtlBytes);
+    const lb::Control &hc = *reinterpret_cast<const lb::Control *>(host.data());
+    for (;;)
+    {
+        if (cap > 0xfffffff0ull) throw std::length_error("adaptive_octree: level build arena exceeds 32-bit indices");
+        m.lvRows.reserve(cap * lb::kRow * sizeof(u32), s);
+        if (nf) m.lvVal.reserve(cap * 8 * sizeof(u32), s);
+        m.lvChild.reserve(cap * 8 * sizeof(u32), s);
+        m.lvLeaves.reserve(cap * sizeof(u32), s);
+        m.lvOffset.reserve(cap * sizeof(u32), s);
+        const size_t scanWords = (cap + lb::kThreads - 1) / lb::kThreads + 64;
+        m.lvScan.reserve(scanWords * sizeof(u64), s);
+        m.lvCtl.reserve(kCtlBytes, s);
+        m.lvCap = cap;
+        lb::Arena a{};
+        a.rows = m.lvRows.as<u32>();
+        a.val = nf ? m.lvVal.as<u32>() : nullptr;
+        a.child = m.lvChild.as<u32>();
+        a.leaves = m.lvLeaves.as<u32>();
+        a.offset = m.lvOffset.as<u32>();
+        a.scan = m.lvScan.as<u64>();
+        a.ctl = m.lvCtl.as<lb::Control>();
+        a.contrib = reinterpret_cast<unsigned long long *>(m.lvCtl.as<unsigned char>() + kHeadBytes);
+        a.landed = a.contrib + lb::kContribBins;
+        a.cap = u32(cap);
+        AOT_CHECK(cudaMemsetAsync(m.lvCtl.p, 0, kCtlBytes, s));
+        AOT_CHECK(cudaMemsetAsync(m.lvScan.p, 0, scanWords * sizeof(u64), s));
+        const rb::NodeTable gt{m.nodeRows.as<u32>(), m.nodeSlots};
+        if (nf)
+        {
+            AOT_CHECK(cudaMemsetAsync(gt.rows, 0, size_t(gt.slots) * rb::kGroupRow * sizeof(u32), s));
+            ensureDigitPos();
+        }
+        m.nodeStale = true;  // the table holds this build's nodes only; an update refills it
+        lb::rootKernel<<<1, 1, 0, s>>>(a, m.bufs(), P, n_, cfg_.bucket, nf ? 1 : 0), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        int levels = 0;  // levels whose units have been classified
+        while (levels < int(kOctLevels))
+        {
+            const int stop = std::min(int(kOctLevels), levels + 4);
+            for (; levels < stop; ++levels)
+            {
+                const int l = levels;
+                if (nf) lb::expandKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
+                else lb::expandKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
+                if (nf)
+                {
+                    if (cfg_.hilbert)
+                        lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
+                    else
+                        lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
+                    lb::classifyKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
+                }
+                else
+                {
+                    lb::classifyKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
+                }
+                AOT_LAUNCH_CHECK();
+            }
+            AOT_CHECK(cudaMemcpyAsync(host.data(), m.lvCtl.p, sizeof(lb::Control), cudaMemcpyDeviceToHost, s));
+            waitStream(s);
+            if (hc.overflow || hc.late || hc.error || hc.levelCount[levels] == 0) break;
+        }
+        if (hc.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
+        if (hc.overflow)
+        {
+            cap *= 2;
+            continue;
+        }
+        if (hc.late) return false;
+        int deepest = -1;  // deepest level holding units
+        for (int l = 0; l < int(kOctLevels); ++l)
+            if (hc.levelCount[l]) deepest = l;
+        for (int l = deepest; l >= 0; --l) lb::leafCountKernel<<<blocks, lb::kThreads, 0, s>>>(a, l), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        u32 rootLeaves = 1;
+        if (deepest >= 0)
+            AOT_CHECK(cudaMemcpyAsync(&rootLeaves, a.leaves, sizeof(u32), cudaMemcpyDeviceToHost, s));
+        AOT_CHECK(cudaMemcpyAsync(host.data() + kHeadBytes, a.contrib,
+                                  (lb::kContribBins + lb::kArrivals) * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, s));
+        waitStream(s);
+        // leaves after every round that changed the tree
+        const auto *contrib = reinterpret_cast<const unsigned long long *>(host.data() + kHeadBytes);
+        const auto *landed = contrib + lb::kContribBins;
+        int rounds = 0;
+        for (int ai = 0; ai < lb::kArrivals; ++ai)
+            for (int k = 1; k < lb::kJumps; ++k)
+                for (int j = 1; j <= k; ++j)
+                    if (contrib[(ai * lb::kJumps + k) * lb::kJumps + j]) rounds = std::max(rounds, ai + 1 + (k - j));
+        if (rounds > int(cfg_.maxDepth)) return false;  // the rounds stop before converging
+        proposals.assign(size_t(rounds), 0);
+        for (int t = 1; t <= rounds; ++t)
+        {
+            unsigned long long leavesAt = landed[t];
+            for (int ai = 0; ai + 1 <= t && ai < lb::kArrivals; ++ai)
+                for (int k = 1; k < lb::kJumps; ++k)
+                    for (int j = 1; j <= k; ++j)
+                    {
+                        const unsigned long long c = contrib[(ai * lb::kJumps + k) * lb::kJumps + j];
+                        if (!c) continue;
+                        const int e = k - (t - ai - 1) - j;
+                        leavesAt += c << (3 * std::max(e, 0));
+                    }
+            proposals[size_t(t - 1)] = (long long)leavesAt;
+        }
+        if (rounds && proposals.back() != (long long)rootLeaves)
+            throw std::logic_error("adaptive_octree: level build history does not end at the tree");
+        hostLeaves_ = rootLeaves;
+        ensurePhysical(std::max<size_t>(physCap_, rootLeaves));
+        const rb::TreeBufs tb = m.bufs();
+        for (int l = 0; l <= deepest; ++l)
+        {
+            if (nf) lb::placeKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, tb, l), noteLaunch();
+            else lb::placeKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, tb, l), noteLaunch();
+        }
+        lb::finishKernel<<<1, 1, 0, s>>>(a, tb, rounds), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        if (nf) AOT_CHECK(cudaMemsetAsync(m.G[0].p, 0, m.G[0].bytes, s));  // no group of the converged tree may merge
+        return true;
+    }
 }
 
 void TreeEngine::binaryBuild()

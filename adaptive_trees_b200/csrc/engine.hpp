@@ -142,6 +142,12 @@ public:
     const EngineConfig &config() const { return cfg_; }
     // diagnostics: committed build rounds, physical leaf capacity
     int buildRounds() const { return buildRounds_; }
+    // How an octree build() reaches its tree: 0 (default) builds the
+    // converged tree level by level where that gives the rounds' result and
+    // falls back to the rounds otherwise; 1 always runs the rounds.
+    void setBuildMode(int mode);
+    // true when the last build() used the level-by-level builder
+    bool lastBuildByLevels() const { return lastBuildByLevels_; }
     size_t physicalCapacity() const { return physCap_; }
     // kernel launches issued by the engine in this process
     static unsigned long long kernelLaunches();
@@ -202,6 +208,8 @@ private:
     int hostActiveBuffer_ = 0;
     bool built_ = false;
     int buildRounds_ = 0;
+    int buildMode_ = 0;
+    bool lastBuildByLevels_ = false;
     // thrust capacity model of K_d / tmpTree (octree.cu:453-457)
     OctreeCapacity capModel_;  // reference K_d / tmpTree capacities (octree)
     adaptive_octree::ViewConfig prepared_{};
@@ -215,6 +223,11 @@ private:
     void markNearField(bool begin);
 
     void sortParticles();
+    // the converged octree by levels (levelbuild.cuh); false when the rounds
+    // must run instead (the tree would not converge within maxDepth rounds,
+    // or LeafCount thresholds wrap in 32 bits); fills the build's round
+    // proposals
+    bool octreeLevelBuild(std::vector<long long> &proposals);
     void sortKeys(int config);
     void octreeBuild();
     void binaryBuild();

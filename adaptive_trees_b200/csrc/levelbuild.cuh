@@ -1,0 +1,573 @@
+// levelbuild.cuh -- device kernels of the converged octree build.
+//
+// The reference builds an octree from the root by rounds of split/merge
+// decisions until a round changes nothing (rebalanceBuild, octree.cu:159-180;
+// calculateNodeOp, octree_rebalance.cuh:174-249).  The decision value of a
+// cell -- its particle count (LeafCount) or its near-field count NF = count x
+// population of the 27 periodic same-level cells around it (NFCount,
+// octree_rebalance.cuh:579-634) -- depends only on the particles, and it
+// never grows from a cell to its children.  So the tree the rounds converge
+// to is unique: a cell is an internal node exactly when its value exceeds the
+// bucket and its level is below 21.  This file builds that tree one level at
+// a time, without the rounds:
+//   expand    the internal cells ("units") of level l get the begin indices
+//             of their 8 children in the sorted keys (and, for NFCount, a row
+//             in the node table of the near-field lookups);
+//   nearField NFCount: the near-field counts of the children of the level-l
+//             units, one unit per parent cell as in the refresh of the
+//             rounds (octNearFieldKernel);
+//   classify  the children whose value exceeds the bucket become the units of
+//             level l + 1 (an order-preserving compaction with decoupled
+//             look-back); the others are leaves of the tree;
+//   leafCount, place: subtree leaf counts bottom-up, then every leaf's
+//             position in the cornerstone array top-down.
+//
+// The capacity the reference ends with depends on how many leaves each round
+// proposed (resizeWithHeadroom history, octree.cu:159-180 and 453-457).  That
+// history follows from the same cells: the rounds start at the root; a leaf
+// whose value exceeds the bucket splits in the next round by 1-4 levels at
+// once (the level jump of calculateNodeOp), and a group of 8 leaves whose
+// parent does not exceed it merges.  Call a cell reached by a split "landed"
+// and the levels a split spans its "region".  A landed cell arrives at round
+// a; if it is an internal node it splits at once, and its region's 8^k cells
+// arrive at round a + 1; every leaf f of the final tree in that region, at
+// relative depth j <= k, is then represented by its 8^(k-j) descendants at
+// the landing level, which merge up one level per round, so f stands for
+// 8^max(0, k - (t - a - 1) - j) leaves at round t >= a + 1.  The classify
+// kernel counts the final leaves per (a, k, j) and the landed internal nodes
+// per round; the host sums the leaf counts of every round from them.
+#pragma once
+
+#include "rebalance.cuh"
+
+namespace aot
+{
+namespace lb
+{
+constexpr int kThreads = 256;
+constexpr u32 kLeaf = 0xffffffffu;     // child slot: the child is a leaf
+constexpr int kArrivals = 32;          // arrival rounds tracked (>= kOctLevels + 2)
+constexpr int kJumps = 5;              // split depth k = 1..4
+constexpr int kContribBins = kArrivals * kJumps * kJumps;
+constexpr int kRow = rb::kGroupRow;    // unit row: key (2 words), 9 child begins, region word
+
+// Device control block of one build.
+struct Control
+{
+    u32 levelStart[kOctLevels + 2];
+    u32 levelCount[kOctLevels + 2];
+    u32 tileCounter[kOctLevels + 2];
+    int overflow;  // the unit arena is too small
+    int late;      // an arrival round beyond the tracked ones
+    int error;     // a bounded look-back gave up
+    int pad;
+};
+
+// The unit arena: units of all levels, level l at
+// [levelStart[l], levelStart[l] + levelCount[l]).
+struct Arena
+{
+    u32 *rows;       // [cap][kRow]
+    u32 *val;        // [cap][8] value of each child (NF or count)
+    u32 *child;      // [cap][8] unit index of an internal child, or kLeaf
+    u32 *leaves;     // [cap] leaves in the unit's subtree
+    u32 *offset;     // [cap] cornerstone index of the unit's first leaf
+    u64 *scan;       // look-back status of the classify tiles of every level
+    Control *ctl;
+    unsigned long long *contrib;  // [kArrivals][kJumps][kJumps] final leaves per (a, k, j)
+    unsigned long long *landed;   // [kArrivals] internal nodes landing in round t
+    u32 cap;
+};
+
+// Region word of a unit, describing the region its children belong to:
+// arrival round of the region's landed cell (8 bits), that cell's level
+// (5 bits) and the region's depth k (3 bits).
+__host__ __device__ __forceinline__ u32 regionWord(u32 a, u32 level, u32 k) { return a | (level << 8) | (k << 16); }
+__device__ __forceinline__ u32 regionArrival(u32 w) { return w & 0xffu; }
+__device__ __forceinline__ u32 regionLevel(u32 w) { return (w >> 8) & 0x1fu; }
+__device__ __forceinline__ u32 regionDepth(u32 w) { return (w >> 16) & 7u; }
+
+// Levels a leaf of value x at level m splits by (calculateNodeOp,
+// octree_rebalance.cuh:188-249: 8, 64, 512 or 4096 children), given that it
+// splits (x > bucket, m < 21).  LeafCount compares with 32-bit products of
+// the bucket, NFCount with 64-bit ones.
+__host__ __device__ __forceinline__ u32 splitDepth(bool nf, u32 x, u32 bucket, unsigned m)
+{
+    if (nf)
+    {
+        const u64 c = x, b = bucket;
+        if (c > b * 262144 && m + 3 < kOctLevels) return 4;
+        if (c > b * 4096 && m + 2 < kOctLevels) return 3;
+        if (c > b * 64 && m + 1 < kOctLevels) return 2;
+        return 1;
+    }
+    if (x > bucket * 512u && m + 3 < kOctLevels) return 4;
+    if (x > bucket * 64u && m + 2 < kOctLevels) return 3;
+    if (x > bucket * 8u && m + 1 < kOctLevels) return 2;
+    return 1;
+}
+
+__device__ __forceinline__ u64 rowKey(const u32 *row) { return (u64(row[1]) << 32) | row[0]; }
+
+// The root: a unit at level 0 when its value exceeds the bucket (NF of the
+// root: 27 x count^2, clamped, octree.cu:23-38), else the whole tree is the
+// root leaf, written straight to the cornerstone buffers.
+static __global__ void rootKernel(Arena a, rb::TreeBufs tb, const u64 *P, size_t n, unsigned bucket, int nf)
+{
+    DeviceState *st = tb.st;
+    const unsigned active = n ? unsigned(lowerBoundDev(P, n, kMaxKey)) : 0u;
+    const u64 sq = u64(active) * active;
+    const u32 nfRoot = sq > 0xffffffffull / 27ull ? 0xffffffffu : u32(27ull * sq);
+    const u32 x = nf ? nfRoot : active;
+    const int err = st->error;
+    *st = DeviceState{};
+    st->error = err;
+    st->numActiveParticles = active;
+    Control &c = *a.ctl;
+    c.levelStart[0] = 0;
+    if (x > bucket)
+    {
+        u32 *row = a.rows;
+        row[0] = 0;
+        row[1] = 0;
+        row[2] = 0;
+        row[10] = active;
+        row[11] = regionWord(0, 0, splitDepth(nf != 0, x, bucket, 0));
+        c.levelCount[0] = 1;
+        a.offset[0] = 0;
+        st->numLeaves = 0;  // set when the tree is placed
+    }
+    else
+    {
+        c.levelCount[0] = 0;
+        tb.K[0][0] = 0;
+        tb.K[0][1] = kMaxKey;
+        tb.B[0][0] = 0;
+        tb.B[0][1] = active;
+        tb.NF[0][0] = nf ? nfRoot : 0u;
+        st->numLeaves = 1;
+    }
+}
+
+// 9 child begins of the units of level l.  A unit with few keys is counted
+// by one lane; a unit with many is searched by the whole warp, each of its 9
+// boundaries by a group of 3 lanes (4-ary search).  NFCount also enters the
+// unit in the node table.
+template <bool NF>
+static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u64 *__restrict__ P, int l,
+                                                              rb::NodeTable gt)
+{
+    const Control &c = *a.ctl;
+    if (c.overflow | c.late | c.error) return;
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    const unsigned m = unsigned(l) + 1;
+    const u64 cr = octRange(m);
+    const int lane = threadIdx.x & 31;
+    const u32 warpsTotal = gridDim.x * (blockDim.x / 32);
+    const u32 w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    for (u32 base = w0 * 32; base < count; base += warpsTotal * 32)
+    {
+        const u32 g = start + base + u32(lane);
+        const bool valid = base + u32(lane) < count;
+        u32 *row = a.rows + size_t(valid ? g : start) * kRow;
+        const u64 key = valid ? rowKey(row) : 0;
+        const u32 lo = valid ? row[2] : 0, hi = valid ? row[10] : 0;
+        const bool wide = valid && hi - lo > rb::kNFScanMax;
+        u32 b[rb::kGroupBegins];
+        if (valid && !wide) rb::childBeginsWithin(P, lo, hi, key, m, b);
+        // wide units one after the other, by the whole warp
+        unsigned pending = __ballot_sync(0xffffffffu, wide);
+        while (pending)
+        {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const u64 k0 = __shfl_sync(0xffffffffu, key, src);
+            u32 slo = __shfl_sync(0xffffffffu, lo, src), shi = __shfl_sync(0xffffffffu, hi, src);
+            const int grp = lane / 3, sub = lane - grp * 3;
+            const u64 v = k0 + u64(grp < 9 ? grp : 8) * cr;
+            // 4-ary search of the first key >= v in [slo, shi]: the 3 lanes of
+            // a group test 3 pivots per step (lanes 27-31 follow group 8)
+            while (__any_sync(0xffffffffu, slo < shi))
+            {
+                const u32 len = shi - slo;
+                const u32 piv = slo + u32((u64(sub + 1) * len) / 4);
+                const bool less = slo < shi && piv < shi && __ldg(P + piv) < v;
+                const int gl = (lane / 3) * 3;
+                const bool l0 = __shfl_sync(0xffffffffu, less, gl < 32 ? gl : 31);
+                const bool l1 = __shfl_sync(0xffffffffu, less, gl + 1 < 32 ? gl + 1 : 31);
+                const bool l2 = __shfl_sync(0xffffffffu, less, gl + 2 < 32 ? gl + 2 : 31);
+                if (slo < shi && lane < 27)
+                {
+                    const u32 p0 = slo + u32(len / 4), p1 = slo + u32((2ull * len) / 4), p2 = slo + u32((3ull * len) / 4);
+                    if (l2) slo = p2 + 1;
+                    else if (l1)
+                    {
+                        slo = p1 + 1;
+                        shi = p2;
+                    }
+                    else if (l0)
+                    {
+                        slo = p0 + 1;
+                        shi = p1;
+                    }
+                    else
+                    {
+                        shi = p0;
+                    }
+                }
+                if (lane >= 27) slo = shi;
+            }
+            // lane 3d holds the boundary of digit d
+#pragma unroll
+            for (int d = 0; d < rb::kGroupBegins; ++d)
+            {
+                const u32 bd = __shfl_sync(0xffffffffu, slo, 3 * d);
+                if (lane == src) b[d] = bd;
+            }
+        }
+        if (valid)
+        {
+#pragma unroll
+            for (int d = 1; d < 8; ++d) row[2 + d] = b[d];
+            if constexpr (NF)
+            {
+                u32 *t = rb::nodeRow(gt, rb::cellCode(key, unsigned(l)));
+                if (t)
+                {
+#pragma unroll
+                    for (int d = 0; d < rb::kGroupBegins; ++d) t[d] = b[d];
+                }
+            }
+        }
+    }
+}
+
+// Near-field counts of the children of the level-l units: per unit, the 27
+// parent-level cells around it give the 4 x 4 x 4 block of child counts (from
+// the node table, or counted inside the leaf that holds them), and each child
+// sums its 3 x 3 x 3 sub-block (octNearFieldKernel, here with the units taken
+// from the arena instead of the leaves of a tree).
+template <bool Hilbert>
+static __global__ void __launch_bounds__(kThreads, 4)
+    nearFieldKernel(Arena a, KeyIndex idx, int l, HilbertTables h, rb::NodeTable gt)
+{
+    using rb::kUnitBatch;
+    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
+    __shared__ rb::UnitScratch sWarp[kThreads / 32];
+    const Control &c = *a.ctl;
+    if (c.overflow | c.late | c.error) return;
+    if constexpr (Hilbert)
+    {
+        for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
+        {
+            sEnc[k] = h.enc[k];
+            sNext[k] = h.encNext[k];
+            sDec[k] = h.decOct[k];
+        }
+    }
+    __syncthreads();
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    const unsigned m = unsigned(l) + 1;
+    rb::UnitScratch &w = sWarp[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const unsigned ltMask = (1u << lane) - 1u;
+    const u32 warpsTotal = gridDim.x * (blockDim.x / 32);
+    const u32 w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    for (u32 base = w0 * kUnitBatch; base < count; base += warpsTotal * kUnitBatch)
+    {
+        const int nb = int(min(u32(kUnitBatch), count - base));
+        if (lane < nb)
+        {
+            const u32 *row = a.rows + size_t(start + base + u32(lane)) * kRow;
+            const u64 key = rowKey(row);
+            const rb::CellPath path = rb::decodeCell<Hilbert>(key, unsigned(l), sNext, sDec);
+            w.active[lane] = 1;
+            w.pStart[lane] = key;
+            w.level[lane] = int(m);
+            w.cx[lane] = path.x;
+            w.cy[lane] = path.y;
+            w.cz[lane] = path.z;
+            w.st0[lane] = path.st0;
+            w.st1[lane] = path.st1;
+            w.st2[lane] = path.st2;
+            w.childState[lane] = path.childState;
+            w.hintB[lane] = row[2];
+        }
+        if (lane == 0) w.nSlow = 0;
+        __syncwarp();
+        // phase A: (unit, Q) pairs over the lanes, internal Q from the table
+        const int items = nb * 27;
+        for (int ib = 0; ib < items; ib += 32)
+        {
+            const int it = ib + lane;
+            const int u = it / 27, q = it - (it / 27) * 27;
+            bool slow = false;
+            u64 qKey = 0;
+            int qState = 0;
+            if (it < items)
+            {
+                qKey = rb::neighbourCell<Hilbert>(w, u, q, qState, sEnc, sNext);
+                u32 gb[rb::kGroupBegins];
+                if (rb::nodeBegins(gt, rb::cellCode(qKey, unsigned(l)), gb))
+                {
+                    rb::childrenFromPacked<Hilbert>(gb, q, qState, w.block[u]);
+                }
+                else
+                {
+                    slow = true;
+                }
+            }
+            const unsigned slowMask = __ballot_sync(0xffffffffu, slow);
+            if (slow)
+            {
+                const int k = w.nSlow + __popc(slowMask & ltMask);
+                w.slowKey[k] = qKey;
+                w.slowItem[k] = (unsigned short)it;
+                w.slowState[k] = (unsigned char)qState;
+            }
+            __syncwarp();
+            if (lane == 0) w.nSlow += __popc(slowMask);
+            __syncwarp();
+        }
+        // phase B: Q that are no internal node, counted inside their leaf
+        const int nSlow = w.nSlow;
+        for (int k = lane; k < nSlow; k += 32)
+        {
+            const int it = w.slowItem[k];
+            const int u = it / 27, q = it - u * 27;
+            const u64 qKey = w.slowKey[k];
+            const int qState = int(w.slowState[k]);
+            u32 begins[rb::kGroupBegins];
+            if (!rb::beginsInside(gt, idx.keys, u32(idx.n), qKey, m, begins))
+            {
+                const u32 lo = idx.lowerNear<rb::kNFGallop>(w.hintB[u], qKey);
+                const u32 hi = rb::lowerFrom(idx, lo, qKey + octRange(m - 1));
+                rb::childBeginsWithin(idx.keys, lo, hi, qKey, m, begins);
+            }
+            rb::childrenFromPacked<Hilbert>(begins, q, qState, w.block[u]);
+        }
+        __syncwarp();
+        // phase C: the 8 children of each unit, two per lane
+        for (int e = lane; e < nb * 8; e += 32)
+        {
+            const int u = e >> 3, d = e & 7;
+            const u32 g = start + base + u32(u);
+            const u32 *row = a.rows + size_t(g) * kRow;
+            const u32 cnt = row[2 + d + 1] - row[2 + d];
+            u32 out = 0;
+            if (cnt)
+            {
+                const unsigned o = Hilbert ? unsigned(sDec[w.childState[u] * 8 + d]) : unsigned(d);
+                const u32 *sub = w.block[u] + (o >> 2) * 16 + ((o >> 1) & 1u) * 4 + (o & 1u);
+                u64 pop = 0;
+                if (m > 1)
+                {
+                    u32 p32 = 0;
+#pragma unroll
+                    for (int x = 0; x < 3; ++x)
+#pragma unroll
+                        for (int y = 0; y < 3; ++y)
+#pragma unroll
+                            for (int z = 0; z < 3; ++z) p32 += sub[x * 16 + y * 4 + z];
+                    pop = p32;
+                }
+                else
+                {
+                    // level 1: the periodic wrap repeats cells, the sum may exceed 2^32
+                    for (int x = 0; x < 3; ++x)
+                        for (int y = 0; y < 3; ++y)
+                            for (int z = 0; z < 3; ++z) pop += sub[x * 16 + y * 4 + z];
+                }
+                const u64 v = u64(cnt) * pop;
+                out = v > 0xffffffffull ? 0xffffffffu : u32(v);
+            }
+            a.val[size_t(g) * 8 + d] = out;
+        }
+        __syncwarp();
+    }
+}
+
+// Children of the level-l units: those whose value exceeds the bucket (below
+// level 21) become the units of level l + 1, in key order; the others are
+// leaves, counted into the round history by (arrival, depth, relative level).
+template <bool NF>
+static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l, unsigned bucket)
+{
+    __shared__ i64 sWarp[kThreads / 32];
+    __shared__ u32 sTile;
+    __shared__ i64 sPrefix;
+    __shared__ u32 sContrib[kContribBins];
+    __shared__ u32 sLanded[kArrivals];
+    Control &c = *a.ctl;
+    if (c.overflow | c.late | c.error) return;
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    const u32 next = start + count;
+    const unsigned m = unsigned(l) + 1;
+    const u64 cr = octRange(m);
+    const u32 numTiles = (count + kThreads - 1) / kThreads;
+    u64 *status = a.scan + (start + kThreads - 1) / kThreads + u32(l);
+    for (int k = threadIdx.x; k < kContribBins; k += kThreads) sContrib[k] = 0;
+    if (threadIdx.x < kArrivals) sLanded[threadIdx.x] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) c.levelStart[l + 1] = next;
+    for (;;)
+    {
+        __syncthreads();
+        if (threadIdx.x == 0) sTile = atomicAdd(&c.tileCounter[l], 1u);
+        __syncthreads();
+        const u32 tile = sTile;
+        if (tile >= numTiles) break;
+        const u32 i = tile * kThreads + threadIdx.x;
+        const bool valid = i < count;
+        const u32 g = start + (valid ? i : 0);
+        const u32 *row = a.rows + size_t(g) * kRow;
+        u32 b[rb::kGroupBegins], x[8];
+        u32 reg = 0;
+        u64 key = 0;
+        unsigned highMask = 0;
+        if (valid)
+        {
+            key = rowKey(row);
+#pragma unroll
+            for (int d = 0; d < rb::kGroupBegins; ++d) b[d] = row[2 + d];
+            reg = row[11];
+#pragma unroll
+            for (int d = 0; d < 8; ++d)
+            {
+                x[d] = NF ? a.val[size_t(g) * 8 + d] : b[d + 1] - b[d];
+                if (x[d] > bucket && m < kOctLevels) highMask |= 1u << d;
+            }
+        }
+        i64 total;
+        const i64 excl = rb::blockExclusiveScan(i64(__popc(highMask)), sWarp, total);
+        if (threadIdx.x == 0) sPrefix = rb::lookback(status, tile, total, &c.error);
+        __syncthreads();
+        if (valid)
+        {
+            const u32 aR = regionArrival(reg), lR = regionLevel(reg), kR = regionDepth(reg);
+            const u32 j = m - lR;  // 1 <= j <= kR
+            u32 rank = u32(sPrefix + excl);
+#pragma unroll
+            for (int d = 0; d < 8; ++d)
+            {
+                u32 slot = kLeaf;
+                if (highMask & (1u << d))
+                {
+                    const u32 gc = next + rank++;
+                    if (gc < a.cap)
+                    {
+                        u32 creg = reg;
+                        if (j == kR)
+                        {
+                            // a landed internal node: a leaf in round aR + 1, splitting at once
+                            creg = regionWord(aR + 1, m, splitDepth(NF, x[d], bucket, m));
+                            if (aR + 2 < u32(kArrivals)) atomicAdd(&sLanded[aR + 1], 1u);
+                            else c.late = 1;
+                        }
+                        u32 *crow = a.rows + size_t(gc) * kRow;
+                        const u64 ck = key + u64(d) * cr;
+                        crow[0] = u32(ck);
+                        crow[1] = u32(ck >> 32);
+                        crow[2] = b[d];
+                        crow[10] = b[d + 1];
+                        crow[11] = creg;
+                        slot = gc;
+                    }
+                    else
+                    {
+                        c.overflow = 1;
+                    }
+                }
+                else
+                {
+                    atomicAdd(&sContrib[(aR * kJumps + kR) * kJumps + j], 1u);
+                }
+                a.child[size_t(g) * 8 + d] = slot;
+            }
+        }
+        if (tile == numTiles - 1 && threadIdx.x == kThreads - 1) c.levelCount[l + 1] = u32(sPrefix + excl) + u32(__popc(highMask));
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kContribBins; k += kThreads)
+        if (sContrib[k]) atomicAdd(a.contrib + k, (unsigned long long)sContrib[k]);
+    if (threadIdx.x < kArrivals && sLanded[threadIdx.x])
+        atomicAdd(a.landed + threadIdx.x, (unsigned long long)sLanded[threadIdx.x]);
+}
+
+// Leaves below each unit of level l (the units of level l + 1 are done).
+static __global__ void leafCountKernel(Arena a, int l)
+{
+    const Control &c = *a.ctl;
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    {
+        const u32 g = start + i;
+        u32 s = 0;
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
+        {
+            const u32 ch = a.child[size_t(g) * 8 + d];
+            s += ch == kLeaf ? 1u : a.leaves[ch];
+        }
+        a.leaves[g] = s;
+    }
+}
+
+// Cornerstone entries of the leaf children of the level-l units, and the
+// first leaf index of their internal children.
+template <bool NF>
+static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l)
+{
+    const Control &c = *a.ctl;
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    const u64 cr = octRange(unsigned(l) + 1);
+    u64 *K = tb.K[0];
+    u32 *B = tb.B[0];
+    u32 *NFo = tb.NF[0];
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    {
+        const u32 g = start + i;
+        const u32 *row = a.rows + size_t(g) * kRow;
+        const u64 key = rowKey(row);
+        u32 o = a.offset[g];
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
+        {
+            const u32 ch = a.child[size_t(g) * 8 + d];
+            if (ch == kLeaf)
+            {
+                K[o] = key + u64(d) * cr;
+                B[o] = row[2 + d];
+                if constexpr (NF) NFo[o] = a.val[size_t(g) * 8 + d];
+                ++o;
+            }
+            else
+            {
+                a.offset[ch] = o;
+                o += a.leaves[ch];
+            }
+        }
+    }
+}
+
+// The finished tree: sentinel boundary and the state of a converged build
+// (finishBuildStateKernel, octree.cu:40-47, after `rounds` changing rounds).
+static __global__ void finishKernel(Arena a, rb::TreeBufs tb, int rounds)
+{
+    DeviceState *st = tb.st;
+    const Control &c = *a.ctl;
+    const int leaves = c.levelCount[0] ? int(a.leaves[0]) : 1;
+    tb.K[0][leaves] = kMaxKey;
+    tb.B[0][leaves] = st->numActiveParticles;
+    st->numLeaves = leaves;
+    st->newNumLeaves = leaves;
+    st->proposal = leaves;
+    st->iteration = rounds;
+    st->rounds = rounds + 1;
+    st->changed = st->converged = st->needsResize = 0;
+    st->numNodes = 0;
+    st->activeBuffer = 0;
+    st->overflow = 0;
+    st->dirtyCount = 0;
+}
+}  // namespace lb
+}  // namespace aot

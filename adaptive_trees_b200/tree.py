@@ -160,6 +160,17 @@ class Tree:
         C.check(C.load().ao_tree_update_until_converged(self._h, int(max_passes), ctypes.byref(out)))
         return out.value
 
+    def setBuildMode(self, mode: int):
+        """Octree build() path: 0 the converged tree level by level (falling
+        back to rounds where needed), 1 the reference's split/merge rounds."""
+        C.check(C.load().ao_tree_set_build_mode(self._h, int(mode)))
+
+    def buildPath(self):
+        """(built by levels, build rounds that changed the tree) of the last build()."""
+        lv, rounds = ctypes.c_int(), ctypes.c_int()
+        C.check(C.load().ao_tree_build_path(self._h, ctypes.byref(lv), ctypes.byref(rounds)))
+        return bool(lv.value), rounds.value
+
     def setProfiling(self, on: bool = True):
         """Stage timing of octree build() and update() with CUDA events and
         NVTX ranges (the reference's ADAPTIVE_OCTREE_PROFILING ranges,

@@ -141,6 +141,21 @@ AO_API ao_status ao_tree_set_profiling(ao_tree *tree, int on);
 /* Waits for the last profiled build() or update() and reads its stage times. */
 AO_API ao_status ao_tree_stage_times(ao_tree *tree, ao_stage_times *out);
 
+/* How an octree build() reaches its tree (no counterpart in the reference,
+ * whose build runs split/merge rounds until one changes nothing,
+ * octree.cu:159-180).  Mode 0 (default) builds the converged tree directly,
+ * one level of internal nodes at a time, and derives from the same cells how
+ * many leaves each of the reference's rounds would have held (the capacity
+ * history behind leafCapacity); it falls back to the rounds when the tree
+ * would not converge within max_depth rounds or when LeafCount's 32-bit split
+ * thresholds wrap (bucket >= 2^23).  Mode 1 always runs the rounds.  Both
+ * give the same tree, counts and capacity.  Binary trees always run rounds. */
+AO_API ao_status ao_tree_set_build_mode(ao_tree *tree, int mode);
+/* The last build(): *by_levels = 1 when it used the level builder; *rounds =
+ * the build rounds that changed the tree (the reference's history length).
+ * Either pointer may be NULL. */
+AO_API ao_status ao_tree_build_path(ao_tree *tree, int *by_levels, int *rounds);
+
 /* Opt-in extension with no reference counterpart: update() that keeps
  * passing until a pass changes nothing or would exceed the leaf capacity
  * (then doBuffersNeedResize() reports it, as after update()), at most
