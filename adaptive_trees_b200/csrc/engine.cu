@@ -1539,10 +1539,12 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
                 else lb::expandKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
                 if (nf)
                 {
+                    markNearField(true);
                     if (cfg_.hilbert)
                         lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
                     else
                         lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
+                    markNearField(false);
                     lb::classifyKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
                 }
                 else
