@@ -149,10 +149,15 @@ static __global__ void rootKernel(Arena a, rb::TreeBufs tb, const u64 *P, size_t
     }
 }
 
-// 9 child begins of the units of level l.  A unit with few keys is counted
-// by one lane; a unit with many is searched by the whole warp, each of its 9
+// 9 child begins of the units of level l, one warp per unit.  A unit with
+// few keys is read by the warp 32 keys at a time (coalesced): a key whose
+// child digit differs from the previous key's begins that child and every
+// empty child before it, and the children after the last key begin at the
+// unit's end.  A unit with many keys is searched instead, each of its 9
 // boundaries by a group of 3 lanes (4-ary search).  NFCount also enters the
 // unit in the node table.
+constexpr u32 kExpandScanMax = 1024;  // keys scanned per unit; more are searched
+
 template <bool NF>
 static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u64 *__restrict__ P, int l,
                                                               rb::NodeTable gt)
@@ -161,44 +166,55 @@ static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u
     if (c.overflow | c.late | c.error) return;
     const u32 start = c.levelStart[l], count = c.levelCount[l];
     const unsigned m = unsigned(l) + 1;
+    const unsigned shift = 3u * (kOctLevels - m);
     const u64 cr = octRange(m);
     const int lane = threadIdx.x & 31;
     const u32 warpsTotal = gridDim.x * (blockDim.x / 32);
-    const u32 w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    for (u32 base = w0 * 32; base < count; base += warpsTotal * 32)
+    for (u32 i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); i < count; i += warpsTotal)
     {
-        const u32 g = start + base + u32(lane);
-        const bool valid = base + u32(lane) < count;
-        u32 *row = a.rows + size_t(valid ? g : start) * kRow;
-        const u64 key = valid ? rowKey(row) : 0;
-        const u32 lo = valid ? row[2] : 0, hi = valid ? row[10] : 0;
-        const bool wide = valid && hi - lo > rb::kNFScanMax;
-        u32 b[rb::kGroupBegins];
-        if (valid && !wide) rb::childBeginsWithin(P, lo, hi, key, m, b);
-        // wide units one after the other, by the whole warp
-        unsigned pending = __ballot_sync(0xffffffffu, wide);
-        while (pending)
+        u32 *row = a.rows + size_t(start + i) * kRow;
+        const u64 key = rowKey(row);
+        const u32 lo = row[2], hi = row[10];
+        if (hi - lo <= kExpandScanMax)
         {
-            const int src = __ffs(pending) - 1;
-            pending &= pending - 1;
-            const u64 k0 = __shfl_sync(0xffffffffu, key, src);
-            u32 slo = __shfl_sync(0xffffffffu, lo, src), shi = __shfl_sync(0xffffffffu, hi, src);
-            const int grp = lane / 3, sub = lane - grp * 3;
-            const u64 v = k0 + u64(grp < 9 ? grp : 8) * cr;
+            int prev = -1;  // child digit of the key before the current chunk
+            for (u32 off = lo; off < hi; off += 32)
+            {
+                const u32 idx = off + u32(lane);
+                const int dig = idx < hi ? int((__ldg(P + idx) >> shift) & 7u) : 8;
+                int before = __shfl_up_sync(0xffffffffu, dig, 1);
+                if (lane == 0) before = prev;
+                if (idx < hi)
+                    for (int d = before + 1; d <= dig; ++d) row[2 + d] = idx;
+                prev = __shfl_sync(0xffffffffu, dig, 31);
+                if (prev == 8)  // the chunk ran past the end: the last key's digit
+                {
+                    const unsigned inRange = __ballot_sync(0xffffffffu, idx < hi);
+                    prev = __shfl_sync(0xffffffffu, dig, 31 - __clz(inRange));
+                }
+            }
+            if (lane == 0)
+                for (int d = prev + 1; d < 8; ++d) row[2 + d] = hi;
+        }
+        else
+        {
             // 4-ary search of the first key >= v in [slo, shi]: the 3 lanes of
-            // a group test 3 pivots per step (lanes 27-31 follow group 8)
+            // a group test 3 pivots per step (lanes 27-31 idle)
+            const int grp = lane / 3, sub = lane - grp * 3;
+            const u64 v = key + u64(grp < 9 ? grp : 8) * cr;
+            u32 slo = lane < 27 ? lo : hi, shi = hi;
             while (__any_sync(0xffffffffu, slo < shi))
             {
                 const u32 len = shi - slo;
                 const u32 piv = slo + u32((u64(sub + 1) * len) / 4);
                 const bool less = slo < shi && piv < shi && __ldg(P + piv) < v;
-                const int gl = (lane / 3) * 3;
+                const int gl = grp * 3;
                 const bool l0 = __shfl_sync(0xffffffffu, less, gl < 32 ? gl : 31);
                 const bool l1 = __shfl_sync(0xffffffffu, less, gl + 1 < 32 ? gl + 1 : 31);
                 const bool l2 = __shfl_sync(0xffffffffu, less, gl + 2 < 32 ? gl + 2 : 31);
-                if (slo < shi && lane < 27)
+                if (slo < shi)
                 {
-                    const u32 p0 = slo + u32(len / 4), p1 = slo + u32((2ull * len) / 4), p2 = slo + u32((3ull * len) / 4);
+                    const u32 p0 = slo + len / 4, p1 = slo + u32((2ull * len) / 4), p2 = slo + u32((3ull * len) / 4);
                     if (l2) slo = p2 + 1;
                     else if (l1)
                     {
@@ -215,30 +231,24 @@ static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u
                         shi = p0;
                     }
                 }
-                if (lane >= 27) slo = shi;
             }
             // lane 3d holds the boundary of digit d
-#pragma unroll
-            for (int d = 0; d < rb::kGroupBegins; ++d)
-            {
-                const u32 bd = __shfl_sync(0xffffffffu, slo, 3 * d);
-                if (lane == src) b[d] = bd;
-            }
+            if (lane < 27 && sub == 0 && grp >= 1 && grp <= 7) row[2 + grp] = slo;
         }
-        if (valid)
+        __syncwarp();
+        if constexpr (NF)
         {
-#pragma unroll
-            for (int d = 1; d < 8; ++d) row[2 + d] = b[d];
-            if constexpr (NF)
+            if (lane == 0)
             {
                 u32 *t = rb::nodeRow(gt, rb::cellCode(key, unsigned(l)));
                 if (t)
                 {
 #pragma unroll
-                    for (int d = 0; d < rb::kGroupBegins; ++d) t[d] = b[d];
+                    for (int d = 0; d < rb::kGroupBegins; ++d) t[d] = row[2 + d];
                 }
             }
         }
+        __syncwarp();
     }
 }
 

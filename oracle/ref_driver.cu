@@ -23,9 +23,12 @@
 //   build_ms (median of `reps` later builds of the same tree, its buffers
 //   already grown), update_ms (median of captured-graph replays of update()
 //   over frame 1).
+// `ref_driver --cub-sort keys.bin reps` instead times cub::DeviceRadixSort::
+// SortPairs on the keys of keys.bin, the sort the reference's build calls.
 #include <cuda_runtime.h>
 #include <thrust/device_vector.h>
 #include <thrust/host_vector.h>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <chrono>
@@ -247,8 +250,65 @@ int run(const Header &h, const std::vector<char> &payload, const char *outPath)
 }
 }  // namespace
 
+// CUB's pair sort, as the reference calls it (octree.cu:301-304: 64-bit keys
+// carrying 32-bit indices over bits [0, 64)), timed on the keys of `path`
+// (u64 count, then the keys): prints {"cub_sort_ms": median, ...}.
+int cubSort(const char *path, int reps)
+{
+    std::ifstream in(path, std::ios::binary);
+    std::uint64_t n = 0;
+    in.read(reinterpret_cast<char *>(&n), 8);
+    std::vector<unsigned long long> keys(n);
+    in.read(reinterpret_cast<char *>(keys.data()), std::streamsize(n * 8));
+    if (!in) throw std::runtime_error("short key file");
+    std::vector<unsigned> iota(n);
+    for (std::uint64_t i = 0; i < n; ++i) iota[i] = unsigned(i);
+    thrust::device_vector<unsigned long long> kin(keys.begin(), keys.end()), kout(n);
+    thrust::device_vector<unsigned> vin(iota.begin(), iota.end()), vout(n);
+    size_t tempBytes = 0;
+    check(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, thrust::raw_pointer_cast(kin.data()),
+                                          thrust::raw_pointer_cast(kout.data()), thrust::raw_pointer_cast(vin.data()),
+                                          thrust::raw_pointer_cast(vout.data()), n, 0, 64),
+          "sort size");
+    thrust::device_vector<unsigned char> temp(tempBytes);
+    cudaEvent_t a, b;
+    check(cudaEventCreate(&a), "ev");
+    check(cudaEventCreate(&b), "ev");
+    std::vector<double> ms;
+    for (int r = 0; r < reps + 3; ++r)
+    {
+        check(cudaEventRecord(a), "rec");
+        check(cub::DeviceRadixSort::SortPairs(thrust::raw_pointer_cast(temp.data()), tempBytes,
+                                              thrust::raw_pointer_cast(kin.data()), thrust::raw_pointer_cast(kout.data()),
+                                              thrust::raw_pointer_cast(vin.data()), thrust::raw_pointer_cast(vout.data()),
+                                              n, 0, 64),
+              "sort");
+        check(cudaEventRecord(b), "rec");
+        check(cudaEventSynchronize(b), "sync");
+        float t = 0;
+        check(cudaEventElapsedTime(&t, a, b), "elapsed");
+        if (r >= 3) ms.push_back(t);
+    }
+    std::sort(ms.begin(), ms.end());
+    std::printf("{\"cub_sort_ms\": %.6f, \"cub_sort_min_ms\": %.6f, \"n\": %llu, \"reps\": %d}\n", ms[ms.size() / 2],
+                ms.front(), (unsigned long long)n, reps);
+    return 0;
+}
+
 int main(int argc, char **argv)
 {
+    if (argc == 4 && std::strcmp(argv[1], "--cub-sort") == 0)
+    {
+        try
+        {
+            return cubSort(argv[2], std::atoi(argv[3]));
+        }
+        catch (const std::exception &e)
+        {
+            std::fprintf(stderr, "ref_driver: %s\n", e.what());
+            return 1;
+        }
+    }
     if (argc < 3 || (argc > 3 && std::strcmp(argv[3], "--digest") != 0))
     {
         std::fprintf(stderr, "usage: ref_driver scenario.bin out.bin [--digest]\n");

@@ -113,3 +113,17 @@ def time_reference(kind, frames, reps=10, timeout=1800, **cfg):
         if r.returncode != 0:
             raise RuntimeError(f"ref_driver failed ({r.returncode}): {r.stderr.strip()}")
         return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def time_cub_sort(keys, reps=10, timeout=600):
+    """CUB's SortPairs (64-bit keys carrying 32-bit indices, bits [0, 64), the
+    reference's particle sort) on `keys` (numpy uint64) on this GPU: median ms."""
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "keys.bin")
+        with open(path, "wb") as f:
+            f.write(np.uint64(keys.size).tobytes())
+            f.write(np.ascontiguousarray(keys, dtype=np.uint64).tobytes())
+        r = subprocess.run([DRIVER, "--cub-sort", path, str(reps)], capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_driver failed ({r.returncode}): {r.stderr.strip()}")
+        return json.loads(r.stdout.strip().splitlines()[-1])
