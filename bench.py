@@ -14,7 +14,13 @@ the slowest rank's time.
 Prints one JSON line (rank 0).  --impl reference times the CPU oracle port of
 the reference algorithm on a bounded sample (the reference has no CPU
 implementation of this path); the reference library's own GPU time on this
-box is reported by the default run under "reference_gpu".
+box is reported by the default run under "reference_gpu", CUB's pair sort on
+the same keys under "roofline_sort", and bit-exact parity of the timed tree
+with the reference library under "parity".  A single-GPU default run then
+adds the metric's other configurations under "configs": c1 (2^20 uniform fp64
+LeafCount octree), c3 (8Mi binary k-d tree), c4 (512 batched octrees against
+a per-tree loop) and c5 (serving, --c5-seconds of requests), each with its
+own clock record (--no-extras skips them).
 """
 from __future__ import annotations
 
@@ -315,10 +321,21 @@ def mixture(n, seed, clusters=8):
 
 
 def single_config_bench(args):
+    """C1 / C3 as their own line."""
+    line = single_config_record(args.config, args.steps, args.warmup, args.cpu_sample, not args.no_cpu_baseline,
+                                not args.no_reference_gpu)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def single_config_record(config, steps, warmup, cpu_sample, cpu_baseline=True, reference_gpu=True):
     """C1 / C3: one tree of the configuration, next to the reference library on the same GPU."""
     import torch
 
     import adaptive_trees_b200 as ab
+    from types import SimpleNamespace
+    args = SimpleNamespace(config=config, steps=steps, warmup=warmup, cpu_sample=cpu_sample,
+                           no_cpu_baseline=not cpu_baseline, no_reference_gpu=not reference_gpu)
     spec = SINGLE_CONFIGS[args.config]
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
@@ -428,8 +445,8 @@ def single_config_bench(args):
                                          "what": "reference library compiled for sm_100a, same inputs and GPU"}
         except Exception as e:  # informational
             line["reference_gpu"] = {"error": str(e)[:200]}
-    print(json.dumps(line), flush=True)
-    return 0
+    tree.close()
+    return line
 
 
 C4_SYSTEMS = 512
@@ -447,12 +464,24 @@ def c4_systems():
 
 
 def batched_bench(args):
-    """C4: Batch (one set of launches for all systems) against a loop of plain trees."""
+    """C4 as its own line (every rank; rank 0 prints)."""
+    line, same = batched_record(args.steps, args.warmup)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0 if same else 1
+
+
+def batched_record(steps, warmup, distributed=True):
+    """C4: Batch (one set of launches for all systems) against a loop of plain trees.
+
+    Returns (line or None on ranks other than 0, identical outputs)."""
     import torch
     import torch.distributed as dist
 
     import adaptive_trees_b200 as ab
-    world, rank, local = rank_env()
+    from types import SimpleNamespace
+    args = SimpleNamespace(steps=steps, warmup=warmup)
+    world, rank, local = rank_env() if distributed else (1, 0, 0)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
@@ -511,6 +540,8 @@ def batched_bench(args):
             for t in trees:
                 t.build()
         l0 = launches()
+        clocks = ClockSampler(local)
+        clocks.__enter__()
         b_build = [timed(batch.build) for _ in range(args.steps)]
         batch_launches = launches() - l0
 
@@ -556,8 +587,11 @@ def batched_bench(args):
                 del graph
                 graph = capture()
             same = same and identical(batch, trees)
+        clocks.__exit__(None, None, None)
         del graph
         batch.close()
+        for t in trees:
+            t.close()
     bb = max_over_ranks(statistics.median(b_build), world, dev)
     pb = max_over_ranks(statistics.median(p_build), world, dev)
     bu = max_over_ranks(statistics.median(b_upd), world, dev)
@@ -567,7 +601,7 @@ def batched_bench(args):
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
-        return 0 if same else 1
+        return None, same
     line = {"metric": C4_METRIC, "value": job_rate(total_all, bb), "unit": "particles/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": bb, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
@@ -580,19 +614,28 @@ def batched_bench(args):
                         "build_launches": batch_launches // max(1, args.steps)},
             "plain_loop": {"build_ms": pb, "update_ms": pu, "build_value": job_rate(total_all, pb),
                            "update_value": job_rate(total_all, pu)},
-            "speedup": {"build": pb / bb, "update": pu / bu}, "identical_outputs": bool(same), "resizes": resizes}
-    print(json.dumps(line), flush=True)
-    return 0 if same else 1
+            "speedup": {"build": pb / bb, "update": pu / bu}, "identical_outputs": bool(same), "resizes": resizes,
+            "clocks": clocks.summary()}
+    return line, same
 
 
 C5_METRIC = "particles/s served (Poisson 2000 req/s, 30% builds / 70% updates, 120 GB budget)"
 
 
 def serving_bench(args):
+    """C5 as its own line."""
+    line = serving_record(args.duration, args.warm_seconds, args.slots, args.live_trees)
+    print(json.dumps(line), flush=True)
+    return 0 if not line["requests"]["failed"] else 1
+
+
+def serving_record(duration, warm_seconds, slots, live_trees):
     """C5: a Server fed by an open-loop Poisson client; latency from submit to result."""
     import torch
 
     import adaptive_trees_b200 as ab
+    from types import SimpleNamespace
+    args = SimpleNamespace(duration=duration, warm_seconds=warm_seconds, slots=slots, live_trees=live_trees)
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
     rate, budget, max_n = 2000.0, 120 << 30, 4_000_000
@@ -702,8 +745,10 @@ def serving_bench(args):
             "host_cpus": os.cpu_count(),
             "offered_particles_per_s": offered / args.duration, "span_s": st["span_s"],
             "peak_bytes": st["peak_bytes"], "clocks": clocks.summary()}
-    print(json.dumps(line), flush=True)
-    return 0 if not failed else 1
+    if args.duration < 60:
+        line["config"]["window_note"] = (f"{args.duration:g} s of requests, shorter than the configured 60 s, "
+                                         "to keep the default benchmark run within minutes")
+    return line
 
 
 def reference_parity(tree, xs, frames, stream):
@@ -777,8 +822,11 @@ def main():
                          "c5: serving under a Poisson request stream")
     ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of requests")
     ap.add_argument("--warm-seconds", type=float, default=2.0, help="c5: seconds of untimed requests first")
-    ap.add_argument("--slots", type=int, default=8, help="c5: server worker threads")
+    ap.add_argument("--slots", type=int, default=32, help="c5: server worker threads")
     ap.add_argument("--live-trees", type=int, default=256, help="c5: resident trees the client keeps")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default run: skip the c1/c3/c4/c5 records that follow the headline")
+    ap.add_argument("--c5-seconds", type=float, default=20.0, help="default run: seconds of the c5 record")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -933,8 +981,9 @@ def main():
 
         # ---------------- roofline: onesweep pass timed live via ao_sort_pairs,
         # replayed from CUDA graphs so no host launch time is inside the events
-        keys_ptr = tree.buffer_info("particleKeys_d")[0]
-        keys_in = ab.device_tensor(keys_ptr, n, "<u8").clone()
+        # the keys as the build's sort receives them: unsorted, from the coordinates
+        keys_in = ab.compute_sfc_keys(0, *xs, sfc_kind=ab.SfcKind.Hilbert, stream=s)
+        s.synchronize()
         rig = SortRig(keys_in, s)
         t64 = graph_ms(lambda: rig(64), s, 7)
         t8 = graph_ms(lambda: rig(8), s, 7)
@@ -951,9 +1000,21 @@ def main():
     achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
     roof_sort = {"bound": "hbm", "kernel": "onesweepKernel (one 8-bit pass of the 64-bit key + 32-bit value sort)",
                  "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                 "traffic": ONESWEEP_TRAFFIC_BYTES, "algorithmic_bytes_per_launch": pass_bytes,
+                 "traffic": ONESWEEP_TRAFFIC_BYTES, "traffic_kind": "ncu capture of one 16Mi pass, not re-measured",
+                 "algorithmic_bytes_per_launch": pass_bytes,
                  "launch_ms": pass_ms, "sort_64bit_ms": t64,
                  "keygen": {"ms": keygen_ms, "achieved_gbs": (20.0 * n) / (keygen_ms * 1e-3) / 1e9}}
+    if rank == 0 and not args.no_reference_gpu:
+        try:
+            from oracle import refrun
+            if refrun.available():
+                kh = keys_in.view(torch.int64).cpu().numpy().view(np.uint64)
+                cub = refrun.time_cub_sort(kh, reps=10)
+                roof_sort["cub_sort_64bit_ms"] = cub["cub_sort_ms"]
+                roof_sort["cub_what"] = ("cub::DeviceRadixSort::SortPairs (CCCL 3.3, the reference's call, "
+                                         "octree.cu:301-304) on the same unsorted keys, same GPU")
+        except Exception as e:  # informational
+            roof_sort["cub_error"] = str(e)[:200]
 
     def med(rows, key):
         return statistics.median(r[key] for r in rows)
@@ -977,6 +1038,15 @@ def main():
         "build_near_field_launches": build_stages[-1]["near_field_launches"],
         "update_near_field_launches": update_stages[-1]["near_field_launches"],
         "how": "CUDA events on the tree's stream around each stage (ao_tree_set_profiling), direct calls"}
+    # the whole build on the byte model of the path: per particle the
+    # coordinates read (3 x 4 B), key + index written (12 B), the upfront
+    # histogram read (8 B), 24 B per radix pass (8 passes), one streaming read
+    # of the sorted keys (8 B); per leaf K and N written (12 B)
+    model_bytes = n * (3 * 4 + 12 + 8 + 24 * 8 + 8) + 12 * leaves
+    model_gbs = model_bytes / (step_ms * 1e-3) / 1e9
+    roof_build = {"bound": "hbm", "what": "whole build() on the byte model N(3 s_r + 12 + 8 + 24 R + 8) + 12 L "
+                                          "(s_r = 4, R = 8)", "bytes": model_bytes, "ms": step_ms,
+                  "achieved": model_gbs, "peak": hbm, "unit": "GB/s", "frac": model_gbs / hbm, "peak_kind": peak_kind}
     line = {"metric": METRIC, "value": total / (step_ms * 1e-3), "unit": "particles/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
@@ -988,7 +1058,10 @@ def main():
                        "graph_replayed": True, "resizes": resizes},
             "e2e": {"value": total / (e2e * 1e-3), "unit": "particles/s", "ms_per_step": e2e,
                     "h2d_bytes_per_step": 3 * 4 * n, "d2h_bytes_per_step": 12},
-            "roofline": roof, "roofline_sort": roof_sort, "stages": stages}
+            "roofline": roof, "roofline_sort": roof_sort, "roofline_build": roof_build, "stages": stages}
+    if hasattr(tree, "buildPath"):
+        lv, rounds = tree.buildPath()
+        line["config"]["build_path"] = {"by_levels": lv, "reference_rounds": rounds}
     if rank == 0 and not args.no_cpu_baseline:
         v, dt = cpu_oracle_build(args.cpu_sample)
         line["cpu_baseline"] = {"value": v, "unit": "particles/s", "cores": 1, "kind": "port",
@@ -1017,6 +1090,26 @@ def main():
             line["reference_gpu"] = {"error": str(e)[:200]}
     if world > 1:
         dist.destroy_process_group()
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the other configurations of the metric, each with its own clocks
+        tree.close()
+        del rig, keys_in
+        ab.release_cached_memory()
+        torch.cuda.empty_cache()
+        extras = {}
+        for name, fn in (("c1", lambda: single_config_record("c1", args.steps, args.warmup, 1 << 18, True,
+                                                             not args.no_reference_gpu)),
+                         ("c3", lambda: single_config_record("c3", args.steps, args.warmup, 1 << 16, True,
+                                                             not args.no_reference_gpu)),
+                         ("c4", lambda: batched_record(args.steps, args.warmup, distributed=False)[0]),
+                         ("c5", lambda: serving_record(args.c5_seconds, 2.0, 32, 256))):
+            try:
+                extras[name] = fn()
+            except Exception as e:  # a failed leg is reported, the headline stands
+                extras[name] = {"error": str(e)[:300]}
+            ab.release_cached_memory()
+            torch.cuda.empty_cache()
+        line["configs"] = extras
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
