@@ -144,6 +144,13 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def wait_first(self, timeout=3.0):
+        """Waits until nvidia-smi has printed its first sample, so a short
+        timed region is still covered."""
+        t0 = time.perf_counter()
+        while self.proc and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
@@ -366,8 +373,12 @@ def single_config_record(config, steps, warmup, cpu_sample, cpu_baseline=True, r
             tree.build()
         launches0 = tree.info().kernel_launches
         with ClockSampler(0) as clocks:
-            build_ms = [timed(tree.build) for _ in range(args.steps)]
-        launches = (tree.info().kernel_launches - launches0) // max(1, args.steps)
+            # at least half a second of builds, so the clock record covers them
+            clocks.wait_first()
+            build_ms, t0 = [], time.perf_counter()
+            while len(build_ms) < args.steps or time.perf_counter() - t0 < 0.5:
+                build_ms.append(timed(tree.build))
+        launches = (tree.info().kernel_launches - launches0) // max(1, len(build_ms))
         info = tree.info()
         leaves = info.num_leaves
         # end to end: pinned host coordinates in, build, the counters out
@@ -414,7 +425,7 @@ def single_config_record(config, steps, warmup, cpu_sample, cpu_baseline=True, r
                     graph = capture()
             del graph
     line = {"metric": spec["metric"], "value": n / (statistics.median(build_ms) * 1e-3), "unit": "particles/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(build_ms),
+            "n_gpus": 1, "steps": len(build_ms), "warmup": args.warmup, "ms_per_step": statistics.median(build_ms),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": spec["workload"], "n": n, "coords": "float64", "leaves": int(leaves),
                        "parallelism": "replicas1", "sort": ab.sort_tuning(n)},
