@@ -149,15 +149,10 @@ static __global__ void rootKernel(Arena a, rb::TreeBufs tb, const u64 *P, size_t
     }
 }
 
-// 9 child begins of the units of level l, one warp per unit.  A unit with
-// few keys is read by the warp 32 keys at a time (coalesced): a key whose
-// child digit differs from the previous key's begins that child and every
-// empty child before it, and the children after the last key begin at the
-// unit's end.  A unit with many keys is searched instead, each of its 9
-// boundaries by a group of 3 lanes (4-ary search).  NFCount also enters the
-// unit in the node table.
-constexpr u32 kExpandScanMax = 1024;  // keys scanned per unit; more are searched
-
+// 9 child begins of the units of level l, one thread per unit: the 7 inner
+// boundaries are lower bounds of the children's first keys in the unit's key
+// range, searched side by side (7 independent loads per step, log2 of the
+// unit's count steps).  NFCount also enters the unit in the node table.
 template <bool NF>
 static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u64 *__restrict__ P, int l,
                                                               rb::NodeTable gt)
@@ -165,90 +160,53 @@ static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u
     const Control &c = *a.ctl;
     if (c.overflow | c.late | c.error) return;
     const u32 start = c.levelStart[l], count = c.levelCount[l];
-    const unsigned m = unsigned(l) + 1;
-    const unsigned shift = 3u * (kOctLevels - m);
-    const u64 cr = octRange(m);
-    const int lane = threadIdx.x & 31;
-    const u32 warpsTotal = gridDim.x * (blockDim.x / 32);
-    for (u32 i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); i < count; i += warpsTotal)
+    const u64 cr = octRange(unsigned(l) + 1);
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
     {
         u32 *row = a.rows + size_t(start + i) * kRow;
         const u64 key = rowKey(row);
         const u32 lo = row[2], hi = row[10];
-        if (hi - lo <= kExpandScanMax)
+        u32 b[7], len[7];
+#pragma unroll
+        for (int d = 0; d < 7; ++d)
         {
-            int prev = -1;  // child digit of the key before the current chunk
-            for (u32 off = lo; off < hi; off += 32)
+            b[d] = lo;
+            len[d] = hi - lo;
+        }
+        // halving steps of all 7 searches side by side; the range lengths
+        // drift apart by at most one per step, so a search that has ended
+        // skips the remaining steps of the others
+        for (;;)
+        {
+            u32 live = 0;
+#pragma unroll
+            for (int d = 0; d < 7; ++d) live |= len[d];
+            if (!live) break;
+#pragma unroll
+            for (int d = 0; d < 7; ++d)
             {
-                const u32 idx = off + u32(lane);
-                const int dig = idx < hi ? int((__ldg(P + idx) >> shift) & 7u) : 8;
-                int before = __shfl_up_sync(0xffffffffu, dig, 1);
-                if (lane == 0) before = prev;
-                if (idx < hi)
-                    for (int d = before + 1; d <= dig; ++d) row[2 + d] = idx;
-                prev = __shfl_sync(0xffffffffu, dig, 31);
-                if (prev == 8)  // the chunk ran past the end: the last key's digit
+                if (len[d])
                 {
-                    const unsigned inRange = __ballot_sync(0xffffffffu, idx < hi);
-                    prev = __shfl_sync(0xffffffffu, dig, 31 - __clz(inRange));
+                    const u32 half = len[d] >> 1;
+                    const bool less = __ldg(P + b[d] + half) < key + u64(d + 1) * cr;
+                    b[d] = less ? b[d] + half + 1 : b[d];
+                    len[d] = less ? len[d] - half - 1 : half;
                 }
             }
-            if (lane == 0)
-                for (int d = prev + 1; d < 8; ++d) row[2 + d] = hi;
         }
-        else
-        {
-            // 4-ary search of the first key >= v in [slo, shi]: the 3 lanes of
-            // a group test 3 pivots per step (lanes 27-31 idle)
-            const int grp = lane / 3, sub = lane - grp * 3;
-            const u64 v = key + u64(grp < 9 ? grp : 8) * cr;
-            u32 slo = lane < 27 ? lo : hi, shi = hi;
-            while (__any_sync(0xffffffffu, slo < shi))
-            {
-                const u32 len = shi - slo;
-                const u32 piv = slo + u32((u64(sub + 1) * len) / 4);
-                const bool less = slo < shi && piv < shi && __ldg(P + piv) < v;
-                const int gl = grp * 3;
-                const bool l0 = __shfl_sync(0xffffffffu, less, gl < 32 ? gl : 31);
-                const bool l1 = __shfl_sync(0xffffffffu, less, gl + 1 < 32 ? gl + 1 : 31);
-                const bool l2 = __shfl_sync(0xffffffffu, less, gl + 2 < 32 ? gl + 2 : 31);
-                if (slo < shi)
-                {
-                    const u32 p0 = slo + len / 4, p1 = slo + u32((2ull * len) / 4), p2 = slo + u32((3ull * len) / 4);
-                    if (l2) slo = p2 + 1;
-                    else if (l1)
-                    {
-                        slo = p1 + 1;
-                        shi = p2;
-                    }
-                    else if (l0)
-                    {
-                        slo = p0 + 1;
-                        shi = p1;
-                    }
-                    else
-                    {
-                        shi = p0;
-                    }
-                }
-            }
-            // lane 3d holds the boundary of digit d
-            if (lane < 27 && sub == 0 && grp >= 1 && grp <= 7) row[2 + grp] = slo;
-        }
-        __syncwarp();
+#pragma unroll
+        for (int d = 0; d < 7; ++d) row[3 + d] = b[d];
         if constexpr (NF)
         {
-            if (lane == 0)
+            u32 *t = rb::nodeRow(gt, rb::cellCode(key, unsigned(l)));
+            if (t)
             {
-                u32 *t = rb::nodeRow(gt, rb::cellCode(key, unsigned(l)));
-                if (t)
-                {
+                t[0] = lo;
 #pragma unroll
-                    for (int d = 0; d < rb::kGroupBegins; ++d) t[d] = row[2 + d];
-                }
+                for (int d = 0; d < 7; ++d) t[1 + d] = b[d];
+                t[8] = hi;
             }
         }
-        __syncwarp();
     }
 }
 
@@ -257,13 +215,28 @@ static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u
 // the node table, or counted inside the leaf that holds them), and each child
 // sums its 3 x 3 x 3 sub-block (octNearFieldKernel, here with the units taken
 // from the arena instead of the leaves of a tree).
+// Per-warp scratch of the units in flight (the refresh's scratch without the
+// group-flag populations, so that five CTAs fit on an SM).
+struct UnitScratch
+{
+    u64 pStart[rb::kUnitBatch], st0[rb::kUnitBatch], st1[rb::kUnitBatch], st2[rb::kUnitBatch];
+    u32 cx[rb::kUnitBatch], cy[rb::kUnitBatch], cz[rb::kUnitBatch];
+    u32 hintB[rb::kUnitBatch];
+    int childState[rb::kUnitBatch], level[rb::kUnitBatch];
+    u32 block[rb::kUnitBatch][64];
+    u64 slowKey[rb::kUnitBatch * 27];
+    unsigned short slowItem[rb::kUnitBatch * 27];
+    unsigned char slowState[rb::kUnitBatch * 27];
+    int nSlow;
+};
+
 template <bool Hilbert>
-static __global__ void __launch_bounds__(kThreads, 4)
+static __global__ void __launch_bounds__(kThreads, 5)
     nearFieldKernel(Arena a, KeyIndex idx, int l, HilbertTables h, rb::NodeTable gt)
 {
     using rb::kUnitBatch;
     __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
-    __shared__ rb::UnitScratch sWarp[kThreads / 32];
+    __shared__ UnitScratch sWarp[kThreads / 32];
     const Control &c = *a.ctl;
     if (c.overflow | c.late | c.error) return;
     if constexpr (Hilbert)
@@ -278,7 +251,7 @@ static __global__ void __launch_bounds__(kThreads, 4)
     __syncthreads();
     const u32 start = c.levelStart[l], count = c.levelCount[l];
     const unsigned m = unsigned(l) + 1;
-    rb::UnitScratch &w = sWarp[threadIdx.x >> 5];
+    UnitScratch &w = sWarp[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const unsigned ltMask = (1u << lane) - 1u;
     const u32 warpsTotal = gridDim.x * (blockDim.x / 32);
@@ -291,7 +264,6 @@ static __global__ void __launch_bounds__(kThreads, 4)
             const u32 *row = a.rows + size_t(start + base + u32(lane)) * kRow;
             const u64 key = rowKey(row);
             const rb::CellPath path = rb::decodeCell<Hilbert>(key, unsigned(l), sNext, sDec);
-            w.active[lane] = 1;
             w.pStart[lane] = key;
             w.level[lane] = int(m);
             w.cx[lane] = path.x;
@@ -503,27 +475,32 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
         atomicAdd(a.landed + threadIdx.x, (unsigned long long)sLanded[threadIdx.x]);
 }
 
-// Leaves below each unit of level l (the units of level l + 1 are done).
+// Leaves below each unit of level l (the units of level l + 1 are done),
+// eight lanes per unit.
 static __global__ void leafCountKernel(Arena a, int l)
 {
     const Control &c = *a.ctl;
     const u32 start = c.levelStart[l], count = c.levelCount[l];
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31, d = lane & 7;
+    const size_t total = size_t(count) * 8;
+    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t e0 = size_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); e0 < total; e0 += stride)
     {
-        const u32 g = start + i;
-        u32 s = 0;
+        const size_t e = e0 + size_t(lane);
+        const bool valid = e < total;
+        const u32 g = start + u32(valid ? e >> 3 : 0);
+        const u32 ch = valid ? a.child[size_t(g) * 8 + d] : kLeaf;
+        u32 s = ch == kLeaf ? 1u : a.leaves[ch];
 #pragma unroll
-        for (int d = 0; d < 8; ++d)
-        {
-            const u32 ch = a.child[size_t(g) * 8 + d];
-            s += ch == kLeaf ? 1u : a.leaves[ch];
-        }
-        a.leaves[g] = s;
+        for (int off = 4; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (valid && d == 0) a.leaves[g] = s;
     }
 }
 
 // Cornerstone entries of the leaf children of the level-l units, and the
-// first leaf index of their internal children.
+// first leaf index of their internal children.  Eight lanes per unit, one per
+// child: a segmented scan of the children's leaf counts gives each child's
+// position, so a warp writes the entries of four units at once.
 template <bool NF>
 static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l)
 {
@@ -533,28 +510,36 @@ static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l)
     u64 *K = tb.K[0];
     u32 *B = tb.B[0];
     u32 *NFo = tb.NF[0];
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31, d = lane & 7;
+    const size_t total = size_t(count) * 8;
+    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t e0 = size_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); e0 < total; e0 += stride)
     {
-        const u32 g = start + i;
-        const u32 *row = a.rows + size_t(g) * kRow;
-        const u64 key = rowKey(row);
-        u32 o = a.offset[g];
+        const size_t e = e0 + size_t(lane);
+        const bool valid = e < total;
+        const u32 g = start + u32(valid ? e >> 3 : 0);
+        const u32 ch = valid ? a.child[size_t(g) * 8 + d] : kLeaf;
+        const u32 mine = ch == kLeaf ? 1u : a.leaves[ch];
+        // exclusive prefix of the leaf counts within the unit's 8 lanes
+        u32 inc = mine;
 #pragma unroll
-        for (int d = 0; d < 8; ++d)
+        for (int off = 1; off < 8; off <<= 1)
         {
-            const u32 ch = a.child[size_t(g) * 8 + d];
-            if (ch == kLeaf)
-            {
-                K[o] = key + u64(d) * cr;
-                B[o] = row[2 + d];
-                if constexpr (NF) NFo[o] = a.val[size_t(g) * 8 + d];
-                ++o;
-            }
-            else
-            {
-                a.offset[ch] = o;
-                o += a.leaves[ch];
-            }
+            const u32 t = __shfl_up_sync(0xffffffffu, inc, off);
+            if (d >= off) inc += t;
+        }
+        if (!valid) continue;
+        const u32 o = a.offset[g] + inc - mine;
+        if (ch == kLeaf)
+        {
+            const u32 *row = a.rows + size_t(g) * kRow;
+            K[o] = rowKey(row) + u64(d) * cr;
+            B[o] = row[2 + d];
+            if constexpr (NF) NFo[o] = a.val[size_t(g) * 8 + d];
+        }
+        else
+        {
+            a.offset[ch] = o;
         }
     }
 }

@@ -840,8 +840,8 @@ struct UnitScratch
 
 // Key and child Hilbert state of the parent-level cell at offset q around the
 // parent of unit u.
-template <bool Hilbert>
-__device__ __forceinline__ u64 neighbourCell(const UnitScratch &w, int u, int q, int &qState,
+template <bool Hilbert, class Scratch>
+__device__ __forceinline__ u64 neighbourCell(const Scratch &w, int u, int q, int &qState,
                                              const unsigned char *sEnc, const unsigned char *sNext)
 {
     const unsigned pl = unsigned(w.level[u]) - 1;
