@@ -744,6 +744,7 @@ struct TreeEngine::Impl
     // converged build by levels (levelbuild.cuh): unit arena and its control
     DevMem lvRows, lvVal, lvChild, lvLeaves, lvOffset, lvScan, lvCtl;
     size_t lvCap = 0;
+    int lvLevels = int(kOctLevels);  // levels the last level build needed, with one to spare
     u32 nodeSlots = 0;
     bool nodeStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
@@ -1528,35 +1529,51 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         m.nodeStale = true;  // the table holds this build's nodes only; an update refills it
         lb::rootKernel<<<1, 1, 0, s>>>(a, m.bufs(), P, n_, cfg_.bucket, nf ? 1 : 0), noteLaunch();
         AOT_LAUNCH_CHECK();
-        int levels = 0;  // levels whose units have been classified
-        while (levels < int(kOctLevels))
+        // Every kernel reads its level's size on the device, so the whole
+        // build is queued without a host wait: the levels the last build
+        // needed (all 21 the first time), their subtree counts and the
+        // placement; one readback at the end checks that no deeper level
+        // was left out.
+        const int levels = std::max(1, std::min(int(kOctLevels), m.lvLevels));
+        for (int l = 0; l < levels; ++l)
         {
-            const int stop = std::min(int(kOctLevels), levels + 4);
-            for (; levels < stop; ++levels)
+            if (nf) lb::expandKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
+            else lb::expandKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
+            if (nf)
             {
-                const int l = levels;
-                if (nf) lb::expandKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
-                else lb::expandKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
-                if (nf)
-                {
-                    markNearField(true);
-                    if (cfg_.hilbert)
-                        lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
-                    else
-                        lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
-                    markNearField(false);
-                    lb::classifyKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
-                }
+                markNearField(true);
+                if (cfg_.hilbert)
+                    lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
                 else
-                {
-                    lb::classifyKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
-                }
-                AOT_LAUNCH_CHECK();
+                    lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
+                markNearField(false);
+                lb::classifyKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
             }
-            AOT_CHECK(cudaMemcpyAsync(host.data(), m.lvCtl.p, sizeof(lb::Control), cudaMemcpyDeviceToHost, s));
-            waitStream(s);
-            if (hc.overflow || hc.late || hc.error || hc.levelCount[levels] == 0) break;
+            else
+            {
+                lb::classifyKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
+            }
+            AOT_LAUNCH_CHECK();
         }
+        for (int l = levels - 1; l >= 0; --l)
+            lb::leafCountKernel<<<blocks, lb::kThreads, 0, s>>>(a, l, levels), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        auto place = [&]() {
+            const rb::TreeBufs tb = m.bufs();
+            for (int l = 0; l < levels; ++l)
+            {
+                if (nf) lb::placeKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, tb, l, levels, u32(physCap_)), noteLaunch();
+                else lb::placeKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, tb, l, levels, u32(physCap_)), noteLaunch();
+            }
+            AOT_LAUNCH_CHECK();
+        };
+        place();
+        // the round history is needed before finishKernel writes it; read
+        // everything once
+        AOT_CHECK(cudaMemcpyAsync(host.data(), m.lvCtl.p, kCtlBytes, cudaMemcpyDeviceToHost, s));
+        u32 rootLeaves = 1;
+        AOT_CHECK(cudaMemcpyAsync(&rootLeaves, a.leaves, sizeof(u32), cudaMemcpyDeviceToHost, s));
+        waitStream(s);
         if (hc.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
         if (hc.overflow)
         {
@@ -1564,18 +1581,15 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
             continue;
         }
         if (hc.late) return false;
+        if (hc.levelCount[levels] != 0)
+        {
+            m.lvLevels = int(kOctLevels);  // deeper than the last build: all levels again
+            continue;
+        }
         int deepest = -1;  // deepest level holding units
-        for (int l = 0; l < int(kOctLevels); ++l)
+        for (int l = 0; l < levels; ++l)
             if (hc.levelCount[l]) deepest = l;
-        for (int l = deepest; l >= 0; --l) lb::leafCountKernel<<<blocks, lb::kThreads, 0, s>>>(a, l), noteLaunch();
-        AOT_LAUNCH_CHECK();
-        u32 rootLeaves = 1;
-        if (deepest >= 0)
-            AOT_CHECK(cudaMemcpyAsync(&rootLeaves, a.leaves, sizeof(u32), cudaMemcpyDeviceToHost, s));
-        AOT_CHECK(cudaMemcpyAsync(host.data() + kHeadBytes, a.contrib,
-                                  (lb::kContribBins + lb::kArrivals) * sizeof(unsigned long long),
-                                  cudaMemcpyDeviceToHost, s));
-        waitStream(s);
+        if (deepest < 0) rootLeaves = 1;
         // leaves after every round that changed the tree
         const auto *contrib = reinterpret_cast<const unsigned long long *>(host.data() + kHeadBytes);
         const auto *landed = contrib + lb::kContribBins;
@@ -1602,15 +1616,15 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         }
         if (rounds && proposals.back() != (long long)rootLeaves)
             throw std::logic_error("adaptive_octree: level build history does not end at the tree");
-        hostLeaves_ = rootLeaves;
-        ensurePhysical(std::max<size_t>(physCap_, rootLeaves));
-        const rb::TreeBufs tb = m.bufs();
-        for (int l = 0; l <= deepest; ++l)
+        if (hc.placeOverflow)
         {
-            if (nf) lb::placeKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, tb, l), noteLaunch();
-            else lb::placeKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, tb, l), noteLaunch();
+            ensurePhysical(rootLeaves);
+            AOT_CHECK(cudaMemsetAsync(&a.ctl->placeOverflow, 0, sizeof(int), s));
+            place();
         }
-        lb::finishKernel<<<1, 1, 0, s>>>(a, tb, rounds), noteLaunch();
+        hostLeaves_ = rootLeaves;
+        m.lvLevels = std::min(int(kOctLevels), deepest + 2);
+        lb::finishKernel<<<1, 1, 0, s>>>(a, m.bufs(), rounds, levels, u32(physCap_)), noteLaunch();
         AOT_LAUNCH_CHECK();
         if (nf) AOT_CHECK(cudaMemsetAsync(m.G[0].p, 0, m.G[0].bytes, s));  // no group of the converged tree may merge
         return true;

@@ -44,7 +44,6 @@ __device__ __forceinline__ u64 particleKey(Real x, Real y, Real z, const KeygenP
 }
 
 constexpr int kKeygenThreads = 256;
-constexpr int kAggregatedPass = 5;  // digit passes from here on are counted warp-aggregated
 
 // Vec: particles per thread step (4 for float4, 2 for double2, 1 scalar).
 template <class Real, Curve C, int Vec>
@@ -62,29 +61,10 @@ static __global__ void __launch_bounds__(kKeygenThreads)
     }
     __syncthreads();
 
-    // Digit counts of a key.  The high digits (levels 1-8 of the curve) are
-    // shared by most keys of a cluster, so a warp's same-digit lanes add
-    // their count once (one shared atomic per distinct digit instead of a
-    // replay per conflicting lane); the low digits are spread out and add
-    // directly.
-    const int lane = threadIdx.x & 31;
     auto count = [&](u64 k) {
-        const unsigned mask = __activemask();
 #pragma unroll
         for (int p = 0; p < sort::kMaxPasses; ++p)
-        {
-            if (p >= histPasses) continue;
-            const unsigned d = unsigned(k >> (p * sort::kRadixBits)) & (sort::kRadix - 1);
-            if (p < kAggregatedPass)
-            {
-                atomicAdd(&sh[p][d], 1u);
-            }
-            else
-            {
-                const unsigned peers = __match_any_sync(mask, d);
-                if (lane == __ffs(peers) - 1) atomicAdd(&sh[p][d], unsigned(__popc(peers)));
-            }
-        }
+            if (p < histPasses) atomicAdd(&sh[p][(k >> (p * sort::kRadixBits)) & (sort::kRadix - 1)], 1u);
     };
 
     const size_t groups = n / Vec;

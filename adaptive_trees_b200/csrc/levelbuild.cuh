@@ -57,10 +57,10 @@ struct Control
     u32 levelStart[kOctLevels + 2];
     u32 levelCount[kOctLevels + 2];
     u32 tileCounter[kOctLevels + 2];
-    int overflow;  // the unit arena is too small
-    int late;      // an arrival round beyond the tracked ones
-    int error;     // a bounded look-back gave up
-    int pad;
+    int overflow;       // the unit arena is too small
+    int late;           // an arrival round beyond the tracked ones
+    int error;          // a bounded look-back gave up
+    int placeOverflow;  // the tree has more leaves than the cornerstone buffers hold
 };
 
 // The unit arena: units of all levels, level l at
@@ -216,7 +216,7 @@ static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u
 // sums its 3 x 3 x 3 sub-block (octNearFieldKernel, here with the units taken
 // from the arena instead of the leaves of a tree).
 // Per-warp scratch of the units in flight (the refresh's scratch without the
-// group-flag populations, so that five CTAs fit on an SM).
+// group-flag populations, which leaves more of the SM's shared storage to L1).
 struct UnitScratch
 {
     u64 pStart[rb::kUnitBatch], st0[rb::kUnitBatch], st1[rb::kUnitBatch], st2[rb::kUnitBatch];
@@ -231,7 +231,7 @@ struct UnitScratch
 };
 
 template <bool Hilbert>
-static __global__ void __launch_bounds__(kThreads, 5)
+static __global__ void __launch_bounds__(kThreads, 4)
     nearFieldKernel(Arena a, KeyIndex idx, int l, HilbertTables h, rb::NodeTable gt)
 {
     using rb::kUnitBatch;
@@ -475,25 +475,25 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
         atomicAdd(a.landed + threadIdx.x, (unsigned long long)sLanded[threadIdx.x]);
 }
 
-// Leaves below each unit of level l (the units of level l + 1 are done),
-// eight lanes per unit.
-static __global__ void leafCountKernel(Arena a, int l)
+// Leaves below each unit of level l (the units of level l + 1 are done).
+// `levels` is the number of levels the build expanded: units below them mean
+// the build is incomplete, and nothing is counted.
+static __global__ void leafCountKernel(Arena a, int l, int levels)
 {
     const Control &c = *a.ctl;
+    if (c.levelCount[levels] | c.overflow | c.late | c.error) return;
     const u32 start = c.levelStart[l], count = c.levelCount[l];
-    const int lane = threadIdx.x & 31, d = lane & 7;
-    const size_t total = size_t(count) * 8;
-    const size_t stride = size_t(gridDim.x) * blockDim.x;
-    for (size_t e0 = size_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); e0 < total; e0 += stride)
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
     {
-        const size_t e = e0 + size_t(lane);
-        const bool valid = e < total;
-        const u32 g = start + u32(valid ? e >> 3 : 0);
-        const u32 ch = valid ? a.child[size_t(g) * 8 + d] : kLeaf;
-        u32 s = ch == kLeaf ? 1u : a.leaves[ch];
+        const u32 g = start + i;
+        u32 s = 0;
 #pragma unroll
-        for (int off = 4; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-        if (valid && d == 0) a.leaves[g] = s;
+        for (int d = 0; d < 8; ++d)
+        {
+            const u32 ch = a.child[size_t(g) * 8 + d];
+            s += ch == kLeaf ? 1u : a.leaves[ch];
+        }
+        a.leaves[g] = s;
     }
 }
 
@@ -502,9 +502,10 @@ static __global__ void leafCountKernel(Arena a, int l)
 // child: a segmented scan of the children's leaf counts gives each child's
 // position, so a warp writes the entries of four units at once.
 template <bool NF>
-static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l)
+static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l, int levels, u32 capacity)
 {
-    const Control &c = *a.ctl;
+    Control &c = *a.ctl;
+    if (c.levelCount[levels] | c.overflow | c.late | c.error) return;
     const u32 start = c.levelStart[l], count = c.levelCount[l];
     const u64 cr = octRange(unsigned(l) + 1);
     u64 *K = tb.K[0];
@@ -530,7 +531,11 @@ static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l)
         }
         if (!valid) continue;
         const u32 o = a.offset[g] + inc - mine;
-        if (ch == kLeaf)
+        if (ch == kLeaf && o >= capacity)
+        {
+            c.placeOverflow = 1;  // the host grows the buffers and places again
+        }
+        else if (ch == kLeaf)
         {
             const u32 *row = a.rows + size_t(g) * kRow;
             K[o] = rowKey(row) + u64(d) * cr;
@@ -546,11 +551,13 @@ static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l)
 
 // The finished tree: sentinel boundary and the state of a converged build
 // (finishBuildStateKernel, octree.cu:40-47, after `rounds` changing rounds).
-static __global__ void finishKernel(Arena a, rb::TreeBufs tb, int rounds)
+static __global__ void finishKernel(Arena a, rb::TreeBufs tb, int rounds, int levels, u32 capacity)
 {
     DeviceState *st = tb.st;
     const Control &c = *a.ctl;
+    if (c.levelCount[levels] | c.overflow | c.late | c.error | c.placeOverflow) return;
     const int leaves = c.levelCount[0] ? int(a.leaves[0]) : 1;
+    if (u32(leaves) > capacity) return;
     tb.K[0][leaves] = kMaxKey;
     tb.B[0][leaves] = st->numActiveParticles;
     st->numLeaves = leaves;

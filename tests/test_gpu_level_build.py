@@ -148,3 +148,25 @@ def test_escaped_particles_sort_last():
     assert t.buildPath()[0]
     compare(t, o)
     t.close()
+
+
+def test_deeper_tree_after_a_shallow_one():
+    """The level build queues as many levels as the tree's last build needed;
+    a deeper tree on the same object must still come out complete."""
+    import adaptive_trees_b200 as ab
+    from oracle import oracle as O
+    shallow = S.uniform_cube(20_000, seed=35)
+    deep = _stacked(20_000, 36)
+    xs = [to_dev(a) for a in shallow]
+    cfg = dict(bucket=32, nf=True, hilbert=True)
+    t = ab.Tree(0, *xs, tree_config(**cfg))
+    t.build()
+    for d, a in zip(xs, deep):
+        d.copy_(torch.from_numpy(np.ascontiguousarray(a)).to("cuda"))
+    t.build()
+    o = O.OracleTree(0, *deep, oracle_config(**cfg))
+    o.build()
+    assert t.buildPath()[0]
+    compare(t, o)
+    assert t.maxAchievedDepth() == 21 or t.info().num_leaves > 1000
+    t.close()
