@@ -1542,17 +1542,10 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
             if (nf)
             {
                 markNearField(true);
-                // the root's children by the unit kernel, deeper levels by sibling group
-                if (l == 0 && cfg_.hilbert)
+                if (cfg_.hilbert)
                     lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
-                else if (l == 0)
-                    lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
-                else if (cfg_.hilbert)
-                    lb::groupNearFieldKernel<true><<<unsigned(smCount()) * 6u, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt),
-                        noteLaunch();
                 else
-                    lb::groupNearFieldKernel<false><<<unsigned(smCount()) * 6u, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt),
-                        noteLaunch();
+                    lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
                 markNearField(false);
                 lb::classifyKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
             }

@@ -239,6 +239,8 @@ static __global__ void __launch_bounds__(kThreads, 4)
     __shared__ UnitScratch sWarp[kThreads / 32];
     const Control &c = *a.ctl;
     if (c.overflow | c.late | c.error) return;
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    if (count <= blockIdx.x * u32(kThreads / 32) * u32(rb::kUnitBatch)) return;  // no units for this CTA
     if constexpr (Hilbert)
     {
         for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
@@ -249,7 +251,6 @@ static __global__ void __launch_bounds__(kThreads, 4)
         }
     }
     __syncthreads();
-    const u32 start = c.levelStart[l], count = c.levelCount[l];
     const unsigned m = unsigned(l) + 1;
     UnitScratch &w = sWarp[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -366,244 +367,6 @@ static __global__ void __launch_bounds__(kThreads, 4)
             a.val[size_t(g) * 8 + d] = out;
         }
         __syncwarp();
-    }
-}
-
-// Near-field counts of the children of the level-l units (l >= 1), one
-// sibling group at a time.  The units of a level are in key order, so the
-// (at most 8) units that share a parent G at level l - 1 are consecutive.
-// Their children's 27-cell stencils all lie in the 8 x 8 x 8 block of level
-// l + 1 cells formed by the children of the 4 x 4 x 4 level-l cells around
-// G, so each of those cells is looked up once for the whole group (64
-// lookups for a full group instead of 8 x 27), and only where some unit of
-// the group touches it.  A cell that is an internal node gives its child
-// counts from the node table; any other cell is a leaf or lies inside one
-// and is counted within that leaf's few keys, as in nearFieldKernel.
-struct GroupScratch
-{
-    u32 block[512];  // child counts of the 8 x 8 x 8 level-(l+1) block, x-major
-    u64 slowKey[64];
-    unsigned char slowCell[64], slowState[64];
-    u64 gKey, gst0, gst1, gst2;
-    u32 gx, gy, gz;
-    int gState;                    // G's child state (Hilbert)
-    int unitOct[8], unitState[8];  // octant of each unit in G and its child state
-    u32 unitBegin;                 // first key of the group (fallback search hint)
-    int nSlow;
-};
-
-// Key of the level-l cell at 21-bit grid coordinates (x, y, z), encoded from
-// G's path (G at level l - 1 with grid origin gx, gy, gz): the key agrees with
-// G's up to the first level where the coordinates differ.  Also gives the
-// cell's child state.
-template <bool Hilbert>
-__device__ __forceinline__ u64 cellFromGroup(const GroupScratch &w, unsigned l, u32 x, u32 y, u32 z, int &state,
-                                             const unsigned char *sEnc, const unsigned char *sNext)
-{
-    if constexpr (!Hilbert)
-    {
-        state = kHilbertStart;
-        return mortonKey(x, y, z);
-    }
-    else
-    {
-        const unsigned pl = l - 1;  // G's level
-        const u32 diff = (x ^ w.gx) | (y ^ w.gy) | (z ^ w.gz);
-        unsigned m = diff ? unsigned(__clz(diff)) - (32u - kOctLevels) : pl;
-        if (m > pl) m = pl;  // inside G: only the last level is encoded
-        int st;
-        if (m == pl)
-        {
-            st = w.gState;
-        }
-        else
-        {
-            const u64 word = m < 10 ? w.gst0 : (m < 20 ? w.gst1 : w.gst2);
-            st = int((word >> (6 * (m < 10 ? m : (m < 20 ? m - 10 : m - 20)))) & 63u);
-        }
-        u64 suffix = 0;
-        for (unsigned k = m; k < l; ++k)
-        {
-            const unsigned b = kOctLevels - 1 - k;
-            const unsigned o = (((x >> b) & 1u) << 2) | (((y >> b) & 1u) << 1) | ((z >> b) & 1u);
-            const int e = st * 8 + int(o);
-            suffix = (suffix << 3) | sEnc[e];
-            st = sNext[e];
-        }
-        state = st;
-        const unsigned keep = 3u * m;
-        const u64 prefix = keep ? (w.gKey >> (63u - keep)) << (63u - keep) : 0ull;
-        return prefix | (suffix << (3u * (kOctLevels - l)));
-    }
-}
-
-// The 8 child counts of the level-l cell at block position (bx, by, bz)
-// into the group block, children placed by their octant.
-template <bool Hilbert>
-__device__ __forceinline__ void placeChildren(u32 *block, const u32 (&b)[rb::kGroupBegins], int bx, int by, int bz,
-                                              int state, const unsigned char *sDec)
-{
-#pragma unroll
-    for (int d = 0; d < 8; ++d)
-    {
-        const unsigned o = Hilbert ? unsigned(sDec[state * 8 + d]) : unsigned(d);
-        const int px = 2 * bx + int(o >> 2), py = 2 * by + int((o >> 1) & 1u), pz = 2 * bz + int(o & 1u);
-        block[(px * 8 + py) * 8 + pz] = b[d + 1] - b[d];
-    }
-}
-
-template <bool Hilbert>
-static __global__ void __launch_bounds__(kThreads, 6)
-    groupNearFieldKernel(Arena a, KeyIndex idx, int l, HilbertTables h, rb::NodeTable gt)
-{
-    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
-    __shared__ GroupScratch sWarp[kThreads / 32];
-    const Control &c = *a.ctl;
-    if (c.overflow | c.late | c.error) return;
-    if constexpr (Hilbert)
-    {
-        for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
-        {
-            sEnc[k] = h.enc[k];
-            sNext[k] = h.encNext[k];
-            sDec[k] = h.decOct[k];
-        }
-    }
-    __syncthreads();
-    const u32 start = c.levelStart[l], count = c.levelCount[l];
-    const unsigned ul = unsigned(l), m = ul + 1;
-    const u64 gRange = octRange(ul - 1);
-    const u32 cubeL = 1u << (kOctLevels - ul);  // level-l cell edge in grid units
-    GroupScratch &w = sWarp[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const unsigned ltMask = (1u << lane) - 1u;
-    const u32 warpsTotal = gridDim.x * (blockDim.x / 32);
-    const u32 w0 = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    for (u32 base = w0 * 32; base < count; base += warpsTotal * 32)
-    {
-        const u32 i = base + u32(lane);
-        const bool valid = i < count;
-        const u32 *row = a.rows + size_t(start + (valid ? i : 0)) * kRow;
-        const u64 key = valid ? rowKey(row) : 0;
-        const u64 gk = key & ~(gRange - 1);
-        const u64 gkPrev = __shfl_up_sync(0xffffffffu, gk, 1);
-        const bool head = valid && (lane == 0 || gk != gkPrev);
-        unsigned heads = __ballot_sync(0xffffffffu, head);
-        const unsigned validMask = __ballot_sync(0xffffffffu, valid);
-        while (heads)
-        {
-            const int g0 = __ffs(heads) - 1;
-            heads &= heads - 1;
-            const int g1 = heads ? __ffs(heads) - 1 : 32 - __clz(validMask);
-            const int k = g1 - g0;  // units of the group (<= 8)
-            // ---- G's path and the units' octants
-            if (lane == g0)
-            {
-                const rb::CellPath p = rb::decodeCell<Hilbert>(gk, ul - 1, sNext, sDec);
-                w.gKey = gk;
-                w.gx = p.x;
-                w.gy = p.y;
-                w.gz = p.z;
-                w.gst0 = p.st0;
-                w.gst1 = p.st1;
-                w.gst2 = p.st2;
-                w.gState = p.childState;
-                w.unitBegin = row[2];
-                w.nSlow = 0;
-            }
-            __syncwarp();
-            if (lane >= g0 && lane < g1)
-            {
-                const int u = lane - g0;
-                const unsigned dg = octDigit(key, ul);
-                const int o = Hilbert ? int(sDec[w.gState * 8 + int(dg)]) : int(dg);
-                w.unitOct[u] = o;
-                w.unitState[u] = Hilbert ? int(sNext[w.gState * 8 + o]) : kHilbertStart;
-            }
-            __syncwarp();
-            // ---- the 64 level-l cells around G: lookups where a unit needs them
-            for (int cc = lane; cc < 64; cc += 32)
-            {
-                const int bx = cc >> 4, by = (cc >> 2) & 3, bz = cc & 3;
-                bool need = false;
-                for (int u = 0; u < k; ++u)
-                {
-                    const int o = w.unitOct[u];
-                    const int ux = 1 + (o >> 2), uy = 1 + ((o >> 1) & 1), uz = 1 + (o & 1);
-                    need |= abs(bx - ux) <= 1 && abs(by - uy) <= 1 && abs(bz - uz) <= 1;
-                }
-                bool slow = false;
-                u64 cKey = 0;
-                int cState = 0;
-                if (need)
-                {
-                    const u32 x = (w.gx + u32(bx - 1) * cubeL) & 0x1fffffu;
-                    const u32 y = (w.gy + u32(by - 1) * cubeL) & 0x1fffffu;
-                    const u32 z = (w.gz + u32(bz - 1) * cubeL) & 0x1fffffu;
-                    cKey = cellFromGroup<Hilbert>(w, ul, x, y, z, cState, sEnc, sNext);
-                    u32 gb[rb::kGroupBegins];
-                    if (rb::nodeBegins(gt, rb::cellCode(cKey, ul), gb)) placeChildren<Hilbert>(w.block, gb, bx, by, bz, cState, sDec);
-                    else slow = true;
-                }
-                // every lane runs both iterations: the warp is converged here
-                const unsigned slowMask = __ballot_sync(0xffffffffu, slow);
-                if (slow)
-                {
-                    const int s = w.nSlow + __popc(slowMask & ltMask);
-                    w.slowKey[s] = cKey;
-                    w.slowCell[s] = (unsigned char)cc;
-                    w.slowState[s] = (unsigned char)cState;
-                }
-                __syncwarp();
-                if (lane == 0) w.nSlow += __popc(slowMask);
-                __syncwarp();
-            }
-            __syncwarp();
-            // ---- cells that are no internal node: counted inside their leaf
-            const int nSlow = w.nSlow;
-            for (int t = lane; t < nSlow; t += 32)
-            {
-                const int cc = w.slowCell[t];
-                const u64 cKey = w.slowKey[t];
-                u32 begins[rb::kGroupBegins];
-                if (!rb::beginsInside(gt, idx.keys, u32(idx.n), cKey, m, begins))
-                {
-                    const u32 lo = idx.lowerNear<rb::kNFGallop>(w.unitBegin, cKey);
-                    const u32 hi = rb::lowerFrom(idx, lo, cKey + octRange(ul));
-                    rb::childBeginsWithin(idx.keys, lo, hi, cKey, m, begins);
-                }
-                placeChildren<Hilbert>(w.block, begins, cc >> 4, (cc >> 2) & 3, cc & 3, int(w.slowState[t]), sDec);
-            }
-            __syncwarp();
-            // ---- the 8 children of each unit: count x 3 x 3 x 3 block sum
-            for (int e = lane; e < k * 8; e += 32)
-            {
-                const int u = e >> 3, d = e & 7;
-                const u32 g = start + base + u32(g0 + u);
-                const u32 *urow = a.rows + size_t(g) * kRow;
-                const u32 cnt = urow[2 + d + 1] - urow[2 + d];
-                u32 out = 0;
-                if (cnt)
-                {
-                    const int o = w.unitOct[u];
-                    const unsigned co = Hilbert ? unsigned(sDec[w.unitState[u] * 8 + d]) : unsigned(d);
-                    const int px = 2 * (1 + (o >> 2)) + int(co >> 2);
-                    const int py = 2 * (1 + ((o >> 1) & 1)) + int((co >> 1) & 1u);
-                    const int pz = 2 * (1 + (o & 1)) + int(co & 1u);
-                    u32 p32 = 0;
-#pragma unroll
-                    for (int dx = -1; dx <= 1; ++dx)
-#pragma unroll
-                        for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-                            for (int dz = -1; dz <= 1; ++dz) p32 += w.block[((px + dx) * 8 + (py + dy)) * 8 + (pz + dz)];
-                    const u64 v = u64(cnt) * p32;
-                    out = v > 0xffffffffull ? 0xffffffffu : u32(v);
-                }
-                a.val[size_t(g) * 8 + d] = out;
-            }
-            __syncwarp();
-        }
     }
 }
 
