@@ -713,7 +713,7 @@ void TreeEngine::sortPairsPreload()
     AOT_CHECK(cudaFuncGetAttributes(&a, sort::binsKernel));
     AOT_CHECK(cudaFuncGetAttributes(&a, sort::histogramKernel<8>));
     AOT_CHECK(cudaFuncGetAttributes(&a, sort::histogramKernel<7>));
-#define AOT_CASE(i, B, I) AOT_CHECK(cudaFuncGetAttributes(&a, sort::onesweepKernel<B, I>));
+#define AOT_CASE(i, B, I, M) AOT_CHECK(cudaFuncGetAttributes(&a, sort::onesweepKernel<B, I, M>));
     AOT_SORT_CONFIGS(AOT_CASE)
 #undef AOT_CASE
     sort::setPassSmemAll();
@@ -1537,8 +1537,8 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         const int levels = std::max(1, std::min(int(kOctLevels), m.lvLevels));
         for (int l = 0; l < levels; ++l)
         {
-            if (nf) lb::expandKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
-            else lb::expandKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, P, l, gt), noteLaunch();
+            if (nf) lb::expandKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, idx, l, gt), noteLaunch();
+            else lb::expandKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, idx, l, gt), noteLaunch();
             if (nf)
             {
                 markNearField(true);

@@ -149,13 +149,72 @@ static __global__ void rootKernel(Arena a, rb::TreeBufs tb, const u64 *P, size_t
     }
 }
 
-// 9 child begins of the units of level l, one thread per unit: the 7 inner
-// boundaries are lower bounds of the children's first keys in the unit's key
-// range, searched side by side (7 independent loads per step, log2 of the
-// unit's count steps).  NFCount also enters the unit in the node table.
+// Lower bounds of the 7 inner child boundaries key + (d + 1) * cr of a unit
+// whose keys are P[lo, hi), searched side by side (7 independent loads per
+// step): first among the sampled keys (every 32nd key, a small array that
+// stays in L2), then in the window of at most 31 keys the sample leaves.
+__device__ __forceinline__ void innerBegins(const KeyIndex &idx, u32 lo, u32 hi, u64 key, u64 cr, u32 (&b)[7])
+{
+    const u32 jA = (lo + kSampleStride - 1) >> kSampleShift, jB = (hi + kSampleStride - 1) >> kSampleShift;
+    u32 len[7];
+#pragma unroll
+    for (int d = 0; d < 7; ++d)
+    {
+        b[d] = jA;
+        len[d] = jB > jA ? jB - jA : 0;
+    }
+    for (;;)  // first sample >= target among samples jA..jB-1
+    {
+        u32 live = 0;
+#pragma unroll
+        for (int d = 0; d < 7; ++d) live |= len[d];
+        if (!live) break;
+#pragma unroll
+        for (int d = 0; d < 7; ++d)
+        {
+            if (len[d])
+            {
+                const u32 half = len[d] >> 1;
+                const bool less = __ldg(idx.sample + b[d] + half) < key + u64(d + 1) * cr;
+                b[d] = less ? b[d] + half + 1 : b[d];
+                len[d] = less ? len[d] - half - 1 : half;
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 7; ++d)
+    {
+        // the answer lies after the last sample below the target and at or
+        // before the first one at or above it
+        const u32 wlo = b[d] > jA ? ((b[d] - 1) << kSampleShift) + 1 : lo;
+        const u32 whi = b[d] < jB ? (b[d] << kSampleShift) : hi;
+        len[d] = whi - wlo;
+        b[d] = wlo;
+    }
+    for (;;)
+    {
+        u32 live = 0;
+#pragma unroll
+        for (int d = 0; d < 7; ++d) live |= len[d];
+        if (!live) break;
+#pragma unroll
+        for (int d = 0; d < 7; ++d)
+        {
+            if (len[d])
+            {
+                const u32 half = len[d] >> 1;
+                const bool less = __ldg(idx.keys + b[d] + half) < key + u64(d + 1) * cr;
+                b[d] = less ? b[d] + half + 1 : b[d];
+                len[d] = less ? len[d] - half - 1 : half;
+            }
+        }
+    }
+}
+
+// 9 child begins of the units of level l, one thread per unit (the 7 inner
+// ones by innerBegins).  NFCount also enters the unit in the node table.
 template <bool NF>
-static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u64 *__restrict__ P, int l,
-                                                              rb::NodeTable gt)
+static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, KeyIndex idx, int l, rb::NodeTable gt)
 {
     const Control &c = *a.ctl;
     if (c.overflow | c.late | c.error) return;
@@ -166,34 +225,8 @@ static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, const u
         u32 *row = a.rows + size_t(start + i) * kRow;
         const u64 key = rowKey(row);
         const u32 lo = row[2], hi = row[10];
-        u32 b[7], len[7];
-#pragma unroll
-        for (int d = 0; d < 7; ++d)
-        {
-            b[d] = lo;
-            len[d] = hi - lo;
-        }
-        // halving steps of all 7 searches side by side; the range lengths
-        // drift apart by at most one per step, so a search that has ended
-        // skips the remaining steps of the others
-        for (;;)
-        {
-            u32 live = 0;
-#pragma unroll
-            for (int d = 0; d < 7; ++d) live |= len[d];
-            if (!live) break;
-#pragma unroll
-            for (int d = 0; d < 7; ++d)
-            {
-                if (len[d])
-                {
-                    const u32 half = len[d] >> 1;
-                    const bool less = __ldg(P + b[d] + half) < key + u64(d + 1) * cr;
-                    b[d] = less ? b[d] + half + 1 : b[d];
-                    len[d] = less ? len[d] - half - 1 : half;
-                }
-            }
-        }
+        u32 b[7];
+        innerBegins(idx, lo, hi, key, cr, b);
 #pragma unroll
         for (int d = 0; d < 7; ++d) row[3 + d] = b[d];
         if constexpr (NF)
