@@ -713,7 +713,7 @@ void TreeEngine::sortPairsPreload()
     AOT_CHECK(cudaFuncGetAttributes(&a, sort::binsKernel));
     AOT_CHECK(cudaFuncGetAttributes(&a, sort::histogramKernel<8>));
     AOT_CHECK(cudaFuncGetAttributes(&a, sort::histogramKernel<7>));
-#define AOT_CASE(i, B, I, M) AOT_CHECK(cudaFuncGetAttributes(&a, sort::onesweepKernel<B, I, M>));
+#define AOT_CASE(i, B, I) AOT_CHECK(cudaFuncGetAttributes(&a, sort::onesweepKernel<B, I>));
     AOT_SORT_CONFIGS(AOT_CASE)
 #undef AOT_CASE
     sort::setPassSmemAll();

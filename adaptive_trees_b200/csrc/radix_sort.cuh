@@ -144,37 +144,15 @@ struct SharedPass
     u32 tile;
 };
 
-// Shared memory of a mode-1 pass: one buffer for the ordered keys, then the
-// ordered values, and the digit of every ordered position.
-template <int Bits, int Items>
-struct SharedPass1
-{
-    static constexpr int R = 1 << Bits;
-    static constexpr int T = kThreads * Items;
-    u64 keys[T];                // ordered keys; then, as u32, the ordered values
-    unsigned char digit[T];     // digit of each ordered position
-    u32 warpHist[kWarps][R];    // per-warp digit counts, then exclusive warp offsets
-    u32 localStart[R];
-    u32 gstart[R];
-    u32 count[R];
-    u32 warpSums[kWarps];
-    u32 tile;
-};
-
 // The compiled configurations: digit width, keys per thread and the CTAs per
 // SM they are built for (their shared memory and a 64-register budget allow
 // 4 CTAs for tiles of up to 3072 keys).  Each gives an even number of passes
 // over 64-bit keys (8 or 10), so the sorted data ends where it started.
-// mode 0: the tile's keys and values are reordered in shared memory side by
-// side (values staged by a bulk copy); mode 1: two phases through one buffer
-// (the keys go out first, then the values, re-read from global memory, take
-// their place), which halves the shared memory of a tile so more CTAs fit.
 struct SortConfig
 {
-    int bits, items, mode;
+    int bits, items;
 };
-constexpr SortConfig kSortConfigs[] = {{8, 10, 0}, {8, 16, 0}, {8, 8, 0}, {7, 12, 0},
-                                       {7, 16, 0}, {8, 10, 1}, {8, 8, 1},  {8, 12, 1}};
+constexpr SortConfig kSortConfigs[] = {{8, 10}, {8, 16}, {8, 8}, {7, 12}, {7, 16}};
 constexpr int kNumSortConfigs = int(sizeof(kSortConfigs) / sizeof(kSortConfigs[0]));
 constexpr int kDefaultSortConfig = 0;
 constexpr int configTile(int c) { return kThreads * kSortConfigs[c].items; }
@@ -504,248 +482,49 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
     }
 }
 
-// One mode-1 onesweep pass (see SortConfig): ranking, digit publication and
-// look-back as in onesweepTile; the keys are reordered in shared memory and
-// written out, then the values are read in tile order, reordered through the
-// same buffer and written out.
-template <int Bits, int Items, class Tiles>
-__device__ __forceinline__ void onesweepTile1(const Tiles &tiles, const u64 *__restrict__ keysIn,
-                                              const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
-                                              u32 *__restrict__ valsOut, int shift, u32 *tileCounter, u64 *status,
-                                              int *error, int bits, unsigned spinLimit = kLookbackSpins)
-{
-    using Smem = SharedPass1<Bits, Items>;
-    constexpr int R = Smem::R;
-    constexpr int T = Smem::T;
-    static_assert(R <= kThreads && R <= kRadix && Bits <= 8, "one digit per thread, digits in a byte");
-    static_assert(Items % 2 == 0, "ranks are packed in pairs");
-    const unsigned dmask = (1u << bits) - 1;
-    extern __shared__ __align__(16) unsigned char smemRaw[];
-    Smem &sm = *reinterpret_cast<Smem *>(smemRaw);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-    for (int i = tid; i < kWarps * R; i += kThreads) (&sm.warpHist[0][0])[i] = 0;
-    if (tid == 0) sm.tile = atomicAdd(tileCounter, 1u);
-    __syncthreads();
-    const size_t tile = sm.tile;
-    const size_t tileBase = tiles.base(tile);
-    const size_t warpBase = tileBase + size_t(warp) * (32 * Items);
-    const size_t tileEnd = tiles.end(tile);
-
-    u64 key[Items];
-#pragma unroll
-    for (int i = 0; i < Items; ++i)
-    {
-        const size_t idx = warpBase + size_t(i) * 32 + lane;
-        key[i] = idx < tileEnd ? __ldcs(keysIn + idx) : 0ull;
-    }
-    u32 *wh = sm.warpHist[warp];
-    const unsigned ltMask = laneMaskLt();
-    u32 rank2[Items / 2];
-    u32 dpack[(Items + 3) / 4];
-#pragma unroll
-    for (int i = 0; i < (Items + 3) / 4; ++i) dpack[i] = 0;
-#pragma unroll
-    for (int i = 0; i < Items; ++i)
-    {
-        const size_t idx = warpBase + size_t(i) * 32 + lane;
-        const bool valid = idx < tileEnd;
-        const unsigned validMask = __ballot_sync(0xffffffffu, valid);
-        const unsigned d = unsigned(key[i] >> shift) & dmask;
-        dpack[i >> 2] |= d << (8 * (i & 3));
-        const unsigned peers = peerLanes(d, bits, validMask);
-        const int leader = __ffs(peers) - 1;
-        u32 base = 0;
-        if (valid && lane == leader) base = atomicAdd(&wh[d], u32(__popc(peers)));
-        base = __shfl_sync(0xffffffffu, base, leader < 0 ? 0 : leader);
-        __syncwarp();
-        const u32 r = base + __popc(peers & ltMask);
-        if (i & 1) rank2[i >> 1] |= r << 16;
-        else rank2[i >> 1] = r;
-    }
-    __syncthreads();
-    if (tid < R)
-    {
-        const int d = tid;
-        u32 acc = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w)
-        {
-            const u32 c = sm.warpHist[w][d];
-            sm.warpHist[w][d] = acc;
-            acc += c;
-        }
-        sm.count[d] = acc;
-    }
-    __syncthreads();
-    {
-        const int d = tid;
-        const u32 cnt = d < R ? sm.count[d] : 0u;
-        if (d < R) stRelaxed(status + tile * R + d, (tiles.chainStart(tile) ? kFlagPrefix : kFlagAgg) | u64(cnt));
-        u32 v = cnt;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1)
-        {
-            const u32 t = __shfl_up_sync(0xffffffffu, v, off);
-            if (lane >= off) v += t;
-        }
-        if (lane == 31) sm.warpSums[warp] = v;
-        __syncthreads();
-        u32 wOff = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w)
-            if (w < warp) wOff += sm.warpSums[w];
-        if (d < R) sm.localStart[d] = wOff + v - cnt;
-    }
-    __syncthreads();
-    // keys (and their digits) in tile order
-#pragma unroll
-    for (int i = 0; i < Items; ++i)
-    {
-        const size_t idx = warpBase + size_t(i) * 32 + lane;
-        if (idx < tileEnd)
-        {
-            const unsigned d = (dpack[i >> 2] >> (8 * (i & 3))) & 0xffu;
-            const u32 r = (rank2[i >> 1] >> ((i & 1) * 16)) & 0xffffu;
-            const u32 pos = sm.localStart[d] + sm.warpHist[warp][d] + r;
-            sm.keys[pos] = key[i];
-            sm.digit[pos] = (unsigned char)d;
-        }
-    }
-    // look-back: global start of each digit for this tile
-    if (tid < R)
-    {
-        const int d = tid;
-        const u64 total = sm.count[d];
-        u64 excl = 0;
-        if (!tiles.chainStart(tile))
-        {
-            long long j = (long long)tile - 1;
-            unsigned spins = 0;
-            while (j >= 0)
-            {
-                u64 w8[kLookbackWindow];
-#pragma unroll
-                for (int k = 0; k < kLookbackWindow; ++k)
-                    w8[k] = j - k >= 0 ? ldRelaxed(status + size_t(j - k) * R + d) : kFlagPrefix;
-                int k = 0;
-                bool done = false;
-                for (; k < kLookbackWindow; ++k)
-                {
-                    const u64 flag = w8[k] & ~kValueMask;
-                    if (flag == 0) break;
-                    excl += w8[k] & kValueMask;
-                    if (flag == kFlagPrefix)
-                    {
-                        done = true;
-                        break;
-                    }
-                }
-                if (done) break;
-                j -= k;
-                if (k < kLookbackWindow)
-                {
-                    if (++spins > spinLimit)
-                    {
-                        atomicExch(error, kErrLookback);
-                        break;
-                    }
-                    if (spins > 64) __nanosleep(64);
-                }
-            }
-            stRelaxed(status + tile * R + d, kFlagPrefix | (excl + total));
-        }
-        sm.gstart[d] = tiles.digitBase(tile)[d] + u32(excl) - sm.localStart[d];
-    }
-    __syncthreads();
-    const size_t remain = tileEnd - tileBase;
-    const int valid = remain < size_t(T) ? int(remain) : T;
-#pragma unroll 4
-    for (int j = tid; j < valid; j += kThreads) keysOut[sm.gstart[sm.digit[j]] + u32(j)] = sm.keys[j];
-    __syncthreads();
-    // values: read in tile order, placed like their keys, written out
-    u32 *sv = reinterpret_cast<u32 *>(sm.keys);
-#pragma unroll
-    for (int i = 0; i < Items; ++i)
-    {
-        const size_t idx = warpBase + size_t(i) * 32 + lane;
-        if (idx < tileEnd)
-        {
-            const unsigned d = (dpack[i >> 2] >> (8 * (i & 3))) & 0xffu;
-            const u32 r = (rank2[i >> 1] >> ((i & 1) * 16)) & 0xffffu;
-            const u32 pos = sm.localStart[d] + sm.warpHist[warp][d] + r;
-            sv[pos] = valsIn ? __ldcs(valsIn + idx) : u32(idx) - tiles.valueOffset(tile);
-        }
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int j = tid; j < valid; j += kThreads) valsOut[sm.gstart[sm.digit[j]] + u32(j)] = sv[j];
-}
-
-// CTAs per SM each configuration is built for (mode 0: its shared memory and
-// a 64-register budget allow 4 CTAs for tiles of up to 3072 keys; mode 1
-// needs about half the shared memory).
-template <int Bits, int Items, int Mode>
+// CTAs per SM each configuration is built for.
+template <int Bits, int Items>
 constexpr int passMinBlocks()
 {
-    return Mode == 1 ? (Items <= 8 ? 6 : 5) : (Items <= 12 ? 4 : 3);
-}
-
-template <int Bits, int Items, int Mode>
-constexpr size_t passSmemBytes()
-{
-    return Mode == 1 ? sizeof(SharedPass1<Bits, Items>) : sizeof(SharedPass<Bits, Items>);
-}
-
-template <int Bits, int Items, int Mode, class Tiles>
-__device__ __forceinline__ void onesweepAny(const Tiles &tiles, const u64 *__restrict__ keysIn,
-                                            const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
-                                            u32 *__restrict__ valsOut, int shift, u32 *tileCounter, u64 *status,
-                                            int *error, int bits)
-{
-    if constexpr (Mode == 1)
-        onesweepTile1<Bits, Items>(tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);
-    else
-        onesweepTile<Bits, Items>(tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);
+    return Items <= 12 ? 4 : 3;
 }
 
 // One onesweep pass over keys[0, n): digit at bit `shift` (`bits` wide).
 // valsIn == nullptr means values are the input indices (first pass).  The
 // look-back status holds one word per tile and digit of the radix.
-template <int Bits, int Items, int Mode>
-static __global__ void __launch_bounds__(kThreads, passMinBlocks<Bits, Items, Mode>())
+template <int Bits, int Items>
+static __global__ void __launch_bounds__(kThreads, passMinBlocks<Bits, Items>())
     onesweepKernel(const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
                    u32 *__restrict__ valsOut, size_t n, int shift, const u32 *__restrict__ bins, u32 *tileCounter,
                    u64 *status, int *error, int bits)
 {
-    onesweepAny<Bits, Items, Mode>(ContiguousTiles<kThreads * Items>{n, bins}, keysIn, valsIn, keysOut, valsOut, shift,
-                                   tileCounter, status, error, bits);
+    onesweepTile<Bits, Items>(ContiguousTiles<kThreads * Items>{n, bins}, keysIn, valsIn, keysOut, valsOut, shift,
+                              tileCounter, status, error, bits);
 }
 
 // One onesweep pass over the segments of a forest: every segment is sorted
 // on its own (stable within the segment), in place in the global arrays.
-template <int Bits, int Items, int Mode>
-static __global__ void __launch_bounds__(kThreads, passMinBlocks<Bits, Items, Mode>())
+template <int Bits, int Items>
+static __global__ void __launch_bounds__(kThreads, passMinBlocks<Bits, Items>())
     segmentOnesweepKernel(SegmentTiles tiles, const u64 *__restrict__ keysIn, const u32 *__restrict__ valsIn,
                           u64 *__restrict__ keysOut, u32 *__restrict__ valsOut, int shift, u32 *tileCounter,
                           u64 *status, int *error, int bits)
 {
-    onesweepAny<Bits, Items, Mode>(tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);
+    onesweepTile<Bits, Items>(tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);
 }
 
 // ---------------------------------------------------------------------------
 // Host-side dispatch over kSortConfigs (one instantiation per configuration):
-// X(index, digit bits, keys per thread, mode), in the order of kSortConfigs.
+// X(index, digit bits, keys per thread), in the order of kSortConfigs.
 // ---------------------------------------------------------------------------
-#define AOT_SORT_CONFIGS(X) \
-    X(0, 8, 10, 0) X(1, 8, 16, 0) X(2, 8, 8, 0) X(3, 7, 12, 0) X(4, 7, 16, 0) X(5, 8, 10, 1) X(6, 8, 8, 1) X(7, 8, 12, 1)
+#define AOT_SORT_CONFIGS(X) X(0, 8, 10) X(1, 8, 16) X(2, 8, 8) X(3, 7, 12) X(4, 7, 16)
 
 inline size_t passSmem(int c)
 {
     switch (c)
     {
-#define AOT_CASE(i, B, I, M) \
-    case i: return passSmemBytes<B, I, M>();
+#define AOT_CASE(i, B, I) \
+    case i: return sizeof(SharedPass<B, I>);
         AOT_SORT_CONFIGS(AOT_CASE)
 #undef AOT_CASE
     default: throw std::invalid_argument("sort: unknown configuration");
@@ -760,11 +539,11 @@ static inline void setPassSmemAll()
     int dev = 0;
     AOT_CHECK(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && done[dev]) return;
-#define AOT_CASE(i, B, I, M)                                                                                     \
-    AOT_CHECK(cudaFuncSetAttribute(onesweepKernel<B, I, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
-                                   int(passSmemBytes<B, I, M>())));                                             \
-    AOT_CHECK(cudaFuncSetAttribute(segmentOnesweepKernel<B, I, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                   int(passSmemBytes<B, I, M>())));
+#define AOT_CASE(i, B, I)                                                                                        \
+    AOT_CHECK(cudaFuncSetAttribute(onesweepKernel<B, I>, cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                                   int(sizeof(SharedPass<B, I>))));                                              \
+    AOT_CHECK(cudaFuncSetAttribute(segmentOnesweepKernel<B, I>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                   int(sizeof(SharedPass<B, I>))));
     AOT_SORT_CONFIGS(AOT_CASE)
 #undef AOT_CASE
     if (dev >= 0 && dev < 64) done[dev] = true;
@@ -777,9 +556,9 @@ static inline void launchPass(int c, cudaStream_t s, const u64 *keysIn, const u3
     const unsigned tiles = unsigned((n + size_t(configTile(c)) - 1) / size_t(configTile(c)));
     switch (c)
     {
-#define AOT_CASE(i, B, I, M)                                                                                     \
+#define AOT_CASE(i, B, I)                                                                                        \
     case i:                                                                                                      \
-        onesweepKernel<B, I, M><<<tiles, kThreads, passSmemBytes<B, I, M>(), s>>>(                               \
+        onesweepKernel<B, I><<<tiles, kThreads, sizeof(SharedPass<B, I>), s>>>(                                  \
             keysIn, valsIn, keysOut, valsOut, n, shift, bins, tileCounter, status, error, bits);                 \
         break;
         AOT_SORT_CONFIGS(AOT_CASE)
@@ -795,9 +574,9 @@ static inline void launchSegmentPass(int c, cudaStream_t s, unsigned numTiles, c
 {
     switch (c)
     {
-#define AOT_CASE(i, B, I, M)                                                                                     \
+#define AOT_CASE(i, B, I)                                                                                        \
     case i:                                                                                                      \
-        segmentOnesweepKernel<B, I, M><<<numTiles, kThreads, passSmemBytes<B, I, M>(), s>>>(                     \
+        segmentOnesweepKernel<B, I><<<numTiles, kThreads, sizeof(SharedPass<B, I>), s>>>(                       \
             tiles, keysIn, valsIn, keysOut, valsOut, shift, tileCounter, status, error, bits);                   \
         break;
         AOT_SORT_CONFIGS(AOT_CASE)

@@ -80,7 +80,7 @@ int TreeEngine::boundedWaitProbe(int which, unsigned spinLimit)
         AOT_CHECK(cudaMemsetAsync(status.p, 0, size_t(kProbeTiles) * sort::kRadix * sizeof(u64), s));
         const u32 firstTile = 1;  // tile 0 is never taken, so it never publishes
         AOT_CHECK(cudaMemcpyAsync(counter.p, &firstTile, sizeof(u32), cudaMemcpyHostToDevice, s));
-        const int smem = int(sizeof(sort::SharedPass<8, kProbeItems>));  // a mode-0 pass
+        const int smem = int(sizeof(sort::SharedPass<8, kProbeItems>));
         AOT_CHECK(cudaFuncSetAttribute(sortWaitProbeKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         sortWaitProbeKernel<<<kProbeTiles - 1, sort::kThreads, smem, s>>>(
             keysIn.as<u64>(), keysOut.as<u64>(), valsOut.as<u32>(), n, bins.as<u32>(), counter.as<u32>(),
