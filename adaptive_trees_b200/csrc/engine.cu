@@ -742,7 +742,7 @@ struct TreeEngine::Impl
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
     DevMem nodeRows;  // node table of the near-field refresh (NFCount)
     // converged build by levels (levelbuild.cuh): unit arena and its control
-    DevMem lvRows, lvVal, lvChild, lvLeaves, lvOffset, lvScan, lvCtl;
+    DevMem lvRows, lvVal, lvChild, lvLeaves, lvOffset, lvScan, lvCtl, lvNbr, lvParent;
     size_t lvCap = 0;
     int lvLevels = int(kOctLevels);  // levels the last level build needed, with one to spare
     u32 nodeSlots = 0;
@@ -787,7 +787,7 @@ struct TreeEngine::Impl
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
                                &viewSort.counters, &viewSort.status, &nodeRows, &lvRows, &lvVal, &lvChild,
-                               &lvLeaves, &lvOffset, &lvScan, &lvCtl};
+                               &lvLeaves, &lvOffset, &lvScan, &lvCtl, &lvNbr, &lvParent};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -1497,9 +1497,14 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
     const lb::Control &hc = *reinterpret_cast<const lb::Control *>(host.data());
     for (;;)
     {
-        if (cap > 0xfffffff0ull) throw std::length_error("adaptive_octree: level build arena exceeds 32-bit indices");
+        if (cap >= (size_t(1) << 28)) return false;  // neighbour references hold unit * 8 + digit in 31 bits
         m.lvRows.reserve(cap * lb::kRow * sizeof(u32), s);
-        if (nf) m.lvVal.reserve(cap * 8 * sizeof(u32), s);
+        if (nf)
+        {
+            m.lvVal.reserve(cap * 8 * sizeof(u32), s);
+            m.lvNbr.reserve(cap * 27 * sizeof(u32), s);
+            m.lvParent.reserve(cap * sizeof(u32), s);
+        }
         m.lvChild.reserve(cap * 8 * sizeof(u32), s);
         m.lvLeaves.reserve(cap * sizeof(u32), s);
         m.lvOffset.reserve(cap * sizeof(u32), s);
@@ -1510,6 +1515,8 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         lb::Arena a{};
         a.rows = m.lvRows.as<u32>();
         a.val = nf ? m.lvVal.as<u32>() : nullptr;
+        a.nbr = nf ? m.lvNbr.as<u32>() : nullptr;
+        a.parent = nf ? m.lvParent.as<u32>() : nullptr;
         a.child = m.lvChild.as<u32>();
         a.leaves = m.lvLeaves.as<u32>();
         a.offset = m.lvOffset.as<u32>();
@@ -1520,13 +1527,7 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         a.cap = u32(cap);
         AOT_CHECK(cudaMemsetAsync(m.lvCtl.p, 0, kCtlBytes, s));
         AOT_CHECK(cudaMemsetAsync(m.lvScan.p, 0, scanWords * sizeof(u64), s));
-        const rb::NodeTable gt{m.nodeRows.as<u32>(), m.nodeSlots};
-        if (nf)
-        {
-            AOT_CHECK(cudaMemsetAsync(gt.rows, 0, size_t(gt.slots) * rb::kGroupRow * sizeof(u32), s));
-            ensureDigitPos();
-        }
-        m.nodeStale = true;  // the table holds this build's nodes only; an update refills it
+        if (nf) ensureDigitPos();
         lb::rootKernel<<<1, 1, 0, s>>>(a, m.bufs(), P, n_, cfg_.bucket, nf ? 1 : 0), noteLaunch();
         AOT_LAUNCH_CHECK();
         // Every kernel reads its level's size on the device, so the whole
@@ -1537,21 +1538,29 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         const int levels = std::max(1, std::min(int(kOctLevels), m.lvLevels));
         for (int l = 0; l < levels; ++l)
         {
-            if (nf) lb::expandKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, idx, l, gt), noteLaunch();
-            else lb::expandKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, idx, l, gt), noteLaunch();
+            lb::expandKernel<<<blocks * 2, lb::kThreads, 0, s>>>(a, idx, l), noteLaunch();
             if (nf)
             {
                 markNearField(true);
                 if (cfg_.hilbert)
-                    lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
+                {
+                    if (l > 0) lb::nbrKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, l, m.kpd.h), noteLaunch();
+                    lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h), noteLaunch();
+                }
                 else
-                    lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h, gt), noteLaunch();
+                {
+                    if (l > 0) lb::nbrKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, l, m.kpd.h), noteLaunch();
+                    lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h), noteLaunch();
+                }
                 markNearField(false);
-                lb::classifyKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
+                if (cfg_.hilbert)
+                    lb::classifyKernel<true, true><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket, m.kpd.h), noteLaunch();
+                else
+                    lb::classifyKernel<true, false><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket, m.kpd.h), noteLaunch();
             }
             else
             {
-                lb::classifyKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket), noteLaunch();
+                lb::classifyKernel<false, false><<<blocks, lb::kThreads, 0, s>>>(a, l, cfg_.bucket, m.kpd.h), noteLaunch();
             }
             AOT_LAUNCH_CHECK();
         }

@@ -72,6 +72,8 @@ struct Arena
     u32 *child;      // [cap][8] unit index of an internal child, or kLeaf
     u32 *leaves;     // [cap] leaves in the unit's subtree
     u32 *offset;     // [cap] cornerstone index of the unit's first leaf
+    u32 *nbr;        // NFCount: [cap][27] the cells around each unit (nbrRef)
+    u32 *parent;     // NFCount: [cap] parent unit * 8 + the unit's digit in it
     u64 *scan;       // look-back status of the classify tiles of every level
     Control *ctl;
     unsigned long long *contrib;  // [kArrivals][kJumps][kJumps] final leaves per (a, k, j)
@@ -86,6 +88,19 @@ __host__ __device__ __forceinline__ u32 regionWord(u32 a, u32 level, u32 k) { re
 __device__ __forceinline__ u32 regionArrival(u32 w) { return w & 0xffu; }
 __device__ __forceinline__ u32 regionLevel(u32 w) { return (w >> 8) & 0x1fu; }
 __device__ __forceinline__ u32 regionDepth(u32 w) { return (w >> 16) & 7u; }
+// The same word also holds the unit's own level (bits 19-23) and the curve
+// state that orders its children (bits 24-29, Hilbert).
+__host__ __device__ __forceinline__ u32 withUnit(u32 region, u32 level, u32 state)
+{
+    return (region & 0x7ffffu) | (level << 19) | (state << 24);
+}
+__device__ __forceinline__ u32 unitLevelOf(u32 w) { return (w >> 19) & 0x1fu; }
+__device__ __forceinline__ u32 unitStateOf(u32 w) { return (w >> 24) & 0x3fu; }
+
+// A cell around a unit, at the unit's level: a unit index when the cell is an
+// internal node, else kLeafRef | (parent unit * 8 + digit) naming the leaf
+// of the tree that holds the cell (the cell itself or a coarser leaf).
+constexpr u32 kLeafRef = 0x80000000u;
 
 // Levels a leaf of value x at level m splits by (calculateNodeOp,
 // octree_rebalance.cuh:188-249: 8, 64, 512 or 4096 children), given that it
@@ -132,9 +147,15 @@ static __global__ void rootKernel(Arena a, rb::TreeBufs tb, const u64 *P, size_t
         row[1] = 0;
         row[2] = 0;
         row[10] = active;
-        row[11] = regionWord(0, 0, splitDepth(nf != 0, x, bucket, 0));
+        row[11] = withUnit(regionWord(0, 0, splitDepth(nf != 0, x, bucket, 0)), 0, kHilbertStart);
         c.levelCount[0] = 1;
         a.offset[0] = 0;
+        if (nf)
+        {
+            // every cell around the root is the root (periodic wrap)
+            for (int q = 0; q < 27; ++q) a.nbr[q] = 0;
+            a.parent[0] = kLeaf;
+        }
         st->numLeaves = 0;  // set when the tree is placed
     }
     else
@@ -212,9 +233,8 @@ __device__ __forceinline__ void innerBegins(const KeyIndex &idx, u32 lo, u32 hi,
 }
 
 // 9 child begins of the units of level l, one thread per unit (the 7 inner
-// ones by innerBegins).  NFCount also enters the unit in the node table.
-template <bool NF>
-static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, KeyIndex idx, int l, rb::NodeTable gt)
+// ones by innerBegins).
+static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, KeyIndex idx, int l)
 {
     const Control &c = *a.ctl;
     if (c.overflow | c.late | c.error) return;
@@ -223,49 +243,83 @@ static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, KeyInde
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
     {
         u32 *row = a.rows + size_t(start + i) * kRow;
-        const u64 key = rowKey(row);
-        const u32 lo = row[2], hi = row[10];
         u32 b[7];
-        innerBegins(idx, lo, hi, key, cr, b);
+        innerBegins(idx, row[2], row[10], rowKey(row), cr, b);
 #pragma unroll
         for (int d = 0; d < 7; ++d) row[3 + d] = b[d];
-        if constexpr (NF)
+    }
+}
+
+// The 27 cells around every unit of level l >= 1, from those around its
+// parent U: the cell at offset (dx, dy, dz) of the unit (octant o in U) is
+// child o' of the cell at offset floor((o + d) / 2) around U, o' =
+// (o + d) mod 2 per axis.  That cell is a unit (the child of a unit around
+// U, if internal) or lies in a leaf: a leaf child of a unit around U, or the
+// leaf that already holds U's cell.
+template <bool Hilbert>
+static __global__ void __launch_bounds__(kThreads) nbrKernel(Arena a, int l, HilbertTables h)
+{
+    __shared__ unsigned char sEnc[48 * 8], sDec[48 * 8];
+    const Control &c = *a.ctl;
+    if (c.overflow | c.late | c.error) return;
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    const size_t total = size_t(count) * 27;
+    if (total <= size_t(blockIdx.x) * blockDim.x) return;
+    if constexpr (Hilbert)
+    {
+        for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
         {
-            u32 *t = rb::nodeRow(gt, rb::cellCode(key, unsigned(l)));
-            if (t)
-            {
-                t[0] = lo;
-#pragma unroll
-                for (int d = 0; d < 7; ++d) t[1 + d] = b[d];
-                t[8] = hi;
-            }
+            sEnc[k] = h.enc[k];
+            sDec[k] = h.decOct[k];
         }
+        __syncthreads();
+    }
+    for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += size_t(gridDim.x) * blockDim.x)
+    {
+        const u32 g = start + u32(e / 27);
+        const int q = int(e - size_t(e / 27) * 27);
+        const u32 pr = a.parent[g];
+        const u32 U = pr >> 3, d = pr & 7u;
+        const u32 stU = unitStateOf(a.rows[size_t(U) * kRow + 11]);
+        const int o = Hilbert ? int(sDec[stU * 8 + d]) : int(d);
+        const int tx = (o >> 2) + q % 3 - 1, ty = ((o >> 1) & 1) + (q / 3) % 3 - 1, tz = (o & 1) + q / 9 - 1;
+        const int qp = ((tx + 2) / 2) + 3 * ((ty + 2) / 2) + 9 * ((tz + 2) / 2);  // offset around U
+        const u32 r = a.nbr[size_t(U) * 27 + qp];
+        u32 ref = r;
+        if (!(r & kLeafRef))
+        {
+            const int oc = ((tx & 1) << 2) | ((ty & 1) << 1) | (tz & 1);
+            const u32 stV = unitStateOf(a.rows[size_t(r) * kRow + 11]);
+            const u32 dv = Hilbert ? u32(sEnc[stV * 8 + oc]) : u32(oc);
+            const u32 ch = a.child[size_t(r) * 8 + dv];
+            ref = ch != kLeaf ? ch : (kLeafRef | (r * 8 + dv));
+        }
+        a.nbr[size_t(g) * 27 + q] = ref;
     }
 }
 
 // Near-field counts of the children of the level-l units: per unit, the 27
-// parent-level cells around it give the 4 x 4 x 4 block of child counts (from
-// the node table, or counted inside the leaf that holds them), and each child
-// sums its 3 x 3 x 3 sub-block (octNearFieldKernel, here with the units taken
-// from the arena instead of the leaves of a tree).
+// parent-level cells Q around it (nbrKernel) give the 4 x 4 x 4 block of
+// child counts -- from the 9 child begins of Q when Q is a unit, counted
+// within the keys of the leaf that holds Q otherwise -- and each child sums
+// its 3 x 3 x 3 sub-block (octNearFieldKernel's unit, with the cells around
+// it known instead of looked up).
 // Per-warp scratch of the units in flight (the refresh's scratch without the
 // group-flag populations, which leaves more of the SM's shared storage to L1).
 struct UnitScratch
 {
     u64 pStart[rb::kUnitBatch], st0[rb::kUnitBatch], st1[rb::kUnitBatch], st2[rb::kUnitBatch];
     u32 cx[rb::kUnitBatch], cy[rb::kUnitBatch], cz[rb::kUnitBatch];
-    u32 hintB[rb::kUnitBatch];
     int childState[rb::kUnitBatch], level[rb::kUnitBatch];
     u32 block[rb::kUnitBatch][64];
-    u64 slowKey[rb::kUnitBatch * 27];
+    u32 slowRef[rb::kUnitBatch * 27];
     unsigned short slowItem[rb::kUnitBatch * 27];
-    unsigned char slowState[rb::kUnitBatch * 27];
     int nSlow;
 };
 
 template <bool Hilbert>
 static __global__ void __launch_bounds__(kThreads, 4)
-    nearFieldKernel(Arena a, KeyIndex idx, int l, HilbertTables h, rb::NodeTable gt)
+    nearFieldKernel(Arena a, KeyIndex idx, int l, HilbertTables h)
 {
     using rb::kUnitBatch;
     __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8], sDec[48 * 8];
@@ -307,59 +361,69 @@ static __global__ void __launch_bounds__(kThreads, 4)
             w.st1[lane] = path.st1;
             w.st2[lane] = path.st2;
             w.childState[lane] = path.childState;
-            w.hintB[lane] = row[2];
         }
         if (lane == 0) w.nSlow = 0;
         __syncwarp();
-        // phase A: (unit, Q) pairs over the lanes, internal Q from the table
+        // phase A: (unit, Q) pairs over the lanes; a Q that is a unit gives
+        // its children's counts from its row
         const int items = nb * 27;
         for (int ib = 0; ib < items; ib += 32)
         {
             const int it = ib + lane;
             const int u = it / 27, q = it - (it / 27) * 27;
+            u32 ref = 0;
             bool slow = false;
-            u64 qKey = 0;
-            int qState = 0;
             if (it < items)
             {
-                qKey = rb::neighbourCell<Hilbert>(w, u, q, qState, sEnc, sNext);
-                u32 gb[rb::kGroupBegins];
-                if (rb::nodeBegins(gt, rb::cellCode(qKey, unsigned(l)), gb))
+                ref = a.nbr[size_t(start + base + u32(u)) * 27 + q];
+                if (ref & kLeafRef)
                 {
-                    rb::childrenFromPacked<Hilbert>(gb, q, qState, w.block[u]);
+                    slow = true;
                 }
                 else
                 {
-                    slow = true;
+                    const uint4 *vr = reinterpret_cast<const uint4 *>(a.rows + size_t(ref) * kRow);
+                    const uint4 r0 = vr[0], r1 = vr[1], r2 = vr[2];
+                    const u32 gb[rb::kGroupBegins] = {r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z};
+                    rb::childrenFromPacked<Hilbert>(gb, q, int(unitStateOf(r2.w)), w.block[u]);
                 }
             }
             const unsigned slowMask = __ballot_sync(0xffffffffu, slow);
             if (slow)
             {
                 const int k = w.nSlow + __popc(slowMask & ltMask);
-                w.slowKey[k] = qKey;
+                w.slowRef[k] = ref;
                 w.slowItem[k] = (unsigned short)it;
-                w.slowState[k] = (unsigned char)qState;
             }
             __syncwarp();
             if (lane == 0) w.nSlow += __popc(slowMask);
             __syncwarp();
         }
-        // phase B: Q that are no internal node, counted inside their leaf
+        // phase B: Q in a leaf: its children counted among the leaf's keys
         const int nSlow = w.nSlow;
         for (int k = lane; k < nSlow; k += 32)
         {
             const int it = w.slowItem[k];
             const int u = it / 27, q = it - u * 27;
-            const u64 qKey = w.slowKey[k];
-            const int qState = int(w.slowState[k]);
-            u32 begins[rb::kGroupBegins];
-            if (!rb::beginsInside(gt, idx.keys, u32(idx.n), qKey, m, begins))
+            const u32 lr = w.slowRef[k] & ~kLeafRef;
+            const u32 P = lr >> 3, d = lr & 7u;
+            const u32 *prow = a.rows + size_t(P) * kRow;
+            const u32 preg = prow[11];
+            u64 qKey;
+            int qState;
+            if (unitLevelOf(preg) + 1 == unsigned(l))
             {
-                const u32 lo = idx.lowerNear<rb::kNFGallop>(w.hintB[u], qKey);
-                const u32 hi = rb::lowerFrom(idx, lo, qKey + octRange(m - 1));
-                rb::childBeginsWithin(idx.keys, lo, hi, qKey, m, begins);
+                // the leaf is Q itself: child d of its parent unit
+                qKey = rowKey(prow) + u64(d) * octRange(unsigned(l));
+                const u32 stP = unitStateOf(preg);
+                qState = Hilbert ? int(sNext[stP * 8 + sDec[stP * 8 + d]]) : kHilbertStart;
             }
+            else
+            {
+                qKey = rb::neighbourCell<Hilbert>(w, u, q, qState, sEnc, sNext);
+            }
+            u32 begins[rb::kGroupBegins];
+            rb::childBeginsWithin(idx.keys, prow[2 + d], prow[3 + d], qKey, m, begins);
             rb::childrenFromPacked<Hilbert>(begins, q, qState, w.block[u]);
         }
         __syncwarp();
@@ -406,16 +470,25 @@ static __global__ void __launch_bounds__(kThreads, 4)
 // Children of the level-l units: those whose value exceeds the bucket (below
 // level 21) become the units of level l + 1, in key order; the others are
 // leaves, counted into the round history by (arrival, depth, relative level).
-template <bool NF>
-static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l, unsigned bucket)
+template <bool NF, bool Hilbert>
+static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l, unsigned bucket, HilbertTables h)
 {
     __shared__ i64 sWarp[kThreads / 32];
     __shared__ u32 sTile;
     __shared__ i64 sPrefix;
     __shared__ u32 sContrib[kContribBins];
     __shared__ u32 sLanded[kArrivals];
+    __shared__ unsigned char sNext[48 * 8], sDec[48 * 8];
     Control &c = *a.ctl;
     if (c.overflow | c.late | c.error) return;
+    if constexpr (Hilbert)
+    {
+        for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
+        {
+            sNext[k] = h.encNext[k];
+            sDec[k] = h.decOct[k];
+        }
+    }
     const u32 start = c.levelStart[l], count = c.levelCount[l];
     const u32 next = start + count;
     const unsigned m = unsigned(l) + 1;
@@ -479,6 +552,15 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
                             if (aR + 2 < u32(kArrivals)) atomicAdd(&sLanded[aR + 1], 1u);
                             else c.late = 1;
                         }
+                        // the child's own level and the curve state ordering its children
+                        u32 cst = kHilbertStart;
+                        if constexpr (Hilbert)
+                        {
+                            const u32 st = unitStateOf(reg);
+                            cst = sNext[st * 8 + sDec[st * 8 + d]];
+                        }
+                        creg = withUnit(creg, m, cst);
+                        if constexpr (NF) a.parent[gc] = g * 8 + u32(d);
                         u32 *crow = a.rows + size_t(gc) * kRow;
                         const u64 ck = key + u64(d) * cr;
                         crow[0] = u32(ck);
