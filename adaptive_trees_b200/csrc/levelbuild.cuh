@@ -232,88 +232,21 @@ __device__ __forceinline__ void innerBegins(const KeyIndex &idx, u32 lo, u32 hi,
     }
 }
 
-// The same 7 lower bounds for a unit with many keys, by a whole warp: each
-// boundary by a group of 4 lanes testing 4 pivots per step (5-ary search),
-// first among the samples, then in the window they leave.  Lanes 28-31
-// only take part in the shuffles.  Returns the boundary of group `lane / 4`
-// (meaningful in lanes 0-27).
-__device__ __forceinline__ u32 groupLowerBound(const u64 *arr, u32 b, u32 len, u64 v)
-{
-    // answer in [b, b + len]
-    const int lane = threadIdx.x & 31, sub = lane & 3, base = lane & ~3;
-    while (__any_sync(0xffffffffu, len > 0))
-    {
-        const u32 p = b + u32((u64(sub + 1) * len) / 5);
-        const bool less = len > 0 && p < b + len && __ldg(arr + p) < v;
-        const unsigned bits = (__ballot_sync(0xffffffffu, less) >> base) & 15u;
-        if (len > 0)
-        {
-            // the pivots below the target form a prefix of the group's 4
-            const int below = __popc(bits);
-            const u32 end = b + len;
-            const u32 pLo = below ? b + u32((u64(below) * len) / 5) + 1 : b;
-            const u32 pHi = below < 4 ? b + u32((u64(below + 1) * len) / 5) : end;
-            b = pLo;
-            len = pHi - pLo;
-        }
-    }
-    return b;
-}
-
-__device__ __forceinline__ u32 warpInnerBegin(const KeyIndex &idx, u32 lo, u32 hi, u64 key, u64 cr)
-{
-    const int grp = (threadIdx.x & 31) >> 2;
-    const u64 v = key + u64(grp < 7 ? grp + 1 : 7) * cr;
-    const u32 jA = (lo + kSampleStride - 1) >> kSampleShift, jB = (hi + kSampleStride - 1) >> kSampleShift;
-    const u32 s = groupLowerBound(idx.sample, jA, jB > jA ? jB - jA : 0, v);
-    const u32 wlo = s > jA ? ((s - 1) << kSampleShift) + 1 : lo;
-    const u32 whi = s < jB ? (s << kSampleShift) : hi;
-    return groupLowerBound(idx.keys, wlo, whi - wlo, v);
-}
-
 // 9 child begins of the units of level l, one thread per unit (the 7 inner
-// ones by innerBegins); units with many keys are queued per CTA and searched
-// by whole warps (warpInnerBegin), so that no thread walks a long chain of
-// dependent loads alone.
-constexpr u32 kWarpSearchMin = 1024;  // keys from which a unit is searched by a warp
-constexpr int kWarpQueue = 64;
-
+// ones by innerBegins).
 static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, KeyIndex idx, int l)
 {
-    __shared__ u32 sQueue[kWarpQueue];
-    __shared__ int sQueued;
     const Control &c = *a.ctl;
     if (c.overflow | c.late | c.error) return;
     const u32 start = c.levelStart[l], count = c.levelCount[l];
-    if (count <= blockIdx.x * blockDim.x) return;
     const u64 cr = octRange(unsigned(l) + 1);
-    if (threadIdx.x == 0) sQueued = 0;
-    __syncthreads();
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
     {
         u32 *row = a.rows + size_t(start + i) * kRow;
-        if (row[10] - row[2] >= kWarpSearchMin)
-        {
-            const int k = atomicAdd(&sQueued, 1);
-            if (k < kWarpQueue)
-            {
-                sQueue[k] = i;
-                continue;
-            }
-        }
         u32 b[7];
         innerBegins(idx, row[2], row[10], rowKey(row), cr, b);
 #pragma unroll
         for (int d = 0; d < 7; ++d) row[3 + d] = b[d];
-    }
-    __syncthreads();
-    const int queued = min(sQueued, kWarpQueue);
-    const int lane = threadIdx.x & 31;
-    for (int j = int(threadIdx.x >> 5); j < queued; j += kThreads / 32)
-    {
-        u32 *row = a.rows + size_t(start + sQueue[j]) * kRow;
-        const u32 b = warpInnerBegin(idx, row[2], row[10], rowKey(row), cr);
-        if (lane < 28 && (lane & 3) == 0) row[3 + (lane >> 2)] = b;
     }
 }
 
