@@ -742,7 +742,7 @@ struct TreeEngine::Impl
     DevMem K[2], B[2], NF[2], N[2], G[2], offs, dirty, scan;
     DevMem nodeRows;  // node table of the near-field refresh (NFCount)
     // converged build by levels (levelbuild.cuh): unit arena and its control
-    DevMem lvRows, lvVal, lvChild, lvLeaves, lvOffset, lvScan, lvCtl, lvNbr, lvParent;
+    DevMem lvRows, lvVal, lvChild, lvLeaves, lvOffset, lvCtl, lvNbr, lvParent;
     size_t lvCap = 0;
     int lvLevels = int(kOctLevels);  // levels the last level build needed, with one to spare
     u32 nodeSlots = 0;
@@ -787,7 +787,7 @@ struct TreeEngine::Impl
                                &vLvVals[1],  &vLayKeys[0], &vLayKeys[1],    &vLayVals[0],  &vLayVals[1],
                                &vIntStartSfc, &vIntLevelSfc, &vIntM,        &vIntStartLay, &vIntLevelLay,
                                &viewSort.counters, &viewSort.status, &nodeRows, &lvRows, &lvVal, &lvChild,
-                               &lvLeaves, &lvOffset, &lvScan, &lvCtl, &lvNbr, &lvParent};
+                               &lvLeaves, &lvOffset, &lvCtl, &lvNbr, &lvParent};
         size_t s = 0;
         for (const DevMem *d : all) s += d->bytes;
         return s;
@@ -1508,8 +1508,6 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         m.lvChild.reserve(cap * 8 * sizeof(u32), s);
         m.lvLeaves.reserve(cap * sizeof(u32), s);
         m.lvOffset.reserve(cap * sizeof(u32), s);
-        const size_t scanWords = (cap + lb::kThreads - 1) / lb::kThreads + 64;
-        m.lvScan.reserve(scanWords * sizeof(u64), s);
         m.lvCtl.reserve(kCtlBytes, s);
         m.lvCap = cap;
         lb::Arena a{};
@@ -1520,13 +1518,11 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         a.child = m.lvChild.as<u32>();
         a.leaves = m.lvLeaves.as<u32>();
         a.offset = m.lvOffset.as<u32>();
-        a.scan = m.lvScan.as<u64>();
         a.ctl = m.lvCtl.as<lb::Control>();
         a.contrib = reinterpret_cast<unsigned long long *>(m.lvCtl.as<unsigned char>() + kHeadBytes);
         a.landed = a.contrib + lb::kContribBins;
         a.cap = u32(cap);
         AOT_CHECK(cudaMemsetAsync(m.lvCtl.p, 0, kCtlBytes, s));
-        AOT_CHECK(cudaMemsetAsync(m.lvScan.p, 0, scanWords * sizeof(u64), s));
         if (nf) ensureDigitPos();
         lb::rootKernel<<<1, 1, 0, s>>>(a, m.bufs(), P, n_, cfg_.bucket, nf ? 1 : 0), noteLaunch();
         AOT_LAUNCH_CHECK();

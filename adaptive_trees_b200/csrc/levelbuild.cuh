@@ -17,8 +17,8 @@
 //             units, one unit per parent cell as in the refresh of the
 //             rounds (octNearFieldKernel);
 //   classify  the children whose value exceeds the bucket become the units of
-//             level l + 1 (an order-preserving compaction with decoupled
-//             look-back); the others are leaves of the tree;
+//             level l + 1 (slots taken by warp-aggregated atomics); the
+//             others are leaves of the tree;
 //   leafCount, place: subtree leaf counts bottom-up, then every leaf's
 //             position in the cornerstone array top-down.
 //
@@ -56,10 +56,9 @@ struct Control
 {
     u32 levelStart[kOctLevels + 2];
     u32 levelCount[kOctLevels + 2];
-    u32 tileCounter[kOctLevels + 2];
     int overflow;       // the unit arena is too small
     int late;           // an arrival round beyond the tracked ones
-    int error;          // a bounded look-back gave up
+    int error;          // reserved (the level build has no waits)
     int placeOverflow;  // the tree has more leaves than the cornerstone buffers hold
 };
 
@@ -74,7 +73,6 @@ struct Arena
     u32 *offset;     // [cap] cornerstone index of the unit's first leaf
     u32 *nbr;        // NFCount: [cap][27] the cells around each unit (nbrRef)
     u32 *parent;     // NFCount: [cap] parent unit * 8 + the unit's digit in it
-    u64 *scan;       // look-back status of the classify tiles of every level
     Control *ctl;
     unsigned long long *contrib;  // [kArrivals][kJumps][kJumps] final leaves per (a, k, j)
     unsigned long long *landed;   // [kArrivals] internal nodes landing in round t
@@ -468,19 +466,23 @@ static __global__ void __launch_bounds__(kThreads, 4)
 }
 
 // Children of the level-l units: those whose value exceeds the bucket (below
-// level 21) become the units of level l + 1, in key order; the others are
-// leaves, counted into the round history by (arrival, depth, relative level).
+// level 21) become the units of level l + 1, the others are leaves, counted
+// into the round history by (arrival, depth, relative level).  A warp takes
+// the slots of its new units with one atomic add; the order of the units in
+// a level is free (every later step finds them through the child and parent
+// links, and the placement follows the digits).
 template <bool NF, bool Hilbert>
 static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l, unsigned bucket, HilbertTables h)
 {
-    __shared__ i64 sWarp[kThreads / 32];
-    __shared__ u32 sTile;
-    __shared__ i64 sPrefix;
     __shared__ u32 sContrib[kContribBins];
     __shared__ u32 sLanded[kArrivals];
     __shared__ unsigned char sNext[48 * 8], sDec[48 * 8];
     Control &c = *a.ctl;
     if (c.overflow | c.late | c.error) return;
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    const u32 next = start + count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) c.levelStart[l + 1] = next;
+    if (count <= blockIdx.x * blockDim.x) return;
     if constexpr (Hilbert)
     {
         for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
@@ -489,100 +491,107 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
             sDec[k] = h.decOct[k];
         }
     }
-    const u32 start = c.levelStart[l], count = c.levelCount[l];
-    const u32 next = start + count;
-    const unsigned m = unsigned(l) + 1;
-    const u64 cr = octRange(m);
-    const u32 numTiles = (count + kThreads - 1) / kThreads;
-    u64 *status = a.scan + (start + kThreads - 1) / kThreads + u32(l);
     for (int k = threadIdx.x; k < kContribBins; k += kThreads) sContrib[k] = 0;
     if (threadIdx.x < kArrivals) sLanded[threadIdx.x] = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) c.levelStart[l + 1] = next;
-    for (;;)
+    __syncthreads();
+    const unsigned m = unsigned(l) + 1;
+    const u64 cr = octRange(m);
+    const int lane = threadIdx.x & 31;
+    const u32 stride = gridDim.x * blockDim.x;
+    for (u32 i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < count; i0 += stride)
     {
-        __syncthreads();
-        if (threadIdx.x == 0) sTile = atomicAdd(&c.tileCounter[l], 1u);
-        __syncthreads();
-        const u32 tile = sTile;
-        if (tile >= numTiles) break;
-        const u32 i = tile * kThreads + threadIdx.x;
+        const u32 i = i0 + u32(lane);
         const bool valid = i < count;
         const u32 g = start + (valid ? i : 0);
-        const u32 *row = a.rows + size_t(g) * kRow;
+        const uint4 *row4 = reinterpret_cast<const uint4 *>(a.rows + size_t(g) * kRow);
         u32 b[rb::kGroupBegins], x[8];
         u32 reg = 0;
         u64 key = 0;
         unsigned highMask = 0;
         if (valid)
         {
-            key = rowKey(row);
-#pragma unroll
-            for (int d = 0; d < rb::kGroupBegins; ++d) b[d] = row[2 + d];
-            reg = row[11];
+            const uint4 r0 = row4[0], r1 = row4[1], r2 = row4[2];
+            key = (u64(r0.y) << 32) | r0.x;
+            b[0] = r0.z; b[1] = r0.w;
+            b[2] = r1.x; b[3] = r1.y; b[4] = r1.z; b[5] = r1.w;
+            b[6] = r2.x; b[7] = r2.y; b[8] = r2.z;
+            reg = r2.w;
+            if constexpr (NF)
+            {
+                const uint4 *v4 = reinterpret_cast<const uint4 *>(a.val + size_t(g) * 8);
+                const uint4 v0 = v4[0], v1 = v4[1];
+                x[0] = v0.x; x[1] = v0.y; x[2] = v0.z; x[3] = v0.w;
+                x[4] = v1.x; x[5] = v1.y; x[6] = v1.z; x[7] = v1.w;
+            }
 #pragma unroll
             for (int d = 0; d < 8; ++d)
             {
-                x[d] = NF ? a.val[size_t(g) * 8 + d] : b[d + 1] - b[d];
+                if constexpr (!NF) x[d] = b[d + 1] - b[d];
                 if (x[d] > bucket && m < kOctLevels) highMask |= 1u << d;
             }
         }
-        i64 total;
-        const i64 excl = rb::blockExclusiveScan(i64(__popc(highMask)), sWarp, total);
-        if (threadIdx.x == 0) sPrefix = rb::lookback(status, tile, total, &c.error);
-        __syncthreads();
-        if (valid)
-        {
-            const u32 aR = regionArrival(reg), lR = regionLevel(reg), kR = regionDepth(reg);
-            const u32 j = m - lR;  // 1 <= j <= kR
-            u32 rank = u32(sPrefix + excl);
+        // slots of the warp's new units: one atomic add per warp
+        const u32 nHigh = u32(__popc(highMask));
+        u32 incl = nHigh;
 #pragma unroll
-            for (int d = 0; d < 8; ++d)
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const u32 t = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += t;
+        }
+        u32 base = 0;
+        if (lane == 31 && incl) base = atomicAdd(&c.levelCount[l + 1], incl);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        if (!valid) continue;
+        const u32 aR = regionArrival(reg), lR = regionLevel(reg), kR = regionDepth(reg);
+        const u32 j = m - lR;  // 1 <= j <= kR
+        u32 rank = base + incl - nHigh;
+        u32 slots[8];
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
+        {
+            u32 slot = kLeaf;
+            if (highMask & (1u << d))
             {
-                u32 slot = kLeaf;
-                if (highMask & (1u << d))
+                const u32 gc = next + rank++;
+                if (gc < a.cap)
                 {
-                    const u32 gc = next + rank++;
-                    if (gc < a.cap)
+                    u32 creg = reg;
+                    if (j == kR)
                     {
-                        u32 creg = reg;
-                        if (j == kR)
-                        {
-                            // a landed internal node: a leaf in round aR + 1, splitting at once
-                            creg = regionWord(aR + 1, m, splitDepth(NF, x[d], bucket, m));
-                            if (aR + 2 < u32(kArrivals)) atomicAdd(&sLanded[aR + 1], 1u);
-                            else c.late = 1;
-                        }
-                        // the child's own level and the curve state ordering its children
-                        u32 cst = kHilbertStart;
-                        if constexpr (Hilbert)
-                        {
-                            const u32 st = unitStateOf(reg);
-                            cst = sNext[st * 8 + sDec[st * 8 + d]];
-                        }
-                        creg = withUnit(creg, m, cst);
-                        if constexpr (NF) a.parent[gc] = g * 8 + u32(d);
-                        u32 *crow = a.rows + size_t(gc) * kRow;
-                        const u64 ck = key + u64(d) * cr;
-                        crow[0] = u32(ck);
-                        crow[1] = u32(ck >> 32);
-                        crow[2] = b[d];
-                        crow[10] = b[d + 1];
-                        crow[11] = creg;
-                        slot = gc;
+                        // a landed internal node: a leaf in round aR + 1, splitting at once
+                        creg = regionWord(aR + 1, m, splitDepth(NF, x[d], bucket, m));
+                        if (aR + 2 < u32(kArrivals)) atomicAdd(&sLanded[aR + 1], 1u);
+                        else c.late = 1;
                     }
-                    else
+                    // the child's own level and the curve state ordering its children
+                    u32 cst = kHilbertStart;
+                    if constexpr (Hilbert)
                     {
-                        c.overflow = 1;
+                        const u32 st = unitStateOf(reg);
+                        cst = sNext[st * 8 + sDec[st * 8 + d]];
                     }
+                    if constexpr (NF) a.parent[gc] = g * 8 + u32(d);
+                    const u64 ck = key + u64(d) * cr;
+                    uint4 *crow = reinterpret_cast<uint4 *>(a.rows + size_t(gc) * kRow);
+                    crow[0] = make_uint4(u32(ck), u32(ck >> 32), b[d], 0u);
+                    crow[2] = make_uint4(0u, 0u, b[d + 1], withUnit(creg, m, cst));
+                    slot = gc;
                 }
                 else
                 {
-                    atomicAdd(&sContrib[(aR * kJumps + kR) * kJumps + j], 1u);
+                    c.overflow = 1;
                 }
-                a.child[size_t(g) * 8 + d] = slot;
             }
+            else
+            {
+                atomicAdd(&sContrib[(aR * kJumps + kR) * kJumps + j], 1u);
+            }
+            slots[d] = slot;
         }
-        if (tile == numTiles - 1 && threadIdx.x == kThreads - 1) c.levelCount[l + 1] = u32(sPrefix + excl) + u32(__popc(highMask));
+        uint4 *ch4 = reinterpret_cast<uint4 *>(a.child + size_t(g) * 8);
+        ch4[0] = make_uint4(slots[0], slots[1], slots[2], slots[3]);
+        ch4[1] = make_uint4(slots[4], slots[5], slots[6], slots[7]);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < kContribBins; k += kThreads)
