@@ -37,7 +37,7 @@ constexpr int kItems = 10;                  // keys per thread of the default co
 constexpr int kTile = kThreads * kItems;
 constexpr int kMaxPasses = 8;               // passes of 8-bit digits over 64-bit keys
 constexpr int kPassSlots = 10;              // most passes of any configuration (7-bit digits)
-constexpr int kMinTile = kThreads * 6;      // smallest tile of any configuration
+constexpr int kMinTile = kThreads * 8;      // smallest tile of any configuration
 constexpr u64 kFlagAgg = u64(1) << 62;
 constexpr u64 kFlagPrefix = u64(2) << 62;
 constexpr u64 kValueMask = (u64(1) << 62) - 1;
@@ -152,7 +152,7 @@ struct SortConfig
 {
     int bits, items;
 };
-constexpr SortConfig kSortConfigs[] = {{8, 10}, {8, 16}, {8, 8}, {7, 12}, {7, 16}, {8, 6}};
+constexpr SortConfig kSortConfigs[] = {{8, 10}, {8, 16}, {8, 8}, {7, 12}, {7, 16}};
 constexpr int kNumSortConfigs = int(sizeof(kSortConfigs) / sizeof(kSortConfigs[0]));
 constexpr int kDefaultSortConfig = 0;
 constexpr int configTile(int c) { return kThreads * kSortConfigs[c].items; }
@@ -486,7 +486,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
 template <int Bits, int Items>
 constexpr int passMinBlocks()
 {
-    return Items <= 6 ? 6 : (Items <= 12 ? 4 : 3);
+    return Items <= 12 ? 4 : 3;
 }
 
 // One onesweep pass over keys[0, n): digit at bit `shift` (`bits` wide).
@@ -517,7 +517,7 @@ static __global__ void __launch_bounds__(kThreads, passMinBlocks<Bits, Items>())
 // Host-side dispatch over kSortConfigs (one instantiation per configuration):
 // X(index, digit bits, keys per thread), in the order of kSortConfigs.
 // ---------------------------------------------------------------------------
-#define AOT_SORT_CONFIGS(X) X(0, 8, 10) X(1, 8, 16) X(2, 8, 8) X(3, 7, 12) X(4, 7, 16) X(5, 8, 6)
+#define AOT_SORT_CONFIGS(X) X(0, 8, 10) X(1, 8, 16) X(2, 8, 8) X(3, 7, 12) X(4, 7, 16)
 
 inline size_t passSmem(int c)
 {
