@@ -98,6 +98,8 @@ PROTOTYPES = {
                         ctypes.POINTER(AoConfig), vp, ctypes.POINTER(vp)],
     "ao_batch_destroy": [vp],
     "ao_batch_build": [vp],
+    "ao_batch_set_build_mode": [vp, ci],
+    "ao_batch_build_path": [vp, ctypes.POINTER(ci)],
     "ao_batch_update": [vp, vp],
     "ao_batch_update_until_converged": [vp, vp, ci, ctypes.POINTER(ci)],
     "ao_batch_needs_resize": [vp, ctypes.POINTER(ci)],

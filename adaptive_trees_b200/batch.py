@@ -65,6 +65,17 @@ class Batch:
     def build(self):
         C.check(C.load().ao_batch_build(self._h))
 
+    def setBuildMode(self, mode: int):
+        """build() path: 0 every system's converged tree by levels in one
+        persistent launch (falling back to rounds where needed), 1 the rounds."""
+        C.check(C.load().ao_batch_set_build_mode(self._h, int(mode)))
+
+    def buildPath(self) -> bool:
+        """True when the last build() used the level builder."""
+        out = ctypes.c_int()
+        C.check(C.load().ao_batch_build_path(self._h, ctypes.byref(out)))
+        return bool(out.value)
+
     def update(self, frozen=None):
         """update() of every system; `frozen` (sequence of bools) keeps the marked systems' trees."""
         if frozen is None:

@@ -638,6 +638,22 @@ ao_status ao_batch_build(ao_batch *batch)
     });
 }
 
+ao_status ao_batch_set_build_mode(ao_batch *batch, int mode)
+{
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("ao_batch_set_build_mode: null batch");
+        batch->engine->setBuildMode(mode);
+    });
+}
+
+ao_status ao_batch_build_path(ao_batch *batch, int *by_levels)
+{
+    return guarded([&] {
+        if (!batch) throw std::invalid_argument("ao_batch_build_path: null batch");
+        if (by_levels) *by_levels = batch->engine->lastBuildByLevels() ? 1 : 0;
+    });
+}
+
 ao_status ao_batch_update(ao_batch *batch, const unsigned char *frozen)
 {
     return guarded([&] {

@@ -1515,6 +1515,8 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         a.val = nf ? m.lvVal.as<u32>() : nullptr;
         a.nbr = nf ? m.lvNbr.as<u32>() : nullptr;
         a.parent = nf ? m.lvParent.as<u32>() : nullptr;
+        a.usys = nullptr;
+        a.sysRoot = nullptr;
         a.child = m.lvChild.as<u32>();
         a.leaves = m.lvLeaves.as<u32>();
         a.offset = m.lvOffset.as<u32>();
@@ -1567,8 +1569,14 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
             const rb::TreeBufs tb = m.bufs();
             for (int l = 0; l < levels; ++l)
             {
-                if (nf) lb::placeKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, tb, l, levels, u32(physCap_)), noteLaunch();
-                else lb::placeKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, tb, l, levels, u32(physCap_)), noteLaunch();
+                if (nf)
+                    lb::placeKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, tb.K[0], tb.B[0], tb.NF[0], nullptr, l, levels,
+                                                                          u32(physCap_)),
+                        noteLaunch();
+                else
+                    lb::placeKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, tb.K[0], tb.B[0], nullptr, nullptr, l, levels,
+                                                                           u32(physCap_)),
+                        noteLaunch();
             }
             AOT_LAUNCH_CHECK();
         };

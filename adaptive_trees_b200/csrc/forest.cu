@@ -21,6 +21,7 @@
 #include "capacity.hpp"
 #include "engine_util.cuh"
 #include "forest.cuh"
+#include "forest_levels.cuh"
 
 namespace aot
 {
@@ -48,6 +49,12 @@ struct ForestEngine::Impl
     std::vector<OctreeCapacity> capModel;
     std::vector<size_t> leafCap;
     bool built = false;
+    // build by levels: the unit arena, the key sample and the control words
+    DevMem lvRows, lvChild, lvLeaves, lvOffset, lvUsys, lvSysRoot, lvBins, lvCtl, sample;
+    size_t lvCap = 0;
+    size_t lastEntries = 0;  // entries of the last build (the first guess of the next)
+    int buildMode = 0;
+    bool lastByLevels = false;
     KeygenParams<float> kpf{};
     KeygenParams<double> kpd{};
 
@@ -231,7 +238,7 @@ void ForestEngine::ensurePhysical(size_t entries)
     m.entryCap = c;
 }
 
-void ForestEngine::sortParticles()
+void ForestEngine::sortParticles(bool withSample)
 {
     Impl &m = *m_;
     cudaStream_t s = m.cfg.stream;
@@ -271,7 +278,11 @@ void ForestEngine::sortParticles()
             sortKeys(config);
         }
     }
-    forest::activeKernel<<<gridFor(size_t(m.S), 256), 256, 0, s>>>(m.bufs()), noteLaunch();
+    const size_t ns = withSample ? (m.total + kSampleStride - 1) >> kSampleShift : 0;
+    if (ns) m.sample.reserve(ns * sizeof(u64), s);
+    const unsigned grid = std::min<unsigned>(gridFor(std::max(size_t(m.S), ns), 256), unsigned(smCount()) * 8u);
+    forest::activeKernel<<<std::max(grid, 1u), 256, 0, s>>>(m.bufs(), ns ? m.sample.as<u64>() : nullptr, ns),
+        noteLaunch();
     AOT_LAUNCH_CHECK();
 }
 
@@ -385,21 +396,116 @@ void ForestEngine::readState(bool model)
         for (int i = 0; i < m.S; ++i) m.capModel[i].stateRead(size_t(std::max(m.hsys[i].leaves, 0)));
 }
 
+void ForestEngine::setBuildMode(int mode)
+{
+    if (mode != 0 && mode != 1) throw std::invalid_argument("forest: build mode must be 0 (levels) or 1 (rounds)");
+    m_->buildMode = mode;
+}
+
+bool ForestEngine::lastBuildByLevels() const { return m_->lastByLevels; }
+
+// The converged build of all systems in one cooperative launch
+// (forest::levelBuildKernel).  False where the rounds must run instead: a
+// system whose rounds stop at maxDepth before converging, an arrival round
+// beyond the tracked ones, LeafCount thresholds that wrap, or a device that
+// cannot hold the grid.
+bool ForestEngine::levelBuild()
+{
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    if (u64(m.cfg.bucket) * 512u > 0xffffffffull) return false;
+    const bool hil = m.cfg.hilbert;
+    const void *fn = hil ? reinterpret_cast<const void *>(&forest::levelBuildKernel<true>)
+                         : reinterpret_cast<const void *>(&forest::levelBuildKernel<false>);
+    int perSm = 0;
+    AOT_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, lb::kThreads, 0));
+    if (perSm <= 0) return false;
+    const unsigned grid = unsigned(perSm) * unsigned(smCount());
+    const size_t S = size_t(m.S);
+    constexpr size_t kHeadBytes = (sizeof(lb::Control) + 255) & ~size_t(255);
+    constexpr size_t kCtlBytes = kHeadBytes + sizeof(forest::LevelStatus);
+    size_t cap = std::max<size_t>(m.lvCap, m.total / std::max(1u, m.cfg.bucket) + 4096);
+    ensurePhysical(std::max(m.lastEntries, 2 * S + 4 * (m.total / std::max(1u, m.cfg.bucket)) + 4096));
+    lb::Control hc{};
+    forest::LevelStatus hl{};
+    for (;;)
+    {
+        if (cap >= (size_t(1) << 31)) return false;
+        m.lvRows.reserve(cap * lb::kRow * sizeof(u32), s);
+        m.lvChild.reserve(cap * 8 * sizeof(u32), s);
+        m.lvLeaves.reserve(cap * sizeof(u32), s);
+        m.lvOffset.reserve(cap * sizeof(u32), s);
+        m.lvUsys.reserve(cap * sizeof(u32), s);
+        m.lvSysRoot.reserve(S * sizeof(u32), s);
+        m.lvBins.reserve(S * (lb::kContribBins + lb::kArrivals) * sizeof(unsigned long long), s);
+        m.lvCtl.reserve(kCtlBytes, s);
+        m.lvCap = cap;
+        forest::LevelArgs p{};
+        lb::Arena &a = p.a;
+        a.rows = m.lvRows.as<u32>();
+        a.child = m.lvChild.as<u32>();
+        a.leaves = m.lvLeaves.as<u32>();
+        a.offset = m.lvOffset.as<u32>();
+        a.usys = m.lvUsys.as<u32>();
+        a.sysRoot = m.lvSysRoot.as<u32>();
+        a.ctl = m.lvCtl.as<lb::Control>();
+        a.contrib = m.lvBins.as<unsigned long long>();
+        a.landed = a.contrib + S * lb::kContribBins;
+        a.cap = u32(cap);
+        p.idx = KeyIndex{m.P[0].as<u64>(), m.sample.as<u64>(), m.total, (m.total + kSampleStride - 1) >> kSampleShift};
+        p.f = m.bufs();
+        p.ls = reinterpret_cast<forest::LevelStatus *>(m.lvCtl.as<unsigned char>() + kHeadBytes);
+        p.capacity = u32(std::min<size_t>(m.entryCap, 0xffffffffu));
+        p.bucket = m.cfg.bucket;
+        p.maxDepth = int(m.cfg.maxDepth);
+        p.h = m.kpd.h;
+        AOT_CHECK(cudaMemsetAsync(m.lvCtl.p, 0, kCtlBytes, s));
+        void *args[] = {&p};
+        AOT_CHECK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(lb::kThreads), args, 0, s));
+        noteLaunch();
+        AOT_LAUNCH_CHECK();
+        AOT_CHECK(cudaMemcpyAsync(&hc, m.lvCtl.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
+        AOT_CHECK(cudaMemcpyAsync(&hl, p.ls, sizeof(hl), cudaMemcpyDeviceToHost, s));
+        waitStream(s);
+        if (hl.barrierError) throw std::runtime_error("forest: a grid barrier of the level build gave up waiting");
+        if (hc.overflow)
+        {
+            cap *= 2;
+            continue;
+        }
+        if (hc.late) return false;
+        if (hl.entriesOverflow)
+        {
+            ensurePhysical(size_t(hl.entries));
+            continue;
+        }
+        if (hl.tooManyRounds) return false;
+        if (hl.historyMismatch) throw std::logic_error("forest: level build history does not end at the tree");
+        m.lastEntries = size_t(hl.entries);
+        return true;
+    }
+}
+
 void ForestEngine::build()
 {
     Impl &m = *m_;
     cudaStream_t s = m.cfg.stream;
     waitStream(s);
     for (auto &c : m.capModel) c.buildStart();
-    sortParticles();
-    ensurePhysical(size_t(2) * m.S);
-    const forest::Bufs f = m.bufs();
-    forest::initKernel<<<gridFor(size_t(m.S), 256), 256, 0, s>>>(f), noteLaunch();
-    AOT_LAUNCH_CHECK();
-    for (unsigned r = 0; r < m.cfg.maxDepth; ++r)
+    const bool tryLevels = m.buildMode == 0;
+    sortParticles(tryLevels);
+    m.lastByLevels = tryLevels && levelBuild();
+    if (!m.lastByLevels)
     {
-        pass(true, nullptr);
-        if (!m.hst->changed) break;
+        ensurePhysical(size_t(2) * m.S);
+        const forest::Bufs f = m.bufs();
+        forest::initKernel<<<gridFor(size_t(m.S), 256), 256, 0, s>>>(f), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        for (unsigned r = 0; r < m.cfg.maxDepth; ++r)
+        {
+            pass(true, nullptr);
+            if (!m.hst->changed) break;
+        }
     }
     // per-system leafCapacity from each system's round history
     readState(false);
@@ -423,8 +529,11 @@ void ForestEngine::build()
     }
     AOT_CHECK(cudaMemcpyAsync(m.sys.p, m.hsys, size_t(m.S) * sizeof(forest::SysState), cudaMemcpyHostToDevice, s));
     ensurePhysical(entries);
-    forest::materializeKernel<<<unsigned(smCount()) * 8u, 256, 0, s>>>(m.bufs()), noteLaunch();
-    AOT_LAUNCH_CHECK();
+    if (!m.lastByLevels)  // the level build writes the counts itself
+    {
+        forest::materializeKernel<<<unsigned(smCount()) * 8u, 256, 0, s>>>(m.bufs()), noteLaunch();
+        AOT_LAUNCH_CHECK();
+    }
     m.built = true;
     readState(true);
 }
@@ -439,7 +548,7 @@ void ForestEngine::beginUpdate(const unsigned char *frozen)
     else
         AOT_CHECK(cudaMemsetAsync(m.frozen.p, 0, size_t(m.S), s));
     AOT_CHECK(cudaMemsetAsync(&m.st.as<forest::State>()->changedPasses, 0, sizeof(int), s));
-    sortParticles();
+    sortParticles(false);
     const forest::Bufs f = m.bufs();
     forest::refreshKernel<true><<<unsigned(smCount()) * 8u, forest::kThreads, 0, s>>>(f), noteLaunch();
     AOT_LAUNCH_CHECK();

@@ -221,12 +221,18 @@ static __global__ void __launch_bounds__(sort::kRadix)
 
 // Active particles of every system: escaped keys (~0) sort past 2^63
 // (initRootOctreeKernel, octree.cu:23-38).
-static __global__ void activeKernel(Bufs f)
+// With a sample array: also every 32nd key of the concatenated sorted keys
+// (the key index of a build by levels).
+static __global__ void activeKernel(Bufs f, u64 *sample, size_t ns)
 {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= f.numSystems) return;
-    const System sy = f.systems[s];
-    f.sys[s].active = sy.n ? u32(lowerBoundDev(f.P + sy.base, sy.n, kMaxKey)) : 0u;
+    const size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x, size = size_t(gridDim.x) * blockDim.x;
+    for (size_t s = r; s < size_t(f.numSystems); s += size)
+    {
+        const System sy = f.systems[s];
+        f.sys[s].active = sy.n ? u32(lowerBoundDev(f.P + sy.base, sy.n, kMaxKey)) : 0u;
+    }
+    if (sample)
+        for (size_t j = r; j < ns; j += size) sample[j] = f.P[j << kSampleShift];
 }
 
 // --------------------------------------------------------------------------

@@ -40,6 +40,11 @@ public:
     bool needsResize();                  // any system (reads the device state)
     void resizeBuffers();                // grows the systems that need it
     void setCoordinates(int s, const void *x, const void *y, const void *z);
+    // 0 (default): build() builds every system's converged tree by levels in
+    // one persistent launch, falling back to the rounds where they would not
+    // converge within maxDepth; 1: always the rounds.  Both give the same trees.
+    void setBuildMode(int mode);
+    bool lastBuildByLevels() const;
 
     enum Buffer { ParticleKeys = 0, Perm = 1, Cornerstone = 2, LeafCounts = 3 };
     // device view of a system's buffer as of the last state readback
@@ -56,7 +61,8 @@ public:
 private:
     struct Impl;
     std::unique_ptr<Impl> m_;
-    void sortParticles();
+    void sortParticles(bool withSample);
+    bool levelBuild();
     void sortKeys(int config);
     void pass(bool build, const unsigned char *frozenDevice);
     void beginUpdate(const unsigned char *frozen);

@@ -73,6 +73,8 @@ struct Arena
     u32 *offset;     // [cap] cornerstone index of the unit's first leaf
     u32 *nbr;        // NFCount: [cap][27] the cells around each unit (nbrRef)
     u32 *parent;     // NFCount: [cap] parent unit * 8 + the unit's digit in it
+    u32 *usys;       // batch of trees: [cap] the tree (system) of each unit
+    u32 *sysRoot;    // batch of trees: [systems] each system's root unit, or kLeaf
     Control *ctl;
     unsigned long long *contrib;  // [kArrivals][kJumps][kJumps] final leaves per (a, k, j)
     unsigned long long *landed;   // [kArrivals] internal nodes landing in round t
@@ -230,15 +232,60 @@ __device__ __forceinline__ void innerBegins(const KeyIndex &idx, u32 lo, u32 hi,
     }
 }
 
-// 9 child begins of the units of level l, one thread per unit (the 7 inner
-// ones by innerBegins).
-static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, KeyIndex idx, int l)
+// Lower bound of t in the sorted A[b, e) by a whole warp: each step probes 32
+// points that split the range into 33 parts and keeps the part the ballot
+// points to, so a range of n keys takes about log33(n) dependent loads
+// instead of log2(n).  Every lane returns the answer.
+__device__ __forceinline__ u32 warpLowerBound(const u64 *A, u32 b, u32 e, u64 t, int lane)
 {
-    const Control &c = *a.ctl;
-    if (c.overflow | c.late | c.error) return;
-    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    while (e > b)
+    {
+        const u32 n = e - b;
+        const u32 p = b + u32((u64(lane) + 1) * n / 33u);  // p < e; p_k = b + k when n <= 32
+        const unsigned below = __ballot_sync(0xffffffffu, __ldg(A + p) < t);
+        const int c = __popc(below);  // a prefix of the lanes: A is sorted
+        const u32 pLow = __shfl_sync(0xffffffffu, p, c > 0 ? c - 1 : 0);
+        const u32 pHigh = __shfl_sync(0xffffffffu, p, c < 32 ? c : 31);
+        if (c > 0) b = pLow + 1;
+        if (c < 32) e = pHigh;
+    }
+    return b;
+}
+
+// Levels with at most this many units expand by warps (a warp per inner
+// child boundary); the chains of dependent loads of the per-thread searches
+// dominate there, and the keys of a unit span most of the array.
+constexpr u32 kWideUnits = 4096;
+
+// 9 child begins of the units of level l: one thread per unit (the 7 inner
+// ones by innerBegins), or one warp per inner boundary on levels of few units.
+// `rank` and `size` number the threads taking part (a grid, or the grid of a
+// persistent kernel).
+__device__ __forceinline__ void expandUnits(const Arena &a, const KeyIndex &idx, int l, u32 start, u32 count, u32 rank,
+                                            u32 size)
+{
     const u64 cr = octRange(unsigned(l) + 1);
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    if (count <= kWideUnits)
+    {
+        const int lane = threadIdx.x & 31;
+        for (u32 w = rank >> 5; w < count * 7; w += size >> 5)
+        {
+            const u32 i = w / 7, d = w - i * 7;
+            u32 *row = a.rows + size_t(start + i) * kRow;
+            const u32 lo = row[2], hi = row[10];
+            const u64 t = rowKey(row) + u64(d + 1) * cr;
+            // first sampled key >= t among the samples inside [lo, hi), then
+            // the window of at most 31 keys before it
+            const u32 jA = (lo + kSampleStride - 1) >> kSampleShift, jB = (hi + kSampleStride - 1) >> kSampleShift;
+            const u32 sIdx = warpLowerBound(idx.sample, jA, jB > jA ? jB : jA, t, lane);
+            const u32 wlo = sIdx > jA ? ((sIdx - 1) << kSampleShift) + 1 : lo;
+            const u32 whi = sIdx < jB ? (sIdx << kSampleShift) : hi;
+            const u32 r = warpLowerBound(idx.keys, wlo, whi, t, lane);
+            if (lane == 0) row[3 + d] = r;
+        }
+        return;
+    }
+    for (u32 i = rank; i < count; i += size)
     {
         u32 *row = a.rows + size_t(start + i) * kRow;
         u32 b[7];
@@ -246,6 +293,14 @@ static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, KeyInde
 #pragma unroll
         for (int d = 0; d < 7; ++d) row[3 + d] = b[d];
     }
+}
+
+static __global__ void __launch_bounds__(kThreads) expandKernel(Arena a, KeyIndex idx, int l)
+{
+    const Control &c = *a.ctl;
+    if (c.overflow | c.late | c.error) return;
+    expandUnits(a, idx, l, c.levelStart[l], c.levelCount[l], blockIdx.x * blockDim.x + threadIdx.x,
+                gridDim.x * blockDim.x);
 }
 
 // The 27 cells around every unit of level l >= 1, from those around its
@@ -471,34 +526,20 @@ static __global__ void __launch_bounds__(kThreads, 4)
 // the slots of its new units with one atomic add; the order of the units in
 // a level is free (every later step finds them through the child and parent
 // links, and the placement follows the digits).
-template <bool NF, bool Hilbert>
-static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l, unsigned bucket, HilbertTables h)
+// Forest: the history counts go to the unit's system's bins in global memory
+// (sContrib / sLanded unused); otherwise to the CTA's shared bins.
+template <bool NF, bool Hilbert, bool Forest>
+__device__ __forceinline__ void classifyUnits(const Arena &a, int l, unsigned bucket, u32 start, u32 count,
+                                              const unsigned char *sNext, const unsigned char *sDec, u32 *sContrib,
+                                              u32 *sLanded, u32 rank, u32 size)
 {
-    __shared__ u32 sContrib[kContribBins];
-    __shared__ u32 sLanded[kArrivals];
-    __shared__ unsigned char sNext[48 * 8], sDec[48 * 8];
     Control &c = *a.ctl;
-    if (c.overflow | c.late | c.error) return;
-    const u32 start = c.levelStart[l], count = c.levelCount[l];
     const u32 next = start + count;
-    if (blockIdx.x == 0 && threadIdx.x == 0) c.levelStart[l + 1] = next;
-    if (count <= blockIdx.x * blockDim.x) return;
-    if constexpr (Hilbert)
-    {
-        for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
-        {
-            sNext[k] = h.encNext[k];
-            sDec[k] = h.decOct[k];
-        }
-    }
-    for (int k = threadIdx.x; k < kContribBins; k += kThreads) sContrib[k] = 0;
-    if (threadIdx.x < kArrivals) sLanded[threadIdx.x] = 0;
-    __syncthreads();
+    if (rank == 0) c.levelStart[l + 1] = next;
     const unsigned m = unsigned(l) + 1;
     const u64 cr = octRange(m);
     const int lane = threadIdx.x & 31;
-    const u32 stride = gridDim.x * blockDim.x;
-    for (u32 i0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); i0 < count; i0 += stride)
+    for (u32 i0 = rank & ~31u; i0 < count; i0 += size)
     {
         const u32 i = i0 + u32(lane);
         const bool valid = i < count;
@@ -545,6 +586,7 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
         if (!valid) continue;
         const u32 aR = regionArrival(reg), lR = regionLevel(reg), kR = regionDepth(reg);
         const u32 j = m - lR;  // 1 <= j <= kR
+        const u32 sys = Forest ? a.usys[g] : 0u;
         u32 rank = base + incl - nHigh;
         u32 slots[8];
 #pragma unroll
@@ -561,9 +603,11 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
                     {
                         // a landed internal node: a leaf in round aR + 1, splitting at once
                         creg = regionWord(aR + 1, m, splitDepth(NF, x[d], bucket, m));
-                        if (aR + 2 < u32(kArrivals)) atomicAdd(&sLanded[aR + 1], 1u);
-                        else c.late = 1;
+                        if (aR + 2 >= u32(kArrivals)) c.late = 1;
+                        else if (Forest) atomicAdd(a.landed + size_t(sys) * kArrivals + aR + 1, 1ull);
+                        else atomicAdd(&sLanded[aR + 1], 1u);
                     }
+                    if constexpr (Forest) a.usys[gc] = sys;
                     // the child's own level and the curve state ordering its children
                     u32 cst = kHilbertStart;
                     if constexpr (Hilbert)
@@ -583,6 +627,10 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
                     c.overflow = 1;
                 }
             }
+            else if constexpr (Forest)
+            {
+                atomicAdd(a.contrib + size_t(sys) * kContribBins + (aR * kJumps + kR) * kJumps + j, 1ull);
+            }
             else
             {
                 atomicAdd(&sContrib[(aR * kJumps + kR) * kJumps + j], 1u);
@@ -593,6 +641,32 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
         ch4[0] = make_uint4(slots[0], slots[1], slots[2], slots[3]);
         ch4[1] = make_uint4(slots[4], slots[5], slots[6], slots[7]);
     }
+}
+
+template <bool NF, bool Hilbert>
+static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l, unsigned bucket, HilbertTables h)
+{
+    __shared__ u32 sContrib[kContribBins];
+    __shared__ u32 sLanded[kArrivals];
+    __shared__ unsigned char sNext[48 * 8], sDec[48 * 8];
+    Control &c = *a.ctl;
+    if (c.overflow | c.late | c.error) return;
+    const u32 start = c.levelStart[l], count = c.levelCount[l];
+    if (blockIdx.x == 0 && threadIdx.x == 0) c.levelStart[l + 1] = start + count;
+    if (count <= blockIdx.x * blockDim.x) return;
+    if constexpr (Hilbert)
+    {
+        for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
+        {
+            sNext[k] = h.encNext[k];
+            sDec[k] = h.decOct[k];
+        }
+    }
+    for (int k = threadIdx.x; k < kContribBins; k += kThreads) sContrib[k] = 0;
+    if (threadIdx.x < kArrivals) sLanded[threadIdx.x] = 0;
+    __syncthreads();
+    classifyUnits<NF, Hilbert, false>(a, l, bucket, start, count, sNext, sDec, sContrib, sLanded,
+                                      blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
     __syncthreads();
     for (int k = threadIdx.x; k < kContribBins; k += kThreads)
         if (sContrib[k]) atomicAdd(a.contrib + k, (unsigned long long)sContrib[k]);
@@ -603,12 +677,9 @@ static __global__ void __launch_bounds__(kThreads) classifyKernel(Arena a, int l
 // Leaves below each unit of level l (the units of level l + 1 are done).
 // `levels` is the number of levels the build expanded: units below them mean
 // the build is incomplete, and nothing is counted.
-static __global__ void leafCountKernel(Arena a, int l, int levels)
+__device__ __forceinline__ void leafCountUnits(const Arena &a, u32 start, u32 count, u32 rank, u32 size)
 {
-    const Control &c = *a.ctl;
-    if (c.levelCount[levels] | c.overflow | c.late | c.error) return;
-    const u32 start = c.levelStart[l], count = c.levelCount[l];
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    for (u32 i = rank; i < count; i += size)
     {
         const u32 g = start + i;
         u32 s = 0;
@@ -622,24 +693,28 @@ static __global__ void leafCountKernel(Arena a, int l, int levels)
     }
 }
 
+static __global__ void leafCountKernel(Arena a, int l, int levels)
+{
+    const Control &c = *a.ctl;
+    if (c.levelCount[levels] | c.overflow | c.late | c.error) return;
+    leafCountUnits(a, c.levelStart[l], c.levelCount[l], blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
 // Cornerstone entries of the leaf children of the level-l units, and the
 // first leaf index of their internal children.  Eight lanes per unit, one per
 // child: a segmented scan of the children's leaf counts gives each child's
 // position, so a warp writes the entries of four units at once.
+// K, B (and NF, SEG where given) are the cornerstone arrays written; SEG
+// receives each leaf's tree (system) in a batch of trees.
 template <bool NF>
-static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l, int levels, u32 capacity)
+__device__ __forceinline__ void placeUnits(const Arena &a, u64 *K, u32 *B, u32 *NFo, int *SEG, int l, u32 start,
+                                           u32 count, u32 capacity, u32 rank, u32 size)
 {
     Control &c = *a.ctl;
-    if (c.levelCount[levels] | c.overflow | c.late | c.error) return;
-    const u32 start = c.levelStart[l], count = c.levelCount[l];
     const u64 cr = octRange(unsigned(l) + 1);
-    u64 *K = tb.K[0];
-    u32 *B = tb.B[0];
-    u32 *NFo = tb.NF[0];
     const int lane = threadIdx.x & 31, d = lane & 7;
     const size_t total = size_t(count) * 8;
-    const size_t stride = size_t(gridDim.x) * blockDim.x;
-    for (size_t e0 = size_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); e0 < total; e0 += stride)
+    for (size_t e0 = rank & ~31u; e0 < total; e0 += size)
     {
         const size_t e = e0 + size_t(lane);
         const bool valid = e < total;
@@ -666,12 +741,22 @@ static __global__ void placeKernel(Arena a, rb::TreeBufs tb, int l, int levels, 
             K[o] = rowKey(row) + u64(d) * cr;
             B[o] = row[2 + d];
             if constexpr (NF) NFo[o] = a.val[size_t(g) * 8 + d];
+            if (SEG) SEG[o] = int(a.usys[g]);
         }
         else
         {
             a.offset[ch] = o;
         }
     }
+}
+
+template <bool NF>
+static __global__ void placeKernel(Arena a, u64 *K, u32 *B, u32 *NFo, int *SEG, int l, int levels, u32 capacity)
+{
+    const Control &c = *a.ctl;
+    if (c.levelCount[levels] | c.overflow | c.late | c.error) return;
+    placeUnits<NF>(a, K, B, NFo, SEG, l, c.levelStart[l], c.levelCount[l], capacity,
+                   blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 // The finished tree: sentinel boundary and the state of a converged build

@@ -307,6 +307,13 @@ AO_API ao_status ao_batch_create(int real_type, int num_systems, const void *con
 AO_API ao_status ao_batch_destroy(ao_batch *batch);
 /* build() of every system (octree.cu:427-457). */
 AO_API ao_status ao_batch_build(ao_batch *batch);
+/* Mode 0 (default): build() makes every system's converged tree by levels in
+ * one persistent launch after the sort, falling back to the rounds where a
+ * system's rounds would not converge within max_depth; mode 1: always the
+ * rounds.  Both give the same trees, counts and capacities. */
+AO_API ao_status ao_batch_set_build_mode(ao_batch *batch, int mode);
+/* *by_levels = 1 when the last build() used the level builder. */
+AO_API ao_status ao_batch_build_path(ao_batch *batch, int *by_levels);
 /* update() of every system (octree.cu:459-496); capturable when frozen is
  * NULL.  frozen: optional host array of num_systems bytes; a system marked
  * non-zero keeps its tree, as if update() were not called on it (for the
