@@ -22,6 +22,7 @@
 #include "engine_util.cuh"
 #include "forest.cuh"
 #include "forest_levels.cuh"
+#include "forest_sort.cuh"
 
 namespace aot
 {
@@ -50,7 +51,7 @@ struct ForestEngine::Impl
     std::vector<size_t> leafCap;
     bool built = false;
     // build by levels: the unit arena, the key sample and the control words
-    DevMem lvRows, lvChild, lvLeaves, lvOffset, lvUsys, lvSysRoot, lvBins, lvCtl, sample;
+    DevMem lvRows, lvChild, lvLeaves, lvOffset, lvUsys, lvSysRoot, lvBins, lvCtl, sample, sortBar;
     size_t lvCap = 0;
     size_t lastEntries = 0;  // entries of the last build (the first guess of the next)
     int buildMode = 0;
@@ -275,6 +276,7 @@ void ForestEngine::sortParticles(bool withSample)
         {
             const int config = sortTuning(true, m.total).config;
             m.buildTiles(config, s);
+            if (withSample && sortPersistent(config)) return;  // keys, sort, active counts and sample in one launch
             sortKeys(config);
         }
     }
@@ -286,25 +288,14 @@ void ForestEngine::sortParticles(bool withSample)
     AOT_LAUNCH_CHECK();
 }
 
-// Keys of every system and the segmented sort with sort configuration
-// `config`, whose tile table must be in place; the result lands in P[0] /
-// Perm[0] (an even pass count).
-void ForestEngine::sortKeys(int config)
+// Keys of every system into P[0] (hist: with the 8-bit digit histograms).
+void ForestEngine::launchKeygen(bool hist)
 {
     Impl &m = *m_;
     cudaStream_t s = m.cfg.stream;
-    if (config != m.tileConfig) throw std::logic_error("forest: the tile table is not the sort configuration's");
-    const int bitsPer = sort::kSortConfigs[config].bits;
-    const int passes = sort::configPasses(config);
-    if (passes & 1) throw std::logic_error("forest: sort configurations must have an even pass count");
-    AOT_CHECK(cudaMemsetAsync(m.hist.p, 0, size_t(m.S) * sort::kPassSlots * sort::kRadix * 4, s));
-    AOT_CHECK(cudaMemsetAsync(m.tileCounters.p, 0, sort::kPassSlots * 4, s));
-    AOT_CHECK(cudaMemsetAsync(m.status.p, 0, size_t(m.numTiles) * passes * sort::kRadix * 8, s));
     const unsigned grid = std::max(1u, std::min<unsigned>(m.numTiles, unsigned(smCount()) * 8u));
     u64 *keys = m.P[0].as<u64>();
-    // 8-bit digits: the histograms come with the keys; otherwise a pass of their own
-    const bool fused = bitsPer == sort::kRadixBits;
-    u32 *keygenHist = fused ? m.hist.as<u32>() : nullptr;
+    u32 *keygenHist = hist ? m.hist.as<u32>() : nullptr;
     const Impl &cm = m;
     auto launch = [&](auto real) {
         using Real = decltype(real);
@@ -323,6 +314,96 @@ void ForestEngine::sortKeys(int config)
     };
     if (m.cfg.real == 0) launch(float{});
     else launch(double{});
+    AOT_LAUNCH_CHECK();
+}
+
+// Keys (one launch), then the segmented sort, the active counts and the key
+// sample of a build by levels in one cooperative launch (forest::sortKernel),
+// for the 8-bit sort configurations; false (nothing done) for the others.
+bool ForestEngine::sortPersistent(int config)
+{
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    const sort::SortConfig sc = sort::kSortConfigs[config];
+    if (sc.bits != sort::kRadixBits || config != m.tileConfig || sort::configPasses(config) != sort::kMaxPasses)
+        return false;
+    const void *fn = nullptr;
+    size_t smem = 0;
+    // 3 CTAs per SM: the pass loop stays in registers (at 4 it spills and
+    // runs slower)
+    switch (sc.items)
+    {
+    case 8:
+        fn = reinterpret_cast<const void *>(&forest::sortKernel<8>);
+        smem = sizeof(sort::SharedPass<8, 8>);
+        break;
+    case 10:
+        fn = reinterpret_cast<const void *>(&forest::sortKernel<10>);
+        smem = sizeof(sort::SharedPass<8, 10>);
+        break;
+    case 16:
+        fn = reinterpret_cast<const void *>(&forest::sortKernel<16>);
+        smem = sizeof(sort::SharedPass<8, 16>);
+        break;
+    default: return false;
+    }
+    AOT_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int perSm = 0;
+    AOT_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, sort::kThreads, smem));
+    if (perSm <= 0) return false;
+    const unsigned grid = unsigned(perSm) * unsigned(smCount());
+    const int passes = sort::configPasses(config);
+    const size_t ns = (m.total + kSampleStride - 1) >> kSampleShift;
+    m.sample.reserve(std::max<size_t>(ns, 1) * sizeof(u64), s);
+    m.sortBar.reserve(sizeof(GridBarrier), s);
+    AOT_CHECK(cudaMemsetAsync(m.hist.p, 0, size_t(m.S) * sort::kPassSlots * sort::kRadix * 4, s));
+    AOT_CHECK(cudaMemsetAsync(m.tileCounters.p, 0, sort::kPassSlots * 4, s));
+    AOT_CHECK(cudaMemsetAsync(m.status.p, 0, size_t(m.numTiles) * passes * sort::kRadix * 8, s));
+    AOT_CHECK(cudaMemsetAsync(m.sortBar.p, 0, sizeof(GridBarrier), s));
+    launchKeygen(true);
+    forest::SortArgs p{};
+    p.f = m.bufs();
+    p.tiles = sort::SegmentTiles{m.tileSys.as<u32>(),      m.tileBegin.as<u32>(), m.tileEnd.as<u32>(),
+                                 m.segFirstTile.as<u32>(), m.segBase.as<u32>(),  nullptr};
+    p.numTiles = m.numTiles;
+    for (int k = 0; k < 2; ++k)
+    {
+        p.keys[k] = m.P[k].as<u64>();
+        p.vals[k] = m.Perm[k].as<u32>();
+    }
+    p.hist = m.hist.as<u32>();
+    p.bins = m.bins.as<u32>();
+    p.tileCounters = m.tileCounters.as<u32>();
+    p.status = m.status.as<u64>();
+    p.error = &m.st.as<forest::State>()->error;
+    p.sample = m.sample.as<u64>();
+    p.ns = ns;
+    p.bar = m.sortBar.as<GridBarrier>();
+    void *args[] = {&p};
+    AOT_CHECK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(sort::kThreads), args, smem, s));
+    noteLaunch();
+    AOT_LAUNCH_CHECK();
+    return true;
+}
+
+// Keys of every system and the segmented sort with sort configuration
+// `config`, whose tile table must be in place; the result lands in P[0] /
+// Perm[0] (an even pass count).
+void ForestEngine::sortKeys(int config)
+{
+    Impl &m = *m_;
+    cudaStream_t s = m.cfg.stream;
+    if (config != m.tileConfig) throw std::logic_error("forest: the tile table is not the sort configuration's");
+    const int bitsPer = sort::kSortConfigs[config].bits;
+    const int passes = sort::configPasses(config);
+    if (passes & 1) throw std::logic_error("forest: sort configurations must have an even pass count");
+    AOT_CHECK(cudaMemsetAsync(m.hist.p, 0, size_t(m.S) * sort::kPassSlots * sort::kRadix * 4, s));
+    AOT_CHECK(cudaMemsetAsync(m.tileCounters.p, 0, sort::kPassSlots * 4, s));
+    AOT_CHECK(cudaMemsetAsync(m.status.p, 0, size_t(m.numTiles) * passes * sort::kRadix * 8, s));
+    u64 *keys = m.P[0].as<u64>();
+    // 8-bit digits: the histograms come with the keys; otherwise a pass of their own
+    const bool fused = bitsPer == sort::kRadixBits;
+    launchKeygen(fused);
     if (!fused)
         forest::segHistKernel<7><<<m.numTiles, forest::kThreads, 0, s>>>(m.tileSys.as<u32>(), m.tileBegin.as<u32>(),
                                                                       m.tileEnd.as<u32>(), keys, passes,
@@ -467,7 +548,7 @@ bool ForestEngine::levelBuild()
         AOT_CHECK(cudaMemcpyAsync(&hc, m.lvCtl.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
         AOT_CHECK(cudaMemcpyAsync(&hl, p.ls, sizeof(hl), cudaMemcpyDeviceToHost, s));
         waitStream(s);
-        if (hl.barrierError) throw std::runtime_error("forest: a grid barrier of the level build gave up waiting");
+        if (hl.bar.error) throw std::runtime_error("forest: a grid barrier of the level build gave up waiting");
         if (hc.overflow)
         {
             cap *= 2;

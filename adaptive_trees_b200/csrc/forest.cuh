@@ -96,24 +96,16 @@ struct Bufs
 // histograms of the eight 8-bit digits, hist[system][pass slot][digit].  Each
 // CTA takes a contiguous range of tiles, so its shared histogram is flushed
 // only where the system changes.
+// The keys of tiles [t0, t1) (a CTA's share), with the digit histograms
+// counted in sh[kMaxPasses][kRadix] (zero on entry and on return) and flushed
+// where the system changes.  sEnc / sNext hold the Hilbert tables.
 template <class Real, Curve C>
-static __global__ void __launch_bounds__(kThreads)
-    keygenKernel(const System *__restrict__ systems, const u32 *__restrict__ tileSys,
-                 const u32 *__restrict__ tileBegin, const u32 *__restrict__ tileEnd, u32 numTiles,
-                 const KeygenParams<Real> prm, u64 *__restrict__ keys, u32 *__restrict__ hist)
+__device__ __forceinline__ void keygenTiles(const System *__restrict__ systems, const u32 *__restrict__ tileSys,
+                                            const u32 *__restrict__ tileBegin, const u32 *__restrict__ tileEnd,
+                                            u32 t0, u32 t1, const KeygenParams<Real> &prm, u64 *__restrict__ keys,
+                                            u32 *__restrict__ hist, u32 *sh, const unsigned char *sEnc,
+                                            const unsigned char *sNext)
 {
-    __shared__ u32 sh[sort::kMaxPasses * sort::kRadix];
-    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8];
-    for (int i = threadIdx.x; i < sort::kMaxPasses * sort::kRadix; i += blockDim.x) sh[i] = 0;
-    for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x)
-    {
-        sEnc[i] = prm.h.enc[i];
-        sNext[i] = prm.h.encNext[i];
-    }
-    __syncthreads();
-    const u32 per = (numTiles + gridDim.x - 1) / gridDim.x;
-    const u32 t0 = blockIdx.x * per;
-    const u32 t1 = min(numTiles, t0 + per);
     int cur = -1;
     auto flush = [&]() {
         __syncthreads();
@@ -161,6 +153,27 @@ static __global__ void __launch_bounds__(kThreads)
     flush();
 }
 
+template <class Real, Curve C>
+static __global__ void __launch_bounds__(kThreads)
+    keygenKernel(const System *__restrict__ systems, const u32 *__restrict__ tileSys,
+                 const u32 *__restrict__ tileBegin, const u32 *__restrict__ tileEnd, u32 numTiles,
+                 const KeygenParams<Real> prm, u64 *__restrict__ keys, u32 *__restrict__ hist)
+{
+    __shared__ u32 sh[sort::kMaxPasses * sort::kRadix];
+    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8];
+    for (int i = threadIdx.x; i < sort::kMaxPasses * sort::kRadix; i += blockDim.x) sh[i] = 0;
+    for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x)
+    {
+        sEnc[i] = prm.h.enc[i];
+        sNext[i] = prm.h.encNext[i];
+    }
+    __syncthreads();
+    const u32 per = (numTiles + gridDim.x - 1) / gridDim.x;
+    const u32 t0 = blockIdx.x * per;
+    keygenTiles<Real, C>(systems, tileSys, tileBegin, tileEnd, t0, min(numTiles, t0 + per), prm, keys, hist, sh, sEnc,
+                         sNext);
+}
+
 // Per-system histograms of Bits-wide digits for `passes` passes, one CTA per
 // tile of the segmented sort (the sort configurations whose digits are not
 // the 8 bits key generation counts).  hist[system][pass slot][digit].
@@ -194,13 +207,12 @@ static __global__ void __launch_bounds__(kThreads)
 }
 
 // Per system and pass: global start of each digit = base + exclusive scan of
-// the system's digit counts.  bins[pass][system][digit].
-static __global__ void __launch_bounds__(sort::kRadix)
-    binsKernel(const System *__restrict__ systems, int numSystems, const u32 *__restrict__ hist,
-               u32 *__restrict__ bins, int passes)
+// the system's digit counts.  bins[pass][system][digit].  One CTA of kRadix
+// threads per system; s: kRadix words of shared scratch.
+__device__ __forceinline__ void systemBins(const System *__restrict__ systems, int numSystems, int sys,
+                                           const u32 *__restrict__ hist, u32 *__restrict__ bins, int passes, u32 *s)
 {
-    __shared__ u32 s[sort::kRadix];
-    const int sys = blockIdx.x, d = threadIdx.x;
+    const int d = threadIdx.x;
     const u32 base = systems[sys].base;
     for (int p = 0; p < passes; ++p)
     {
@@ -219,13 +231,18 @@ static __global__ void __launch_bounds__(sort::kRadix)
     }
 }
 
-// Active particles of every system: escaped keys (~0) sort past 2^63
-// (initRootOctreeKernel, octree.cu:23-38).
+static __global__ void __launch_bounds__(sort::kRadix)
+    binsKernel(const System *__restrict__ systems, int numSystems, const u32 *__restrict__ hist,
+               u32 *__restrict__ bins, int passes)
+{
+    __shared__ u32 s[sort::kRadix];
+    systemBins(systems, numSystems, blockIdx.x, hist, bins, passes, s);
+}
+
 // With a sample array: also every 32nd key of the concatenated sorted keys
 // (the key index of a build by levels).
-static __global__ void activeKernel(Bufs f, u64 *sample, size_t ns)
+__device__ __forceinline__ void activeAndSample(const Bufs &f, u64 *sample, size_t ns, size_t r, size_t size)
 {
-    const size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x, size = size_t(gridDim.x) * blockDim.x;
     for (size_t s = r; s < size_t(f.numSystems); s += size)
     {
         const System sy = f.systems[s];
@@ -233,6 +250,11 @@ static __global__ void activeKernel(Bufs f, u64 *sample, size_t ns)
     }
     if (sample)
         for (size_t j = r; j < ns; j += size) sample[j] = f.P[j << kSampleShift];
+}
+
+static __global__ void activeKernel(Bufs f, u64 *sample, size_t ns)
+{
+    activeAndSample(f, sample, ns, size_t(blockIdx.x) * blockDim.x + threadIdx.x, size_t(gridDim.x) * blockDim.x);
 }
 
 // --------------------------------------------------------------------------

@@ -62,6 +62,8 @@ private:
     struct Impl;
     std::unique_ptr<Impl> m_;
     void sortParticles(bool withSample);
+    bool sortPersistent(int config);
+    void launchKeygen(bool hist);
     bool levelBuild();
     void sortKeys(int config);
     void pass(bool build, const unsigned char *frozenDevice);

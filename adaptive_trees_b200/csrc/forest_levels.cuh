@@ -27,65 +27,23 @@
 #pragma once
 
 #include "forest.cuh"
+#include "grid_barrier.cuh"
 #include "levelbuild.cuh"
 
 namespace aot
 {
 namespace forest
 {
-// Barrier words and the outcome of one persistent build (zeroed before the launch).
+// The barrier and the outcome of one persistent build (zeroed before the launch).
 struct LevelStatus
 {
-    u32 arrived;         // CTAs at the current barrier
-    u32 generation;      // barriers passed
-    int barrierError;    // a barrier wait gave up
+    GridBarrier bar;
     int entriesOverflow; // the leaf arrays hold fewer entries than the forest needs
     int tooManyRounds;   // a system's rounds would not converge within maxDepth
     int historyMismatch; // a system's derived history does not end at its tree
-    long long entries;   // entries of all systems (leaves and sentinels)
     int deepest;         // deepest level holding units
-    int pad;
+    long long entries;   // entries of all systems (leaves and sentinels)
 };
-
-constexpr u32 kBarrierSpins = 1u << 22;  // polls of 128 ns or more: well over 0.5 s
-
-// Grid-wide barrier of a cooperative launch.  False when some CTA gave up
-// waiting; the caller returns.
-__device__ __forceinline__ bool gridBarrier(LevelStatus *ls)
-{
-    __shared__ int sOk;
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        volatile u32 *gen = &ls->generation;
-        volatile int *err = &ls->barrierError;
-        const u32 g = *gen;
-        __threadfence();
-        if (atomicAdd(&ls->arrived, 1u) == gridDim.x - 1)
-        {
-            atomicExch(&ls->arrived, 0u);
-            __threadfence();
-            atomicAdd(&ls->generation, 1u);
-        }
-        else
-        {
-            u32 spins = 0;
-            while (*gen == g)
-            {
-                if (*err || ++spins > kBarrierSpins)
-                {
-                    atomicExch(&ls->barrierError, 1);
-                    break;
-                }
-                __nanosleep(128);
-            }
-        }
-        __threadfence();
-        sOk = *err == 0;
-    }
-    __syncthreads();
-    return sOk != 0;
-}
 
 struct LevelArgs
 {
@@ -98,12 +56,6 @@ struct LevelArgs
     int maxDepth;
     HilbertTables h;
 };
-
-template <class T>
-__device__ __forceinline__ T vload(const T &x)
-{
-    return *static_cast<const volatile T *>(&x);
-}
 
 template <bool Hilbert>
 static __global__ void __launch_bounds__(lb::kThreads) levelBuildKernel(LevelArgs p)
@@ -120,6 +72,7 @@ static __global__ void __launch_bounds__(lb::kThreads) levelBuildKernel(LevelArg
     LevelStatus *ls = p.ls;
     const u32 rank = blockIdx.x * blockDim.x + threadIdx.x, size = gridDim.x * blockDim.x;
     const int S = p.f.numSystems;
+    if (vload(p.f.st->error)) return;  // the sort gave up: the host reports it
     if constexpr (Hilbert)
     {
         for (int k = threadIdx.x; k < 48 * 8; k += blockDim.x)
@@ -157,7 +110,7 @@ static __global__ void __launch_bounds__(lb::kThreads) levelBuildKernel(LevelArg
         }
         a.sysRoot[s] = root;
     }
-    if (!gridBarrier(ls)) return;
+    if (!gridBarrier(&ls->bar)) return;
     // levels: every CTA reads the same counts and flags after a barrier
     int deepest = -1;
     for (int l = 0; l < int(kOctLevels); ++l)
@@ -166,15 +119,15 @@ static __global__ void __launch_bounds__(lb::kThreads) levelBuildKernel(LevelArg
         if (vload(c.overflow) | vload(c.late) || count == 0) break;
         deepest = l;
         expandUnits(a, p.idx, l, start, count, rank, size);
-        if (!gridBarrier(ls)) return;
+        if (!gridBarrier(&ls->bar)) return;
         classifyUnits<false, Hilbert, true>(a, l, p.bucket, start, count, sNext, sDec, nullptr, nullptr, rank, size);
-        if (!gridBarrier(ls)) return;
+        if (!gridBarrier(&ls->bar)) return;
     }
     if (vload(c.overflow) | vload(c.late)) return;
     for (int l = deepest; l >= 0; --l)
     {
         leafCountUnits(a, vload(c.levelStart[l]), vload(c.levelCount[l]), rank, size);
-        if (!gridBarrier(ls)) return;
+        if (!gridBarrier(&ls->bar)) return;
     }
     // layout (CTA 0): systems one after the other, each followed by its sentinel
     if (blockIdx.x == 0)
@@ -238,7 +191,7 @@ static __global__ void __launch_bounds__(lb::kThreads) levelBuildKernel(LevelArg
             st.proposal = entries;
         }
     }
-    if (!gridBarrier(ls)) return;
+    if (!gridBarrier(&ls->bar)) return;
     if (vload(ls->entriesOverflow)) return;
     // each system's leaves after every round that changes it: a final leaf at
     // (arrival a, region depth k, relative level j) stands for
@@ -292,7 +245,7 @@ static __global__ void __launch_bounds__(lb::kThreads) levelBuildKernel(LevelArg
     {
         placeUnits<false>(a, p.f.K[0], p.f.B[0], nullptr, p.f.SEG[0], l, vload(c.levelStart[l]),
                           vload(c.levelCount[l]), p.capacity, rank, size);
-        if (!gridBarrier(ls)) return;
+        if (!gridBarrier(&ls->bar)) return;
     }
     const i64 E = vload(ls->entries);
     for (i64 i = rank; i < E; i += size)

@@ -209,7 +209,7 @@ __device__ __forceinline__ void innerBegins(const KeyIndex &idx, u32 lo, u32 hi,
         // before the first one at or above it
         const u32 wlo = b[d] > jA ? ((b[d] - 1) << kSampleShift) + 1 : lo;
         const u32 whi = b[d] < jB ? (b[d] << kSampleShift) : hi;
-        len[d] = whi - wlo;
+        len[d] = whi > wlo ? whi - wlo : 0;  // empty unless the keys are sorted (a failed sort stays in bounds)
         b[d] = wlo;
     }
     for (;;)

@@ -259,12 +259,16 @@ struct SegmentTiles
 // digit each in the per-digit steps.  A look-back that polls an unpublished
 // tile more than spinLimit times records kErrLookback and goes on with the
 // prefix it has: every write stays inside the output, the result is wrong
-// and the host reports the error.
+// and the host reports the error.  A persistent CTA calls it until it returns
+// false: the tile counter has passed numTiles (which a launch of one CTA per
+// tile never reaches).  Persistent use needs unstaged values
+// (Tiles::kStageValues false): the staging barrier is not set up again.
 template <int Bits, int Items, class Tiles>
-__device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__restrict__ keysIn,
+__device__ __forceinline__ bool onesweepTile(const Tiles &tiles, const u64 *__restrict__ keysIn,
                                              const u32 *__restrict__ valsIn, u64 *__restrict__ keysOut,
                                              u32 *__restrict__ valsOut, int shift, u32 *tileCounter, u64 *status,
-                                             int *error, int bits, unsigned spinLimit = kLookbackSpins)
+                                             int *error, int bits, unsigned spinLimit = kLookbackSpins,
+                                             u32 numTiles = 0xffffffffu)
 {
     using Smem = SharedPass<Bits, Items>;
     constexpr int R = Smem::R;
@@ -289,6 +293,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
     }
     __syncthreads();
     const size_t tile = sm.tile;
+    if (tile >= numTiles) return false;
     const size_t tileBase = tiles.base(tile);
     const size_t warpBase = tileBase + size_t(warp) * (32 * Items);
     if (stage && tid == 0)
@@ -480,6 +485,7 @@ __device__ __forceinline__ void onesweepTile(const Tiles &tiles, const u64 *__re
         {
         }
     }
+    return true;
 }
 
 // CTAs per SM each configuration is built for.

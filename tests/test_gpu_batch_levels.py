@@ -155,3 +155,28 @@ def test_second_build_grows_buffers():
     _same(lv, rd, 3, "second build")
     lv.close()
     rd.close()
+
+
+def test_build_is_three_launches():
+    """Keys, the persistent sort and the persistent level build: three kernel
+    launches for the whole batch (after the first build has tuned the sort)."""
+    import adaptive_trees_b200 as ab
+    rng = np.random.default_rng(21)
+    host = [_system(rng, k, n, np.float32) for k, n in enumerate([30_000, 5, 70_000, 0, 12_345])]
+    cfg = tree_config(bucket=64, hilbert=False)
+    b, dev = _batch(host, cfg, 0)
+    probe = ab.Tree(0, *dev[0], cfg)  # the launch counter is process-wide
+    b.build()
+    torch.cuda.synchronize()
+    before = probe.info().kernel_launches
+    b.build()
+    torch.cuda.synchronize()
+    assert b.buildPath()
+    assert probe.info().kernel_launches - before == 3
+    rd, _ = _batch(host, cfg, 1)
+    b.doBuffersNeedResize()
+    rd.doBuffersNeedResize()
+    _same(b, rd, len(host), "build")
+    probe.close()
+    b.close()
+    rd.close()
