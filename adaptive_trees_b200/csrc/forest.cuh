@@ -98,13 +98,12 @@ struct Bufs
 // only where the system changes.
 // The keys of tiles [t0, t1) (a CTA's share), with the digit histograms
 // counted in sh[kMaxPasses][kRadix] (zero on entry and on return) and flushed
-// where the system changes.  sEnc / sNext hold the Hilbert tables.
+// where the system changes.  sPair holds the two-level Hilbert table.
 template <class Real, Curve C>
 __device__ __forceinline__ void keygenTiles(const System *__restrict__ systems, const u32 *__restrict__ tileSys,
                                             const u32 *__restrict__ tileBegin, const u32 *__restrict__ tileEnd,
                                             u32 t0, u32 t1, const KeygenParams<Real> &prm, u64 *__restrict__ keys,
-                                            u32 *__restrict__ hist, u32 *sh, const unsigned char *sEnc,
-                                            const unsigned char *sNext)
+                                            u32 *__restrict__ hist, u32 *sh, const unsigned short *sPair)
 {
     int cur = -1;
     auto flush = [&]() {
@@ -140,7 +139,7 @@ __device__ __forceinline__ void keygenTiles(const System *__restrict__ systems, 
         for (u32 g = tileBegin[t] + threadIdx.x; g < end; g += blockDim.x)
         {
             const u32 l = g - sy.base;
-            const u64 k = particleKey<Real, C>(x[l], y[l], z[l], prm, sEnc, sNext);
+            const u64 k = particleKey<Real, C>(x[l], y[l], z[l], prm, sPair);
             keys[g] = k;
             if (hist)
             {
@@ -160,18 +159,25 @@ static __global__ void __launch_bounds__(kThreads)
                  const KeygenParams<Real> prm, u64 *__restrict__ keys, u32 *__restrict__ hist)
 {
     __shared__ u32 sh[sort::kMaxPasses * sort::kRadix];
-    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8];
+    __shared__ unsigned short sPair[C == Curve::Hilbert ? kHilbertPairEntries : 1];
     for (int i = threadIdx.x; i < sort::kMaxPasses * sort::kRadix; i += blockDim.x) sh[i] = 0;
-    for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x)
+    if constexpr (C == Curve::Hilbert)
     {
-        sEnc[i] = prm.h.enc[i];
-        sNext[i] = prm.h.encNext[i];
+        // the one-level tables staged in shared memory, then the pair table from them
+        __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8];
+        for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x)
+        {
+            sEnc[i] = prm.h.enc[i];
+            sNext[i] = prm.h.encNext[i];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kHilbertPairEntries; i += blockDim.x)
+            sPair[i] = hilbertPairEntry(i, sEnc, sNext);
     }
     __syncthreads();
     const u32 per = (numTiles + gridDim.x - 1) / gridDim.x;
     const u32 t0 = blockIdx.x * per;
-    keygenTiles<Real, C>(systems, tileSys, tileBegin, tileEnd, t0, min(numTiles, t0 + per), prm, keys, hist, sh, sEnc,
-                         sNext);
+    keygenTiles<Real, C>(systems, tileSys, tileBegin, tileEnd, t0, min(numTiles, t0 + per), prm, keys, hist, sh, sPair);
 }
 
 // Per-system histograms of Bits-wide digits for `passes` passes, one CTA per

@@ -24,9 +24,10 @@ struct KeygenParams
     HilbertTables h;
 };
 
+// sPair: the two-level Hilbert table (hilbertPairEntry) in shared memory.
 template <class Real, Curve C>
 __device__ __forceinline__ u64 particleKey(Real x, Real y, Real z, const KeygenParams<Real> &p,
-                                           const unsigned char *sEnc, const unsigned char *sNext)
+                                           const unsigned short *sPair)
 {
     if constexpr (C == Curve::Binary)
     {
@@ -38,7 +39,7 @@ __device__ __forceinline__ u64 particleKey(Real x, Real y, Real z, const KeygenP
         const u32 ix = quantise(x, p.q.xmin, p.q.ilx, p.q.bx);
         const u32 iy = quantise(y, p.q.ymin, p.q.ily, p.q.by);
         const u32 iz = quantise(z, p.q.zmin, p.q.ilz, p.q.bz);
-        if constexpr (C == Curve::Hilbert) return hilbertPrefix(ix, iy, iz, kOctLevels, sEnc, sNext);
+        if constexpr (C == Curve::Hilbert) return hilbertKeyPairs(ix, iy, iz, sPair);
         else return mortonKey(ix, iy, iz);
     }
 }
@@ -52,12 +53,20 @@ static __global__ void __launch_bounds__(kKeygenThreads)
                  const KeygenParams<Real> prm, u64 *__restrict__ keys, u32 *__restrict__ hist, int histPasses)
 {
     __shared__ u32 sh[sort::kMaxPasses][sort::kRadix];
-    __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8];
+    __shared__ unsigned short sPair[C == Curve::Hilbert ? kHilbertPairEntries : 1];
     for (int i = threadIdx.x; i < sort::kMaxPasses * sort::kRadix; i += blockDim.x) (&sh[0][0])[i] = 0;
-    for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x)
+    if constexpr (C == Curve::Hilbert)
     {
-        sEnc[i] = prm.h.enc[i];
-        sNext[i] = prm.h.encNext[i];
+        // the one-level tables staged in shared memory, then the pair table from them
+        __shared__ unsigned char sEnc[48 * 8], sNext[48 * 8];
+        for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x)
+        {
+            sEnc[i] = prm.h.enc[i];
+            sNext[i] = prm.h.encNext[i];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kHilbertPairEntries; i += blockDim.x)
+            sPair[i] = hilbertPairEntry(i, sEnc, sNext);
     }
     __syncthreads();
 
@@ -101,7 +110,7 @@ static __global__ void __launch_bounds__(kKeygenThreads)
 #pragma unroll
         for (int j = 0; j < Vec; ++j)
         {
-            k[j] = particleKey<Real, C>(vx[j], vy[j], vz[j], prm, sEnc, sNext);
+            k[j] = particleKey<Real, C>(vx[j], vy[j], vz[j], prm, sPair);
             count(k[j]);
         }
         if constexpr (Vec == 4)
@@ -122,7 +131,7 @@ static __global__ void __launch_bounds__(kKeygenThreads)
     // tail particles that do not fill a vector
     for (size_t i = groups * Vec + blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += stride)
     {
-        const u64 k = particleKey<Real, C>(x[i], y[i], z[i], prm, sEnc, sNext);
+        const u64 k = particleKey<Real, C>(x[i], y[i], z[i], prm, sPair);
         keys[i] = k;
         count(k);
     }

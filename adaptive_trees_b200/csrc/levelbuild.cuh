@@ -256,9 +256,41 @@ __device__ __forceinline__ u32 warpLowerBound(const u64 *A, u32 b, u32 e, u64 t,
 // child boundary); the chains of dependent loads of the per-thread searches
 // dominate there, and the keys of a unit span most of the array.
 constexpr u32 kWideUnits = 4096;
+// Up to this many units, a lane per inner boundary (8 lanes per unit): more
+// searches in flight where the units are too few to fill the GPU one thread
+// each.
+constexpr u32 kLaneUnits = 1u << 18;
+
+// Lower bound of t among the keys P[lo, hi): first among the sampled keys in
+// the range, then in the window of at most 31 keys they leave.
+__device__ __forceinline__ u32 boundaryIn(const KeyIndex &idx, u32 lo, u32 hi, u64 t)
+{
+    const u32 jA = (lo + kSampleStride - 1) >> kSampleShift, jB = (hi + kSampleStride - 1) >> kSampleShift;
+    u32 b = jA, len = jB > jA ? jB - jA : 0;
+    while (len)
+    {
+        const u32 half = len >> 1;
+        const bool less = __ldg(idx.sample + b + half) < t;
+        b = less ? b + half + 1 : b;
+        len = less ? len - half - 1 : half;
+    }
+    const u32 wlo = b > jA ? ((b - 1) << kSampleShift) + 1 : lo;
+    const u32 whi = b < jB ? (b << kSampleShift) : hi;
+    b = wlo;
+    len = whi > wlo ? whi - wlo : 0;
+    while (len)
+    {
+        const u32 half = len >> 1;
+        const bool less = __ldg(idx.keys + b + half) < t;
+        b = less ? b + half + 1 : b;
+        len = less ? len - half - 1 : half;
+    }
+    return b;
+}
 
 // 9 child begins of the units of level l: one thread per unit (the 7 inner
-// ones by innerBegins), or one warp per inner boundary on levels of few units.
+// ones by innerBegins), one lane per inner boundary on levels of fewer units,
+// one warp per inner boundary on levels of few units.
 // `rank` and `size` number the threads taking part (a grid, or the grid of a
 // persistent kernel).
 __device__ __forceinline__ void expandUnits(const Arena &a, const KeyIndex &idx, int l, u32 start, u32 count, u32 rank,
@@ -282,6 +314,17 @@ __device__ __forceinline__ void expandUnits(const Arena &a, const KeyIndex &idx,
             const u32 whi = sIdx < jB ? (sIdx << kSampleShift) : hi;
             const u32 r = warpLowerBound(idx.keys, wlo, whi, t, lane);
             if (lane == 0) row[3 + d] = r;
+        }
+        return;
+    }
+    if (count <= kLaneUnits)
+    {
+        for (u32 e = rank; e < count * 8; e += size)
+        {
+            const u32 i = e >> 3, d = e & 7;
+            if (d == 7) continue;
+            u32 *row = a.rows + size_t(start + i) * kRow;
+            row[3 + d] = boundaryIn(idx, row[2], row[10], rowKey(row) + u64(d + 1) * cr);
         }
         return;
     }

@@ -130,6 +130,40 @@ __host__ __device__ __forceinline__ u64 hilbertPrefix(u32 x, u32 y, u32 z, unsig
     return key << (3u * (kOctLevels - levels));
 }
 
+// Two levels per lookup: pair[state * 64 + (o1 << 3 | o2)] = the two emitted
+// digits (d1 << 3 | d2) | the state after both << 6, for the original octants
+// o1, o2 of two consecutive levels.  3072 entries built from enc / encNext.
+constexpr int kHilbertPairEntries = 48 * 64;
+__host__ __device__ __forceinline__ unsigned short hilbertPairEntry(int i, const unsigned char *enc,
+                                                                   const unsigned char *encNext)
+{
+    const int s = i >> 6, o1 = (i >> 3) & 7, o2 = i & 7;
+    const int a = s * 8 + o1;
+    const int b = int(encNext[a]) * 8 + o2;
+    return (unsigned short)((enc[a] << 3) | enc[b] | (encNext[b] << 6));
+}
+
+// The full 21-level Hilbert key of (x, y, z) with the pair table: the Morton
+// interleave of the words puts each level's original octant (x << 2 | y << 1
+// | z) in consecutive bits, so two levels are one 6-bit field.  Equal to
+// hilbertPrefix(x, y, z, kOctLevels, ...).
+__host__ __device__ __forceinline__ u64 hilbertKeyPairs(u32 x, u32 y, u32 z, const unsigned short *sPair)
+{
+    const u64 m = mortonKey(x, y, z);
+    u64 key = 0;
+    unsigned s = kHilbertStart;
+#pragma unroll
+    for (int i = 0; i < int(kOctLevels) / 2; ++i)  // levels 2i and 2i + 1 from the top
+    {
+        const unsigned v = sPair[s * 64 + (unsigned(m >> (3 * (kOctLevels - 2 - 2 * i))) & 63u)];
+        key = (key << 6) | (v & 63u);
+        s = v >> 6;
+    }
+    // the last level alone: the first digit of the entry with o2 = 0
+    const unsigned v = sPair[s * 64 + ((unsigned(m) & 7u) << 3)];
+    return (key << 3) | ((v >> 3) & 7u);
+}
+
 // Decode the top `levels` levels of a Hilbert key to the cell's corner in
 // 21-bit integer coordinates (bits below the level are zero).
 __host__ __device__ __forceinline__ void hilbertCorner(u64 key, unsigned levels, const unsigned char *sDec,
