@@ -404,10 +404,9 @@ static __global__ void __launch_bounds__(kThreads) nbrKernel(Arena a, int l, Hil
 // group-flag populations, which leaves more of the SM's shared storage to L1).
 struct UnitScratch
 {
-    u64 pStart[rb::kUnitBatch], st0[rb::kUnitBatch], st1[rb::kUnitBatch], st2[rb::kUnitBatch];
-    u32 cx[rb::kUnitBatch], cy[rb::kUnitBatch], cz[rb::kUnitBatch];
-    int childState[rb::kUnitBatch], level[rb::kUnitBatch];
-    u32 block[rb::kUnitBatch][64];
+    u64 pStart[rb::kUnitBatch];
+    int childState[rb::kUnitBatch];
+    rb::UnitBlocks block;
     u32 slowRef[rb::kUnitBatch * 27];
     unsigned short slowItem[rb::kUnitBatch * 27];
     int nSlow;
@@ -445,18 +444,11 @@ static __global__ void __launch_bounds__(kThreads, 4)
         const int nb = int(min(u32(kUnitBatch), count - base));
         if (lane < nb)
         {
+            // the cell's path is decoded only where a neighbour lies inside a
+            // coarser leaf (phase B); the children's curve state is in the row
             const u32 *row = a.rows + size_t(start + base + u32(lane)) * kRow;
-            const u64 key = rowKey(row);
-            const rb::CellPath path = rb::decodeCell<Hilbert>(key, unsigned(l), sNext, sDec);
-            w.pStart[lane] = key;
-            w.level[lane] = int(m);
-            w.cx[lane] = path.x;
-            w.cy[lane] = path.y;
-            w.cz[lane] = path.z;
-            w.st0[lane] = path.st0;
-            w.st1[lane] = path.st1;
-            w.st2[lane] = path.st2;
-            w.childState[lane] = path.childState;
+            w.pStart[lane] = rowKey(row);
+            w.childState[lane] = int(unitStateOf(row[11]));
         }
         if (lane == 0) w.nSlow = 0;
         __syncwarp();
@@ -516,7 +508,8 @@ static __global__ void __launch_bounds__(kThreads, 4)
             }
             else
             {
-                qKey = rb::neighbourCell<Hilbert>(w, u, q, qState, sEnc, sNext);
+                const rb::CellPath path = rb::decodeCell<Hilbert>(w.pStart[u], unsigned(l), sNext, sDec);
+                qKey = rb::neighbourCellOf<Hilbert>(path, w.pStart[u], unsigned(l), q, qState, sEnc, sNext);
             }
             u32 begins[rb::kGroupBegins];
             rb::childBeginsWithin(idx.keys, prow[2 + d], prow[3 + d], qKey, m, begins);

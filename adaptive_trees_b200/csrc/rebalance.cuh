@@ -824,6 +824,24 @@ __device__ __forceinline__ bool beginsInside(const NodeTable &gt, const u64 *P, 
 }
 
 // Per-warp scratch of the units in flight.
+// The 4 x 4 x 4 child-count blocks of a warp's units in shared memory.  The 8
+// children of a unit read their 3 x 3 x 3 sub-blocks from offsets {0, 1, 4, 5,
+// 16, 17, 20, 21} (plus a common offset), the same banks for every unit of a
+// dense [unit][64] array; unit u starts at u * 64 + {0, 2, 8, 10}[u % 4] +
+// 16 * (u / 4) instead, so the sub-block reads of 4 consecutive units (one
+// warp instruction) fall in 32 distinct banks.
+__host__ __device__ __forceinline__ int unitBlockBase(int u)
+{
+    return u * 64 + ((0xA820 >> (4 * (u & 3))) & 15) + 16 * (u >> 2);
+}
+constexpr int kUnitBlockWords = (kUnitBatch - 1) * 64 + 10 + 16 * ((kUnitBatch - 1) / 4) + 64;
+
+struct UnitBlocks
+{
+    u32 mem[kUnitBlockWords];
+    __device__ __forceinline__ u32 *operator[](int u) { return mem + unitBlockBase(u); }
+};
+
 struct UnitScratch
 {
     u64 pStart[kUnitBatch], st0[kUnitBatch], st1[kUnitBatch], st2[kUnitBatch];
@@ -831,7 +849,7 @@ struct UnitScratch
     u32 cx[kUnitBatch], cy[kUnitBatch], cz[kUnitBatch];
     u32 hintB[kUnitBatch];                // begin index of the unit's first leaf
     int childState[kUnitBatch], level[kUnitBatch], active[kUnitBatch];
-    u32 block[kUnitBatch][64];
+    UnitBlocks block;
     u64 slowKey[kUnitBatch * 27];
     unsigned short slowItem[kUnitBatch * 27];  // unit * 27 + q
     unsigned char slowState[kUnitBatch * 27];
@@ -840,19 +858,18 @@ struct UnitScratch
 
 // Key and child Hilbert state of the parent-level cell at offset q around the
 // parent of unit u.
-template <bool Hilbert, class Scratch>
-__device__ __forceinline__ u64 neighbourCell(const Scratch &w, int u, int q, int &qState,
-                                             const unsigned char *sEnc, const unsigned char *sNext)
+// The same from the decoded path of the parent cell P (key pStart at level pl).
+template <bool Hilbert>
+__device__ __forceinline__ u64 neighbourCellOf(const CellPath &path, u64 pStart, unsigned pl, int q, int &qState,
+                                               const unsigned char *sEnc, const unsigned char *sNext)
 {
-    const unsigned pl = unsigned(w.level[u]) - 1;
-    const u64 pStart = w.pStart[u];
     const int dx = q % 3 - 1, dy = (q / 3) % 3 - 1, dz = q / 9 - 1;
     const u32 cube = 1u << (kOctLevels - pl);
-    const u32 cx = w.cx[u], cy = w.cy[u], cz = w.cz[u];
+    const u32 cx = path.x, cy = path.y, cz = path.z;
     const u32 x = (cx + u32(dx) * cube) & 0x1fffffu;
     const u32 y = (cy + u32(dy) * cube) & 0x1fffffu;
     const u32 z = (cz + u32(dz) * cube) & 0x1fffffu;
-    qState = w.childState[u];
+    qState = path.childState;
     const u32 diff = (x ^ cx) | (y ^ cy) | (z ^ cz);  // zero only when the wrap maps Q onto P
     if (diff == 0) return pStart;
     if constexpr (Hilbert)
@@ -860,7 +877,7 @@ __device__ __forceinline__ u64 neighbourCell(const Scratch &w, int u, int q, int
         // Q agrees with P on the levels above the first differing bit: keep
         // that key prefix and encode the suffix from P's state there
         const unsigned m = unsigned(__clz(diff)) - (32u - kOctLevels);
-        const u64 word = m < 10 ? w.st0[u] : (m < 20 ? w.st1[u] : w.st2[u]);
+        const u64 word = m < 10 ? path.st0 : (m < 20 ? path.st1 : path.st2);
         int st = int((word >> (6 * (m < 10 ? m : (m < 20 ? m - 10 : m - 20)))) & 63u);
         u64 suffix = 0;
         for (unsigned k = m; k < pl; ++k)
@@ -880,6 +897,14 @@ __device__ __forceinline__ u64 neighbourCell(const Scratch &w, int u, int q, int
     {
         return mortonKey(x, y, z);
     }
+}
+
+template <bool Hilbert, class Scratch>
+__device__ __forceinline__ u64 neighbourCell(const Scratch &w, int u, int q, int &qState,
+                                             const unsigned char *sEnc, const unsigned char *sNext)
+{
+    const CellPath path{w.cx[u], w.cy[u], w.cz[u], w.st0[u], w.st1[u], w.st2[u], w.childState[u]};
+    return neighbourCellOf<Hilbert>(path, w.pStart[u], unsigned(w.level[u]) - 1, q, qState, sEnc, sNext);
 }
 
 // Where the children of the neighbour cell at offset q land in the unit's
