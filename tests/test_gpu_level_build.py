@@ -49,11 +49,15 @@ CONFIGS = [
 
 
 def _build(xyz, mode, **cfg):
+    """Mode 0 builds twice: the second build queues only the levels the first
+    one needed (and must still come out whole)."""
     import adaptive_trees_b200 as ab
     xs = [to_dev(a) for a in xyz]
     t = ab.Tree(0, *xs, tree_config(**cfg))
     t.setBuildMode(mode)
     t.build()
+    if mode == 0:
+        t.build()
     return t, xs
 
 
@@ -148,6 +152,33 @@ def test_escaped_particles_sort_last():
     assert t.buildPath()[0]
     compare(t, o)
     t.close()
+
+
+@pytest.mark.parametrize("first,second", [("uniform", "stacked"), ("stacked", "uniform"), ("plummer", "mixture")])
+@pytest.mark.parametrize("nf", [True, False])
+def test_second_build_of_another_tree(first, second, nf):
+    """The second build queues the levels the first tree needed; a tree of
+    another shape (deeper, shallower, denser) must still come out equal to
+    the rounds."""
+    import adaptive_trees_b200 as ab
+    gen = {"uniform": lambda: S.uniform_cube(60_000, seed=41), "stacked": lambda: _stacked(60_000, 42),
+           "plummer": lambda: S.plummer_sphere(80_000, seed=43), "mixture": lambda: S.gaussian_mixture(80_000, seed=44)}
+    a, b = gen[first](), gen[second]()
+    cfg = dict(bucket=16, nf=nf, hilbert=True)
+    trees = []
+    for mode in (0, 1):  # the same two builds by levels and by rounds (leafCapacity keeps its history)
+        xs = [to_dev(v) for v in a]
+        t = ab.Tree(0, *xs, tree_config(**cfg))
+        t.setBuildMode(mode)
+        t.build()
+        for d, v in zip(xs, b):
+            d.copy_(torch.from_numpy(np.ascontiguousarray(v)).to("cuda"))
+        t.build()
+        trees.append(t)
+    assert trees[0].buildPath()[0]
+    _same(trees[0], trees[1], nf)
+    for t in trees:
+        t.close()
 
 
 def test_deeper_tree_after_a_shallow_one():
