@@ -745,6 +745,7 @@ struct TreeEngine::Impl
     DevMem lvRows, lvVal, lvChild, lvLeaves, lvOffset, lvCtl, lvNbr, lvParent;
     size_t lvCap = 0;
     int lvLevels = int(kOctLevels);  // levels the last level build needed, with one to spare
+    DevMem mergeSplits;              // merge-path cuts of the full begin refresh
     u32 nodeSlots = 0;
     bool nodeStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
@@ -1282,8 +1283,21 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
     cudaStream_t s = cfg_.stream;
     const rb::TreeBufs tb = m_->bufs();
     const KeyIndex idx = m_->keyIndex(n_);
-    if (all) rb::octBeginKernel<true><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx), noteLaunch();
-    else rb::octBeginKernel<false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx), noteLaunch();
+    if (all)
+    {
+        // every leaf: a merge of the leaf keys with the particle keys
+        const size_t chunks = (physCap_ + 1 + n_) / rb::kMergeChunk + 2;
+        m_->mergeSplits.reserve((chunks + 1) * sizeof(u32), s);
+        const u64 *P = m_->P[0].as<u64>();
+        rb::mergeSplitKernel<<<gridFor(chunks + 1, 256), 256, 0, s>>>(tb, P, m_->mergeSplits.as<u32>()), noteLaunch();
+        rb::mergeBeginKernel<<<unsigned(std::min<size_t>(chunks, size_t(smCount()) * 8u)), 256, 0, s>>>(
+            tb, P, m_->mergeSplits.as<u32>()),
+            noteLaunch();
+    }
+    else
+    {
+        rb::octBeginKernel<false><<<blocks, rb::kRefreshThreads, 0, s>>>(tb, idx), noteLaunch();
+    }
     if (cfg_.nf)
     {
         const HilbertTables &h = m_->kpd.h;

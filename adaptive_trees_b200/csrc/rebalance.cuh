@@ -535,6 +535,80 @@ static __global__ void __launch_bounds__(kRefreshThreads) octBeginKernel(TreeBuf
     }
 }
 
+// The begin index of every leaf (and B[L] = the active count) by merging the
+// sorted leaf keys K with the sorted particle keys P, the refresh of all
+// leaves at the start of an update: B[i] = #{j : P[j] < K[i]}.  In the merged
+// order (a leaf key before an equal particle key) K[i] sits at i + B[i].  The
+// merged sequence of L + nActive entries is cut into chunks of kMergeChunk; a
+// first kernel finds each cut's leaf count by a binary search of the merge
+// path, and a second one takes a chunk per CTA: its particle keys into shared
+// memory, each of its leaf keys a search there.  Every key is read once and
+// coalesced, where lower bounds one leaf at a time read the sampled index and
+// a window per leaf.
+constexpr int kMergeChunk = 2048;
+
+// Leaves among the first d entries of the merged order.
+__device__ __forceinline__ u32 mergeSplit(const u64 *K, u32 L, const u64 *P, u32 nA, u64 d)
+{
+    u32 lo = d > nA ? u32(d - nA) : 0u, hi = d < L ? u32(d) : L;
+    while (lo < hi)
+    {
+        const u32 mid = (lo + hi) >> 1;
+        // leaf mid comes before particle d - mid - 1: more than mid leaves
+        if (K[mid] <= P[d - mid - 1]) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+static __global__ void mergeSplitKernel(TreeBufs tb, const u64 *P, u32 *splits)
+{
+    const DeviceState *st = tb.st;
+    if (halted(st)) return;
+    const u32 L = u32(st->numLeaves), nA = st->numActiveParticles;
+    const u64 M = u64(L) + nA;
+    const u64 chunks = (M + kMergeChunk - 1) / kMergeChunk;
+    const u64 *K = tb.k(st->activeBuffer);
+    for (u64 c = blockIdx.x * u64(blockDim.x) + threadIdx.x; c <= chunks; c += u64(gridDim.x) * blockDim.x)
+        splits[c] = mergeSplit(K, L, P, nA, c * kMergeChunk < M ? c * kMergeChunk : M);
+}
+
+static __global__ void __launch_bounds__(256) mergeBeginKernel(TreeBufs tb, const u64 *P, const u32 *splits)
+{
+    __shared__ u64 sP[kMergeChunk];
+    const DeviceState *st = tb.st;
+    if (halted(st)) return;
+    const int a = st->activeBuffer;
+    const u32 L = u32(st->numLeaves), nA = st->numActiveParticles;
+    const u64 M = u64(L) + nA;
+    const u64 chunks = (M + kMergeChunk - 1) / kMergeChunk;
+    const u64 *K = tb.k(a);
+    u32 *B = tb.b(a);
+    if (blockIdx.x == 0 && threadIdx.x == 0) B[L] = nA;
+    for (u64 c = blockIdx.x; c < chunks; c += gridDim.x)
+    {
+        const u64 d0 = c * kMergeChunk, d1 = d0 + kMergeChunk < M ? d0 + kMergeChunk : M;
+        const u32 i0 = splits[c], i1 = splits[c + 1];
+        const u32 j0 = u32(d0 - i0), j1 = u32(d1 - i1);
+        __syncthreads();  // the previous chunk's searches are done
+        for (u32 j = j0 + threadIdx.x; j < j1; j += blockDim.x) sP[j - j0] = P[j];
+        __syncthreads();
+        for (u32 i = i0 + threadIdx.x; i < i1; i += blockDim.x)
+        {
+            const u64 k = K[i];
+            u32 lo = 0, len = j1 - j0;
+            while (len)
+            {
+                const u32 half = len >> 1;
+                const bool less = sP[lo + half] < k;
+                lo = less ? lo + half + 1 : lo;
+                len = less ? len - half - 1 : half;
+            }
+            B[i] = j0 + lo;
+        }
+    }
+}
+
 // Near-field counts by parent cell.
 //
 // NF(leaf) = own x (population of the 27 periodic same-level cells around the
