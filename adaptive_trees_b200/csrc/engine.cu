@@ -734,6 +734,10 @@ struct TreeEngine::Impl
     size_t hstBytes = 0;
     cudaStream_t d2h = nullptr;
     cudaEvent_t ready = nullptr;
+    // level build: the neighbour references of a level run on `side` beside
+    // the expansion of the same level (neither needs the other)
+    cudaStream_t side = nullptr;
+    cudaEvent_t sideFork = nullptr, sideJoin = nullptr;
     cudaEvent_t marks[8] = {};              // stage events (profiling)
     cudaEvent_t tuneStart = nullptr, tuneEnd = nullptr;  // sort tuner timing
     std::vector<cudaEvent_t> nfMarks;       // begin/end pairs around near-field launches
@@ -772,6 +776,9 @@ struct TreeEngine::Impl
         if (tuneEnd) cudaEventDestroy(tuneEnd);
         for (cudaEvent_t e : nfMarks) cudaEventDestroy(e);
         if (d2h) cudaStreamDestroy(d2h);
+        if (sideFork) cudaEventDestroy(sideFork);
+        if (sideJoin) cudaEventDestroy(sideJoin);
+        if (side) cudaStreamDestroy(side);
     }
 
     // device bytes held by this tree
@@ -959,6 +966,7 @@ TreeEngine::~TreeEngine()
     {
         (void)cudaStreamSynchronize(cfg_.stream);
         if (m_->d2h) (void)cudaStreamSynchronize(m_->d2h);
+        if (m_->side) (void)cudaStreamSynchronize(m_->side);
     }
 }
 
@@ -1548,20 +1556,38 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         // placement; one readback at the end checks that no deeper level
         // was left out.
         const int levels = std::max(1, std::min(int(kOctLevels), m.lvLevels));
+        const bool useSide = nf;
+        if (useSide && !m.side)
+        {
+            AOT_CHECK(cudaStreamCreateWithFlags(&m.side, cudaStreamNonBlocking));
+            AOT_CHECK(cudaEventCreateWithFlags(&m.sideFork, cudaEventDisableTiming));
+            AOT_CHECK(cudaEventCreateWithFlags(&m.sideJoin, cudaEventDisableTiming));
+        }
         for (int l = 0; l < levels; ++l)
         {
+            const bool fork = nf && l > 0 && useSide;
+            if (fork)
+            {
+                // the neighbour references of level l need level l - 1 only
+                AOT_CHECK(cudaEventRecord(m.sideFork, s));
+                AOT_CHECK(cudaStreamWaitEvent(m.side, m.sideFork, 0));
+                if (cfg_.hilbert) lb::nbrKernel<true><<<blocks * 2, lb::kThreads, 0, m.side>>>(a, l, m.kpd.h), noteLaunch();
+                else lb::nbrKernel<false><<<blocks * 2, lb::kThreads, 0, m.side>>>(a, l, m.kpd.h), noteLaunch();
+                AOT_CHECK(cudaEventRecord(m.sideJoin, m.side));
+            }
             lb::expandKernel<<<blocks * 2, lb::kThreads, 0, s>>>(a, idx, l), noteLaunch();
+            if (fork) AOT_CHECK(cudaStreamWaitEvent(s, m.sideJoin, 0));
             if (nf)
             {
                 markNearField(true);
                 if (cfg_.hilbert)
                 {
-                    if (l > 0) lb::nbrKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, l, m.kpd.h), noteLaunch();
+                    if (l > 0 && !fork) lb::nbrKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, l, m.kpd.h), noteLaunch();
                     lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h), noteLaunch();
                 }
                 else
                 {
-                    if (l > 0) lb::nbrKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, l, m.kpd.h), noteLaunch();
+                    if (l > 0 && !fork) lb::nbrKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, l, m.kpd.h), noteLaunch();
                     lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h), noteLaunch();
                 }
                 markNearField(false);
