@@ -750,6 +750,8 @@ struct TreeEngine::Impl
     size_t lvCap = 0;
     int lvLevels = int(kOctLevels);  // levels the last level build needed, with one to spare
     DevMem mergeSplits;              // merge-path cuts of the full begin refresh
+    unsigned char *lvHost = nullptr; // pinned: the level build's one readback
+    size_t lvHostBytes = 0;
     u32 nodeSlots = 0;
     bool nodeStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
@@ -769,6 +771,7 @@ struct TreeEngine::Impl
     ~Impl()
     {
         if (hst) blockcache::giveHost(hst, hstBytes);
+        if (lvHost) blockcache::giveHost(lvHost, lvHostBytes);
         if (ready) cudaEventDestroy(ready);
         for (cudaEvent_t e : marks)
             if (e) cudaEventDestroy(e);
@@ -1349,6 +1352,13 @@ void TreeEngine::readState()
     AOT_CHECK(cudaStreamWaitEvent(m_->d2h, m_->ready, 0));
     AOT_CHECK(cudaMemcpyAsync(m_->hst, m_->st, sizeof(DeviceState), cudaMemcpyDeviceToHost, m_->d2h));
     waitStream(m_->d2h);
+    applyState();
+}
+
+// The host's copies of the state from the mirror (filled by a readback, or
+// by the host where it knows every value).
+void TreeEngine::applyState()
+{
     const DeviceState &h = *m_->hst;
     if (h.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
     hostActiveBuffer_ = h.activeBuffer;
@@ -1491,7 +1501,11 @@ void TreeEngine::octreeBuild()
     materializeCounts();
     buildViews(cfg_.views);
     mark(MarkEnd);
-    (void)doBuffersNeedResize();
+    // the state read at the end of a build (doBuffersNeedResize); a build by
+    // levels without views already knows every value of the state
+    const bool views = cfg_.views.treeStructure | cfg_.views.particleCountsPerBox | cfg_.views.particleMapping;
+    if (lastBuildByLevels_ && !views) applyState();
+    else (void)doBuffersNeedResize();
 }
 
 void TreeEngine::setBuildMode(int mode)
@@ -1515,8 +1529,10 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
     size_t cap = std::max<size_t>(m.lvCap, n_ / 4 + 4096);
     constexpr size_t kHeadBytes = (sizeof(lb::Control) + 255) & ~size_t(255);
     constexpr size_t kCtlBytes = kHeadBytes + (lb::kContribBins + lb::kArrivals) * sizeof(unsigned long long);
-    std::vector<unsigned char> host(kCtlBytes);
-    const lb::Control &hc = *reinterpret_cast<const lb::Control *>(host.data());
+    if (!m.lvHost)
+        m.lvHost = static_cast<unsigned char *>(blockcache::takeHost(kCtlBytes + 16, &m.lvHostBytes));
+    unsigned char *host = m.lvHost;
+    const lb::Control &hc = *reinterpret_cast<const lb::Control *>(host);
     for (;;)
     {
         if (cap >= (size_t(1) << 28)) return false;  // neighbour references hold unit * 8 + digit in 31 bits
@@ -1623,10 +1639,13 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         place();
         // the round history is needed before finishKernel writes it; read
         // everything once
-        AOT_CHECK(cudaMemcpyAsync(host.data(), m.lvCtl.p, kCtlBytes, cudaMemcpyDeviceToHost, s));
-        u32 rootLeaves = 1;
-        AOT_CHECK(cudaMemcpyAsync(&rootLeaves, a.leaves, sizeof(u32), cudaMemcpyDeviceToHost, s));
+        // (with the device state: its active count, set by the root kernel)
+        AOT_CHECK(cudaMemcpyAsync(host, m.lvCtl.p, kCtlBytes, cudaMemcpyDeviceToHost, s));
+        AOT_CHECK(cudaMemcpyAsync(host + kCtlBytes, a.leaves, sizeof(u32), cudaMemcpyDeviceToHost, s));
+        AOT_CHECK(cudaMemcpyAsync(m.hst, m.st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
         waitStream(s);
+        u32 rootLeaves = 1;
+        std::memcpy(&rootLeaves, host + kCtlBytes, sizeof(u32));
         if (hc.error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
         if (hc.overflow)
         {
@@ -1644,7 +1663,7 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
             if (hc.levelCount[l]) deepest = l;
         if (deepest < 0) rootLeaves = 1;
         // leaves after every round that changed the tree
-        const auto *contrib = reinterpret_cast<const unsigned long long *>(host.data() + kHeadBytes);
+        const auto *contrib = reinterpret_cast<const unsigned long long *>(host + kHeadBytes);
         const auto *landed = contrib + lb::kContribBins;
         int rounds = 0;
         for (int ai = 0; ai < lb::kArrivals; ++ai)
@@ -1679,6 +1698,18 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         m.lvLevels = std::min(int(kOctLevels), deepest + 2);
         lb::finishKernel<<<1, 1, 0, s>>>(a, m.bufs(), rounds, levels, u32(physCap_)), noteLaunch();
         AOT_LAUNCH_CHECK();
+        // the host mirror of what finishKernel writes (the readback above
+        // brought the active count), so the build needs no second readback
+        DeviceState &h = *m.hst;
+        h.numLeaves = h.newNumLeaves = int(rootLeaves);
+        h.proposal = (long long)rootLeaves;
+        h.iteration = rounds;
+        h.rounds = rounds + 1;
+        h.changed = h.converged = h.needsResize = 0;
+        h.numNodes = 0;
+        h.activeBuffer = 0;
+        h.overflow = 0;
+        h.dirtyCount = 0;
         if (nf) AOT_CHECK(cudaMemsetAsync(m.G[0].p, 0, m.G[0].bytes, s));  // no group of the converged tree may merge
         return true;
     }

@@ -241,6 +241,7 @@ private:
     void prepareViews(size_t capacity, const adaptive_octree::ViewConfig &v);
     void syncViewSizes();
     void readState();
+    void applyState();
     void materializeCounts();
 };
 
