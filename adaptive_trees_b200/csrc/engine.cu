@@ -1498,7 +1498,7 @@ void TreeEngine::octreeBuild()
     const size_t cap = capModel_.finishBuild(proposals.data(), proposals.size(), leaves);
     prepareGraphBuffers(cap);
     built_ = true;
-    materializeCounts();
+    if (!lastBuildByLevels_) materializeCounts();  // the placement of a build by levels writes the counts
     buildViews(cfg_.views);
     mark(MarkEnd);
     // the state read at the end of a build (doBuffersNeedResize); a build by
@@ -1626,11 +1626,11 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
             for (int l = 0; l < levels; ++l)
             {
                 if (nf)
-                    lb::placeKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, tb.K[0], tb.B[0], tb.NF[0], nullptr, l, levels,
+                    lb::placeKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, tb.K[0], tb.B[0], tb.NF[0], tb.N[0], l, levels,
                                                                           u32(physCap_)),
                         noteLaunch();
                 else
-                    lb::placeKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, tb.K[0], tb.B[0], nullptr, nullptr, l, levels,
+                    lb::placeKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, tb.K[0], tb.B[0], nullptr, tb.N[0], l, levels,
                                                                            u32(physCap_)),
                         noteLaunch();
             }

@@ -243,7 +243,7 @@ static __global__ void __launch_bounds__(lb::kThreads) levelBuildKernel(LevelArg
     // placement, shallowest level first (a unit's first entry comes from its parent)
     for (int l = 0; l <= deepest; ++l)
     {
-        placeUnits<false>(a, p.f.K[0], p.f.B[0], nullptr, p.f.SEG[0], l, vload(c.levelStart[l]),
+        placeUnits<false>(a, p.f.K[0], p.f.B[0], nullptr, nullptr, p.f.SEG[0], l, vload(c.levelStart[l]),
                           vload(c.levelCount[l]), p.capacity, rank, size);
         if (!gridBarrier(&ls->bar)) return;
     }

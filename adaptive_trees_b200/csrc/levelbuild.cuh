@@ -166,6 +166,7 @@ static __global__ void rootKernel(Arena a, rb::TreeBufs tb, const u64 *P, size_t
         tb.B[0][0] = 0;
         tb.B[0][1] = active;
         tb.NF[0][0] = nf ? nfRoot : 0u;
+        tb.N[0][0] = active;
         st->numLeaves = 1;
     }
 }
@@ -740,11 +741,11 @@ static __global__ void leafCountKernel(Arena a, int l, int levels)
 // first leaf index of their internal children.  Eight lanes per unit, one per
 // child: a segmented scan of the children's leaf counts gives each child's
 // position, so a warp writes the entries of four units at once.
-// K, B (and NF, SEG where given) are the cornerstone arrays written; SEG
-// receives each leaf's tree (system) in a batch of trees.
+// K, B (and NF, N, SEG where given) are the cornerstone arrays written: N the
+// leaf counts, SEG each leaf's tree (system) in a batch of trees.
 template <bool NF>
-__device__ __forceinline__ void placeUnits(const Arena &a, u64 *K, u32 *B, u32 *NFo, int *SEG, int l, u32 start,
-                                           u32 count, u32 capacity, u32 rank, u32 size)
+__device__ __forceinline__ void placeUnits(const Arena &a, u64 *K, u32 *B, u32 *NFo, u32 *N, int *SEG, int l,
+                                           u32 start, u32 count, u32 capacity, u32 rank, u32 size)
 {
     Control &c = *a.ctl;
     const u64 cr = octRange(unsigned(l) + 1);
@@ -777,6 +778,7 @@ __device__ __forceinline__ void placeUnits(const Arena &a, u64 *K, u32 *B, u32 *
             K[o] = rowKey(row) + u64(d) * cr;
             B[o] = row[2 + d];
             if constexpr (NF) NFo[o] = a.val[size_t(g) * 8 + d];
+            if (N) N[o] = row[3 + d] - row[2 + d];
             if (SEG) SEG[o] = int(a.usys[g]);
         }
         else
@@ -787,11 +789,11 @@ __device__ __forceinline__ void placeUnits(const Arena &a, u64 *K, u32 *B, u32 *
 }
 
 template <bool NF>
-static __global__ void placeKernel(Arena a, u64 *K, u32 *B, u32 *NFo, int *SEG, int l, int levels, u32 capacity)
+static __global__ void placeKernel(Arena a, u64 *K, u32 *B, u32 *NFo, u32 *N, int l, int levels, u32 capacity)
 {
     const Control &c = *a.ctl;
     if (c.levelCount[levels] | c.overflow | c.late | c.error) return;
-    placeUnits<NF>(a, K, B, NFo, SEG, l, c.levelStart[l], c.levelCount[l], capacity,
+    placeUnits<NF>(a, K, B, NFo, N, nullptr, l, c.levelStart[l], c.levelCount[l], capacity,
                    blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
