@@ -135,6 +135,26 @@ __device__ __forceinline__ u32 lowerBound32(const u64 *__restrict__ a, u32 n, u6
 constexpr unsigned kSampleShift = 5;
 constexpr unsigned kSampleStride = 1u << kSampleShift;
 
+// Lower bound of t in the sorted A[b, e) by a whole warp: each step probes 32
+// points that split the range into 33 parts and keeps the part the ballot
+// points to, so a range of n keys takes about log33(n) dependent loads
+// instead of log2(n).  Every lane returns the answer.
+__device__ __forceinline__ u32 warpLowerBound(const u64 *A, u32 b, u32 e, u64 t, int lane)
+{
+    while (e > b)
+    {
+        const u32 n = e - b;
+        const u32 p = b + u32((u64(lane) + 1) * n / 33u);  // p < e; p_k = b + k when n <= 32
+        const unsigned below = __ballot_sync(0xffffffffu, __ldg(A + p) < t);
+        const int c = __popc(below);  // a prefix of the lanes: A is sorted
+        const u32 pLow = __shfl_sync(0xffffffffu, p, c > 0 ? c - 1 : 0);
+        const u32 pHigh = __shfl_sync(0xffffffffu, p, c < 32 ? c : 31);
+        if (c > 0) b = pLow + 1;
+        if (c < 32) e = pHigh;
+    }
+    return b;
+}
+
 struct KeyIndex
 {
     const u64 *keys;

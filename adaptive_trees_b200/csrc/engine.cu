@@ -1236,7 +1236,7 @@ void TreeEngine::refreshAll()
     cudaStream_t s = cfg_.stream;
     const rb::TreeBufs tb = m_->bufs();
     const KeyIndex idx = m_->keyIndex(n_);
-    rb::resetForUpdateKernel<<<1, 1, 0, s>>>(m_->st, m_->P[0].as<u64>(), n_), noteLaunch();
+    rb::resetForUpdateKernel<<<1, 32, 0, s>>>(m_->st, m_->P[0].as<u64>(), n_), noteLaunch();
     const unsigned blocks = unsigned(smCount()) * 8u;
     if (cfg_.kind == 1)
     {
@@ -1564,7 +1564,7 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         a.cap = u32(cap);
         AOT_CHECK(cudaMemsetAsync(m.lvCtl.p, 0, kCtlBytes, s));
         if (nf) ensureDigitPos();
-        lb::rootKernel<<<1, 1, 0, s>>>(a, m.bufs(), P, n_, cfg_.bucket, nf ? 1 : 0), noteLaunch();
+        lb::rootKernel<<<1, 32, 0, s>>>(a, m.bufs(), P, n_, cfg_.bucket, nf ? 1 : 0), noteLaunch();
         AOT_LAUNCH_CHECK();
         // Every kernel reads its level's size on the device, so the whole
         // build is queued without a host wait: the levels the last build

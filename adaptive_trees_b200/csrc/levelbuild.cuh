@@ -127,10 +127,12 @@ __device__ __forceinline__ u64 rowKey(const u32 *row) { return (u64(row[1]) << 3
 // The root: a unit at level 0 when its value exceeds the bucket (NF of the
 // root: 27 x count^2, clamped, octree.cu:23-38), else the whole tree is the
 // root leaf, written straight to the cornerstone buffers.
+// One warp: the active count by a warp-wide search, then lane 0.
 static __global__ void rootKernel(Arena a, rb::TreeBufs tb, const u64 *P, size_t n, unsigned bucket, int nf)
 {
     DeviceState *st = tb.st;
-    const unsigned active = n ? unsigned(lowerBoundDev(P, n, kMaxKey)) : 0u;
+    const unsigned active = n ? warpLowerBound(P, 0, u32(n), kMaxKey, int(threadIdx.x & 31)) : 0u;
+    if (threadIdx.x != 0) return;
     const u64 sq = u64(active) * active;
     const u32 nfRoot = sq > 0xffffffffull / 27ull ? 0xffffffffu : u32(27ull * sq);
     const u32 x = nf ? nfRoot : active;
@@ -231,26 +233,6 @@ __device__ __forceinline__ void innerBegins(const KeyIndex &idx, u32 lo, u32 hi,
             }
         }
     }
-}
-
-// Lower bound of t in the sorted A[b, e) by a whole warp: each step probes 32
-// points that split the range into 33 parts and keeps the part the ballot
-// points to, so a range of n keys takes about log33(n) dependent loads
-// instead of log2(n).  Every lane returns the answer.
-__device__ __forceinline__ u32 warpLowerBound(const u64 *A, u32 b, u32 e, u64 t, int lane)
-{
-    while (e > b)
-    {
-        const u32 n = e - b;
-        const u32 p = b + u32((u64(lane) + 1) * n / 33u);  // p < e; p_k = b + k when n <= 32
-        const unsigned below = __ballot_sync(0xffffffffu, __ldg(A + p) < t);
-        const int c = __popc(below);  // a prefix of the lanes: A is sorted
-        const u32 pLow = __shfl_sync(0xffffffffu, p, c > 0 ? c - 1 : 0);
-        const u32 pHigh = __shfl_sync(0xffffffffu, p, c < 32 ? c : 31);
-        if (c > 0) b = pLow + 1;
-        if (c < 32) e = pHigh;
-    }
-    return b;
 }
 
 // Levels with at most this many units expand by warps (a warp per inner

@@ -1330,11 +1330,14 @@ static __global__ void binRefreshKernel(TreeBufs tb, KeyIndex idx)
 
 // Reset at the start of update() (resetRebalanceStateKernel,
 // octree_rebalance.cuh:62-73): changed, converged and the active count.
+// One warp (the active count by a warp-wide search).
 static __global__ void resetForUpdateKernel(DeviceState *st, const u64 *P, size_t n)
 {
+    const unsigned active = n ? warpLowerBound(P, 0, u32(n), kMaxKey, int(threadIdx.x & 31)) : 0u;
+    if (threadIdx.x != 0) return;
     st->changed = 0;
     st->converged = 0;
-    st->numActiveParticles = n ? u32(lowerBoundDev(P, n, kMaxKey)) : 0u;
+    st->numActiveParticles = active;
     st->dirtyCount = 0;
     st->updatePasses = 0;
 }
