@@ -209,6 +209,77 @@ void trim()
     k.dev.clear();
     k.devBytes = 0;
 }
+
+namespace
+{
+struct Handles
+{
+    std::mutex mu;
+    std::map<int, std::vector<cudaStream_t>> streams;
+    std::map<int, std::vector<cudaEvent_t>> events;
+};
+Handles &handles()
+{
+    static Handles *h = new Handles;  // lives as long as the process (streams outlive static teardown)
+    return *h;
+}
+}  // namespace
+
+cudaStream_t takeStream()
+{
+    int d = 0;
+    AOT_CHECK(cudaGetDevice(&d));
+    Handles &h = handles();
+    {
+        std::lock_guard<std::mutex> lock(h.mu);
+        auto &v = h.streams[d];
+        if (!v.empty())
+        {
+            const cudaStream_t s = v.back();
+            v.pop_back();
+            return s;
+        }
+    }
+    cudaStream_t s = nullptr;
+    AOT_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+void giveStream(cudaStream_t s, int device)
+{
+    if (!s) return;
+    Handles &h = handles();
+    std::lock_guard<std::mutex> lock(h.mu);
+    h.streams[device].push_back(s);
+}
+
+cudaEvent_t takeEvent()
+{
+    int d = 0;
+    AOT_CHECK(cudaGetDevice(&d));
+    Handles &h = handles();
+    {
+        std::lock_guard<std::mutex> lock(h.mu);
+        auto &v = h.events[d];
+        if (!v.empty())
+        {
+            const cudaEvent_t e = v.back();
+            v.pop_back();
+            return e;
+        }
+    }
+    cudaEvent_t e = nullptr;
+    AOT_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return e;
+}
+
+void giveEvent(cudaEvent_t e, int device)
+{
+    if (!e) return;
+    Handles &h = handles();
+    std::lock_guard<std::mutex> lock(h.mu);
+    h.events[device].push_back(e);
+}
 }  // namespace blockcache
 
 namespace
@@ -738,6 +809,7 @@ struct TreeEngine::Impl
     // the expansion of the same level (neither needs the other)
     cudaStream_t side = nullptr;
     cudaEvent_t sideFork = nullptr, sideJoin = nullptr;
+    int device = 0;  // the device of the pooled streams and events
     cudaEvent_t marks[8] = {};              // stage events (profiling)
     cudaEvent_t tuneStart = nullptr, tuneEnd = nullptr;  // sort tuner timing
     std::vector<cudaEvent_t> nfMarks;       // begin/end pairs around near-field launches
@@ -772,16 +844,16 @@ struct TreeEngine::Impl
     {
         if (hst) blockcache::giveHost(hst, hstBytes);
         if (lvHost) blockcache::giveHost(lvHost, lvHostBytes);
-        if (ready) cudaEventDestroy(ready);
+        blockcache::giveEvent(ready, device);
         for (cudaEvent_t e : marks)
             if (e) cudaEventDestroy(e);
         if (tuneStart) cudaEventDestroy(tuneStart);
         if (tuneEnd) cudaEventDestroy(tuneEnd);
         for (cudaEvent_t e : nfMarks) cudaEventDestroy(e);
-        if (d2h) cudaStreamDestroy(d2h);
-        if (sideFork) cudaEventDestroy(sideFork);
-        if (sideJoin) cudaEventDestroy(sideJoin);
-        if (side) cudaStreamDestroy(side);
+        blockcache::giveStream(d2h, device);
+        blockcache::giveEvent(sideFork, device);
+        blockcache::giveEvent(sideJoin, device);
+        blockcache::giveStream(side, device);
     }
 
     // device bytes held by this tree
@@ -897,8 +969,9 @@ TreeEngine::TreeEngine(const void *x, const void *y, const void *z, size_t n, co
     AOT_CHECK(cudaMemsetAsync(m_->st, 0, sizeof(DeviceState), cfg.stream));
     m_->hst = static_cast<DeviceState *>(blockcache::takeHost(sizeof(DeviceState), &m_->hstBytes));
     std::memset(m_->hst, 0, sizeof(DeviceState));
-    AOT_CHECK(cudaStreamCreateWithFlags(&m_->d2h, cudaStreamNonBlocking));
-    AOT_CHECK(cudaEventCreateWithFlags(&m_->ready, cudaEventDisableTiming));
+    AOT_CHECK(cudaGetDevice(&m_->device));
+    m_->d2h = blockcache::takeStream();
+    m_->ready = blockcache::takeEvent();
     if (n)
     {
         for (int k = 0; k < 2; ++k)
@@ -1575,9 +1648,9 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
         const bool useSide = nf;
         if (useSide && !m.side)
         {
-            AOT_CHECK(cudaStreamCreateWithFlags(&m.side, cudaStreamNonBlocking));
-            AOT_CHECK(cudaEventCreateWithFlags(&m.sideFork, cudaEventDisableTiming));
-            AOT_CHECK(cudaEventCreateWithFlags(&m.sideJoin, cudaEventDisableTiming));
+            m.side = blockcache::takeStream();
+            m.sideFork = blockcache::takeEvent();
+            m.sideJoin = blockcache::takeEvent();
         }
         for (int l = 0; l < levels; ++l)
         {

@@ -75,6 +75,14 @@ void *takeHost(size_t bytes, size_t *classBytes);  // pinned host block
 void giveHost(void *p, size_t classBytes);
 size_t cachedBytes();  // device bytes held for reuse
 void trim();           // returns every cached block to the driver
+// Non-blocking streams and timing-free events of the current device, kept
+// for reuse as the blocks are: creating and destroying them for every tree
+// takes driver locks that the threads of a server would contend on.  A
+// stream is given back once the work its owner queued is done.
+cudaStream_t takeStream();
+void giveStream(cudaStream_t s, int device);
+cudaEvent_t takeEvent();
+void giveEvent(cudaEvent_t e, int device);
 }  // namespace blockcache
 
 // Host wait for the work queued on `s` so far.  By default the thread spins

@@ -127,7 +127,7 @@ Server::~Server()
     for (auto &kv : trees_)
     {
         kv.second->engine.reset();
-        if (kv.second->stream) (void)cudaStreamDestroy(kv.second->stream);
+        if (kv.second->stream) blockcache::giveStream(kv.second->stream, device_);
     }
 }
 
@@ -270,7 +270,7 @@ void Server::run(Job &job, ServeResult &res)
                 if (t) throw std::invalid_argument("server: a resident tree already has this id");
                 throw std::length_error("server: the build needs more device memory than the whole budget");
             }
-            AOT_CHECK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
+            t->stream = blockcache::takeStream();
             EngineConfig cfg = r.cfg;
             cfg.tuneSort = false;  // no timing runs inside a request
             cfg.stream = t->stream;
@@ -309,7 +309,7 @@ void Server::run(Job &job, ServeResult &res)
             if (!t || !t->engine) throw std::invalid_argument("server: no resident tree with this id");
             t->engine.reset();  // synchronises the tree's stream
             for (DevMem &c : t->coords) c.release();
-            (void)cudaStreamDestroy(t->stream);
+            blockcache::giveStream(t->stream, device_);
             t->stream = nullptr;
         }
         if (t && t->engine)
@@ -334,7 +334,7 @@ void Server::run(Job &job, ServeResult &res)
         {
             // a failed build leaves no tree behind
             t->engine.reset();
-            if (t->stream) (void)cudaStreamDestroy(t->stream);
+            if (t->stream) blockcache::giveStream(t->stream, device_);
             trees_.erase(r.tree);
             return;
         }
