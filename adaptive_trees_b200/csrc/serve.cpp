@@ -105,6 +105,15 @@ Server::Server(int slots, size_t budgetBytes) : budget_(budgetBytes)
     if (slots <= 0) throw std::invalid_argument("server: need at least one slot");
     if (budgetBytes == 0) throw std::invalid_argument("server: the memory budget must be positive");
     AOT_CHECK(cudaGetDevice(&device_));
+    // the streams and events of `slots` requests in flight (a tree's stream,
+    // its engine's read-back and side streams, three events), created now
+    // rather than by the first requests
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+    for (int i = 0; i < 3 * slots; ++i) streams.push_back(blockcache::takeStream());
+    for (int i = 0; i < 3 * slots; ++i) events.push_back(blockcache::takeEvent());
+    for (cudaStream_t st : streams) blockcache::giveStream(st, device_);
+    for (cudaEvent_t e : events) blockcache::giveEvent(e, device_);
     for (int i = 0; i < slots; ++i) workers_.emplace_back([this] { worker(); });
 }
 
