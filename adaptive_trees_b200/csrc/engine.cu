@@ -32,6 +32,7 @@
 
 #include "engine_util.cuh"
 #include "keygen.cuh"
+#include "binlevel.cuh"
 #include "levelbuild.cuh"
 #include "rebalance.cuh"
 #include "tree_view.cuh"
@@ -824,6 +825,12 @@ struct TreeEngine::Impl
     DevMem mergeSplits;              // merge-path cuts of the full begin refresh
     unsigned char *lvHost = nullptr; // pinned: the level build's one readback
     size_t lvHostBytes = 0;
+    // binary tree by levels (binlevel.cuh)
+    DevMem blRows, blMid, blChild, blLeaves, blOffset, blCtl;
+    size_t blCap = 0;
+    int blLevels = bl::kLevels;      // depths the last binary build needed, with one to spare
+    bl::Control *blHost = nullptr;   // pinned readback
+    size_t blHostBytes = 0;
     u32 nodeSlots = 0;
     bool nodeStale = true;         // the keys changed or the table moved: clear before use
     size_t scanTiles = 0;
@@ -844,6 +851,7 @@ struct TreeEngine::Impl
     {
         if (hst) blockcache::giveHost(hst, hstBytes);
         if (lvHost) blockcache::giveHost(lvHost, lvHostBytes);
+        if (blHost) blockcache::giveHost(blHost, blHostBytes);
         blockcache::giveEvent(ready, device);
         for (cudaEvent_t e : marks)
             if (e) cudaEventDestroy(e);
@@ -1798,6 +1806,18 @@ void TreeEngine::binaryBuild()
     sortParticles();
     const size_t estimate = std::max<size_t>(4096, 4 * (n_ / std::max(1u, cfg_.bucket)) + 4096);
     ensurePhysical(std::max({physCap_, estimate, leafCapacity_}));
+    lastBuildByLevels_ = buildMode_ == 0 && binaryLevelBuild();
+    if (lastBuildByLevels_)
+    {
+        built_ = true;
+        if (prepared_.treeStructure | prepared_.particleCountsPerBox | prepared_.particleMapping)
+            prepareViews(leafCapacity_, prepared_);
+        buildViews(cfg_.views);  // the placement wrote the counts
+        const bool views = cfg_.views.treeStructure | cfg_.views.particleCountsPerBox | cfg_.views.particleMapping;
+        if (views) readState();
+        else applyState();  // the finish kernel's state, known on the host
+        return;
+    }
     rb::TreeBufs tb = m_->bufs();
     binInitRootKernel<<<1, 1, 0, s>>>(tb, (long long)leafCapacity_), noteLaunch();
     AOT_LAUNCH_CHECK();
@@ -1832,6 +1852,111 @@ void TreeEngine::binaryBuild()
     materializeCounts();
     buildViews(cfg_.views);
     readState();
+}
+
+// The converged binary tree, level by level (binlevel.cuh): the tree the
+// reference's build passes end with, its pass count and its leaf capacity.
+// False where the passes must run: a depth limit beyond the 63 key bits.
+bool TreeEngine::binaryLevelBuild()
+{
+    if (cfg_.maxDepth > 63) return false;
+    cudaStream_t s = cfg_.stream;
+    Impl &m = *m_;
+    const unsigned blocks = unsigned(smCount()) * 4u;
+    const KeyIndex idx = m.keyIndex(n_);
+    const u64 *P = m.P[0].as<u64>();
+    size_t cap = std::max<size_t>(m.blCap, 2 * (n_ / std::max(1u, cfg_.bucket)) + 4096);
+    if (!m.blHost) m.blHost = static_cast<bl::Control *>(blockcache::takeHost(sizeof(bl::Control), &m.blHostBytes));
+    const bl::Control &hc = *m.blHost;
+    for (;;)
+    {
+        if (cap >= (size_t(1) << 31)) return false;
+        m.blRows.reserve(cap * sizeof(uint4), s);
+        m.blMid.reserve(cap * sizeof(u32), s);
+        m.blChild.reserve(cap * 2 * sizeof(u32), s);
+        m.blLeaves.reserve(cap * sizeof(u32), s);
+        m.blOffset.reserve(cap * sizeof(u32), s);
+        m.blCtl.reserve(sizeof(bl::Control), s);
+        m.blCap = cap;
+        bl::Arena a{};
+        a.rows = m.blRows.as<uint4>();
+        a.mid = m.blMid.as<u32>();
+        a.child = m.blChild.as<u32>();
+        a.leaves = m.blLeaves.as<u32>();
+        a.offset = m.blOffset.as<u32>();
+        a.ctl = m.blCtl.as<bl::Control>();
+        a.cap = u32(cap);
+        AOT_CHECK(cudaMemsetAsync(m.blCtl.p, 0, sizeof(bl::Control), s));
+        bl::rootKernel<<<1, 32, 0, s>>>(a, m.bufs(), P, n_, cfg_.bucket, cfg_.maxDepth), noteLaunch();
+        // as many depths as the last build needed (all 64 the first time);
+        // the readback tells whether the tree went deeper
+        const int levels = std::max(1, std::min(bl::kLevels, m.blLevels));
+        for (int l = 0; l < levels; ++l)
+            bl::levelKernel<<<blocks * 2, bl::kThreads, 0, s>>>(a, idx, l, cfg_.bucket, cfg_.maxDepth), noteLaunch();
+        for (int l = levels - 1; l >= 0; --l)
+            bl::leafCountKernel<<<blocks, bl::kThreads, 0, s>>>(a, l, levels), noteLaunch();
+        auto place = [&]() {
+            const rb::TreeBufs tb = m.bufs();
+            for (int l = 0; l < levels; ++l)
+                bl::placeKernel<<<blocks, bl::kThreads, 0, s>>>(a, tb.K[0], tb.B[0], tb.N[0], l, levels,
+                                                               u32(physCap_)),
+                    noteLaunch();
+            AOT_LAUNCH_CHECK();
+        };
+        place();
+        AOT_CHECK(cudaMemcpyAsync(m.blHost, m.blCtl.p, sizeof(bl::Control), cudaMemcpyDeviceToHost, s));
+        u32 rootLeaves = 1;
+        AOT_CHECK(cudaMemcpyAsync(m.hst, m.st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
+        waitStream(s);
+        if (m.hst->error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
+        if (hc.overflow)
+        {
+            cap *= 2;
+            continue;
+        }
+        if (hc.levelCount[levels] != 0)
+        {
+            m.blLevels = bl::kLevels;  // deeper than the last build: all depths again
+            continue;
+        }
+        int deepest = -1;  // deepest depth holding units
+        for (int l = 0; l < levels; ++l)
+            if (hc.levelCount[l]) deepest = l;
+        if (deepest >= 0)
+            AOT_CHECK(cudaMemcpy(&rootLeaves, a.leaves, sizeof(u32), cudaMemcpyDeviceToHost));
+        if (hc.placeOverflow)
+        {
+            ensurePhysical(rootLeaves);
+            AOT_CHECK(cudaMemsetAsync(&a.ctl->placeOverflow, 0, sizeof(int), s));
+            place();
+        }
+        // one pass per depth of units; the capacity's 25 % steps end at the
+        // first step at or above the final leaf count (the counts only grow)
+        const int passes = deepest + 1;
+        long long c = std::max<long long>((long long)leafCapacity_, 1);
+        while ((long long)rootLeaves > c) c += (c + 3) / 4;
+        m.blLevels = std::min(bl::kLevels, deepest + 2);
+        bl::finishKernel<<<1, 1, 0, s>>>(a, m.bufs(), int(rootLeaves), passes, c), noteLaunch();
+        AOT_LAUNCH_CHECK();
+        // the host mirror of the finished state
+        DeviceState &h = *m.hst;
+        h.numLeaves = h.newNumLeaves = int(rootLeaves);
+        h.numNodes = (int(rootLeaves) - 1) * 2 + 1;
+        h.proposal = (long long)rootLeaves;
+        h.iteration = passes;
+        h.rounds = passes + 1;
+        h.converged = 1;
+        h.changed = h.needsResize = 0;
+        h.activeBuffer = 0;
+        h.overflow = 0;
+        h.dirtyCount = 0;
+        h.logicalCap = c;
+        buildRounds_ = passes;
+        hostLeaves_ = rootLeaves;
+        leafCapacity_ = size_t(c);
+        ensurePhysical(leafCapacity_);
+        return true;
+    }
 }
 
 void TreeEngine::update()

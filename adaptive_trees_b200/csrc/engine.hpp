@@ -236,6 +236,7 @@ private:
     // or LeafCount thresholds wrap in 32 bits); fills the build's round
     // proposals
     bool octreeLevelBuild(std::vector<long long> &proposals);
+    bool binaryLevelBuild();
     void sortKeys(int config);
     void octreeBuild();
     void binaryBuild();

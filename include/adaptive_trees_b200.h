@@ -149,7 +149,10 @@ AO_API ao_status ao_tree_stage_times(ao_tree *tree, ao_stage_times *out);
  * history behind leafCapacity); it falls back to the rounds when the tree
  * would not converge within max_depth rounds or when LeafCount's 32-bit split
  * thresholds wrap (bucket >= 2^23).  Mode 1 always runs the rounds.  Both
- * give the same tree, counts and capacity.  Binary trees always run rounds. */
+ * give the same tree, counts and capacity.  Binary (k-d) trees likewise:
+ * mode 0 builds the converged tree a depth at a time (the reference's build
+ * passes, kdtree3d.cu:239-249, split one depth per pass), falling back to
+ * the passes for a max_depth above 63; mode 1 always runs the passes. */
 AO_API ao_status ao_tree_set_build_mode(ao_tree *tree, int mode);
 /* The last build(): *by_levels = 1 when it used the level builder; *rounds =
  * the build rounds that changed the tree (the reference's history length).

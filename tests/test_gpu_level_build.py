@@ -204,3 +204,83 @@ def test_deeper_tree_after_a_shallow_one():
     assert t.buildPath()[0]
     compare(t, o)
     t.close()
+
+
+# ---------------------------------------------------------------------------
+# binary (k-d) trees: the converged tree a depth at a time against the passes
+# ---------------------------------------------------------------------------
+BIN_CASES = [
+    ("mixture_f64", lambda: S.gaussian_mixture(200_000, seed=51)),
+    ("uniform_f64", lambda: S.uniform_cube(150_000, seed=52)),
+    ("plummer_f32", lambda: S.plummer_sphere(150_000, seed=53, dtype=np.float32)),
+    ("stacked_f64", lambda: _stacked(40_000, 54)),
+]
+
+
+def _binary(xyz, mode, builds=1, **cfg):
+    import adaptive_trees_b200 as ab
+    xs = [to_dev(a) for a in xyz]
+    t = ab.Tree(1, *xs, tree_config(**cfg))
+    t.setBuildMode(mode)
+    for _ in range(builds):
+        t.build()
+    return t, xs
+
+
+def _same_binary(a, b):
+    for name in ("particleKeys", "perm", "cornerstone", "leafCounts"):
+        x, y = gpu_get(a, name), gpu_get(b, name)
+        assert x.size == y.size and np.array_equal(x, y), name
+    ia, ib = a.info(), b.info()
+    assert (ia.num_leaves, ia.num_nodes, ia.leaf_capacity, ia.max_achieved_depth) == \
+        (ib.num_leaves, ib.num_nodes, ib.leaf_capacity, ib.max_achieved_depth)
+    assert a.buildPath()[1] == b.buildPath()[1]
+    assert a.doBuffersNeedResize() == b.doBuffersNeedResize()
+
+
+@pytest.mark.parametrize("case", BIN_CASES, ids=[c[0] for c in BIN_CASES])
+@pytest.mark.parametrize("bucket,max_depth", [(32, -1), (1, -1), (64, 12), (8, 5)])
+def test_binary_levels_equal_passes(case, bucket, max_depth):
+    xyz = case[1]()
+    lv, xs_l = _binary(xyz, 0, builds=2, bucket=bucket, max_depth=max_depth)
+    rd, xs_r = _binary(xyz, 1, builds=2, bucket=bucket, max_depth=max_depth)
+    assert lv.buildPath()[0] and not rd.buildPath()[0]
+    _same_binary(lv, rd)
+    moved = S.jitter(xyz, 2e-3, seed=9)
+    for xs in (xs_l, xs_r):
+        for d, a in zip(xs, moved):
+            d.copy_(torch.from_numpy(np.ascontiguousarray(a)).to("cuda"))
+    for t in (lv, rd):
+        t.update()
+        while t.doBuffersNeedResize():
+            t.resizeBuffers()
+            t.update()
+    _same_binary(lv, rd)
+    lv.close()
+    rd.close()
+
+
+@pytest.mark.parametrize("n", [1, 7, 33, 600])
+def test_binary_small_trees(n):
+    xyz = S.uniform_cube(n, seed=55)
+    lv, _ = _binary(xyz, 0, bucket=4)
+    rd, _ = _binary(xyz, 1, bucket=4)
+    _same_binary(lv, rd)
+    lv.close()
+    rd.close()
+
+
+def test_binary_escaped_and_views():
+    from oracle import oracle as O
+    x, y, z = S.gaussian_mixture(30_000, seed=56)
+    x, y, z = x.copy(), y.copy(), z.copy()
+    esc = np.finfo(np.float64).max
+    for a in (x, y, z):
+        a[::9] = esc
+    cfg = dict(bucket=16, views=(1, 1, 1))
+    t, _ = _binary((x, y, z), 0, **cfg)
+    o = O.OracleTree(1, x, y, z, oracle_config(**cfg))
+    o.build()
+    assert t.buildPath()[0]
+    compare(t, o)
+    t.close()
