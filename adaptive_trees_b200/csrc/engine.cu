@@ -1091,6 +1091,9 @@ void TreeEngine::ensurePhysical(size_t capacity)
     }
     m_->offs.reserve((c + 1) * sizeof(i64), s);
     m_->dirty.reserve((c + 1) * sizeof(int), s);
+    // the merge-path cuts of the full begin refresh (reserved here: an update
+    // may run under stream capture, where nothing may be allocated)
+    m_->mergeSplits.reserve(((c + 1 + n_) / rb::kMergeChunk + 3) * sizeof(u32), s);
     // candidate group leaders are first children of distinct internal nodes: <= (L - 1) / 7
     m_->scanTiles = (c + 1 + rb::kScanTile - 1) / rb::kScanTile;
     m_->scan.reserve((m_->scanTiles + 1) * sizeof(u64), s);
@@ -1378,8 +1381,7 @@ void TreeEngine::refreshCounts(bool all, unsigned blocks)
     if (all)
     {
         // every leaf: a merge of the leaf keys with the particle keys
-        const size_t chunks = (physCap_ + 1 + n_) / rb::kMergeChunk + 2;
-        m_->mergeSplits.reserve((chunks + 1) * sizeof(u32), s);
+        const size_t chunks = (physCap_ + 1 + n_) / rb::kMergeChunk + 2;  // cuts: reserved by ensurePhysical
         const u64 *P = m_->P[0].as<u64>();
         rb::mergeSplitKernel<<<gridFor(chunks + 1, 256), 256, 0, s>>>(tb, P, m_->mergeSplits.as<u32>()), noteLaunch();
         rb::mergeBeginKernel<<<unsigned(std::min<size_t>(chunks, size_t(smCount()) * 8u)), 256, 0, s>>>(
