@@ -1868,7 +1868,9 @@ bool TreeEngine::binaryLevelBuild()
     const KeyIndex idx = m.keyIndex(n_);
     const u64 *P = m.P[0].as<u64>();
     size_t cap = std::max<size_t>(m.blCap, 2 * (n_ / std::max(1u, cfg_.bucket)) + 4096);
-    if (!m.blHost) m.blHost = static_cast<bl::Control *>(blockcache::takeHost(sizeof(bl::Control), &m.blHostBytes));
+    // pinned readback: the control block, then the root's subtree leaf count
+    constexpr size_t kLeavesAt = (sizeof(bl::Control) + 15) & ~size_t(15);
+    if (!m.blHost) m.blHost = static_cast<bl::Control *>(blockcache::takeHost(kLeavesAt + 16, &m.blHostBytes));
     const bl::Control &hc = *m.blHost;
     for (;;)
     {
@@ -1907,9 +1909,11 @@ bool TreeEngine::binaryLevelBuild()
         };
         place();
         AOT_CHECK(cudaMemcpyAsync(m.blHost, m.blCtl.p, sizeof(bl::Control), cudaMemcpyDeviceToHost, s));
-        u32 rootLeaves = 1;
+        unsigned char *leavesHost = reinterpret_cast<unsigned char *>(m.blHost) + kLeavesAt;
+        AOT_CHECK(cudaMemcpyAsync(leavesHost, a.leaves, sizeof(u32), cudaMemcpyDeviceToHost, s));
         AOT_CHECK(cudaMemcpyAsync(m.hst, m.st, sizeof(DeviceState), cudaMemcpyDeviceToHost, s));
         waitStream(s);
+        u32 rootLeaves = 1;
         if (m.hst->error) throw std::runtime_error("adaptive_octree: a device scan gave up waiting (bounded look-back)");
         if (hc.overflow)
         {
@@ -1924,8 +1928,7 @@ bool TreeEngine::binaryLevelBuild()
         int deepest = -1;  // deepest depth holding units
         for (int l = 0; l < levels; ++l)
             if (hc.levelCount[l]) deepest = l;
-        if (deepest >= 0)
-            AOT_CHECK(cudaMemcpy(&rootLeaves, a.leaves, sizeof(u32), cudaMemcpyDeviceToHost));
+        if (deepest >= 0) std::memcpy(&rootLeaves, leavesHost, sizeof(u32));
         if (hc.placeOverflow)
         {
             ensurePhysical(rootLeaves);
