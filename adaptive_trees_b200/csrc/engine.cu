@@ -1682,12 +1682,12 @@ bool TreeEngine::octreeLevelBuild(std::vector<long long> &proposals)
                 if (cfg_.hilbert)
                 {
                     if (l > 0 && !fork) lb::nbrKernel<true><<<blocks * 2, lb::kThreads, 0, s>>>(a, l, m.kpd.h), noteLaunch();
-                    lb::nearFieldKernel<true><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h), noteLaunch();
+                    lb::nearFieldKernel<true><<<blocks / 4 * 5, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h), noteLaunch();
                 }
                 else
                 {
                     if (l > 0 && !fork) lb::nbrKernel<false><<<blocks * 2, lb::kThreads, 0, s>>>(a, l, m.kpd.h), noteLaunch();
-                    lb::nearFieldKernel<false><<<blocks, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h), noteLaunch();
+                    lb::nearFieldKernel<false><<<blocks / 4 * 5, lb::kThreads, 0, s>>>(a, idx, l, m.kpd.h), noteLaunch();
                 }
                 markNearField(false);
                 if (cfg_.hilbert)

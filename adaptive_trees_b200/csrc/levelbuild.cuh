@@ -395,8 +395,10 @@ struct UnitScratch
     int nSlow;
 };
 
+// 5 CTAs per SM (48 registers, 29.6 KB of scratch each): 0.7 % faster builds
+// at 16 Mi than 4.
 template <bool Hilbert>
-static __global__ void __launch_bounds__(kThreads, 4)
+static __global__ void __launch_bounds__(kThreads, 5)
     nearFieldKernel(Arena a, KeyIndex idx, int l, HilbertTables h)
 {
     using rb::kUnitBatch;
