@@ -382,6 +382,7 @@ def single_config_record(config, steps, warmup, cpu_sample, cpu_baseline=True, r
         launches = (tree.info().kernel_launches - launches0) // max(1, len(build_ms))
         info = tree.info()
         leaves = info.num_leaves
+        by_levels, passes = tree.buildPath()
         # end to end: pinned host coordinates in, build, the counters out
         host_counters = torch.zeros(3, dtype=torch.int32).pin_memory()
         cnt = tree.counters()
@@ -429,7 +430,8 @@ def single_config_record(config, steps, warmup, cpu_sample, cpu_baseline=True, r
             "n_gpus": 1, "steps": len(build_ms), "warmup": args.warmup, "ms_per_step": statistics.median(build_ms),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": spec["workload"], "n": n, "coords": "float64", "leaves": int(leaves),
-                       "parallelism": "replicas1", "sort": ab.sort_tuning(n)},
+                       "parallelism": "replicas1", "sort": ab.sort_tuning(n),
+                       "build_path": {"by_levels": bool(by_levels), "reference_rounds": int(passes)}},
             "clocks": clocks.summary(), "gpu_launches": int(launches),
             "e2e": {"value": n / (e2e_ms * 1e-3), "unit": "particles/s", "ms_per_step": e2e_ms,
                     "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 12}}
